@@ -1,0 +1,398 @@
+#!/usr/bin/env python3
+"""Benchmark of the BN254 prover hot path at k = 22 (one GPU per process).
+
+A step is one pass of the full-size single-kernel workload:
+  * MSM over 2^22 SRS points [tau^i] G (seeded tau) with the witness-like
+    scalar mix 50% uniform / 30% < 2^64 / 20% in {0, 1};
+  * coeff_to_extended: coset NTT 2^22 -> 2^24 (extension factor 4);
+  * batch_invert over 2^24 nonzero uniform Fr.
+The headline metric is MSM points/s; NTT GB/s (algorithmic bytes
+2^22*32 + 2^24*32 per transform) and batch-invert elements/s are reported
+beside it from the same timed steps.  Inputs (128 MB scalars + 256 MB bases,
+512 MB NTT output, 512 MB inversion array) exceed the 126 MB L2, so no flush
+is needed between steps.
+
+`--impl reference` times the CPU restatement of the reference's CPU path
+(best_multiexp_cpu, the radix-2 FFT, the chunked Montgomery trick) on a
+bounded sample of the same workload, with all host threads.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+K_MSM, K_NTT, K_EXT, K_BI = 22, 22, 24, 24
+METRIC = "MSM pts/s at k=22 (step: MSM 2^22 + coset NTT 2^22->2^24 + batch_invert 2^24)"
+UNIT = "points/s"
+WORKLOAD = {
+    "workload": "k22_single_kernels",
+    "msm_points": 1 << K_MSM,
+    "msm_scalar_mix": "50% uniform Fr / 30% < 2^64 / 20% {0,1}",
+    "ntt": "coset 2^22 -> 2^24",
+    "batch_invert": 1 << K_BI,
+    "l2": "inputs larger than L2 (no flush)",
+}
+
+
+def load_pkg():
+    name = "halo2_gpu_b200"
+    pkg = os.path.join(ROOT, "halo2-gpu_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, mx, reasons = [], None, set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        sms.sort()
+        med = sms[len(sms) // 2] if sms else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def ncu_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline_msm(threads=None, log_n=16, reps=None):
+    """Oracle (C restatement of best_multiexp_cpu) on a 2^log_n sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import numpy as np
+    f = load_pkg().fields if "halo2_gpu_b200" not in sys.modules else sys.modules["halo2_gpu_b200"].fields
+    n = 1 << log_n
+    tau = f.fr_mont_limbs([0x5EED])
+    bases = orc.srs(tau, n)
+    sc = orc.chacha_fr(22, n)
+    # witness-like mix as in the GPU workload
+    rng = np.random.default_rng(22)
+    cls = rng.integers(0, 10, n)
+    small = rng.integers(0, 2**63, n, dtype=np.uint64)
+    sc_plain = np.zeros((n, 4), np.uint64)
+    sc_plain[:, 0] = np.where(cls >= 8, small & np.uint64(1), small)
+    mix = orc.lib()
+    smallm = np.zeros_like(sc_plain)
+    mix.o_to_mont(0, sc_plain.ctypes.data, smallm.ctypes.data, n)
+    sc = np.where((cls < 5)[:, None], sc, smallm)
+    threads = threads or orc.num_threads()
+    orc.msm(sc[:1024], bases[:1024], threads)
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        orc.msm(sc, bases, threads)
+        done += 1
+        el = time.perf_counter() - t0
+        if (reps is not None and done >= reps) or (reps is None and el > 10.0):
+            break
+    return {"value": n * done / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"best_multiexp_cpu restatement (oracle/oracle.c) over 2^{log_n} SRS points with the same "
+                      f"scalar mix, {done} runs in {el:.1f}s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    for _ in range(args.warmup):
+        pass
+    base = cpu_baseline_msm(reps=None)
+    value = base["value"]
+    ms = (1 << K_MSM) / value * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32-limb Montgomery Fr/Fq (exact)",
+            "data": "synthetic (seeded SRS and scalars)", "config": WORKLOAD,
+            "cpu_baseline": base,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    h2b = load_pkg()
+    L = h2b.lib()
+    f = h2b.fields
+    stream = torch.cuda.current_stream()
+    sh = h2b.stream_handle(stream)
+
+    # ---- setup (untimed) ----
+    n_msm, n_ntt, n_ext, n_bi = 1 << K_MSM, 1 << K_NTT, 1 << K_EXT, 1 << K_BI
+    dom = f.EvaluationDomain(5, K_NTT)
+    assert dom.extended_k == K_EXT
+    d_srs = h2b.srs_device(0x5EED + 0x1000 * rank, n_msm)
+    d_sc = h2b.random_fr_device(n_msm, 1000 + rank, 1)
+    d_ntt_in = h2b.random_fr_device(n_ntt, 2000 + rank, 0)
+    d_ext = h2b.dev_empty(32 * n_ext)
+    d_bi = h2b.random_fr_device(n_bi, 3000 + rank, 0)
+    d_msm_out = h2b.dev_empty(96)
+    ws_msm = h2b.msm_workspace(n_msm)
+    ws_ntt = h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(3, K_NTT, K_EXT))
+    ws_bi = h2b.dev_empty(L.h2b_batch_invert_workspace_size(n_bi))
+    d_om = h2b.to_dev(f.fr_mont_limbs([dom.extended_omega]))
+    one = f.fr_mont_limbs([1])
+    one_ffi = h2b.host_ffi(one)
+    ins = h2b.ffi_array([d_ntt_in.data_ptr()])
+    outs = h2b.ffi_array([d_ext.data_ptr()])
+    d_cnt = h2b.dev_empty(8)
+    h2b.call("h2b_msm_count_entries", h2b.ptr(d_sc), n_msm, h2b.ptr(d_cnt), sh)
+    torch.cuda.synchronize()
+    entries = int(d_cnt.cpu().numpy().view("uint64")[0])
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        h2b.call("h2b_msm_device", h2b.ptr(d_sc), h2b.ptr(d_srs), h2b.ptr(d_msm_out), n_msm, h2b.ptr(ws_msm),
+                 ws_msm.numel(), sh)
+        if ev is not None:
+            ev[1].record(stream)
+        h2b.call("_halo2_fft_many_to_device", 3, 1, K_NTT, K_EXT, ins, outs, h2b.ptr(d_om), ctypes.byref(one_ffi),
+                 True, h2b.ptr(ws_ntt), ws_ntt.numel(), sh)
+        if ev is not None:
+            ev[2].record(stream)
+        h2b.call("h2b_batch_invert", h2b.ptr(d_bi), 0, n_bi, h2b.ptr(ws_bi), ws_bi.numel(), sh)
+        if ev is not None:
+            ev[3].record(stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    # IMAD / modmul pipe probes (untimed), for the roofline denominators
+    sink = h2b.dev_empty(4 * 148 * 64)
+    probe = {}
+    for name, iters, per in (("h2b_probe_imad", 4096, 16), ("h2b_probe_modmul", 64, 4)):
+        h2b.call(name, 148 * 8, 256, 8, h2b.ptr(sink), sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h2b.call(name, 148 * 8, 256, iters, h2b.ptr(sink), sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        probe[name] = 148 * 8 * 256 * iters * per / (e0.elapsed_time(e1) * 1e-3)
+
+    # ---- timed region ----
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    launches0 = L.h2b_launch_count()
+    L.h2b_prof_enable(1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(evs[i])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = L.h2b_launch_count() - launches0
+    total_ms = t0.elapsed_time(t1)
+    msm_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+    ntt_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+    bi_ms = sum(e[2].elapsed_time(e[3]) for e in evs) / args.steps
+    acc_ms, acc_cnt = h2b.prof_read(h2b.PROF_MSM_ACCUMULATE)
+    nttp_ms, nttp_cnt = h2b.prof_read(h2b.PROF_NTT_PASSES)
+    bik_ms, bik_cnt = h2b.prof_read(h2b.PROF_BATCH_INVERT)
+    L.h2b_prof_enable(0)
+
+    step_ms = total_ms / args.steps
+    if dist is not None:
+        t = torch.tensor([step_ms, msm_ms, ntt_ms, bi_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, msm_ms, ntt_ms, bi_ms = t.tolist()
+
+    ntt_bytes = 32 * n_ntt + 32 * n_ext
+    value = world * n_msm / (msm_ms * 1e-3)
+    hbm, hbm_kind = peaks()
+    # dominant kernel: MSM bucket accumulation (one launch per MSM)
+    acc_avg_ms = acc_ms / max(acc_cnt, 1)
+    acc_bytes = entries * (4 + 64) + (1 << 19) * 128          # sorted ids + affine points + bucket sums
+    acc_modmul = entries * 10                                  # XYZZ mixed add 8M + 2S
+    roofline = {"bound": "hbm", "kernel": "k_msm_accumulate", "achieved": acc_bytes / (acc_avg_ms * 1e-3) / 1e9,
+                "peak": hbm, "unit": "GB/s", "peak_source": f"{hbm_kind} MEASURED_PEAKS.json hbm_gbs",
+                "traffic": ncu_traffic("msm_accumulate_k22.md"),
+                "algorithmic_bytes_per_launch": acc_bytes, "launch_ms": acc_avg_ms}
+    roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    imad_peak = probe["h2b_probe_imad"]
+    imad = {"kernel": "k_msm_accumulate", "modmul_per_launch": acc_modmul,
+            "achieved_imad_ops_per_s": acc_modmul * 264 / (acc_avg_ms * 1e-3),
+            "peak_imad_ops_per_s": imad_peak, "peak_source": "measured h2b_probe_imad (mad.lo/mad.hi chains)",
+            "modmul_probe_per_s": probe["h2b_probe_modmul"]}
+    imad["frac"] = imad["achieved_imad_ops_per_s"] / imad_peak
+    ntt_kernel_ms = nttp_ms / max(nttp_cnt, 1)
+    ntt_modmul = (n_ext // 2) * K_EXT
+    bi_kernel_ms = bik_ms / max(bik_cnt, 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32-limb Montgomery Fr/Fq (exact integer)",
+        "data": "synthetic (seeded SRS [tau^i]G and scalars; generated on device)",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}"),
+        "msm": {"ms": msm_ms, "points_per_s": n_msm / (msm_ms * 1e-3), "entries": entries,
+                "window_bits": L.h2b_msm_window_bits(n_msm)},
+        "ntt": {"ms": ntt_ms, "GB_per_s": ntt_bytes / (ntt_ms * 1e-3) / 1e9,
+                "elements_per_s": n_ext / (ntt_ms * 1e-3), "pass_kernels_ms": ntt_kernel_ms,
+                "imad_frac_passes": ntt_modmul * 264 / (ntt_kernel_ms * 1e-3) / imad_peak},
+        "batch_invert": {"ms": bi_ms, "elements_per_s": n_bi / (bi_ms * 1e-3), "apply_kernel_ms": bi_kernel_ms},
+        "roofline": roofline, "imad_roofline": imad, "clocks": clk, "gpu_launches": launches,
+    }
+
+    # ---- end to end through the reference-facing C ABI with host buffers ----
+    if not args.no_e2e:
+        import numpy as np
+        h_sc = torch.empty(32 * n_msm, dtype=torch.uint8).pin_memory()
+        h_sc.copy_(d_sc.cpu())
+        h_ntt = torch.empty(32 * n_ntt, dtype=torch.uint8).pin_memory()
+        h_ntt.copy_(d_ntt_in.cpu())
+        h_ext = torch.empty(32 * n_ext, dtype=torch.uint8).pin_memory()
+        h_bi = torch.empty(32 * n_bi, dtype=torch.uint8).pin_memory()
+        h_bi.copy_(d_bi.cpu())
+        h_out = np.zeros(12, np.uint64)
+        ws_e2e_msm = h2b.dev_empty(L._halo2_multiexp_device_bases_workspace_size(n_msm))
+        ws_e2e_ntt = h2b.dev_empty(L._halo2_fft_normal_workspace_size(3, K_NTT, K_EXT))
+        sc_ffi = h2b.FFITraitObject(ctypes.c_void_p(h_sc.data_ptr()))
+        out_ffi = h2b.host_ffi(h_out)
+        h_om = f.fr_mont_limbs([dom.extended_omega])
+
+        def e2e_step(ev=None):
+            if ev is not None:
+                ev[0].record(stream)
+            h2b.call("_halo2_multiexp_device_bases", ctypes.byref(sc_ffi), h2b.ptr(d_srs), ctypes.byref(out_ffi),
+                     n_msm, h2b.ptr(ws_e2e_msm), ws_e2e_msm.numel(), sh)
+            if ev is not None:
+                ev[1].record(stream)
+            h2b.call("_halo2_cosetfft", 3, K_NTT, K_EXT, ctypes.c_void_p(h_ntt.data_ptr()),
+                     ctypes.c_void_p(h_ext.data_ptr()), h_om.ctypes.data, one.ctypes.data, h2b.ptr(ws_e2e_ntt),
+                     ws_e2e_ntt.numel(), sh)
+            d_bi.copy_(h_bi, non_blocking=True)
+            h2b.call("h2b_batch_invert", h2b.ptr(d_bi), 0, n_bi, h2b.ptr(ws_bi), ws_bi.numel(), sh)
+            h_bi.copy_(d_bi, non_blocking=True)
+            if ev is not None:
+                ev[2].record(stream)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        eevs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        for i in range(args.steps):
+            e2e_step(eevs[i])
+        torch.cuda.synchronize()
+        e_msm = sum(e[0].elapsed_time(e[1]) for e in eevs) / args.steps
+        e_step = sum(e[0].elapsed_time(e[2]) for e in eevs) / args.steps
+        if dist is not None:
+            t = torch.tensor([e_msm, e_step], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_msm, e_step = t.tolist()
+        line["e2e"] = {"value": world * n_msm / (e_msm * 1e-3), "unit": UNIT,
+                       "h2d_bytes_per_step": 32 * n_msm + 32 * n_ntt + 32 * n_bi,
+                       "d2h_bytes_per_step": 96 + 32 * n_ext + 32 * n_bi, "step_ms": e_step,
+                       "api": "_halo2_multiexp_device_bases (host scalars), _halo2_cosetfft (host in/out), "
+                              "h2b_batch_invert with pinned H2D/D2H"}
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_msm()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

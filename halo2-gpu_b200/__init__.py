@@ -1,0 +1,451 @@
+"""halo2-gpu_b200: B200-native BN254 Halo2/KZG prover hot path.
+
+Python host mirror of the reference's GPU wrappers
+(halo2_proofs/src/cuda/funcs/*.rs, halo2_proofs/src/poly/domain.rs) over the
+C ABI in libhalo2_gpu.so (declared in include/halo2_gpu.h).  PyTorch provides
+device memory and streams only; every field operation runs in this package's
+CUDA kernels.  There is no CPU fallback: if the shared library is missing the
+import of `lib()` raises.
+
+Array conventions: field elements are numpy uint64 arrays of shape (n, 4) in
+Montgomery form (the halo2curves memory image); G1 affine points are (n, 8)
+(x limbs then y limbs); an MSM result is the (12,) Jacobian image
+{X, Y, Z} with Z = 1 (or (0, 1, 0) for infinity).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import fields  # noqa: F401  (re-exported helper module)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhalo2_gpu.so")
+
+NTT_FFT, NTT_IFFT, NTT_COSET, NTT_ICOSET, NTT_IFFT_COSET, NTT_COSET_PART = 1, 2, 3, 4, 5, 6
+
+
+class RustError(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int), ("message", ctypes.c_void_p)]
+
+
+class FFITraitObject(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p)]
+
+
+class Halo2GpuError(RuntimeError):
+    def __init__(self, code, message, who):
+        super().__init__(f"{who}: code {code}: {message}")
+        self.code = code
+        self.message = message
+
+
+_u64, _u32, _i32, _vp, _b = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_bool
+_ffi = ctypes.POINTER(FFITraitObject)
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "_halo2_msm_max_length": (_u64, [_u64]),
+    "_halo2_multiexp_workspace_size": (_u64, [_u64]),
+    "_halo2_multiexp": (RustError, [_ffi, _ffi, _ffi, _u64, _vp, _u64, _vp]),
+    "_halo2_multiexp_device_bases_workspace_size": (_u64, [_u64]),
+    "_halo2_multiexp_device_bases": (RustError, [_ffi, _vp, _ffi, _u64, _vp, _u64, _vp]),
+    "_halo2_multiexp_device_scalars_device_bases_workspace_size": (_u64, [_u64]),
+    "_halo2_multiexp_device_scalars_device_bases": (RustError, [_vp, _vp, _ffi, _u64, _vp, _u64, _vp]),
+    "_halo2_batch_invert": (RustError, [_vp, _u32, _u64, _vp]),
+    "_halo2_commit_product_max_len": (_u64, [_u64, _u64]),
+    "_halo2_commit_product_workspace_size": (_u64, [_u64]),
+    "_halo2_commit_product": (RustError, [_ffi, _ffi, _ffi, _ffi, _ffi, _vp, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_commit_product_device_inputs": (RustError, [_ffi, _ffi, _ffi, _ffi, _ffi, _vp, _vp, _u64, _u64, _vp]),
+    "_halo2_permutation_product_max_len": (_u64, [_u64, _u64]),
+    "_halo2_permutation_product_workspace_size": (_u64, [_u64]),
+    "_halo2_permutation_product": (RustError, [_ffi, _ffi, _ffi, _vp, _vp, _vp, _vp, _vp, _u64, _u64, _u64, _vp,
+                                               _u64, _vp]),
+    "_halo2_permutation_product_device_inputs_workspace_size": (_u64, [_u64]),
+    "_halo2_permutation_product_device_inputs": (RustError, [_ffi, _ffi, _ffi, _vp, _vp, _vp, _vp, _vp, _u64, _u64,
+                                                             _u64, _vp, _u64, _vp]),
+    "_halo2_grand_product_max_len": (_u64, [_u64, _u64]),
+    "_halo2_grand_product_workspace_size": (_u64, [_u64]),
+    "_halo2_grand_product": (RustError, [_ffi, _ffi, _ffi, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_grand_product_device_inputs": (RustError, [_ffi, _ffi, _u64, _u64, _vp]),
+    "_halo2_permute_expression_pair_workspace_size": (_u64, [_u64, _u64]),
+    "_halo2_permute_expression_pair": (RustError, [_vp, _vp, _vp, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_poly_multiply_add": (RustError, [_vp, _vp, _vp, _u64, _vp]),
+    "_halo2_poly_elementwise_multiply": (RustError, [_vp, _vp, _vp, _u64, _vp]),
+    "_halo2_poly_fill_one": (RustError, [_vp, _u64, _vp]),
+    "_halo2_divide_by_vanishing_poly": (RustError, [_vp, _vp, _u32, _u64, _vp]),
+    "_halo2_poly_sub_short_inplace": (RustError, [_vp, _vp, _u64, _vp]),
+    "_halo2_poly_sub_short_out_of_place": (RustError, [_vp, _vp, _vp, _u64, _u64, _vp]),
+    "_halo2_poly_sub_scalar_at_zero": (RustError, [_vp, _vp, _vp]),
+    "_halo2_extended_from_lagrange_vec_device": (RustError, [_vp, _vp, _u32, _u64, _vp]),
+    "_halo2_distribute_powers_zeta": (RustError, [_vp, _vp, _u32, _u64, _vp]),
+    "_halo2_fft_normal_workspace_size": (_u64, [_u32, _u32, _u32]),
+    "_halo2_fft_normal": (RustError, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _vp]),
+    "_halo2_fft_normal_check_memory": (_b, [_u32, _vp, _u32, _u32]),
+    "_halo2_fft_normal_to_device_workspace_size": (_u64, [_u32, _u32, _u32]),
+    "_halo2_fft_normal_to_device": (RustError, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _vp]),
+    "_halo2_cosetfft": (RustError, [_u32, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _vp]),
+    "_halo2_fft_many_workspace_size": (_u64, [_u32, _u32, _u32]),
+    "_halo2_fft_many_to_device_workspace_size": (_u64, [_u32, _u32, _u32]),
+    "_halo2_fft_many": (RustError, [_u32, _u32, _u32, _u32, _ffi, _ffi, _vp, _ffi, _vp, _u64, _vp]),
+    "_halo2_fft_many_to_device": (RustError, [_u32, _u32, _u32, _u32, _ffi, _ffi, _vp, _ffi, _b, _vp, _u64, _vp]),
+    "_halo2_fft_many_check_memory": (_b, [_u32, _u32, _u32]),
+    "_halo2_get_fft_split_radix": (_i32, [_u32, _u32, _u32, _u64]),
+    "_halo2_evaluate_h_max_rows": (_u64, [_vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64,
+                                          _u64]),
+    "_halo2_quotient_workspace_size": (_u64, [_vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64,
+                                              _u64]),
+    "_halo2_quotient": (RustError, [_ffi, _u64, _ffi, _u64, _ffi, _u64, FFITraitObject, _u64, FFITraitObject, _u64,
+                                    FFITraitObject, _vp, _u64, _vp, _u64, FFITraitObject, _u64, _u64, _u64, _u64, _vp,
+                                    _u64, _vp]),
+    "_halo2_quotient_device_columns_device_out": (RustError, [_vp, _u64, _vp, _u64, _vp, _u64, FFITraitObject, _u64,
+                                                              FFITraitObject, _u64, FFITraitObject, _vp, _u64, _vp,
+                                                              _u64, _vp, _u64, _vp, _u64, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_quotient_device_columns": (RustError, [_vp, _u64, _vp, _u64, _vp, _u64, FFITraitObject, _u64,
+                                                   FFITraitObject, _u64, FFITraitObject, _vp, _u64, _vp, _u64,
+                                                   FFITraitObject, _u64, _u64, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_quotient_lookups": (RustError, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u64, _vp]),
+    "_halo2_quotient_permutation": (RustError, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                _vp, _u64, _u64, _u64, _i32, _i32, _i32, _u64, _vp]),
+    "h2b_msm_device": (RustError, [_vp, _vp, _vp, _u64, _vp, _u64, _vp]),
+    "h2b_msm_set_tuning": (None, [ctypes.c_int, ctypes.c_int]),
+    "h2b_batch_invert_workspace_size": (_u64, [_u64]),
+    "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
+    "h2b_ntt_set_pass_stages": (None, [ctypes.c_int]),
+    "h2b_ntt_get_pass_stages": (ctypes.c_int, []),
+    "h2b_random_fr": (RustError, [_vp, _u64, _u64, ctypes.c_int, _vp]),
+    "h2b_powers": (RustError, [_vp, _u64, _vp, _vp]),
+    "h2b_srs_from_powers": (RustError, [_vp, _vp, _u64, _vp, _vp]),
+    "h2b_prof_enable": (None, [ctypes.c_int]),
+    "h2b_prof_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
+    "h2b_probe_imad": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "h2b_probe_modmul": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "h2b_launch_count": (_u64, []),
+    "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
+    "h2b_msm_window_bits": (ctypes.c_int, [_u64]),
+}
+
+PROF_MSM_ACCUMULATE, PROF_MSM_TOTAL, PROF_NTT_PASSES, PROF_BATCH_INVERT, PROF_QUOTIENT, PROF_PERMUTE_SORT = range(6)
+
+
+def prof_read(prof_id):
+    ms, cnt = ctypes.c_double(), ctypes.c_int()
+    lib().h2b_prof_read(prof_id, ctypes.byref(ms), ctypes.byref(cnt))
+    return ms.value, cnt.value
+
+_lib = None
+
+
+def lib():
+    """Loads libhalo2_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing; run `python halo2-gpu_b200/build.py` "
+                                    "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return [n for n in _SIGS if hasattr(lib(), n)]
+
+
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+def check(err, who):
+    if err.code != 0:
+        msg = ctypes.string_at(err.message).decode(errors="replace") if err.message else ""
+        if err.message:
+            _libc.free(err.message)
+        raise Halo2GpuError(err.code, msg, who)
+    if err.message:
+        _libc.free(err.message)
+
+
+def call(name, *args):
+    """Calls a RustError-returning entry point and raises on a non-zero code."""
+    check(getattr(lib(), name)(*args), name)
+
+
+# --- device memory helpers (torch as the allocator) ---------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def stream_handle(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def dev_empty(nbytes):
+    torch = _torch()
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+
+
+def to_dev(arr):
+    """numpy (any dtype) -> torch uint8 device tensor with the same bytes."""
+    torch = _torch()
+    a = np.ascontiguousarray(arr)
+    t = torch.from_numpy(a.view(np.uint8).reshape(-1))
+    return t.to("cuda")
+
+
+def to_host(t, shape=None):
+    a = t.cpu().numpy().view(np.uint64)
+    return a.reshape(shape) if shape is not None else a.reshape(-1, 4)
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def ffi(p):
+    return FFITraitObject(ctypes.c_void_p(p) if isinstance(p, int) else p)
+
+
+def host_ffi(arr):
+    """FFITraitObject carrying the address of a numpy array (kept alive by caller)."""
+    return FFITraitObject(ctypes.c_void_p(arr.ctypes.data))
+
+
+def ffi_array(ptrs):
+    arr = (FFITraitObject * max(len(ptrs), 1))()
+    for i, p in enumerate(ptrs):
+        arr[i].ptr = p if isinstance(p, int) else p.value
+    return arr
+
+
+def _scalar_bytes(x):
+    """Accepts a python int (plain value) or 32 Montgomery bytes / (1,4) limbs."""
+    if isinstance(x, int):
+        return np.frombuffer(fields.fr_scalar(x), dtype=np.uint64).copy()
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint64).reshape(4))
+
+
+# --- MSM (halo2_proofs/src/cuda/funcs/multiexp.rs) -------------------------------
+
+def multiexp_gpu(scalars, bases, stream=None):
+    """_halo2_multiexp: host scalars (n,4) and host bases (n,8) -> (12,) Jacobian."""
+    torch = _torch()
+    n = int(scalars.shape[0])
+    sc = np.ascontiguousarray(scalars, dtype=np.uint64)
+    bs = np.ascontiguousarray(bases, dtype=np.uint64)
+    out = np.zeros(12, dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_multiexp_workspace_size(n))
+    a, b, o = host_ffi(sc), host_ffi(bs), host_ffi(out)
+    call("_halo2_multiexp", ctypes.byref(a), ctypes.byref(b), ctypes.byref(o), n, ptr(ws), ws.numel(),
+         stream_handle(stream))
+    del torch
+    return out
+
+
+def multiexp_gpu_device_bases(scalars, d_bases, n=None, stream=None):
+    n = int(scalars.shape[0]) if n is None else n
+    sc = np.ascontiguousarray(scalars, dtype=np.uint64)
+    out = np.zeros(12, dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_multiexp_device_bases_workspace_size(n))
+    a, o = host_ffi(sc), host_ffi(out)
+    call("_halo2_multiexp_device_bases", ctypes.byref(a), ptr(d_bases), ctypes.byref(o), n, ptr(ws), ws.numel(),
+         stream_handle(stream))
+    return out
+
+
+def multiexp_gpu_device_scalars_device_bases(d_scalars, d_bases, n, ws=None, stream=None):
+    out = np.zeros(12, dtype=np.uint64)
+    need = lib()._halo2_multiexp_device_scalars_device_bases_workspace_size(n)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    o = host_ffi(out)
+    call("_halo2_multiexp_device_scalars_device_bases", ptr(d_scalars), ptr(d_bases), ctypes.byref(o), n, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return out
+
+
+def msm_device(d_scalars, d_bases, d_out, n, ws, stream=None):
+    call("h2b_msm_device", ptr(d_scalars), ptr(d_bases), ptr(d_out), n, ptr(ws), ws.numel(), stream_handle(stream))
+
+
+def msm_workspace(n):
+    return dev_empty(lib()._halo2_multiexp_device_scalars_device_bases_workspace_size(n))
+
+
+# --- NTT (halo2_proofs/src/cuda/funcs/ntt.rs, poly/domain.rs) ----------------------
+
+def fft_normal(ntt_type, log_n, values, omega, divisor, stream=None):
+    """_halo2_fft_normal: host in/out (types 1,2,3,4,6 with extend = log_n)."""
+    inp = np.ascontiguousarray(values, dtype=np.uint64)
+    out = np.zeros_like(inp)
+    om, dv = _scalar_bytes(omega), _scalar_bytes(divisor)
+    ws = dev_empty(lib()._halo2_fft_normal_workspace_size(ntt_type, log_n, log_n))
+    call("_halo2_fft_normal", ntt_type, log_n, inp.ctypes.data, out.ctypes.data, om.ctypes.data, dv.ctypes.data,
+         ptr(ws), ws.numel(), stream_handle(stream))
+    return out
+
+
+def fft_normal_to_device(ntt_type, log_n, d_in, d_out, omega, divisor, ws=None, stream=None):
+    d_om = to_dev(_scalar_bytes(omega))
+    dv = _scalar_bytes(divisor)
+    need = lib()._halo2_fft_normal_to_device_workspace_size(ntt_type, log_n, log_n)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    call("_halo2_fft_normal_to_device", ntt_type, log_n, ptr(d_in), ptr(d_out), ptr(d_om), dv.ctypes.data, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return d_out
+
+
+def cosetfft(log_n, extend_log_n, values, extended_omega, stream=None):
+    inp = np.ascontiguousarray(values, dtype=np.uint64)
+    out = np.zeros((1 << extend_log_n, 4), dtype=np.uint64)
+    om = _scalar_bytes(extended_omega)
+    one = _scalar_bytes(1)
+    ws = dev_empty(lib()._halo2_fft_normal_workspace_size(NTT_COSET, log_n, extend_log_n))
+    call("_halo2_cosetfft", NTT_COSET, log_n, extend_log_n, inp.ctypes.data, out.ctypes.data, om.ctypes.data,
+         one.ctypes.data, ptr(ws), ws.numel(), stream_handle(stream))
+    return out
+
+
+def fft_many(ntt_type, log_n, extend_log_n, polys, omega, divisor, stream=None):
+    """_halo2_fft_many: list of host polys -> list of host outputs."""
+    ins = [np.ascontiguousarray(p, dtype=np.uint64) for p in polys]
+    la = extend_log_n if ntt_type in (NTT_COSET, NTT_ICOSET) else log_n
+    outs = [np.zeros((1 << la, 4), dtype=np.uint64) for _ in polys]
+    d_om = to_dev(_scalar_bytes(omega))
+    dv = _scalar_bytes(divisor)
+    dvo = host_ffi(dv)
+    ws = dev_empty(lib()._halo2_fft_many_workspace_size(ntt_type, log_n, extend_log_n))
+    call("_halo2_fft_many", ntt_type, len(ins), log_n, extend_log_n, ffi_array([a.ctypes.data for a in ins]),
+         ffi_array([a.ctypes.data for a in outs]), ptr(d_om), ctypes.byref(dvo), ptr(ws), ws.numel(),
+         stream_handle(stream))
+    return outs
+
+
+def fft_many_to_device(ntt_type, log_n, extend_log_n, d_ins, d_outs, omega, divisor, input_on_device=True,
+                       ws=None, stream=None):
+    d_om = to_dev(_scalar_bytes(omega))
+    dv = _scalar_bytes(divisor)
+    dvo = host_ffi(dv)
+    need = lib()._halo2_fft_many_to_device_workspace_size(ntt_type, log_n, extend_log_n)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    ins = [t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data for t in d_ins]
+    call("_halo2_fft_many_to_device", ntt_type, len(d_ins), log_n, extend_log_n, ffi_array(ins),
+         ffi_array([t.data_ptr() for t in d_outs]), ptr(d_om), ctypes.byref(dvo), bool(input_on_device), ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return d_outs
+
+
+# --- batch inversion and products --------------------------------------------------
+
+def batch_invert_device(d, n, field_type=0, stream=None):
+    call("_halo2_batch_invert", ptr(d), field_type, n, stream_handle(stream))
+
+
+def batch_invert_device_scratch(d, n, field_type=0, ws=None, stream=None):
+    need = lib().h2b_batch_invert_workspace_size(n)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    call("h2b_batch_invert", ptr(d), field_type, n, ptr(ws), ws.numel(), stream_handle(stream))
+
+
+def grand_product(inp, prefix, offset=0, length=None, stream=None):
+    a = np.ascontiguousarray(inp, dtype=np.uint64)
+    length = a.shape[0] - offset if length is None else length
+    out = np.zeros_like(a)
+    pf = _scalar_bytes(prefix)
+    ws = dev_empty(lib()._halo2_grand_product_workspace_size(length))
+    o, i, p = host_ffi(out), host_ffi(a), host_ffi(pf)
+    call("_halo2_grand_product", ctypes.byref(o), ctypes.byref(i), ctypes.byref(p), length, offset, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return out
+
+
+def grand_product_device(d_inout, d_prefix, length, offset=0, stream=None):
+    a, p = ffi(d_inout.data_ptr()), ffi(d_prefix.data_ptr())
+    call("_halo2_grand_product_device_inputs", ctypes.byref(a), ctypes.byref(p), length, offset,
+         stream_handle(stream))
+
+
+def lookup_product(permuted_input, permuted_table, compressed_input, compressed_table, beta, gamma, offset=0,
+                   length=None, stream=None):
+    arrs = [np.ascontiguousarray(x, dtype=np.uint64) for x in
+            (permuted_input, permuted_table, compressed_input, compressed_table)]
+    length = arrs[0].shape[0] - offset if length is None else length
+    out = np.zeros_like(arrs[0])
+    d_b, d_g = to_dev(_scalar_bytes(beta)), to_dev(_scalar_bytes(gamma))
+    ws = dev_empty(lib()._halo2_commit_product_workspace_size(length))
+    objs = [host_ffi(out)] + [host_ffi(a) for a in arrs]
+    call("_halo2_commit_product", *[ctypes.byref(o) for o in objs], ptr(d_b), ptr(d_g), length, offset, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return out
+
+
+def lookup_product_device(d_out, d_pin, d_ptab, d_cin, d_ctab, d_beta, d_gamma, length, offset=0, stream=None):
+    objs = [ffi(t.data_ptr()) for t in (d_out, d_pin, d_ptab, d_cin, d_ctab)]
+    call("_halo2_commit_product_device_inputs", *[ctypes.byref(o) for o in objs], ptr(d_beta), ptr(d_gamma), length,
+         offset, stream_handle(stream))
+
+
+def permutation_product(modified_values, permutations, values, beta, gamma, delta, omega, deltaomega, offset=0,
+                        length=None, stream=None):
+    """Host variant; returns (modified_values, advanced deltaomega limbs)."""
+    mv = np.ascontiguousarray(modified_values, dtype=np.uint64).copy()
+    perms = [np.ascontiguousarray(p, dtype=np.uint64) for p in permutations]
+    vals = [np.ascontiguousarray(v, dtype=np.uint64) for v in values]
+    length = mv.shape[0] if length is None else length
+    d_sc = [to_dev(_scalar_bytes(x)) for x in (beta, gamma, delta, omega, deltaomega)]
+    ws = dev_empty(lib()._halo2_permutation_product_workspace_size(length))
+    m = host_ffi(mv)
+    call("_halo2_permutation_product", ctypes.byref(m), ffi_array([p.ctypes.data for p in perms]),
+         ffi_array([v.ctypes.data for v in vals]), *[ptr(t) for t in d_sc], length, offset, len(perms), ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return mv, to_host(d_sc[4])[0]
+
+
+def permutation_product_device(d_mod, d_perms, d_vals, d_beta, d_gamma, d_delta, d_omega, d_deltaomega, length,
+                               offset=0, stream=None):
+    m = ffi(d_mod.data_ptr())
+    call("_halo2_permutation_product_device_inputs", ctypes.byref(m), ffi_array([t.data_ptr() for t in d_perms]),
+         ffi_array([t.data_ptr() for t in d_vals]), ptr(d_beta), ptr(d_gamma), ptr(d_delta), ptr(d_omega),
+         ptr(d_deltaomega), length, offset, len(d_perms), None, 0, stream_handle(stream))
+
+
+def permute_expression_pair_device(d_in, d_table, d_pin, d_ptab, n, usable_rows, stream=None):
+    ws = dev_empty(lib()._halo2_permute_expression_pair_workspace_size(n, usable_rows))
+    call("_halo2_permute_expression_pair", ptr(d_in), ptr(d_table), ptr(d_pin), ptr(d_ptab), n, usable_rows,
+         ptr(ws), ws.numel(), stream_handle(stream))
+
+
+# --- device-side generators ------------------------------------------------------
+
+def random_fr_device(n, seed, mix=0, stream=None):
+    d = dev_empty(32 * n)
+    call("h2b_random_fr", ptr(d), n, seed, mix, stream_handle(stream))
+    return d
+
+
+def powers_device(x, n, stream=None):
+    d = dev_empty(32 * n)
+    call("h2b_powers", ptr(d), n, ptr(to_dev(_scalar_bytes(x))), stream_handle(stream))
+    return d
+
+
+def srs_device(tau, n, stream=None):
+    """[tau^i] G, i < n, as a device tensor of n affine points (64 bytes each)."""
+    pw = powers_device(tau, n, stream)
+    table = to_dev(fields.g1_pow2_table(256))
+    out = dev_empty(64 * n)
+    call("h2b_srs_from_powers", ptr(out), ptr(pw), n, ptr(table), stream_handle(stream))
+    return out

@@ -1,0 +1,71 @@
+"""Builds libhalo2_gpu.so (sm_100a) in-tree from csrc/*.cu.
+
+Each translation unit is compiled in parallel with
+`nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`, objects go to
+_build/ (rebuilt when a source or header is newer), and the shared library
+lands next to this file so it travels with the repository snapshot.
+"""
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libhalo2_gpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+         "--expt-relaxed-constexpr", "-I", CSRC]
+
+
+def _sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def _newest_header():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    return max((os.path.getmtime(h) for h in hs), default=0.0)
+
+
+def _compile(src, verbose):
+    obj = os.path.join(BUILD, src[:-3] + ".o")
+    path = os.path.join(CSRC, src)
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), _newest_header()):
+        return obj, None
+    cmd = [NVCC, *ARCH, *FLAGS, "-c", path, "-o", obj]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        return None, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"
+    return obj, (r.stderr if verbose else None)
+
+
+def build(verbose=False, jobs=None):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = _sources()
+    jobs = jobs or min(len(srcs), os.cpu_count() or 4)
+    objs, errors = [], []
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        for obj, msg in ex.map(lambda s: _compile(s, verbose), srcs):
+            if obj is None:
+                errors.append(msg)
+            else:
+                objs.append(obj)
+                if msg:
+                    print(msg)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n\n".join(errors))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

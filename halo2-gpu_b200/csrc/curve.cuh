@@ -1,0 +1,202 @@
+// BN254 G1 (y^2 = x^3 + 3 over Fq) point arithmetic for the MSM.
+//
+// Affine points are 64 bytes {x, y} in Montgomery form with the point at
+// infinity encoded as (0, 0) -- the halo2curves `G1Affine` memory image the
+// reference passes to its MSM (halo2_proofs/cuda/include/curve/xyzz_t.hpp:49-50).
+// Bucket accumulators use XYZZ coordinates (x = X/ZZ, y = Y/ZZZ, ZZ^3 = ZZZ^2,
+// infinity <=> ZZ == 0) with the EFD formulas madd-2008-s (8M+2S),
+// add-2008-s (12M+2S), mdbl-2008-s-1 and dbl-2008-s-1, written from the
+// published formulas.  The MSM result leaves the device as the reference's
+// 96-byte Jacobian image {X, Y, Z}: affine coordinates with Z = 1, or
+// (0, 1, 0) for infinity (halo2_proofs/cuda/include/kernel/pippenger.h:659-668,
+// halo2_proofs/cuda/include/curve/jacobian_t.hpp:64-83).
+#pragma once
+#include "field.cuh"
+
+namespace h2b {
+
+struct G1Affine {
+    Fq x, y;
+};
+
+struct G1Xyzz {
+    Fq X, Y, ZZ, ZZZ;
+};
+
+struct G1Jac {
+    Fq X, Y, Z;
+};
+
+H2B_DEV bool is_inf(const G1Affine& p) { return p.x.is_zero() && p.y.is_zero(); }
+H2B_DEV bool is_inf(const G1Xyzz& p) { return p.ZZ.is_zero(); }
+
+H2B_DEV G1Xyzz xyzz_inf()
+{
+    G1Xyzz r;
+    r.X = Fq::zero(); r.Y = Fq::zero(); r.ZZ = Fq::zero(); r.ZZZ = Fq::zero();
+    return r;
+}
+
+H2B_DEV G1Xyzz xyzz_from_affine(const G1Affine& p)
+{
+    if (is_inf(p)) return xyzz_inf();
+    G1Xyzz r;
+    r.X = p.x; r.Y = p.y; r.ZZ = Fq::one(); r.ZZZ = Fq::one();
+    return r;
+}
+
+H2B_DEV G1Affine ld_affine(const G1Affine* p)
+{
+    G1Affine r;
+    r.x = ldg(&p->x);
+    r.y = ldg(&p->y);
+    return r;
+}
+
+H2B_DEV G1Xyzz ld_xyzz(const G1Xyzz* p)
+{
+    G1Xyzz r;
+    r.X = ld(&p->X); r.Y = ld(&p->Y); r.ZZ = ld(&p->ZZ); r.ZZZ = ld(&p->ZZZ);
+    return r;
+}
+H2B_DEV void st_xyzz(G1Xyzz* p, const G1Xyzz& a)
+{
+    st(&p->X, a.X); st(&p->Y, a.Y); st(&p->ZZ, a.ZZ); st(&p->ZZZ, a.ZZZ);
+}
+
+// mdbl-2008-s-1: double an affine point into XYZZ.
+H2B_DEV G1Xyzz xyzz_dbl_affine(const G1Affine& p)
+{
+    if (is_inf(p) || p.y.is_zero()) return xyzz_inf();
+    Fq U = fdbl(p.y);
+    Fq V = fsqr(U);
+    Fq W = U * V;
+    Fq S = p.x * V;
+    Fq xx = fsqr(p.x);
+    Fq M = fdbl(xx) + xx;
+    G1Xyzz r;
+    r.X = fsqr(M) - fdbl(S);
+    r.Y = M * (S - r.X) - W * p.y;
+    r.ZZ = V;
+    r.ZZZ = W;
+    return r;
+}
+
+// dbl-2008-s-1 (a = 0).
+H2B_DEV G1Xyzz xyzz_dbl(const G1Xyzz& p)
+{
+    if (is_inf(p) || p.Y.is_zero()) return xyzz_inf();
+    Fq U = fdbl(p.Y);
+    Fq V = fsqr(U);
+    Fq W = U * V;
+    Fq S = p.X * V;
+    Fq xx = fsqr(p.X);
+    Fq M = fdbl(xx) + xx;
+    G1Xyzz r;
+    r.X = fsqr(M) - fdbl(S);
+    r.Y = M * (S - r.X) - W * p.Y;
+    r.ZZ = V * p.ZZ;
+    r.ZZZ = W * p.ZZZ;
+    return r;
+}
+
+// madd-2008-s: acc += q (q affine), with the exceptional cases handled.
+H2B_DEV void xyzz_madd(G1Xyzz& acc, const G1Affine& q)
+{
+    if (is_inf(q)) return;
+    if (is_inf(acc)) {
+        acc.X = q.x; acc.Y = q.y; acc.ZZ = Fq::one(); acc.ZZZ = Fq::one();
+        return;
+    }
+    Fq U2 = q.x * acc.ZZ;
+    Fq S2 = q.y * acc.ZZZ;
+    Fq P = U2 - acc.X;
+    Fq R = S2 - acc.Y;
+    if (P.is_zero()) {
+        if (R.is_zero()) acc = xyzz_dbl_affine(q);
+        else acc = xyzz_inf();
+        return;
+    }
+    Fq PP = fsqr(P);
+    Fq PPP = P * PP;
+    Fq Q = acc.X * PP;
+    Fq X3 = fsqr(R) - PPP - fdbl(Q);
+    acc.Y = R * (Q - X3) - acc.Y * PPP;
+    acc.X = X3;
+    acc.ZZ = acc.ZZ * PP;
+    acc.ZZZ = acc.ZZZ * PPP;
+}
+
+// add-2008-s: acc += q (both XYZZ).
+H2B_DEV void xyzz_add(G1Xyzz& acc, const G1Xyzz& q)
+{
+    if (is_inf(q)) return;
+    if (is_inf(acc)) { acc = q; return; }
+    Fq U1 = acc.X * q.ZZ;
+    Fq U2 = q.X * acc.ZZ;
+    Fq S1 = acc.Y * q.ZZZ;
+    Fq S2 = q.Y * acc.ZZZ;
+    Fq P = U2 - U1;
+    Fq R = S2 - S1;
+    if (P.is_zero()) {
+        if (R.is_zero()) acc = xyzz_dbl(acc);
+        else acc = xyzz_inf();
+        return;
+    }
+    Fq PP = fsqr(P);
+    Fq PPP = P * PP;
+    Fq Q = U1 * PP;
+    Fq X3 = fsqr(R) - PPP - fdbl(Q);
+    acc.Y = R * (Q - X3) - S1 * PPP;
+    acc.X = X3;
+    acc.ZZ = acc.ZZ * q.ZZ * PP;
+    acc.ZZZ = acc.ZZZ * q.ZZZ * PPP;
+}
+
+H2B_DEV G1Affine affine_neg(const G1Affine& p)
+{
+    G1Affine r;
+    r.x = p.x;
+    r.y = p.y.is_zero() ? p.y : fneg(p.y);
+    return r;
+}
+
+H2B_DEV G1Xyzz xyzz_neg(const G1Xyzz& p)
+{
+    G1Xyzz r = p;
+    if (!is_inf(p)) r.Y = fneg(p.Y);
+    return r;
+}
+
+// XYZZ -> reference Jacobian image (affine with Z = 1; infinity = (0, 1, 0)).
+H2B_DEV G1Jac xyzz_to_jac_affine(const G1Xyzz& p)
+{
+    G1Jac r;
+    if (is_inf(p)) {
+        r.X = Fq::zero(); r.Y = Fq::one(); r.Z = Fq::zero();
+        return r;
+    }
+    Fq inv = finv(p.ZZ * p.ZZZ);      // 1 / (ZZ * ZZZ)
+    Fq izz = inv * p.ZZZ;             // 1 / ZZ
+    Fq izzz = inv * p.ZZ;             // 1 / ZZZ
+    r.X = p.X * izz;
+    r.Y = p.Y * izzz;
+    r.Z = Fq::one();
+    return r;
+}
+
+// Scalar multiplication by a small non-negative integer (double-and-add).
+H2B_DEV G1Xyzz xyzz_mul_u32(const G1Xyzz& p, uint32_t k)
+{
+    G1Xyzz r = xyzz_inf();
+    if (k == 0 || is_inf(p)) return r;
+    int top = 31 - __clz(k);
+#pragma unroll 1
+    for (int i = top; i >= 0; i--) {
+        r = xyzz_dbl(r);
+        if ((k >> i) & 1u) xyzz_add(r, p);
+    }
+    return r;
+}
+
+} // namespace h2b

@@ -1,0 +1,316 @@
+// BN254 prime-field arithmetic for sm_100a: 8 x 32-bit limbs, Montgomery form
+// with R = 2^256, little-endian limb order.  Memory layout is byte-identical to
+// halo2curves' `Fr` / `Fq` (4 x u64 little-endian, Montgomery form), which is
+// what the reference's device type `fr_t` / `fp_t` stores
+// (halo2_proofs/cuda/include/field/alt_bn128.hpp:15-43 pins the moduli,
+// R^2 mod m, R mod m and n0' = -m^-1 mod 2^64).
+//
+// Multiplication is word-serial Montgomery (CIOS): for each word b_i of the
+// multiplier, t += a*b_i, m = t_0 * n0', t += m*p, t >>= 32.  Each step is one
+// inline-PTX block of `mad.lo.cc` / `madc.hi.cc` chains so the carry flag never
+// crosses an asm boundary.  The loop invariant t < 2p (p < 2^254) means the
+// 9th word of t never carries out and the result needs at most one conditional
+// subtraction.  Every value handed out of this header is fully reduced
+// (canonical Montgomery residue), so outputs are bit-exact with any other
+// correct implementation.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace h2b {
+
+#define H2B_DEV __device__ __forceinline__
+
+// Scalar field r (halo2curves bn256::Fr); constants from alt_bn128.hpp:30-43.
+struct FrCfg {
+    static constexpr uint32_t M0 = 0xf0000001u, M1 = 0x43e1f593u, M2 = 0x79b97091u, M3 = 0x2833e848u,
+                              M4 = 0x8181585du, M5 = 0xb85045b6u, M6 = 0xe131a029u, M7 = 0x30644e72u;
+    static constexpr uint32_t N0 = 0xefffffffu;  // low word of 0xc2e1f593efffffff
+    static constexpr uint32_t O0 = 0x4ffffffbu, O1 = 0xac96341cu, O2 = 0x9f60cd29u, O3 = 0x36fc7695u,
+                              O4 = 0x7879462eu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+    static constexpr uint32_t Q0 = 0xae216da7u, Q1 = 0x1bb8e645u, Q2 = 0xe35c59e3u, Q3 = 0x53fe3ab1u,
+                              Q4 = 0x53bb8085u, Q5 = 0x8c49833du, Q6 = 0x7f4e44a5u, Q7 = 0x0216d0b1u;
+};
+
+// Base field p (halo2curves bn256::Fq); constants from alt_bn128.hpp:15-29.
+struct FqCfg {
+    static constexpr uint32_t M0 = 0xd87cfd47u, M1 = 0x3c208c16u, M2 = 0x6871ca8du, M3 = 0x97816a91u,
+                              M4 = 0x8181585du, M5 = 0xb85045b6u, M6 = 0xe131a029u, M7 = 0x30644e72u;
+    static constexpr uint32_t N0 = 0xe4866389u;  // low word of 0x87d20782e4866389
+    static constexpr uint32_t O0 = 0xc58f0d9du, O1 = 0xd35d438du, O2 = 0xf5c70b3du, O3 = 0x0a78eb28u,
+                              O4 = 0x7879462cu, O5 = 0x666ea36fu, O6 = 0x9a07df2fu, O7 = 0x0e0a77c1u;
+    static constexpr uint32_t Q0 = 0x538afa89u, Q1 = 0xf32cfc5bu, Q2 = 0xd44501fbu, Q3 = 0xb5e71911u,
+                              Q4 = 0x0a417ff6u, Q5 = 0x47ab1effu, Q6 = 0xcab8351fu, Q7 = 0x06d89f71u;
+};
+
+template <class C>
+struct Fp {
+    uint32_t v[8];
+
+    H2B_DEV static Fp zero()
+    {
+        Fp r;
+#pragma unroll
+        for (int i = 0; i < 8; i++) r.v[i] = 0;
+        return r;
+    }
+    H2B_DEV static Fp one()
+    {
+        Fp r;
+        r.v[0] = C::O0; r.v[1] = C::O1; r.v[2] = C::O2; r.v[3] = C::O3;
+        r.v[4] = C::O4; r.v[5] = C::O5; r.v[6] = C::O6; r.v[7] = C::O7;
+        return r;
+    }
+    H2B_DEV static Fp r2()
+    {
+        Fp r;
+        r.v[0] = C::Q0; r.v[1] = C::Q1; r.v[2] = C::Q2; r.v[3] = C::Q3;
+        r.v[4] = C::Q4; r.v[5] = C::Q5; r.v[6] = C::Q6; r.v[7] = C::Q7;
+        return r;
+    }
+    H2B_DEV bool is_zero() const
+    {
+        uint32_t acc = v[0] | v[1] | v[2] | v[3] | v[4] | v[5] | v[6] | v[7];
+        return acc == 0;
+    }
+    H2B_DEV bool operator==(const Fp& o) const
+    {
+        uint32_t acc = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc |= v[i] ^ o.v[i];
+        return acc == 0;
+    }
+    H2B_DEV bool operator!=(const Fp& o) const { return !(*this == o); }
+};
+
+using Fr = Fp<FrCfg>;
+using Fq = Fp<FqCfg>;
+
+// One Montgomery word step: t (9 words, t < 2p on entry, t8 == 0) becomes
+// (t + a*b + m*p) / 2^32 with m chosen so the low word vanishes.
+template <class C>
+H2B_DEV void mont_step(uint32_t (&t)[9], const uint32_t (&a)[8], uint32_t b)
+{
+    asm("{\n\t"
+        ".reg .u32 m;\n\t"
+        "mad.lo.cc.u32  %0, %9, %17, %0;\n\t"
+        "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"
+        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
+        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
+        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
+        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
+        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
+        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
+        "addc.u32       %8, %8, 0;\n\t"
+        "mad.hi.cc.u32  %1, %9, %17, %1;\n\t"
+        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
+        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
+        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
+        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
+        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
+        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
+        "madc.hi.u32    %8, %16, %17, %8;\n\t"
+        "mul.lo.u32     m, %0, %26;\n\t"
+        "mad.lo.cc.u32  %0, m, %18, %0;\n\t"
+        "madc.lo.cc.u32 %1, m, %19, %1;\n\t"
+        "madc.lo.cc.u32 %2, m, %20, %2;\n\t"
+        "madc.lo.cc.u32 %3, m, %21, %3;\n\t"
+        "madc.lo.cc.u32 %4, m, %22, %4;\n\t"
+        "madc.lo.cc.u32 %5, m, %23, %5;\n\t"
+        "madc.lo.cc.u32 %6, m, %24, %6;\n\t"
+        "madc.lo.cc.u32 %7, m, %25, %7;\n\t"
+        "addc.u32       %8, %8, 0;\n\t"
+        "mad.hi.cc.u32  %1, m, %18, %1;\n\t"
+        "madc.hi.cc.u32 %2, m, %19, %2;\n\t"
+        "madc.hi.cc.u32 %3, m, %20, %3;\n\t"
+        "madc.hi.cc.u32 %4, m, %21, %4;\n\t"
+        "madc.hi.cc.u32 %5, m, %22, %5;\n\t"
+        "madc.hi.cc.u32 %6, m, %23, %6;\n\t"
+        "madc.hi.cc.u32 %7, m, %24, %7;\n\t"
+        "madc.hi.u32    %8, m, %25, %8;\n\t"
+        "}"
+        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]),
+          "+r"(t[8])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(b),
+          "n"(C::M0), "n"(C::M1), "n"(C::M2), "n"(C::M3), "n"(C::M4), "n"(C::M5), "n"(C::M6), "n"(C::M7),
+          "n"(C::N0));
+    // t0 is now zero; shift one word down.
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = t[i + 1];
+    t[8] = 0;
+}
+
+// r = t - m if t >= m else t  (t < 2m).
+template <class C>
+H2B_DEV void cond_sub(uint32_t (&r)[8], const uint32_t (&t)[8])
+{
+    uint32_t s[8], bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7]),
+          "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+          "n"(C::M0), "n"(C::M1), "n"(C::M2), "n"(C::M3), "n"(C::M4), "n"(C::M5), "n"(C::M6), "n"(C::M7));
+#pragma unroll
+    for (int i = 0; i < 8; i++) r[i] = bw ? t[i] : s[i];
+}
+
+template <class C>
+H2B_DEV Fp<C> operator*(const Fp<C>& a, const Fp<C>& b)
+{
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) mont_step<C>(t, a.v, b.v[i]);
+    Fp<C> r;
+    uint32_t lo[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) lo[i] = t[i];
+    cond_sub<C>(r.v, lo);
+    return r;
+}
+
+template <class C>
+H2B_DEV Fp<C> operator+(const Fp<C>& a, const Fp<C>& b)
+{
+    uint32_t t[8];
+    asm("add.cc.u32  %0, %8, %16;\n\t"
+        "addc.cc.u32 %1, %9, %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7])
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    Fp<C> r;
+    cond_sub<C>(r.v, t);
+    return r;
+}
+
+template <class C>
+H2B_DEV Fp<C> operator-(const Fp<C>& a, const Fp<C>& b)
+{
+    Fp<C> r;
+    uint32_t bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(bw)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    // On borrow add the modulus back (bw is 0 or all-ones).
+    const uint32_t q0 = bw & C::M0, q1 = bw & C::M1, q2 = bw & C::M2, q3 = bw & C::M3;
+    const uint32_t q4 = bw & C::M4, q5 = bw & C::M5, q6 = bw & C::M6, q7 = bw & C::M7;
+    asm("add.cc.u32  %0, %0, %8;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, %10;\n\t"
+        "addc.cc.u32 %3, %3, %11;\n\t"
+        "addc.cc.u32 %4, %4, %12;\n\t"
+        "addc.cc.u32 %5, %5, %13;\n\t"
+        "addc.cc.u32 %6, %6, %14;\n\t"
+        "addc.u32    %7, %7, %15;"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7])
+        : "r"(q0), "r"(q1), "r"(q2), "r"(q3), "r"(q4), "r"(q5), "r"(q6), "r"(q7));
+    return r;
+}
+
+template <class C>
+H2B_DEV Fp<C>& operator*=(Fp<C>& a, const Fp<C>& b) { a = a * b; return a; }
+template <class C>
+H2B_DEV Fp<C>& operator+=(Fp<C>& a, const Fp<C>& b) { a = a + b; return a; }
+template <class C>
+H2B_DEV Fp<C>& operator-=(Fp<C>& a, const Fp<C>& b) { a = a - b; return a; }
+
+template <class C>
+H2B_DEV Fp<C> fneg(const Fp<C>& a) { return Fp<C>::zero() - a; }
+template <class C>
+H2B_DEV Fp<C> fdbl(const Fp<C>& a) { return a + a; }
+template <class C>
+H2B_DEV Fp<C> fsqr(const Fp<C>& a) { return a * a; }
+
+// Montgomery residue -> canonical integer (multiply by 1).
+template <class C>
+H2B_DEV Fp<C> from_mont(const Fp<C>& a)
+{
+    Fp<C> one_int = Fp<C>::zero();
+    one_int.v[0] = 1;
+    return a * one_int;
+}
+template <class C>
+H2B_DEV Fp<C> to_mont(const Fp<C>& a) { return a * Fp<C>::r2(); }
+
+// a^e for a 256-bit exponent given as 8 little-endian words; 4-bit fixed window.
+template <class C>
+H2B_DEV Fp<C> fpow(const Fp<C>& a, const uint32_t (&e)[8])
+{
+    Fp<C> tbl[16];
+    tbl[0] = Fp<C>::one();
+    tbl[1] = a;
+#pragma unroll 1
+    for (int i = 2; i < 16; i++) tbl[i] = tbl[i - 1] * a;
+    Fp<C> r = Fp<C>::one();
+#pragma unroll 1
+    for (int w = 63; w >= 0; w--) {
+        r = r * r; r = r * r; r = r * r; r = r * r;
+        uint32_t d = (e[w >> 3] >> ((w & 7) * 4)) & 15u;
+        if (d) r = r * tbl[d];
+    }
+    return r;
+}
+
+// Fermat inverse a^(m-2); inverse of zero is zero.
+template <class C>
+H2B_DEV Fp<C> finv(const Fp<C>& a)
+{
+    const uint32_t e[8] = {C::M0 - 2u, C::M1, C::M2, C::M3, C::M4, C::M5, C::M6, C::M7};
+    return fpow<C>(a, e);
+}
+
+template <class C>
+H2B_DEV Fp<C> ldg(const Fp<C>* p)
+{
+    Fp<C> r;
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4 x = __ldg(q), y = __ldg(q + 1);
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = x.z; r.v[3] = x.w;
+    r.v[4] = y.x; r.v[5] = y.y; r.v[6] = y.z; r.v[7] = y.w;
+    return r;
+}
+template <class C>
+H2B_DEV Fp<C> ld(const Fp<C>* p)
+{
+    Fp<C> r;
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4 x = q[0], y = q[1];
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = x.z; r.v[3] = x.w;
+    r.v[4] = y.x; r.v[5] = y.y; r.v[6] = y.z; r.v[7] = y.w;
+    return r;
+}
+template <class C>
+H2B_DEV void st(Fp<C>* p, const Fp<C>& a)
+{
+    uint4* q = reinterpret_cast<uint4*>(p);
+    q[0] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+    q[1] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
+}
+
+} // namespace h2b

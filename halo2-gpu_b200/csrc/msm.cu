@@ -1,0 +1,503 @@
+// Pippenger G1 MSM behind Params::commit / commit_lagrange
+// (halo2_proofs/src/poly/kzg/commitment.rs:456-575) and the reference entry
+// points `_halo2_multiexp{,_device_bases,_device_scalars_device_bases}`
+// (halo2_proofs/cuda/src/multiexp.cu:260-525, declared at
+// halo2_proofs/src/cuda/culib.rs:30-70).
+//
+// Pipeline (all stream-ordered, no host round trip until the 96-byte result):
+//  1. canon:   scalars leave Montgomery form (one modmul each) into scratch;
+//              the caller's scalars are never mutated.
+//  2. digits:  signed c-bit windows, digits in [-(2^(c-1)-1), 2^(c-1)], so a
+//              window needs 2^(c-1) buckets; a negative digit adds -P.
+//  3. sort:    counting sort of (window, bucket) keys -- warp-aggregated
+//              histogram, exclusive scan to bucket offsets, warp-aggregated
+//              scatter of point indices (sign in bit 31).
+//  4. accumulate: the sorted entry list is cut into equal chunks of K entries,
+//              one chunk per thread, so dense buckets (e.g. every scalar == 1
+//              landing in one bucket) cost the same as sparse ones.  A chunk
+//              writes finished buckets directly and the partial sum of the
+//              bucket it started in the middle of to a per-chunk slot.
+//  5. fixup:   each bucket adds the per-chunk partials it spans; buckets that
+//              span many chunks are summed by a CTA-wide tree instead.
+//  6. reduce:  per window, buckets are cut into segments; each segment does
+//              the running-sum trick and scales by its offset, a CTA tree
+//              sums the segments, then 2^(c*w) * W_w is summed over windows.
+//  7. output:  XYZZ -> the reference's Jacobian image {x, y, 1} (or (0,1,0)).
+#include <algorithm>
+#include "abi.cuh"
+#include "curve.cuh"
+#include "msm.cuh"
+#include "prof.cuh"
+#include "scan_u32.cuh"
+
+namespace h2b {
+
+static constexpr int SCALAR_BITS = 254;
+static constexpr uint32_t SIGN_BIT = 0x80000000u;
+static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed serially in fixup
+
+static int g_msm_window_override = 0;
+static int g_msm_chunk_override = 0;
+
+void msm_set_tuning(int window_bits, int chunk)
+{
+    g_msm_window_override = window_bits;
+    g_msm_chunk_override = chunk;
+}
+
+MsmPlan msm_plan(uint64_t n)
+{
+    MsmPlan p;
+    p.n = n;
+    int lg = 0;
+    while ((1ull << (lg + 1)) <= n) lg++;
+    int c;
+    if (g_msm_window_override >= 4 && g_msm_window_override <= 20) c = g_msm_window_override;
+    else if (lg >= 21) c = 16;
+    else if (lg >= 19) c = 15;
+    else if (lg >= 17) c = 13;
+    else if (lg >= 14) c = 12;
+    else if (lg >= 10) c = 10;
+    else c = 7;
+    p.c = c;
+    p.W = (SCALAR_BITS + c - 1) / c + ((SCALAR_BITS % c) == 0 ? 1 : 0);
+    p.H = 1u << (c - 1);
+    p.NB = (uint64_t)p.W * p.H;
+    p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 64u;
+    p.max_entries = n * (uint64_t)p.W;
+    p.max_chunks = (p.max_entries + p.K - 1) / p.K + 1;
+    // segments per window for the running-sum reduction
+    uint32_t L = p.H >= 4096 ? 16u : (p.H >= 256 ? 8u : 4u);
+    if (L > p.H) L = p.H;
+    p.L = L;
+    p.S = p.H / L;
+    return p;
+}
+
+void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host)
+{
+    if (bases_host) sp.add(p.n * sizeof(G1Affine));
+    if (scalar_host) sp.add(p.n * sizeof(Fr));       // host scalars staged here
+    sp.add(p.n * sizeof(Fr));                         // canonical scalars
+    sp.add_n<uint32_t>(p.NB);                         // counts
+    sp.add_n<uint32_t>(p.NB + 1);                     // offsets
+    sp.add_n<uint32_t>(p.NB);                         // cursor
+    sp.add_n<uint32_t>(scan_u32_tiles(p.NB) + 1);     // scan tiles
+    sp.add_n<uint32_t>(p.max_entries);                // sorted entries
+    sp.add_n<G1Xyzz>(p.NB);                           // bucket sums
+    sp.add_n<G1Xyzz>(p.max_chunks);                   // chunk head partials
+    sp.add_n<uint32_t>(p.NB + 1);                     // dense list + count
+    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment sums
+    sp.add_n<G1Xyzz>(p.W);                            // window sums
+    sp.add_n<G1Jac>(1);                               // result
+}
+
+MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host)
+{
+    MsmScratch s;
+    s.bases_stage = bases_host ? (G1Affine*)ar.take(p.n * sizeof(G1Affine)) : nullptr;
+    s.scalar_stage = scalar_host ? (Fr*)ar.take(p.n * sizeof(Fr)) : nullptr;
+    s.canon = (Fr*)ar.take(p.n * sizeof(Fr));
+    s.counts = ar.take_n<uint32_t>(p.NB);
+    s.offsets = ar.take_n<uint32_t>(p.NB + 1);
+    s.cursor = ar.take_n<uint32_t>(p.NB);
+    s.scan_tmp = ar.take_n<uint32_t>(scan_u32_tiles(p.NB) + 1);
+    s.sorted = ar.take_n<uint32_t>(p.max_entries);
+    s.buckets = ar.take_n<G1Xyzz>(p.NB);
+    s.heads = ar.take_n<G1Xyzz>(p.max_chunks);
+    s.dense = ar.take_n<uint32_t>(p.NB + 1);
+    s.segs = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
+    s.wins = ar.take_n<G1Xyzz>(p.W);
+    s.result = ar.take_n<G1Jac>(1);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+__global__ void k_msm_canon(const Fr* __restrict__ sc, Fr* __restrict__ canon, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        st(&canon[i], from_mont(ldg(&sc[i])));
+}
+
+__device__ __forceinline__ uint32_t window_bits(const Fr& s, int bit, int c)
+{
+    int li = bit >> 5, sh = bit & 31;
+    uint64_t lo = s.v[li];
+    uint64_t hi = (li + 1 < 8) ? s.v[li + 1] : 0u;
+    uint64_t v = (lo | (hi << 32)) >> sh;
+    return (uint32_t)(v & ((1ull << c) - 1));
+}
+
+// For each digit: key = w*H + |d| - 1 (or ~0 for zero digits), neg = d < 0.
+template <bool SCATTER>
+__global__ void k_msm_sort(const Fr* __restrict__ canon, uint64_t n, int c, int W, uint32_t H,
+                           uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t full = 1u << c;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = base + threadIdx.x;
+        bool valid = i < n;
+        Fr s = valid ? ldg(&canon[i]) : Fr::zero();
+        uint32_t carry = 0;
+        for (int w = 0; w < W; w++) {
+            uint32_t v = window_bits(s, w * c, c) + carry;
+            int32_t d;
+            if (v > H) { d = (int32_t)v - (int32_t)full; carry = 1; }
+            else { d = (int32_t)v; carry = 0; }
+            uint32_t key = 0xffffffffu;
+            if (valid && d != 0) key = (uint32_t)w * H + (uint32_t)(d < 0 ? -d : d) - 1u;
+            unsigned peers = __match_any_sync(0xffffffffu, key);
+            int leader = __ffs(peers) - 1;
+            if (!SCATTER) {
+                if (key != 0xffffffffu && (int)lane == leader) atomicAdd(&counts_or_cursor[key], __popc(peers));
+            } else {
+                uint32_t b = 0;
+                if (key != 0xffffffffu && (int)lane == leader) b = atomicAdd(&counts_or_cursor[key], __popc(peers));
+                b = __shfl_sync(0xffffffffu, b, leader);
+                if (key != 0xffffffffu) {
+                    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+                    sorted[b + rank] = (uint32_t)i | (d < 0 ? SIGN_BIT : 0u);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ G1Affine load_signed_point(const G1Affine* __restrict__ bases, uint32_t e)
+{
+    G1Affine P = ld_affine(&bases[e & ~SIGN_BIT]);
+    if (e & SIGN_BIT) P = affine_neg(P);
+    return P;
+}
+
+// One thread per chunk of K sorted entries.
+__global__ void __launch_bounds__(128) k_msm_accumulate(const uint32_t* __restrict__ sorted,
+                                                        const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
+                                                        const G1Affine* __restrict__ bases, G1Xyzz* __restrict__ buckets,
+                                                        G1Xyzz* __restrict__ heads)
+{
+    const uint32_t M = offsets[NB];
+    const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = (uint32_t)(t * K);
+        const uint32_t end = ((uint64_t)start + K < (uint64_t)M) ? start + K : M;
+        uint64_t lo = 0, hi = NB;  // offsets[lo] <= start < offsets[hi]
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= start) lo = mid; else hi = mid;
+        }
+        uint64_t b = lo;
+        uint32_t next = offsets[b + 1];
+        bool head = offsets[b] < start;
+        G1Xyzz acc = xyzz_inf();
+        for (uint32_t e = start; e < end; e++) {
+            if (e == next) {
+                if (head) st_xyzz(&heads[t], acc); else st_xyzz(&buckets[b], acc);
+                acc = xyzz_inf();
+                head = false;
+                do { b++; next = offsets[b + 1]; } while (next == e);
+            }
+            xyzz_madd(acc, load_signed_point(bases, sorted[e]));
+        }
+        if (head) st_xyzz(&heads[t], acc); else st_xyzz(&buckets[b], acc);
+    }
+}
+
+__global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K, G1Xyzz* __restrict__ buckets,
+                            const G1Xyzz* __restrict__ heads, uint32_t* __restrict__ dense)
+{
+    for (uint64_t gb = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gb < NB; gb += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t s = offsets[gb], e = offsets[gb + 1];
+        if (s == e) { st_xyzz(&buckets[gb], xyzz_inf()); continue; }
+        uint32_t t0 = s / K, t1 = (e - 1) / K;
+        if (t1 == t0) continue;
+        if (t1 - t0 > DENSE_LIMIT) {
+            uint32_t idx = atomicAdd(&dense[NB], 1u);
+            dense[idx] = (uint32_t)gb;
+            continue;
+        }
+        G1Xyzz acc = ld_xyzz(&buckets[gb]);
+        for (uint32_t t = t0 + 1; t <= t1; t++) xyzz_add(acc, ld_xyzz(&heads[t]));
+        st_xyzz(&buckets[gb], acc);
+    }
+}
+
+// CTA-wide tree sum of n XYZZ values produced by get(i); result valid in thread 0.
+template <class Get>
+__device__ G1Xyzz block_sum_xyzz(uint64_t n, Get get)
+{
+    __shared__ G1Xyzz red[256];
+    G1Xyzz acc = xyzz_inf();
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) xyzz_add(acc, get(i));
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            G1Xyzz a = red[threadIdx.x];
+            xyzz_add(a, red[threadIdx.x + h]);
+            red[threadIdx.x] = a;
+        }
+        __syncthreads();
+    }
+    G1Xyzz r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_msm_dense(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
+                                                   G1Xyzz* __restrict__ buckets, const G1Xyzz* __restrict__ heads,
+                                                   const uint32_t* __restrict__ dense)
+{
+    const uint32_t cnt = dense[NB];
+    for (uint32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+        uint32_t gb = dense[i];
+        uint32_t t0 = offsets[gb] / K, t1 = (offsets[gb + 1] - 1) / K;
+        G1Xyzz r = block_sum_xyzz(t1 - t0, [&](uint64_t j) { return ld_xyzz(&heads[t0 + 1 + j]); });
+        if (threadIdx.x == 0) {
+            G1Xyzz acc = ld_xyzz(&buckets[gb]);
+            xyzz_add(acc, r);
+            st_xyzz(&buckets[gb], acc);
+        }
+        __syncthreads();
+    }
+}
+
+// Thread (w, s): sum_{j in segment s} (j + 1) * B_{w, j}, buckets j = s*L .. s*L+L-1.
+__global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__ buckets, int W, uint32_t H, uint32_t L,
+                                                      uint32_t S, G1Xyzz* __restrict__ segs)
+{
+    uint64_t total = (uint64_t)W * S;
+    for (uint64_t id = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; id < total;
+         id += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t w = id / S, s = id % S;
+        const G1Xyzz* B = buckets + w * H + s * L;
+        G1Xyzz run = xyzz_inf(), acc = xyzz_inf();
+        for (int j = (int)L - 1; j >= 0; j--) {
+            xyzz_add(run, ld_xyzz(&B[j]));
+            xyzz_add(acc, run);
+        }
+        // acc = sum (j - sL + 1) B_j ; add (s*L) * run
+        G1Xyzz off = xyzz_mul_u32(run, (uint32_t)(s * L));
+        xyzz_add(acc, off);
+        st_xyzz(&segs[id], acc);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_msm_windows(const G1Xyzz* __restrict__ segs, uint32_t S, G1Xyzz* __restrict__ wins)
+{
+    uint32_t w = blockIdx.x;
+    G1Xyzz r = block_sum_xyzz(S, [&](uint64_t j) { return ld_xyzz(&segs[(uint64_t)w * S + j]); });
+    if (threadIdx.x == 0) st_xyzz(&wins[w], r);
+}
+
+// 2^(c*w) * W_w in parallel over w, then the sum and the affine conversion.
+__global__ void k_msm_final(const G1Xyzz* __restrict__ wins, int W, int c, G1Jac* __restrict__ out)
+{
+    __shared__ G1Xyzz sh[64];
+    int w = threadIdx.x;
+    if (w < W) {
+        G1Xyzz x = ld_xyzz(&wins[w]);
+        for (int d = 0; d < c * w; d++) x = xyzz_dbl(x);
+        sh[w] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        G1Xyzz acc = xyzz_inf();
+        for (int i = 0; i < W; i++) xyzz_add(acc, sh[i]);
+        G1Jac j = xyzz_to_jac_affine(acc);
+        st(&out->X, j.X);
+        st(&out->Y, j.Y);
+        st(&out->Z, j.Z);
+    }
+}
+
+__global__ void k_write_inf(G1Jac* out)
+{
+    if (threadIdx.x == 0) {
+        st(&out->X, Fq::zero());
+        st(&out->Y, Fq::one());
+        st(&out->Z, Fq::zero());
+    }
+}
+
+// Runs steps 1-7 on device buffers; result (96 bytes) lands in s.result.
+RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases, cudaStream_t st)
+{
+    if (p.n == 0) {
+        k_write_inf<<<1, 32, 0, st>>>(s.result);
+        H2B_LAUNCHED("k_write_inf");
+        return ok();
+    }
+    const unsigned sm_cap = 148u * 16u;
+    prof_begin(PROF_MSM_TOTAL, st);
+    k_msm_canon<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, s.canon, p.n);
+    H2B_LAUNCHED("k_msm_canon");
+    H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
+    H2B_CUDA(cudaMemsetAsync(s.dense + p.NB, 0, sizeof(uint32_t), st));
+    k_msm_sort<false><<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(s.canon, p.n, p.c, p.W, p.H, s.counts, nullptr);
+    H2B_LAUNCHED("k_msm_sort<hist>");
+    H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
+    H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    k_msm_sort<true><<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(s.canon, p.n, p.c, p.W, p.H, s.cursor, s.sorted);
+    H2B_LAUNCHED("k_msm_sort<scatter>");
+    uint64_t chunks = (p.max_entries + p.K - 1) / p.K;
+    prof_begin(PROF_MSM_ACCUMULATE, st);
+    k_msm_accumulate<<<grid_for(chunks, 128, 148u * 32u), 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases,
+                                                                       s.buckets, s.heads);
+    prof_end(PROF_MSM_ACCUMULATE, st);
+    H2B_LAUNCHED("k_msm_accumulate");
+    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense);
+    H2B_LAUNCHED("k_msm_fixup");
+    k_msm_dense<<<148, 256, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense);
+    H2B_LAUNCHED("k_msm_dense");
+    uint64_t nseg = (uint64_t)p.W * p.S;
+    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.W, p.H, p.L, p.S, s.segs);
+    H2B_LAUNCHED("k_msm_segments");
+    k_msm_windows<<<p.W, 256, 0, st>>>(s.segs, p.S, s.wins);
+    H2B_LAUNCHED("k_msm_windows");
+    k_msm_final<<<1, 64, 0, st>>>(s.wins, p.W, p.c, s.result);
+    prof_end(PROF_MSM_TOTAL, st);
+    H2B_LAUNCHED("k_msm_final");
+    return ok();
+}
+
+} // namespace h2b
+
+using namespace h2b;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+static uint64_t msm_ws(uint64_t length, bool scalar_host, bool bases_host)
+{
+    MsmPlan p = msm_plan(length);
+    ScratchPlan sp;
+    msm_plan_scratch(p, sp, scalar_host, bases_host);
+    return sp.used;
+}
+
+extern "C" uint64_t _halo2_msm_max_length(uint64_t free_bytes)
+{
+    for (int lg = 28; lg > 0; lg--) {
+        if (msm_ws(1ull << lg, true, true) < free_bytes) return 1ull << lg;
+    }
+    return 0;
+}
+
+extern "C" uint64_t _halo2_multiexp_workspace_size(uint64_t length) { return msm_ws(length, true, true); }
+extern "C" uint64_t _halo2_multiexp_device_bases_workspace_size(uint64_t length) { return msm_ws(length, true, false); }
+extern "C" uint64_t _halo2_multiexp_device_scalars_device_bases_workspace_size(uint64_t length)
+{
+    return msm_ws(length, false, false);
+}
+
+static RustError msm_entry(const void* scalars, bool scalar_host, const void* bases, bool bases_host, void* h_out,
+                           uint64_t length, void* scratch, uint64_t scratch_bytes, cudaStream_t st, const char* who)
+{
+    if (length > 0xffffffffull / 32) return err(cudaErrorInvalidValue, "MSM length too large for 32-bit entry ids");
+    MsmPlan p = msm_plan(length);
+    uint64_t need = msm_ws(length, scalar_host, bases_host);
+    if (scratch_bytes < need) return scratch_too_small(who, scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    MsmScratch s = msm_carve(p, ar, scalar_host, bases_host);
+    if (!ar.good()) return scratch_too_small(who, scratch_bytes, need);
+    const Fr* d_sc = (const Fr*)scalars;
+    const G1Affine* d_b = (const G1Affine*)bases;
+    if (length > 0 && scalar_host) {
+        H2B_CUDA(cudaMemcpyAsync(s.scalar_stage, scalars, length * sizeof(Fr), cudaMemcpyHostToDevice, st));
+        d_sc = s.scalar_stage;
+    }
+    if (length > 0 && bases_host) {
+        H2B_CUDA(cudaMemcpyAsync(s.bases_stage, bases, length * sizeof(G1Affine), cudaMemcpyHostToDevice, st));
+        d_b = s.bases_stage;
+    }
+    H2B_TRY(msm_run(p, s, d_sc, d_b, st));
+    H2B_CUDA(cudaMemcpyAsync(h_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToHost, st));
+    H2B_CUDA(cudaStreamSynchronize(st));
+    return ok();
+}
+
+extern "C" RustError _halo2_multiexp(const FFITraitObject* scalar, const FFITraitObject* point,
+                                     const FFITraitObject* output, uint64_t length, void* scratch,
+                                     uint64_t scratch_bytes, cudaStream_t stream)
+{
+    return msm_entry(scalar->ptr, true, point->ptr, true, output->ptr, length, scratch, scratch_bytes, stream,
+                     "_halo2_multiexp");
+}
+
+extern "C" RustError _halo2_multiexp_device_bases(const FFITraitObject* h_scalar, const void* d_bases,
+                                                  const FFITraitObject* h_output, uint64_t length, void* scratch,
+                                                  uint64_t scratch_bytes, cudaStream_t stream)
+{
+    return msm_entry(h_scalar->ptr, true, d_bases, false, h_output->ptr, length, scratch, scratch_bytes, stream,
+                     "_halo2_multiexp_device_bases");
+}
+
+extern "C" RustError _halo2_multiexp_device_scalars_device_bases(const void* d_scalar, const void* d_bases,
+                                                                 const FFITraitObject* h_output, uint64_t length,
+                                                                 void* scratch, uint64_t scratch_bytes,
+                                                                 cudaStream_t stream)
+{
+    return msm_entry(d_scalar, false, d_bases, false, h_output->ptr, length, scratch, scratch_bytes, stream,
+                     "_halo2_multiexp_device_scalars_device_bases");
+}
+
+// Device-output, sync-free variant: the 96-byte Jacobian image is written to
+// d_out on `stream`.  Same scratch size as the device-scalars entry point.
+extern "C" RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out, uint64_t length,
+                                    void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (length > 0xffffffffull / 32) return err(cudaErrorInvalidValue, "MSM length too large for 32-bit entry ids");
+    MsmPlan p = msm_plan(length);
+    uint64_t need = msm_ws(length, false, false);
+    if (scratch_bytes < need) return scratch_too_small("h2b_msm_device", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    MsmScratch s = msm_carve(p, ar, false, false);
+    H2B_TRY(msm_run(p, s, (const Fr*)d_scalar, (const G1Affine*)d_bases, stream));
+    H2B_CUDA(cudaMemcpyAsync(d_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToDevice, stream));
+    return ok();
+}
+
+extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(window_bits, chunk); }
+
+// Number of nonzero signed window digits (= sorted entries = bucket
+// additions) the MSM of these scalars performs; written to *d_count (u64).
+// Used by the benchmark for its algorithmic work count, untimed.
+namespace h2b {
+__global__ void k_msm_count(const Fr* __restrict__ sc, uint64_t n, int c, int W, uint32_t H,
+                            unsigned long long* __restrict__ cnt)
+{
+    unsigned long long local = 0;
+    const uint32_t full = 1u << c;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        Fr s = from_mont(ldg(&sc[i]));
+        uint32_t carry = 0;
+        for (int w = 0; w < W; w++) {
+            uint32_t v = window_bits(s, w * c, c) + carry;
+            int32_t d = (v > H) ? (int32_t)v - (int32_t)full : (int32_t)v;
+            carry = (v > H) ? 1u : 0u;
+            if (d != 0) local++;
+        }
+    }
+    atomicAdd(cnt, local);
+}
+} // namespace h2b
+
+extern "C" RustError h2b_msm_count_entries(const void* d_scalars, uint64_t n, void* d_count, cudaStream_t stream)
+{
+    MsmPlan p = msm_plan(n);
+    H2B_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), stream));
+    if (n == 0) return ok();
+    k_msm_count<<<grid_for(n, 256, 148u * 8u), 256, 0, stream>>>((const Fr*)d_scalars, n, p.c, p.W, p.H,
+                                                                (unsigned long long*)d_count);
+    H2B_LAUNCHED("k_msm_count");
+    return ok();
+}
+
+extern "C" int h2b_msm_window_bits(uint64_t n) { return msm_plan(n).c; }

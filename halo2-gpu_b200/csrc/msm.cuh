@@ -1,0 +1,47 @@
+// Internal MSM interface shared by the C-ABI launchers and the batched /
+// no-allocation entry points.
+#pragma once
+#include <cstdint>
+#include "abi.cuh"
+#include "curve.cuh"
+
+namespace h2b {
+
+struct MsmPlan {
+    uint64_t n;
+    int c;           // window bits
+    int W;           // windows
+    uint32_t H;      // buckets per window = 2^(c-1)
+    uint64_t NB;     // W * H
+    uint32_t K;      // sorted entries per accumulation chunk
+    uint64_t max_entries;
+    uint64_t max_chunks;
+    uint32_t L;      // buckets per reduction segment
+    uint32_t S;      // segments per window
+};
+
+struct MsmScratch {
+    G1Affine* bases_stage;
+    Fr* scalar_stage;
+    Fr* canon;
+    uint32_t* counts;
+    uint32_t* offsets;
+    uint32_t* cursor;
+    uint32_t* scan_tmp;
+    uint32_t* sorted;
+    G1Xyzz* buckets;
+    G1Xyzz* heads;
+    uint32_t* dense;
+    G1Xyzz* segs;
+    G1Xyzz* wins;
+    G1Jac* result;
+};
+
+MsmPlan msm_plan(uint64_t n);
+void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host);
+MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host);
+RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases,
+                  cudaStream_t st);
+void msm_set_tuning(int window_bits, int chunk);
+
+} // namespace h2b

@@ -1,0 +1,608 @@
+// Fr number-theoretic transforms behind EvaluationDomain (lagrange_to_coeff,
+// coeff_to_extended, coeff_to_extended_part, extended_to_coeff) and the
+// reference's `_halo2_fft_*` entry points (halo2_proofs/cuda/src/ntt.cu:21-962,
+// declared at halo2_proofs/src/cuda/culib.rs:492-600).
+//
+// Transform conventions (identical outputs to the reference):
+//   FFT (1)           A_j = sum_i a_i w^(ij), natural order in and out.
+//   iFFT (2)          FFT with the caller's w (= w^-1), then * divisor.
+//   cosetFFT (3)      zero-pad to 2^ext, a_i *= zeta^(i mod 3), FFT at 2^ext.
+//   icosetFFT (4)     FFT at 2^ext with w, * divisor, a_i *= zeta^-(i mod 3).
+//   CosetFFT_Part (6) a_i *= c^i with c carried in the divisor slot, then FFT.
+//
+// Structure on the device: the radix-2 network runs as a few passes, each
+// pass a shared-memory tile that executes up to 9 consecutive radix-2 stages
+// on groups of 2^b elements gathered at a fixed stride, so HBM is touched once
+// per pass instead of once per stage.  Decimation in time (bit-reversed in,
+// natural out) serves the forward transforms after a fused
+// twist+bit-reversal scatter; decimation in frequency (natural in,
+// bit-reversed out) serves the inverse ones, followed by a fused
+// bit-reversal+scale(+untwist) pass.  Twiddles w^e, e < n/2, are generated
+// into caller scratch once per call (once per batch for the *_many entries).
+#include <algorithm>
+#include <cstring>
+#include "abi.cuh"
+#include "field.cuh"
+#include "hostfield.h"
+#include "ntt.cuh"
+#include "prof.cuh"
+
+namespace h2b {
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// lut[i] = base^(2^i), i < k.  One thread: k sequential squarings.
+__global__ void k_pow2_lut(const Fr* __restrict__ base, Fr* __restrict__ lut, int k)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Fr cur = ld(base);
+        for (int i = 0; i < k; i++) {
+            st(&lut[i], cur);
+            cur = cur * cur;
+        }
+    }
+}
+
+__device__ __forceinline__ Fr pow_from_lut(const Fr* __restrict__ lut, uint64_t e)
+{
+    Fr r = Fr::one();
+    int i = 0;
+    while (e) {
+        if (e & 1) r = r * ldg(&lut[i]);
+        e >>= 1;
+        i++;
+    }
+    return r;
+}
+
+// tw[e] = w^e for e < half, using lut[i] = w^(2^i).
+constexpr int TW_CHUNK = 16;
+__global__ void k_twiddles(const Fr* __restrict__ lut, Fr* __restrict__ tw, uint64_t half)
+{
+    uint64_t nthreads = (half + TW_CHUNK - 1) / TW_CHUNK;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t e0 = t * TW_CHUNK;
+        Fr p = pow_from_lut(lut, e0);
+        Fr w = ldg(&lut[0]);
+        for (int j = 0; j < TW_CHUNK && e0 + j < half; j++) {
+            st(&tw[e0 + j], p);
+            p = p * w;
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t bitrev(uint64_t x, int k)
+{
+    return k == 0 ? 0 : (__brevll(x) >> (64 - k));
+}
+
+// Forward-path input stage: out[rev(i)] = in[i] * f(i) for i < n_out, where
+// in[i] = 0 for i >= n_in (zero padding) and f is
+//   mode 0: 1,   mode 1: c^i (lut_c[j] = c^(2^j)),   mode 2: z3[i mod 3].
+// `out` must not alias `in`.
+constexpr int SC_CHUNK = 8;
+struct Zeta3 {
+    Fr f[3];
+};
+__global__ void k_twist_bitrev_scatter(const Fr* __restrict__ in, Fr* __restrict__ out, uint64_t n_in, int log_out,
+                                       int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
+{
+    uint64_t n_out = 1ull << log_out;
+    uint64_t nthreads = n_out / SC_CHUNK + (n_out % SC_CHUNK ? 1 : 0);
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i0 = t * SC_CHUNK;
+        Fr p;
+        Fr c;
+        if (mode == 1) {
+            p = pow_from_lut(lut_c, i0);
+            c = ldg(&lut_c[0]);
+        }
+        for (int j = 0; j < SC_CHUNK && i0 + j < n_out; j++) {
+            uint64_t i = i0 + j;
+            Fr v = (i < n_in) ? ldg(&in[i]) : Fr::zero();
+            if (mode == 1) {
+                v = v * p;
+                p = p * c;
+            } else if (mode == 2) {
+                v = v * z3.f[i % 3];
+            }
+            st(&out[bitrev(i, log_out)], v);
+        }
+    }
+}
+
+// In-place a_i *= c^i (mode 1) or zeta^(i mod 3) factors (mode 2).
+__global__ void k_twist_inplace(Fr* __restrict__ a, uint64_t n, int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
+{
+    uint64_t nthreads = n / SC_CHUNK + (n % SC_CHUNK ? 1 : 0);
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i0 = t * SC_CHUNK;
+        Fr p, c;
+        if (mode == 1) {
+            p = pow_from_lut(lut_c, i0);
+            c = ldg(&lut_c[0]);
+        }
+        for (int j = 0; j < SC_CHUNK && i0 + j < n; j++) {
+            uint64_t i = i0 + j;
+            Fr v = ld(&a[i]);
+            if (mode == 1) {
+                v = v * p;
+                p = p * c;
+            } else {
+                v = v * z3.f[i % 3];
+            }
+            st(&a[i], v);
+        }
+    }
+}
+
+// In-place bit reversal; when `scale` each element landing at index i is
+// multiplied by z3.f[i mod 3] (used for divisor and divisor*zeta^-(i mod 3)).
+__global__ void k_bitrev_inplace(Fr* __restrict__ a, int k, bool scale, Zeta3 z3)
+{
+    uint64_t n = 1ull << k;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t j = bitrev(i, k);
+        if (i < j) {
+            Fr x = ld(&a[i]), y = ld(&a[j]);
+            if (scale) {
+                y = y * z3.f[i % 3];
+                x = x * z3.f[j % 3];
+            }
+            st(&a[i], y);
+            st(&a[j], x);
+        } else if (i == j && scale) {
+            Fr x = ld(&a[i]);
+            st(&a[i], x * z3.f[i % 3]);
+        }
+    }
+}
+
+// One shared-memory pass of `nst` radix-2 stages starting at stage s0.
+//   DIT: stage s pairs (i, i + 2^s), twiddle w^((i mod 2^s) * n/2^(s+1)),
+//        groups: 2^nst elements at stride S = 2^s0 inside blocks of S*2^nst.
+//   DIF: stage s pairs (i, i + n/2^(s+1)), twiddle w^((i mod n/2^(s+1)) * 2^s),
+//        groups: stride S = n / 2^(s0+nst).
+// A CTA owns G = TILE >> nst consecutive groups (G * 2^nst = TILE elements).
+constexpr int NTT_TILE = 1024;
+constexpr int NTT_THREADS = 512;
+
+template <bool DIT>
+__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(Fr* __restrict__ a, const Fr* __restrict__ tw, int logn,
+                                                          int s0, int nst)
+{
+    extern __shared__ uint4 smem_raw[];
+    Fr* sm = reinterpret_cast<Fr*>(smem_raw);
+    const uint64_t n = 1ull << logn;
+    const int gsize = 1 << nst;
+    const uint64_t S = DIT ? (1ull << s0) : (n >> (s0 + nst));
+    const uint64_t BS = S << nst;
+    const uint64_t ngroups = n >> nst;
+    uint64_t G = (uint64_t)NTT_TILE >> nst;
+    if (G > ngroups) G = ngroups;
+    const uint64_t g0 = blockIdx.x * G;
+    if (g0 >= ngroups) return;
+    const uint64_t elems = G << nst;
+    const bool wide = S >= G;   // the G groups share one block, consecutive r
+
+    // load
+    for (uint64_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint64_t gl, j, addr;
+        if (wide) {
+            gl = idx % G;
+            j = idx / G;
+            uint64_t g = g0 + gl;
+            addr = (g / S) * BS + j * S + (g % S);
+        } else {
+            uint64_t base = (g0 / S) * BS;
+            uint64_t bl = idx / BS, rem = idx % BS;
+            j = rem / S;
+            gl = bl * S + (rem % S);
+            addr = base + idx;
+        }
+        sm[gl * gsize + j] = ld(&a[addr]);
+    }
+    __syncthreads();
+
+    const uint64_t nbf = G << (nst - 1);
+    for (int t = 0; t < nst; t++) {
+        const int s = s0 + t;
+        for (uint64_t u = threadIdx.x; u < nbf; u += blockDim.x) {
+            uint64_t gl = u >> (nst - 1);
+            uint64_t m = u & ((1ull << (nst - 1)) - 1);
+            uint64_t g = g0 + gl;
+            uint64_t r = g % S;
+            if (DIT) {
+                uint64_t lowm = m & ((1ull << t) - 1);
+                uint64_t q = ((m >> t) << (t + 1)) | lowm;
+                uint64_t e = (lowm * S + r) * (n >> (s + 1));
+                Fr* px = &sm[gl * gsize + q];
+                Fr* py = px + (1ull << t);
+                Fr x = *px;
+                Fr y = *py * ldg(&tw[e]);
+                *px = x + y;
+                *py = x - y;
+            } else {
+                int h = nst - t - 1;
+                uint64_t lowm = m & ((1ull << h) - 1);
+                uint64_t q = ((m >> h) << (h + 1)) | lowm;
+                uint64_t e = (lowm * S + r) << s;
+                Fr* px = &sm[gl * gsize + q];
+                Fr* py = px + (1ull << h);
+                Fr x = *px, y = *py;
+                *px = x + y;
+                *py = (x - y) * ldg(&tw[e]);
+            }
+        }
+        __syncthreads();
+    }
+
+    // store
+    for (uint64_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint64_t gl, j, addr;
+        if (wide) {
+            gl = idx % G;
+            j = idx / G;
+            uint64_t g = g0 + gl;
+            addr = (g / S) * BS + j * S + (g % S);
+        } else {
+            uint64_t base = (g0 / S) * BS;
+            uint64_t bl = idx / BS, rem = idx % BS;
+            j = rem / S;
+            gl = bl * S + (rem % S);
+            addr = base + idx;
+        }
+        st(&a[addr], sm[gl * gsize + j]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side pass planning
+// ---------------------------------------------------------------------------
+
+static int g_max_pass_stages = 9;  // tuned per k by ntt_set_pass_stages()
+
+int ntt_pass_stages() { return g_max_pass_stages; }
+void ntt_set_pass_stages(int b)
+{
+    if (b >= 1 && b <= 10) g_max_pass_stages = b;
+}
+
+static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_t st)
+{
+    if (logn == 0) return ok();
+    int passes = (logn + g_max_pass_stages - 1) / g_max_pass_stages;
+    int base = logn / passes, extra = logn % passes;
+    int s0 = 0;
+    prof_begin(PROF_NTT_PASSES, st);
+    for (int p = 0; p < passes; p++) {
+        int nst = base + (p < extra ? 1 : 0);
+        uint64_t n = 1ull << logn;
+        uint64_t G = (uint64_t)NTT_TILE >> nst;
+        uint64_t ngroups = n >> nst;
+        if (G > ngroups) G = ngroups;
+        uint64_t blocks = (ngroups + G - 1) / G;
+        size_t smem = (size_t)(G << nst) * sizeof(Fr);
+        int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, G << (nst - 1)));
+        if (dit)
+            k_ntt_pass<true><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst);
+        else
+            k_ntt_pass<false><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst);
+        H2B_LAUNCHED("k_ntt_pass");
+        s0 += nst;
+    }
+    prof_end(PROF_NTT_PASSES, st);
+    return ok();
+}
+
+// Scratch layout for one transform family: twiddles (n/2), lut_w (64), lut_c
+// (64), omega staging, then (host-input variants) one data slot.
+struct NttScratch {
+    Fr* tw = nullptr;
+    Fr* lut_w = nullptr;
+    Fr* lut_c = nullptr;
+    Fr* omega = nullptr;
+    Fr* data = nullptr;
+};
+
+static void plan_ntt(ScratchPlan& p, int log_size, bool data_slot, int log_data)
+{
+    uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
+    p.add_n<Fr>(half);
+    p.add_n<Fr>(64);
+    p.add_n<Fr>(64);
+    p.add_n<Fr>(1);
+    if (data_slot) p.add_n<Fr>(1ull << log_data);
+}
+
+static NttScratch carve_ntt(ScratchArena& ar, int log_size, bool data_slot, int log_data)
+{
+    NttScratch s;
+    uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
+    s.tw = ar.take_n<Fr>(half);
+    s.lut_w = ar.take_n<Fr>(64);
+    s.lut_c = ar.take_n<Fr>(64);
+    s.omega = ar.take_n<Fr>(1);
+    if (data_slot) s.data = ar.take_n<Fr>(1ull << log_data);
+    return s;
+}
+
+// Builds tw[] (and lut_w) for transforms of size 2^logn from a device omega.
+static RustError make_twiddles(const Fr* d_omega, NttScratch& s, int logn, cudaStream_t st)
+{
+    if (logn == 0) return ok();
+    k_pow2_lut<<<1, 32, 0, st>>>(d_omega, s.lut_w, logn);
+    H2B_LAUNCHED("k_pow2_lut");
+    uint64_t half = 1ull << (logn - 1);
+    uint64_t nthreads = (half + TW_CHUNK - 1) / TW_CHUNK;
+    k_twiddles<<<grid_for(nthreads, 256), 256, 0, st>>>(s.lut_w, s.tw, half);
+    H2B_LAUNCHED("k_twiddles");
+    return ok();
+}
+
+static Zeta3 zeta_factors(const host::Fr64& scale, bool inverse)
+{
+    using namespace host;
+    Fr64 one = fr_const(FR_ONE), z = fr_const(FR_ZETA), z2 = fr_const(FR_ZETA2);
+    Fr64 f[3];
+    f[0] = fr_mul(scale, one);
+    // forward twist: a_i *= zeta^(i mod 3); inverse: zeta^-(i mod 3) = zeta^(2(i mod 3)).
+    f[1] = fr_mul(scale, inverse ? z2 : z);
+    f[2] = fr_mul(scale, inverse ? z : z2);
+    Zeta3 out;
+    for (int i = 0; i < 3; i++) memcpy(out.f[i].v, f[i].v, 32);
+    return out;
+}
+
+static Zeta3 scale_factors(const host::Fr64& scale)
+{
+    Zeta3 out;
+    for (int i = 0; i < 3; i++) memcpy(out.f[i].v, scale.v, 32);
+    return out;
+}
+
+// Core: one transform into `d_out` (device).  `in` may be host (in_host) or
+// device, and may alias d_out only when it is device memory.
+//   log_n   : input length (and transform size except for coset types)
+//   log_ext : transform size for cosetFFT / icosetFFT
+static RustError transform_one(int type, int log_n, int log_ext, const void* in, bool in_host, Fr* d_out,
+                               const host::Fr64* h_divisor, NttScratch& s, cudaStream_t st)
+{
+    using namespace host;
+    const bool coset_full = (type == 3 || type == 4);
+    const int logt = coset_full ? log_ext : log_n;
+    const uint64_t nt = 1ull << logt;
+    const uint64_t nin = 1ull << log_n;
+    Zeta3 none = scale_factors(fr_const(FR_ONE));
+
+    // Stage input on the device when it lives on the host.
+    const Fr* din = (const Fr*)in;
+    if (in_host) {
+        H2B_CUDA(cudaMemcpyAsync(d_out, in, nin * sizeof(Fr), cudaMemcpyHostToDevice, st));
+        din = d_out;
+    }
+    const bool alias = (din == d_out);
+
+    if (type == 1 || type == 6 || type == 3) {
+        int mode = 0;
+        Zeta3 z3 = none;
+        if (type == 6) {
+            Fr64 lut[64];
+            fr_pow2_lut(*h_divisor, logt, lut);
+            H2B_CUDA(cudaMemcpyAsync(s.lut_c, lut, sizeof(Fr) * logt, cudaMemcpyHostToDevice, st));
+            mode = 1;
+        } else if (type == 3) {
+            z3 = zeta_factors(fr_const(FR_ONE), false);
+            mode = 2;
+        }
+        if (!alias) {
+            uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
+            k_twist_bitrev_scatter<<<grid_for(nthreads, 256), 256, 0, st>>>(din, d_out, type == 3 ? nin : nt,
+                                                                            logt, mode, s.lut_c, z3);
+            H2B_LAUNCHED("k_twist_bitrev_scatter");
+        } else {
+            if (type == 3 && nt != nin) {
+                // zero the padding in place, then twist + reverse
+                H2B_CUDA(cudaMemsetAsync(d_out + nin, 0, (nt - nin) * sizeof(Fr), st));
+            }
+            if (mode != 0) {
+                uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
+                k_twist_inplace<<<grid_for(nthreads, 256), 256, 0, st>>>(d_out, nt, mode, s.lut_c, z3);
+                H2B_LAUNCHED("k_twist_inplace");
+            }
+            k_bitrev_inplace<<<grid_for(nt, 256), 256, 0, st>>>(d_out, logt, false, none);
+            H2B_LAUNCHED("k_bitrev_inplace");
+        }
+        return run_passes(d_out, s.tw, logt, true, st);
+    }
+    if (type == 2 || type == 4) {
+        if (!alias) {
+            H2B_CUDA(cudaMemcpyAsync(d_out, din, nin * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
+        }
+        if (type == 4 && nt != nin) {
+            H2B_CUDA(cudaMemsetAsync(d_out + nin, 0, (nt - nin) * sizeof(Fr), st));
+        }
+        H2B_TRY(run_passes(d_out, s.tw, logt, false, st));
+        Zeta3 z3 = (type == 4) ? zeta_factors(*h_divisor, true) : scale_factors(*h_divisor);
+        k_bitrev_inplace<<<grid_for(nt, 256), 256, 0, st>>>(d_out, logt, true, z3);
+        H2B_LAUNCHED("k_bitrev_inplace");
+        return ok();
+    }
+    return err(-1, "unsupported ntt_type");
+}
+
+static RustError check_type(uint32_t t)
+{
+    if (t == 5) return err(-1, "iFFT_cosetFFT not supported");
+    if (t < 1 || t > 6) return err(-6, "unsupported ntt_type");
+    return ok();
+}
+
+} // namespace h2b
+
+using namespace h2b;
+
+// ---------------------------------------------------------------------------
+// C ABI (declarations in include/halo2_gpu.h)
+// ---------------------------------------------------------------------------
+
+static int active_log(uint32_t t, uint32_t log_n, uint32_t ext) { return (t == 3 || t == 4) ? (int)ext : (int)log_n; }
+
+extern "C" uint64_t _halo2_fft_normal_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n)
+{
+    ScratchPlan p;
+    int la = active_log(ntt_type, log_n, extend_log_n);
+    plan_ntt(p, la, true, la);
+    return p.used;
+}
+
+extern "C" bool _halo2_fft_normal_check_memory(uint32_t, const void*, uint32_t, uint32_t) { return true; }
+
+extern "C" RustError _halo2_fft_normal(uint32_t ntt_type, uint32_t log_n, const void* input, void* output,
+                                       const void* omega, const void* divisor, void* scratch, uint64_t scratch_bytes,
+                                       cudaStream_t stream)
+{
+    H2B_TRY(check_type(ntt_type));
+    if (log_n == 0) return err(cudaErrorInvalidValue, "_halo2_fft_normal: log_n must be >= 1");
+    uint64_t need = _halo2_fft_normal_workspace_size(ntt_type, log_n, log_n);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_fft_normal", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    NttScratch s = carve_ntt(ar, log_n, true, log_n);
+    if (!ar.good()) return scratch_too_small("_halo2_fft_normal", scratch_bytes, need);
+    H2B_CUDA(cudaMemcpyAsync(s.omega, omega, sizeof(Fr), cudaMemcpyHostToDevice, stream));
+    H2B_TRY(make_twiddles(s.omega, s, log_n, stream));
+    host::Fr64 div = host::fr_from(divisor);
+    H2B_TRY(transform_one(ntt_type, log_n, log_n, input, true, s.data, &div, s, stream));
+    H2B_CUDA(cudaMemcpyAsync(output, s.data, sizeof(Fr) << log_n, cudaMemcpyDeviceToHost, stream));
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" uint64_t _halo2_fft_normal_to_device_workspace_size(uint32_t ntt_type, uint32_t log_n,
+                                                               uint32_t extend_log_n)
+{
+    ScratchPlan p;
+    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0);
+    return p.used;
+}
+
+extern "C" RustError _halo2_fft_normal_to_device(uint32_t ntt_type, uint32_t log_n, const void* d_input,
+                                                 void* d_output, const void* d_omega, const void* h_divisor,
+                                                 void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (ntt_type != 1 && ntt_type != 2 && ntt_type != 6)
+        return err(cudaErrorInvalidValue, "_halo2_fft_normal_to_device supports only FFT, iFFT, CosetFFT_Part");
+    if (log_n == 0) return err(cudaErrorInvalidValue, "_halo2_fft_normal_to_device: log_n must be >= 1");
+    uint64_t need = _halo2_fft_normal_to_device_workspace_size(ntt_type, log_n, log_n);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_fft_normal_to_device", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    NttScratch s = carve_ntt(ar, log_n, false, 0);
+    H2B_TRY(make_twiddles((const Fr*)d_omega, s, log_n, stream));
+    host::Fr64 div = host::fr_from(h_divisor);
+    return transform_one(ntt_type, log_n, log_n, d_input, false, (Fr*)d_output, &div, s, stream);
+}
+
+extern "C" RustError _halo2_cosetfft(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n, const void* input,
+                                     void* output, const void* omega, const void* divisor, void* scratch,
+                                     uint64_t scratch_bytes, cudaStream_t stream)
+{
+    (void)ntt_type;
+    (void)divisor;
+    if (log_n == 0 || extend_log_n == 0)
+        return err(cudaErrorInvalidValue, "_halo2_cosetfft: log_n and extend_log_n must be >= 1");
+    if (extend_log_n < log_n) return err(cudaErrorInvalidValue, "_halo2_cosetfft: extend_log_n < log_n");
+    // This entry point always runs the forward coset extension (cosetFFT).
+    uint64_t need = _halo2_fft_normal_workspace_size(3, log_n, extend_log_n);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_cosetfft", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    NttScratch s = carve_ntt(ar, extend_log_n, true, extend_log_n);
+    H2B_CUDA(cudaMemcpyAsync(s.omega, omega, sizeof(Fr), cudaMemcpyHostToDevice, stream));
+    H2B_TRY(make_twiddles(s.omega, s, extend_log_n, stream));
+    host::Fr64 one = host::fr_const(host::FR_ONE);
+    H2B_TRY(transform_one(3, log_n, extend_log_n, input, true, s.data, &one, s, stream));
+    H2B_CUDA(cudaMemcpyAsync(output, s.data, sizeof(Fr) << extend_log_n, cudaMemcpyDeviceToHost, stream));
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" uint64_t _halo2_fft_many_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n)
+{
+    ScratchPlan p;
+    int la = active_log(ntt_type, log_n, extend_log_n);
+    plan_ntt(p, la, true, la);
+    return p.used;
+}
+
+extern "C" uint64_t _halo2_fft_many_to_device_workspace_size(uint32_t ntt_type, uint32_t log_n,
+                                                             uint32_t extend_log_n)
+{
+    ScratchPlan p;
+    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0);
+    return p.used;
+}
+
+extern "C" bool _halo2_fft_many_check_memory(uint32_t, uint32_t, uint32_t) { return true; }
+
+static RustError fft_many_impl(uint32_t ntt_type, uint32_t num_many, uint32_t log_n, uint32_t extend_log_n,
+                               const FFITraitObject* input, const FFITraitObject* output, const void* d_omega,
+                               const FFITraitObject* divisor, bool in_on_device, bool out_on_device, void* scratch,
+                               uint64_t scratch_bytes, cudaStream_t stream, const char* who)
+{
+    if (ntt_type == 4) return err(2, "icosetFFT not supported now");
+    H2B_TRY(check_type(ntt_type));
+    if (log_n == 0 || extend_log_n == 0) return err(cudaErrorInvalidValue, "log_n and extend_log_n must be >= 1");
+    int la = active_log(ntt_type, log_n, extend_log_n);
+    uint64_t need = out_on_device ? _halo2_fft_many_to_device_workspace_size(ntt_type, log_n, extend_log_n)
+                                  : _halo2_fft_many_workspace_size(ntt_type, log_n, extend_log_n);
+    if (scratch_bytes < need) return scratch_too_small(who, scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    NttScratch s = carve_ntt(ar, la, !out_on_device, la);
+    H2B_TRY(make_twiddles((const Fr*)d_omega, s, la, stream));
+    host::Fr64 div = (divisor && divisor->ptr) ? host::fr_from(divisor->ptr) : host::fr_const(host::FR_ONE);
+    for (uint32_t i = 0; i < num_many; i++) {
+        Fr* dst = out_on_device ? (Fr*)output[i].ptr : s.data;
+        H2B_TRY(transform_one(ntt_type, log_n, extend_log_n, input[i].ptr, !in_on_device, dst, &div, s, stream));
+        if (!out_on_device) {
+            H2B_CUDA(cudaMemcpyAsync(output[i].ptr, s.data, sizeof(Fr) << la, cudaMemcpyDeviceToHost, stream));
+        }
+    }
+    if (!out_on_device) H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" RustError _halo2_fft_many(uint32_t ntt_type, uint32_t num_many, uint32_t log_n, uint32_t extend_log_n,
+                                     const FFITraitObject* input, const FFITraitObject* output, const void* d_omega,
+                                     const FFITraitObject* divisor, void* scratch, uint64_t scratch_bytes,
+                                     cudaStream_t stream)
+{
+    return fft_many_impl(ntt_type, num_many, log_n, extend_log_n, input, output, d_omega, divisor, false, false,
+                         scratch, scratch_bytes, stream, "_halo2_fft_many");
+}
+
+extern "C" RustError _halo2_fft_many_to_device(uint32_t ntt_type, uint32_t num_many, uint32_t log_n,
+                                               uint32_t extend_log_n, const FFITraitObject* input,
+                                               const FFITraitObject* output, const void* d_omega,
+                                               const FFITraitObject* divisor, bool input_on_device, void* scratch,
+                                               uint64_t scratch_bytes, cudaStream_t stream)
+{
+    return fft_many_impl(ntt_type, num_many, log_n, extend_log_n, input, output, d_omega, divisor, input_on_device,
+                         true, scratch, scratch_bytes, stream, "_halo2_fft_many_to_device");
+}
+
+extern "C" int32_t _halo2_get_fft_split_radix(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n,
+                                              uint64_t free_bytes)
+{
+    for (uint32_t s = 0; s < log_n; s++) {
+        uint64_t need = _halo2_fft_normal_workspace_size(ntt_type, log_n - s, extend_log_n - s);
+        if (need < free_bytes) return (int32_t)s;
+    }
+    return -1;
+}
+
+extern "C" void h2b_ntt_set_pass_stages(int stages) { ntt_set_pass_stages(stages); }
+extern "C" int h2b_ntt_get_pass_stages(void) { return ntt_pass_stages(); }

@@ -1,0 +1,627 @@
+// Batch inversion, grand-product scans and the permutation / lookup products.
+//
+//  * `_halo2_batch_invert` (halo2_proofs/cuda/src/polynomial/operations.cu:16-42,
+//    semantics of halo2_proofs/cuda/include/kernel/inverse.h:10-63): in-place
+//    x_i <- x_i^-1 with zeros preserved, Fr or Fq.  The entry point has no
+//    scratch, so each CTA runs a Montgomery trick over 2048 elements with one
+//    inversion (prefixes in shared memory, a product tree over the 256 thread
+//    totals).  `h2b_batch_invert` adds a scratch-taking variant whose CTAs
+//    publish their totals, which are inverted recursively, so the whole array
+//    costs one inversion.
+//  * `_halo2_grand_product{,_device_inputs}` (halo2_proofs/cuda/src/commitment/
+//    grand_product.cu:45-195): out[i] = prefix * prod_{j<=i} in[j].  In-place
+//    multi-level scan: each level scans tiles of 2048 level entries whose last
+//    element then carries the tile total; a down-sweep multiplies every entry
+//    by the final value at the end of the previous tile.  No scratch.
+//  * `_halo2_commit_product{,_device_inputs}` (halo2_proofs/cuda/src/commitment/
+//    commit_product.cu:51-186): (A+b)(S+g) / ((A'+b)(S'+g)) per row, fused
+//    with the per-CTA inversion.
+//  * `_halo2_permutation_product{,_device_inputs}` (halo2_proofs/cuda/src/
+//    commitment/permutation_commit.cu:51-256): acc_r * prod_i (b*sigma_i+g+v_i)
+//    inverted, times prod_i (deltaomega*delta^i*w^r*b + g + v_i); deltaomega
+//    is advanced by delta^batch in place.
+#include <vector>
+#include "abi.cuh"
+#include "field.cuh"
+#include "inverse.cuh"
+#include "prof.cuh"
+
+namespace h2b {
+
+constexpr int BI_T = 256;
+constexpr int BI_E = 8;
+constexpr int BI_TILE = BI_T * BI_E;  // elements per CTA
+constexpr size_t BI_SMEM = (size_t)(BI_E - 1) * BI_T * 32 + (size_t)2 * BI_T * 32;
+
+// Block Montgomery trick.  Thread t owns tile elements j*BI_T + t (j < BI_E).
+//   fwd(i)   -> x_i (may stash x_i for bwd); zero is treated as one
+//   bwdx(i)  -> x_i again
+//   emit(i, inv_or_zero)
+// The CTA's total inverse comes from *root_inv when non-null, else it is
+// computed here by thread 0.
+template <class C, class Fwd, class Bwdx, class Emit>
+__device__ __forceinline__ void block_mont_trick(uint64_t base, uint64_t n, const Fp<C>* root_inv, Fwd fwd, Bwdx bwdx,
+                                                 Emit emit)
+{
+    using F = Fp<C>;
+    extern __shared__ uint4 bi_smem[];
+    F* pre = reinterpret_cast<F*>(bi_smem);           // (E-1) x T prefixes
+    F* tree = pre + (BI_E - 1) * BI_T;                 // 2T heap: tree[T + t] = thread total
+    const int t = threadIdx.x;
+
+    F acc = F::one();
+#pragma unroll 1
+    for (int j = 0; j < BI_E; j++) {
+        uint64_t i = base + (uint64_t)j * BI_T + t;
+        F x = F::one();
+        if (i < n) {
+            x = fwd(i);
+            if (x.is_zero()) x = F::one();
+        }
+        acc = (j == 0) ? x : acc * x;
+        if (j < BI_E - 1) pre[j * BI_T + t] = acc;
+    }
+    tree[BI_T + t] = acc;
+    __syncthreads();
+    for (int w = BI_T / 2; w >= 1; w >>= 1) {
+        if (t < w) tree[w + t] = tree[2 * (w + t)] * tree[2 * (w + t) + 1];
+        __syncthreads();
+    }
+    if (t == 0) tree[1] = root_inv ? *root_inv : finv_fast<C>(tree[1]);
+    __syncthreads();
+    for (int w = 1; w < BI_T; w <<= 1) {
+        if (t < w) {
+            int k = w + t;
+            F inv = tree[k];
+            F l = tree[2 * k], r = tree[2 * k + 1];
+            tree[2 * k] = inv * r;
+            tree[2 * k + 1] = inv * l;
+        }
+        __syncthreads();
+    }
+    // Backward: x_j^-1 = inv(prefix_j) * prefix_{j-1}; results replace the
+    // consumed prefix slots, then are emitted in ascending j.
+    F inv = tree[BI_T + t];
+    F inv0 = F::zero();
+#pragma unroll 1
+    for (int j = BI_E - 1; j >= 0; j--) {
+        uint64_t i = base + (uint64_t)j * BI_T + t;
+        if (i >= n) continue;
+        F x = bwdx(i);
+        F out;
+        if (x.is_zero()) {
+            out = x;
+        } else {
+            out = (j > 0) ? inv * pre[(j - 1) * BI_T + t] : inv;
+            inv = inv * x;
+        }
+        if (j > 0) pre[(j - 1) * BI_T + t] = out;
+        else inv0 = out;
+    }
+#pragma unroll 1
+    for (int j = 0; j < BI_E; j++) {
+        uint64_t i = base + (uint64_t)j * BI_T + t;
+        if (i >= n) break;
+        emit(i, j == 0 ? inv0 : pre[(j - 1) * BI_T + t], j);
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(BI_T) k_batch_invert(Fp<C>* __restrict__ d, uint64_t n,
+                                                       const Fp<C>* __restrict__ root_inv)
+{
+    using F = Fp<C>;
+    uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
+    block_mont_trick<C>(
+        base, n, root_inv ? root_inv + blockIdx.x : nullptr, [&](uint64_t i) { return ld(&d[i]); },
+        [&](uint64_t i) { return ld(&d[i]); }, [&](uint64_t i, const F& v, int) { st(&d[i], v); });
+}
+
+// Per-CTA product of the (zero-as-one) tile, written to totals[blockIdx.x].
+template <class C>
+__global__ void __launch_bounds__(BI_T) k_tile_product(const Fp<C>* __restrict__ d, uint64_t n,
+                                                       Fp<C>* __restrict__ totals)
+{
+    using F = Fp<C>;
+    __shared__ F red[BI_T];
+    uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
+    F acc = F::one();
+    for (int j = 0; j < BI_E; j++) {
+        uint64_t i = base + (uint64_t)j * BI_T + threadIdx.x;
+        if (i < n) {
+            F x = ld(&d[i]);
+            if (!x.is_zero()) acc = acc * x;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = BI_T / 2; w >= 1; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] * red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) st(&totals[blockIdx.x], red[0]);
+}
+
+template <class Kern>
+static void enable_big_smem(Kern k)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BI_SMEM);
+}
+
+template <class C>
+static RustError batch_invert_local(Fp<C>* d, uint64_t n, cudaStream_t st)
+{
+    if (n == 0) return ok();
+    enable_big_smem(k_batch_invert<C>);
+    uint64_t blocks = (n + BI_TILE - 1) / BI_TILE;
+    k_batch_invert<C><<<(unsigned)blocks, BI_T, BI_SMEM, st>>>(d, n, nullptr);
+    H2B_LAUNCHED("k_batch_invert");
+    return ok();
+}
+
+static uint64_t tiles_of(uint64_t n) { return (n + BI_TILE - 1) / BI_TILE; }
+
+static void plan_batch_invert(ScratchPlan& p, uint64_t n)
+{
+    while (n > BI_TILE) {
+        n = tiles_of(n);
+        p.add(n * 32);
+    }
+}
+
+// Multi-level: tile totals -> recurse -> apply with the inverted totals.
+template <class C>
+static RustError batch_invert_levels(Fp<C>* d, uint64_t n, ScratchArena& ar, cudaStream_t st)
+{
+    if (n <= BI_TILE) return batch_invert_local<C>(d, n, st);
+    uint64_t nt = tiles_of(n);
+    Fp<C>* tot = ar.take_n<Fp<C>>(nt);
+    if (!ar.good()) return err(cudaErrorInvalidValue, "batch_invert: scratch too small");
+    k_tile_product<C><<<(unsigned)nt, BI_T, 0, st>>>(d, n, tot);
+    H2B_LAUNCHED("k_tile_product");
+    H2B_TRY(batch_invert_levels<C>(tot, nt, ar, st));
+    enable_big_smem(k_batch_invert<C>);
+    prof_begin(PROF_BATCH_INVERT, st);
+    k_batch_invert<C><<<(unsigned)nt, BI_T, BI_SMEM, st>>>(d, n, tot);
+    prof_end(PROF_BATCH_INVERT, st);
+    H2B_LAUNCHED("k_batch_invert");
+    return ok();
+}
+
+// ---------------------------------------------------------------------------
+// grand product (in-place multi-level inclusive multiplicative scan)
+// ---------------------------------------------------------------------------
+
+constexpr int GP_T = 256, GP_E = 8, GP_TILE = GP_T * GP_E;
+
+__device__ __forceinline__ uint64_t gp_pos(uint64_t m, uint64_t stride) { return (m + 1) * stride - 1; }
+
+// Scans tiles of GP_TILE level entries (entry m lives at (m+1)*stride-1).
+__global__ void __launch_bounds__(GP_T) k_gp_up(Fr* __restrict__ d, uint64_t count, uint64_t stride,
+                                                 const Fr* __restrict__ prefix)
+{
+    __shared__ Fr tot[GP_T];
+    const int t = threadIdx.x;
+    const uint64_t m0 = (uint64_t)blockIdx.x * GP_TILE + (uint64_t)t * GP_E;
+    Fr q[GP_E];
+    Fr acc = Fr::one();
+#pragma unroll
+    for (int j = 0; j < GP_E; j++) {
+        uint64_t m = m0 + j;
+        Fr x = (m < count) ? ld(&d[gp_pos(m, stride)]) : Fr::one();
+        acc = (j == 0) ? x : acc * x;
+        q[j] = acc;
+    }
+    // exclusive scan of thread totals (Hillis-Steele over 256 entries)
+    tot[t] = acc;
+    __syncthreads();
+    for (int o = 1; o < GP_T; o <<= 1) {
+        Fr v = tot[t];
+        Fr u = (t >= o) ? tot[t - o] : Fr::one();
+        __syncthreads();
+        if (t >= o) tot[t] = u * v;
+        __syncthreads();
+    }
+    Fr ex = (t > 0) ? tot[t - 1] : Fr::one();
+    bool first = (blockIdx.x == 0 && t == 0 && prefix != nullptr);
+    if (first) ex = ld(prefix);
+    bool apply = (t > 0) || first;
+#pragma unroll
+    for (int j = 0; j < GP_E; j++) {
+        uint64_t m = m0 + j;
+        if (m < count) st(&d[gp_pos(m, stride)], apply ? ex * q[j] : q[j]);
+    }
+}
+
+// Entries not on a tile boundary take the final value at the end of the
+// previous tile.
+__global__ void k_gp_down(Fr* __restrict__ d, uint64_t count, uint64_t stride)
+{
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < count;
+         m += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t g = m / GP_TILE;
+        if (g == 0 || ((m + 1) % GP_TILE) == 0) continue;
+        Fr pre = ld(&d[gp_pos(g * GP_TILE - 1, stride)]);
+        uint64_t p = gp_pos(m, stride);
+        st(&d[p], pre * ld(&d[p]));
+    }
+}
+
+static RustError grand_product_inplace(Fr* d, uint64_t n, const Fr* d_prefix, cudaStream_t st)
+{
+    if (n == 0) return ok();
+    std::vector<uint64_t> strides;
+    uint64_t stride = 1, count = n;
+    while (true) {
+        uint64_t blocks = (count + GP_TILE - 1) / GP_TILE;
+        k_gp_up<<<(unsigned)blocks, GP_T, 0, st>>>(d, count, stride, stride == 1 ? d_prefix : nullptr);
+        H2B_LAUNCHED("k_gp_up");
+        strides.push_back(stride);
+        if (count <= GP_TILE) break;
+        stride *= GP_TILE;
+        count = n / stride;
+        if (count == 0) break;
+    }
+    // down-sweep from the second-highest level to level 0
+    for (int l = (int)strides.size() - 2; l >= 0; l--) {
+        uint64_t s = strides[l];
+        uint64_t cnt = (s == 1) ? n : n / s;
+        k_gp_down<<<grid_for(cnt, 256), 256, 0, st>>>(d, cnt, s);
+        H2B_LAUNCHED("k_gp_down");
+    }
+    return ok();
+}
+
+// ---------------------------------------------------------------------------
+// lookup product: (A+b)(S+g) / ((A'+b)(S'+g))
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(BI_T) k_lookup_product(Fr* __restrict__ out, const Fr* __restrict__ pa,
+                                                         const Fr* __restrict__ ps, const Fr* __restrict__ ca,
+                                                         const Fr* __restrict__ cs, const Fr* __restrict__ pbeta,
+                                                         const Fr* __restrict__ pgamma, uint64_t n)
+{
+    const Fr beta = ld(pbeta), gamma = ld(pgamma);
+    uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
+    block_mont_trick<FrCfg>(
+        base, n, nullptr,
+        [&](uint64_t i) {
+            Fr x = (ld(&pa[i]) + beta) * (ld(&ps[i]) + gamma);
+            st(&out[i], x);
+            return x;
+        },
+        [&](uint64_t i) { return ld(&out[i]); },
+        [&](uint64_t i, const Fr& inv, int) {
+            Fr v = inv.is_zero() ? inv : inv * (ld(&ca[i]) + beta) * (ld(&cs[i]) + gamma);
+            st(&out[i], v);
+        });
+}
+
+// ---------------------------------------------------------------------------
+// permutation product
+// ---------------------------------------------------------------------------
+
+constexpr int PP_MAX_COLS = 48;
+struct PermCols {
+    const Fr* sigma[PP_MAX_COLS];
+    const Fr* value[PP_MAX_COLS];
+};
+
+__device__ __forceinline__ Fr pow_u64(const Fr& w, uint64_t e)
+{
+    Fr r = Fr::one(), b = w;
+    while (e) {
+        if (e & 1) r = r * b;
+        b = b * b;
+        e >>= 1;
+    }
+    return r;
+}
+
+// Fused device path: acc_i *= prod_c (b*sigma_c + g + v_c), invert, times
+// prod_c (dw0*delta^c*w^i*b + g + v_c).
+__global__ void __launch_bounds__(BI_T) k_permutation_product(Fr* __restrict__ acc, PermCols cols, int ncols,
+                                                              const Fr* __restrict__ pbeta, const Fr* __restrict__ pgamma,
+                                                              const Fr* __restrict__ pdelta, const Fr* __restrict__ pomega,
+                                                              const Fr* __restrict__ pdeltaomega, uint64_t n)
+{
+    const Fr beta = ld(pbeta), gamma = ld(pgamma), delta = ld(pdelta), omega = ld(pomega);
+    const Fr dw0 = ld(pdeltaomega);
+    const uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
+    Fr wstep = pow_u64(omega, BI_T);   // emit steps i by BI_T
+    Fr wi = Fr::one();
+    block_mont_trick<FrCfg>(
+        base, n, nullptr,
+        [&](uint64_t i) {
+            Fr x = ld(&acc[i]);
+            for (int c = 0; c < ncols; c++) x = x * (beta * ld(&cols.sigma[c][i]) + gamma + ld(&cols.value[c][i]));
+            st(&acc[i], x);
+            return x;
+        },
+        [&](uint64_t i) { return ld(&acc[i]); },
+        [&](uint64_t i, const Fr& inv, int j) {
+            wi = (j == 0) ? dw0 * pow_u64(omega, i) : wi * wstep;
+            if (inv.is_zero()) { st(&acc[i], inv); return; }
+            Fr cur = wi;
+            Fr num = Fr::one();
+            for (int c = 0; c < ncols; c++) {
+                num = num * (cur * beta + gamma + ld(&cols.value[c][i]));
+                cur = cur * delta;
+            }
+            st(&acc[i], inv * num);
+        });
+}
+
+// Host-staged path, one column per launch (the reference's 4-poly workspace):
+// den_i *= b*sigma_i + g + v_i ; num_i = (first ? 1 : num_i) * (dw*w^i*b + g + v_i).
+constexpr int PP_CHUNK = 8;
+__global__ void k_pp_accumulate(Fr* __restrict__ den, Fr* __restrict__ num, const Fr* __restrict__ sigma,
+                                const Fr* __restrict__ value, const Fr* __restrict__ pbeta,
+                                const Fr* __restrict__ pgamma, const Fr* __restrict__ pomega,
+                                const Fr* __restrict__ pdw, uint64_t n, bool first)
+{
+    const Fr beta = ld(pbeta), gamma = ld(pgamma), omega = ld(pomega), dw = ld(pdw);
+    uint64_t nthreads = (n + PP_CHUNK - 1) / PP_CHUNK;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i0 = t * PP_CHUNK;
+        Fr cur = dw * pow_u64(omega, i0);
+        for (int j = 0; j < PP_CHUNK && i0 + j < n; j++) {
+            uint64_t i = i0 + j;
+            Fr v = ld(&value[i]);
+            st(&den[i], ld(&den[i]) * (beta * ld(&sigma[i]) + gamma + v));
+            Fr f = cur * beta + gamma + v;
+            st(&num[i], first ? f : ld(&num[i]) * f);
+            cur = cur * omega;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(BI_T) k_pp_finish(Fr* __restrict__ den, const Fr* __restrict__ num, uint64_t n,
+                                                    bool have_num)
+{
+    uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
+    block_mont_trick<FrCfg>(
+        base, n, nullptr, [&](uint64_t i) { return ld(&den[i]); }, [&](uint64_t i) { return ld(&den[i]); },
+        [&](uint64_t i, const Fr& inv, int) { st(&den[i], have_num ? inv * ld(&num[i]) : inv); });
+}
+
+__global__ void k_advance_deltaomega(Fr* __restrict__ dw, const Fr* __restrict__ pdelta, uint64_t batch)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        Fr x = ld(dw), d = ld(pdelta);
+        for (uint64_t i = 0; i < batch; i++) x = x * d;
+        st(dw, x);
+    }
+}
+
+} // namespace h2b
+
+using namespace h2b;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" RustError _halo2_batch_invert(void* d_data, uint32_t field_type, uint64_t length, cudaStream_t stream)
+{
+    if (field_type != 0 && field_type != 1) return err(cudaErrorInvalidValue, "Invalid scalar type");
+    if (length == 0) return err(cudaErrorInvalidValue, "_halo2_batch_invert: length must be >= 1");
+    if (field_type == 0) return batch_invert_local<FrCfg>((Fr*)d_data, length, stream);
+    return batch_invert_local<FqCfg>((Fq*)d_data, length, stream);
+}
+
+extern "C" uint64_t h2b_batch_invert_workspace_size(uint64_t length)
+{
+    ScratchPlan p;
+    plan_batch_invert(p, length);
+    return p.used;
+}
+
+extern "C" RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_t length, void* scratch,
+                                      uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (field_type != 0 && field_type != 1) return err(cudaErrorInvalidValue, "Invalid scalar type");
+    if (length == 0) return err(cudaErrorInvalidValue, "h2b_batch_invert: length must be >= 1");
+    uint64_t need = h2b_batch_invert_workspace_size(length);
+    if (scratch_bytes < need) return scratch_too_small("h2b_batch_invert", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    if (field_type == 0) return batch_invert_levels<FrCfg>((Fr*)d_data, length, ar, stream);
+    return batch_invert_levels<FqCfg>((Fq*)d_data, length, ar, stream);
+}
+
+// grand product ---------------------------------------------------------------
+
+extern "C" uint64_t _halo2_grand_product_workspace_size(uint64_t poly_length)
+{
+    ScratchPlan p;
+    p.add(poly_length * 32);
+    p.add(32);
+    return p.used;
+}
+
+extern "C" uint64_t _halo2_grand_product_max_len(uint64_t poly_length, uint64_t free_bytes)
+{
+    for (uint64_t l = poly_length; l > 0; l >>= 1)
+        if (_halo2_grand_product_workspace_size(l) < free_bytes) return l;
+    return 0;
+}
+
+extern "C" RustError _halo2_grand_product(const FFITraitObject* output, const FFITraitObject* input,
+                                          const FFITraitObject* prefix, uint64_t poly_length, uint64_t poly_offset,
+                                          void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    uint64_t need = _halo2_grand_product_workspace_size(poly_length);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_grand_product", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    Fr* d = ar.take_n<Fr>(poly_length);
+    Fr* dp = ar.take_n<Fr>(1);
+    const uint8_t* hin = (const uint8_t*)input->ptr + poly_offset * 32;
+    uint8_t* hout = (uint8_t*)output->ptr + poly_offset * 32;
+    H2B_CUDA(cudaMemcpyAsync(d, hin, poly_length * 32, cudaMemcpyHostToDevice, stream));
+    H2B_CUDA(cudaMemcpyAsync(dp, prefix->ptr, 32, cudaMemcpyHostToDevice, stream));
+    H2B_TRY(grand_product_inplace(d, poly_length, dp, stream));
+    H2B_CUDA(cudaMemcpyAsync(hout, d, poly_length * 32, cudaMemcpyDeviceToHost, stream));
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" RustError _halo2_grand_product_device_inputs(const FFITraitObject* d_inout, const FFITraitObject* d_prefix,
+                                                        uint64_t poly_length, uint64_t poly_offset, cudaStream_t stream)
+{
+    Fr* d = (Fr*)((uint8_t*)d_inout->ptr + poly_offset * 32);
+    return grand_product_inplace(d, poly_length, (const Fr*)d_prefix->ptr, stream);
+}
+
+// lookup (commit) product -------------------------------------------------------
+
+static RustError lookup_product_run(Fr* out, const Fr* pa, const Fr* ps, const Fr* ca, const Fr* cs, const Fr* beta,
+                                    const Fr* gamma, uint64_t n, cudaStream_t st)
+{
+    if (n == 0) return ok();
+    enable_big_smem(k_lookup_product);
+    k_lookup_product<<<(unsigned)tiles_of(n), BI_T, BI_SMEM, st>>>(out, pa, ps, ca, cs, beta, gamma, n);
+    H2B_LAUNCHED("k_lookup_product");
+    return ok();
+}
+
+extern "C" uint64_t _halo2_commit_product_workspace_size(uint64_t poly_length)
+{
+    ScratchPlan p;
+    for (int i = 0; i < 5; i++) p.add(poly_length * 32);
+    return p.used;
+}
+
+extern "C" uint64_t _halo2_commit_product_max_len(uint64_t poly_length, uint64_t free_bytes)
+{
+    for (uint64_t l = poly_length; l > 0; l >>= 1)
+        if (_halo2_commit_product_workspace_size(l) < free_bytes) return l;
+    return 0;
+}
+
+extern "C" RustError _halo2_commit_product(const FFITraitObject* lookup_product, const FFITraitObject* permuted_input,
+                                           const FFITraitObject* permuted_table,
+                                           const FFITraitObject* compressed_input,
+                                           const FFITraitObject* compressed_table, const void* beta_device,
+                                           const void* gamma_device, uint64_t length, uint64_t offset, void* scratch,
+                                           uint64_t scratch_bytes, cudaStream_t stream)
+{
+    uint64_t need = _halo2_commit_product_workspace_size(length);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_commit_product", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    Fr* buf[5];
+    for (int i = 0; i < 5; i++) buf[i] = ar.take_n<Fr>(length);
+    const FFITraitObject* srcs[4] = {permuted_input, permuted_table, compressed_input, compressed_table};
+    for (int i = 0; i < 4; i++)
+        H2B_CUDA(cudaMemcpyAsync(buf[i + 1], (const uint8_t*)srcs[i]->ptr + offset * 32, length * 32,
+                                 cudaMemcpyHostToDevice, stream));
+    H2B_TRY(lookup_product_run(buf[0], buf[1], buf[2], buf[3], buf[4], (const Fr*)beta_device,
+                               (const Fr*)gamma_device, length, stream));
+    H2B_CUDA(cudaMemcpyAsync((uint8_t*)lookup_product->ptr + offset * 32, buf[0], length * 32,
+                             cudaMemcpyDeviceToHost, stream));
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" RustError _halo2_commit_product_device_inputs(
+    const FFITraitObject* d_lookup_product, const FFITraitObject* d_permuted_input,
+    const FFITraitObject* d_permuted_table, const FFITraitObject* d_compressed_input,
+    const FFITraitObject* d_compressed_table, const void* beta_device, const void* gamma_device, uint64_t length,
+    uint64_t offset, cudaStream_t stream)
+{
+    auto at = [&](const FFITraitObject* o) { return (Fr*)((uint8_t*)o->ptr + offset * 32); };
+    return lookup_product_run(at(d_lookup_product), at(d_permuted_input), at(d_permuted_table),
+                              at(d_compressed_input), at(d_compressed_table), (const Fr*)beta_device,
+                              (const Fr*)gamma_device, length, stream);
+}
+
+// permutation product -------------------------------------------------------------
+
+extern "C" uint64_t _halo2_permutation_product_workspace_size(uint64_t poly_length)
+{
+    // accumulator, numerators, and one staged (sigma, value) column pair
+    ScratchPlan p;
+    for (int i = 0; i < 4; i++) p.add(poly_length * 32);
+    return p.used;
+}
+
+extern "C" uint64_t _halo2_permutation_product_max_len(uint64_t poly_length, uint64_t free_bytes)
+{
+    for (uint64_t l = poly_length; l > 0; l >>= 1)
+        if (_halo2_permutation_product_workspace_size(l) < free_bytes) return l;
+    return 0;
+}
+
+extern "C" RustError _halo2_permutation_product(const FFITraitObject* modified_values,
+                                                const FFITraitObject* permutations, const FFITraitObject* values,
+                                                const void* beta_device, const void* gamma_device,
+                                                const void* delta_device, const void* omega_device,
+                                                void* deltaomega_device, uint64_t length, uint64_t offset,
+                                                uint64_t batch, void* scratch, uint64_t scratch_bytes,
+                                                cudaStream_t stream)
+{
+    uint64_t need = _halo2_permutation_product_workspace_size(length);
+    if (scratch_bytes < need) return scratch_too_small("_halo2_permutation_product", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    Fr* den = ar.take_n<Fr>(length);
+    Fr* num = ar.take_n<Fr>(length);
+    Fr* sig = ar.take_n<Fr>(length);
+    Fr* val = ar.take_n<Fr>(length);
+    H2B_CUDA(cudaMemcpyAsync(den, modified_values->ptr, length * 32, cudaMemcpyHostToDevice, stream));
+    for (uint64_t c = 0; c < batch; c++) {
+        H2B_CUDA(cudaMemcpyAsync(sig, (const uint8_t*)permutations[c].ptr + offset * 32, length * 32,
+                                 cudaMemcpyHostToDevice, stream));
+        H2B_CUDA(cudaMemcpyAsync(val, (const uint8_t*)values[c].ptr + offset * 32, length * 32,
+                                 cudaMemcpyHostToDevice, stream));
+        if (length > 0) {
+            uint64_t nthreads = (length + PP_CHUNK - 1) / PP_CHUNK;
+            k_pp_accumulate<<<grid_for(nthreads, 256), 256, 0, stream>>>(
+                den, num, sig, val, (const Fr*)beta_device, (const Fr*)gamma_device, (const Fr*)omega_device,
+                (const Fr*)deltaomega_device, length, c == 0);
+            H2B_LAUNCHED("k_pp_accumulate");
+        }
+        k_advance_deltaomega<<<1, 32, 0, stream>>>((Fr*)deltaomega_device, (const Fr*)delta_device, 1);
+        H2B_LAUNCHED("k_advance_deltaomega");
+    }
+    if (length > 0) {
+        enable_big_smem(k_pp_finish);
+        k_pp_finish<<<(unsigned)tiles_of(length), BI_T, BI_SMEM, stream>>>(den, num, length, batch > 0);
+        H2B_LAUNCHED("k_pp_finish");
+    }
+    H2B_CUDA(cudaMemcpyAsync(modified_values->ptr, den, length * 32, cudaMemcpyDeviceToHost, stream));
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    return ok();
+}
+
+extern "C" uint64_t _halo2_permutation_product_device_inputs_workspace_size(uint64_t poly_length)
+{
+    (void)poly_length;
+    return 0;
+}
+
+extern "C" RustError _halo2_permutation_product_device_inputs(
+    const FFITraitObject* modified_values_device, const FFITraitObject* permutations_device,
+    const FFITraitObject* values_device, const void* beta_device, const void* gamma_device, const void* delta_device,
+    const void* omega_device, void* deltaomega_device, uint64_t length, uint64_t offset, uint64_t batch,
+    void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    (void)scratch;
+    (void)scratch_bytes;
+    if (batch > PP_MAX_COLS) return err(cudaErrorInvalidValue, "permutation product: too many columns in one set");
+    PermCols cols;
+    for (uint64_t c = 0; c < batch; c++) {
+        cols.sigma[c] = (const Fr*)((const uint8_t*)permutations_device[c].ptr + offset * 32);
+        cols.value[c] = (const Fr*)((const uint8_t*)values_device[c].ptr + offset * 32);
+    }
+    Fr* acc = (Fr*)modified_values_device->ptr;
+    if (length > 0) {
+        enable_big_smem(k_permutation_product);
+        k_permutation_product<<<(unsigned)tiles_of(length), BI_T, BI_SMEM, stream>>>(
+            acc, cols, (int)batch, (const Fr*)beta_device, (const Fr*)gamma_device, (const Fr*)delta_device,
+            (const Fr*)omega_device, (const Fr*)deltaomega_device, length);
+        H2B_LAUNCHED("k_permutation_product");
+    }
+    k_advance_deltaomega<<<1, 32, 0, stream>>>((Fr*)deltaomega_device, (const Fr*)delta_device, batch);
+    H2B_LAUNCHED("k_advance_deltaomega");
+    return ok();
+}

@@ -1,0 +1,145 @@
+// Event-based kernel timing hook and pipe-throughput probes.
+//
+//  * h2b_prof_enable / h2b_prof_read: see prof.cuh.  Events come from a pool
+//    created on first use; nothing here allocates device memory.
+//  * h2b_probe_imad: independent mad.lo / mad.hi chains at full occupancy,
+//    giving the measured 32-bit integer multiply-add throughput that bounds
+//    every Montgomery-arithmetic kernel in this library.
+//  * h2b_probe_modmul: four independent Montgomery products per thread per
+//    iteration, the achievable Fr multiplication rate of field.cuh.
+#include <mutex>
+#include <vector>
+#include "abi.cuh"
+#include "field.cuh"
+#include "prof.cuh"
+
+namespace h2b {
+
+namespace {
+struct Pair {
+    cudaEvent_t a, b;
+};
+std::mutex g_mu;
+bool g_on = false;
+std::vector<Pair> g_pool;
+std::vector<Pair> g_used[PROF_IDS];
+Pair g_open[PROF_IDS];
+bool g_is_open[PROF_IDS];
+
+Pair take_pair()
+{
+    if (!g_pool.empty()) {
+        Pair p = g_pool.back();
+        g_pool.pop_back();
+        return p;
+    }
+    Pair p;
+    cudaEventCreate(&p.a);
+    cudaEventCreate(&p.b);
+    return p;
+}
+} // namespace
+
+bool prof_on() { return g_on; }
+
+void prof_begin(int id, cudaStream_t st)
+{
+    if (!g_on || id < 0 || id >= PROF_IDS) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Pair p = take_pair();
+    cudaEventRecord(p.a, st);
+    g_open[id] = p;
+    g_is_open[id] = true;
+}
+
+void prof_end(int id, cudaStream_t st)
+{
+    if (!g_on || id < 0 || id >= PROF_IDS) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_is_open[id]) return;
+    cudaEventRecord(g_open[id].b, st);
+    g_used[id].push_back(g_open[id]);
+    g_is_open[id] = false;
+}
+
+// 16 independent 32-bit IMADs per iteration per thread (8 lo, 8 hi).
+__global__ void k_probe_imad(uint32_t* sink, int iters, uint32_t seed)
+{
+    uint32_t a[8];
+    for (int j = 0; j < 8; j++) a[j] = seed * (threadIdx.x + 1) + j * 0x9e3779b9u;
+    const uint32_t m = seed | 1u;
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(m), "r"(a[(j + 1) & 7]));
+            asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(m), "r"(a[(j + 3) & 7]));
+        }
+    }
+    uint32_t x = 0;
+    for (int j = 0; j < 8; j++) x ^= a[j];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
+}
+
+__global__ void k_probe_modmul(uint32_t* sink, int iters)
+{
+    Fr a = Fr::one(), b = Fr::r2(), c = Fr::one(), d = Fr::r2();
+    a.v[0] ^= threadIdx.x;
+    c.v[1] ^= blockIdx.x;
+    const Fr m = Fr::r2();
+    for (int it = 0; it < iters; it++) {
+        a = a * m;
+        b = b * m;
+        c = c * m;
+        d = d * m;
+    }
+    uint32_t x = a.v[0] ^ b.v[1] ^ c.v[2] ^ d.v[3];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
+}
+
+} // namespace h2b
+
+using namespace h2b;
+
+extern "C" void h2b_prof_enable(int on)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int i = 0; i < PROF_IDS; i++) {
+        for (auto& p : g_used[i]) g_pool.push_back(p);
+        g_used[i].clear();
+        g_is_open[i] = false;
+    }
+    g_on = on != 0;
+}
+
+// Sums the recorded intervals of `id` (waits for their completion).
+extern "C" int h2b_prof_read(int id, double* total_ms, int* count)
+{
+    if (id < 0 || id >= PROF_IDS) return -1;
+    std::lock_guard<std::mutex> lk(g_mu);
+    double tot = 0;
+    for (auto& p : g_used[id]) {
+        cudaEventSynchronize(p.b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        tot += ms;
+    }
+    *total_ms = tot;
+    *count = (int)g_used[id].size();
+    return 0;
+}
+
+extern "C" RustError h2b_probe_imad(int blocks, int threads, int iters, void* d_sink, cudaStream_t stream)
+{
+    k_probe_imad<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters, 0x2545f491u);
+    H2B_LAUNCHED("k_probe_imad");
+    return ok();
+}
+
+extern "C" RustError h2b_probe_modmul(int blocks, int threads, int iters, void* d_sink, cudaStream_t stream)
+{
+    k_probe_modmul<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    H2B_LAUNCHED("k_probe_modmul");
+    return ok();
+}
+
+extern "C" uint64_t h2b_launch_count(void) { return g_kernel_launches.load(); }

@@ -1,0 +1,279 @@
+/*
+ * halo2_gpu.h -- C ABI of the B200 (sm_100a) BN254 Halo2/KZG prover hot path.
+ *
+ * Drop-in for the reference's static library `libhalo2_gpu`: every `_halo2_*`
+ * symbol below keeps the name, argument order, argument meaning and error
+ * behaviour of the reference launcher it replaces (cited per entry, paths
+ * relative to the axiom-crypto/halo2-gpu tree).  The Rust crate binds them in
+ * halo2_proofs/src/cuda/culib.rs:28-652 and
+ * halo2_proofs/src/plonk/evaluation.rs:1434-1568.
+ *
+ * Conventions (halo2_proofs/cuda/include/common/halo2_ffi.h:1-62):
+ *  - Field elements are 32-byte Montgomery-form BN254 Fr/Fq, little-endian
+ *    64-bit limbs (the halo2curves memory image).  G1 affine points are 64
+ *    bytes {x, y}, infinity = (0, 0).  MSM results are the 96-byte Jacobian
+ *    image {X, Y, Z} with Z = 1, or (0, 1, 0) for infinity.
+ *  - `void*` arguments named d_* are device pointers; FFITraitObject carries a
+ *    host or device address as documented per entry.
+ *  - `scratch` is caller-owned device memory of at least the matching
+ *    `_workspace_size` bytes (256-byte aligned is best).  Launchers never
+ *    allocate device memory.
+ *  - Work is enqueued on `stream`; entries with host outputs synchronise the
+ *    stream before returning, device-output entries do not.
+ *  - RustError.code == 0 on success; otherwise a cudaError_t value or a
+ *    reference-compatible sentinel (-1 / 2 / -6 for unsupported NTT types).
+ *    A non-null RustError.message is heap memory owned by the caller (free()).
+ */
+#ifndef HALO2_GPU_H
+#define HALO2_GPU_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct RustError {
+    int code;
+    char* message;
+} RustError;
+
+typedef struct FFITraitObject {
+    uint64_t* ptr;
+} FFITraitObject;
+
+typedef void* h2b_stream_t; /* cudaStream_t */
+
+/* ------------------------------------------------------------------ MSM --- */
+
+/* culib.rs:30 ; multiexp.cu:183-188 */
+uint64_t _halo2_msm_max_length(uint64_t free_bytes);
+/* culib.rs:32 ; multiexp.cu:191-195 */
+uint64_t _halo2_multiexp_workspace_size(uint64_t length);
+/* culib.rs:34-43 ; multiexp.cu:260-327 -- host scalars, host bases, host out */
+RustError _halo2_multiexp(const FFITraitObject* scalar, const FFITraitObject* point, const FFITraitObject* output,
+                          uint64_t length, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:45 ; multiexp.cu:333-337 */
+uint64_t _halo2_multiexp_device_bases_workspace_size(uint64_t length);
+/* culib.rs:47-56 ; multiexp.cu:346-412 -- host scalars, device bases, host out */
+RustError _halo2_multiexp_device_bases(const FFITraitObject* h_scalar, const void* d_bases,
+                                       const FFITraitObject* h_output, uint64_t length, void* scratch,
+                                       uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:58 ; multiexp.cu:419-423 */
+uint64_t _halo2_multiexp_device_scalars_device_bases_workspace_size(uint64_t length);
+/* culib.rs:60-70 ; multiexp.cu:436-525 -- device scalars (not mutated), device bases, host out */
+RustError _halo2_multiexp_device_scalars_device_bases(const void* d_scalar, const void* d_bases,
+                                                      const FFITraitObject* h_output, uint64_t length,
+                                                      void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+
+/* ------------------------------------------------------------- batch inv --- */
+
+/* culib.rs:72-79 ; polynomial/operations.cu:16-42 -- in place, zeros stay zero, field_type 0 = Fr, 1 = Fq */
+RustError _halo2_batch_invert(void* d_data, uint32_t field_type, uint64_t length, h2b_stream_t stream);
+
+/* ---------------------------------------------------- products and scans --- */
+
+/* culib.rs:81-82 ; commitment/commit_product.cu:35-50 */
+uint64_t _halo2_commit_product_max_len(uint64_t length, uint64_t free_bytes);
+uint64_t _halo2_commit_product_workspace_size(uint64_t poly_length);
+/* culib.rs:87-100 ; commitment/commit_product.cu:51-139 -- host polys, device beta/gamma */
+RustError _halo2_commit_product(const FFITraitObject* lookup_product, const FFITraitObject* permuted_input,
+                                const FFITraitObject* permuted_table, const FFITraitObject* compressed_input,
+                                const FFITraitObject* compressed_table, const void* beta_device,
+                                const void* gamma_device, uint64_t length, uint64_t offset, void* scratch,
+                                uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:114-125 ; commitment/commit_product.cu:141-186 -- all device, no scratch */
+RustError _halo2_commit_product_device_inputs(const FFITraitObject* d_lookup_product,
+                                              const FFITraitObject* d_permuted_input,
+                                              const FFITraitObject* d_permuted_table,
+                                              const FFITraitObject* d_compressed_input,
+                                              const FFITraitObject* d_compressed_table, const void* beta_device,
+                                              const void* gamma_device, uint64_t length, uint64_t offset,
+                                              h2b_stream_t stream);
+
+/* culib.rs:143-144 ; commitment/permutation_commit.cu:37-50 */
+uint64_t _halo2_permutation_product_max_len(uint64_t length, uint64_t free_bytes);
+uint64_t _halo2_permutation_product_workspace_size(uint64_t poly_length);
+/* culib.rs:147-162 ; commitment/permutation_commit.cu:51-146 -- host polys, device scalars */
+RustError _halo2_permutation_product(const FFITraitObject* modified_values, const FFITraitObject* permutations,
+                                     const FFITraitObject* values, const void* beta_device, const void* gamma_device,
+                                     const void* delta_device, const void* omega_device, void* deltaomega_device,
+                                     uint64_t length, uint64_t offset, uint64_t batch, void* scratch,
+                                     uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:164 ; commitment/permutation_commit.cu:163-167 */
+uint64_t _halo2_permutation_product_device_inputs_workspace_size(uint64_t poly_length);
+/* culib.rs:184-199 ; commitment/permutation_commit.cu:181-256 -- all device */
+RustError _halo2_permutation_product_device_inputs(const FFITraitObject* modified_values_device,
+                                                   const FFITraitObject* permutations_device,
+                                                   const FFITraitObject* values_device, const void* beta_device,
+                                                   const void* gamma_device, const void* delta_device,
+                                                   const void* omega_device, void* deltaomega_device,
+                                                   uint64_t length, uint64_t offset, uint64_t batch, void* scratch,
+                                                   uint64_t scratch_bytes, h2b_stream_t stream);
+
+/* culib.rs:201-202 ; commitment/grand_product.cu:31-49 */
+uint64_t _halo2_grand_product_max_len(uint64_t length, uint64_t free_bytes);
+uint64_t _halo2_grand_product_workspace_size(uint64_t poly_length);
+/* culib.rs:206-215 ; commitment/grand_product.cu:51-132 -- out[i] = prefix * prod_{j<=i} in[j], host polys */
+RustError _halo2_grand_product(const FFITraitObject* output, const FFITraitObject* input,
+                               const FFITraitObject* prefix, uint64_t poly_length, uint64_t poly_offset,
+                               void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:224-230 ; commitment/grand_product.cu:139-195 -- in place on device, device prefix */
+RustError _halo2_grand_product_device_inputs(const FFITraitObject* d_inout, const FFITraitObject* d_prefix,
+                                             uint64_t poly_length, uint64_t poly_offset, h2b_stream_t stream);
+
+/* ------------------------------------------------------ lookup permute --- */
+
+/* culib.rs:127 ; commitment/permute_expression_pair.cu:185-227 */
+uint64_t _halo2_permute_expression_pair_workspace_size(uint64_t n, uint64_t usable_rows);
+/* culib.rs:131-141 ; commitment/permute_expression_pair.cu:229-350 -- device in/out */
+RustError _halo2_permute_expression_pair(const void* d_compressed_input, const void* d_compressed_table,
+                                         void* d_permuted_input, void* d_permuted_table, uint64_t n,
+                                         uint64_t usable_rows, void* scratch, uint64_t scratch_bytes,
+                                         h2b_stream_t stream);
+
+/* -------------------------------------------------------- element-wise --- */
+
+/* culib.rs:276-282 ; polynomial/polynomial.cu:420-455 */
+RustError _halo2_poly_multiply_add(void* d_poly_acc, const void* d_poly_in, const void* d_scalar,
+                                   uint64_t poly_length, h2b_stream_t stream);
+/* culib.rs:285-291 ; polynomial/polynomial.cu:321-341 */
+RustError _halo2_poly_elementwise_multiply(void* d_out, const void* d_a, const void* d_b, uint64_t length,
+                                           h2b_stream_t stream);
+/* culib.rs:294-298 ; polynomial/polynomial.cu:343-361 -- fills with one */
+RustError _halo2_poly_fill_one(void* d_out, uint64_t length, h2b_stream_t stream);
+/* culib.rs:322-328 ; polynomial/polynomial.cu:270-292 */
+RustError _halo2_divide_by_vanishing_poly(void* d_poly, const void* d_t_evals, uint32_t t_len, uint64_t n,
+                                          h2b_stream_t stream);
+/* culib.rs:359-364 ; polynomial/polynomial.cu:363-388 */
+RustError _halo2_poly_sub_short_inplace(void* d_acc, const void* d_short, uint64_t short_len, h2b_stream_t stream);
+/* culib.rs:370-377 ; polynomial/polynomial.cu:390-416 */
+RustError _halo2_poly_sub_short_out_of_place(void* d_out, const void* d_long, const void* d_short,
+                                             uint64_t short_len, uint64_t long_len, h2b_stream_t stream);
+/* culib.rs:381-385 ; polynomial/polynomial.cu:418-433 */
+RustError _halo2_poly_sub_scalar_at_zero(void* d_buf, const void* d_scalar, h2b_stream_t stream);
+/* culib.rs:389-395 ; polynomial/polynomial.cu:247-268 -- d_parts: device array of device pointers */
+RustError _halo2_extended_from_lagrange_vec_device(void* d_out, const void* d_parts, uint32_t num_parts, uint64_t n,
+                                                   h2b_stream_t stream);
+/* culib.rs:399-405 ; polynomial/polynomial.cu:294-319 */
+RustError _halo2_distribute_powers_zeta(void* d_a, const void* d_coset_powers, uint32_t coset_powers_len,
+                                       uint64_t n, h2b_stream_t stream);
+
+/* ------------------------------------------------------------------ NTT --- */
+/* ntt_type: 1 FFT, 2 iFFT, 3 cosetFFT, 4 icosetFFT, 5 unsupported, 6 CosetFFT_Part (ntt.cu:21-28);
+ * for CosetFFT_Part the divisor slot carries the coset factor zeta * w_ext^j (domain.rs:527-540). */
+
+/* culib.rs:492 ; ntt.cu:383-392 */
+uint64_t _halo2_fft_normal_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:494-504 ; ntt.cu:394-477 -- host in/out, host omega/divisor, synchronises */
+RustError _halo2_fft_normal(uint32_t ntt_type, uint32_t log_n, const void* input, void* output, const void* omega,
+                            const void* divisor, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:506-511 ; ntt.cu:149-164 -- always true */
+bool _halo2_fft_normal_check_memory(uint32_t ntt_type, const void* input, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:513-517 ; ntt.cu:483-490 */
+uint64_t _halo2_fft_normal_to_device_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:523-533 ; ntt.cu:510-580 -- device in/out (may alias), device omega, host divisor; FFT/iFFT/CosetFFT_Part */
+RustError _halo2_fft_normal_to_device(uint32_t ntt_type, uint32_t log_n, const void* d_input, void* d_output,
+                                      const void* d_omega, const void* h_divisor, void* scratch,
+                                      uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:535-546 ; ntt.cu:584-648 -- host in (2^log_n) -> host out (2^extend_log_n), forward coset */
+RustError _halo2_cosetfft(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n, const void* input, void* output,
+                          const void* omega, const void* divisor, void* scratch, uint64_t scratch_bytes,
+                          h2b_stream_t stream);
+/* culib.rs:548 ; ntt.cu:758-772 */
+uint64_t _halo2_fft_many_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:550-554 ; ntt.cu:777-787 */
+uint64_t _halo2_fft_many_to_device_workspace_size(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:561-573 ; ntt.cu:829-890 -- host arrays of host polys, device omega, host divisor */
+RustError _halo2_fft_many(uint32_t ntt_type, uint32_t num_many, uint32_t log_n, uint32_t extend_log_n,
+                          const FFITraitObject* input, const FFITraitObject* output, const void* omega_device,
+                          const FFITraitObject* divisor, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:579-592 ; ntt.cu:898-962 -- device outputs, input residency per input_on_device */
+RustError _halo2_fft_many_to_device(uint32_t ntt_type, uint32_t num_many, uint32_t log_n, uint32_t extend_log_n,
+                                    const FFITraitObject* input, const FFITraitObject* output,
+                                    const void* omega_device, const FFITraitObject* divisor, bool input_on_device,
+                                    void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:594 ; ntt.cu:792-800 -- always true */
+bool _halo2_fft_many_check_memory(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n);
+/* culib.rs:596-601 ; ntt.cu:676-690 */
+int32_t _halo2_get_fft_split_radix(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n, uint64_t free_bytes);
+
+/* ------------------------------------------------------------ quotient --- */
+
+/* evaluation.rs:1435-1449 ; quotient.cu:190-222 */
+uint64_t _halo2_evaluate_h_max_rows(const uint64_t* rules, uint64_t num_rules, uint64_t num_vp_rules,
+                                    uint64_t num_quotient, uint64_t num_fixed, uint64_t num_instance,
+                                    uint64_t num_advice, uint64_t num_challenges, uint64_t num_constants,
+                                    uint64_t rotation_scale, uint64_t row_start, uint64_t row_end,
+                                    uint64_t free_bytes);
+/* evaluation.rs:1451-1464 ; quotient.cu:224-260 */
+uint64_t _halo2_quotient_workspace_size(const uint64_t* rules, uint64_t num_rules, uint64_t num_vp_rules,
+                                        uint64_t num_quotient, uint64_t num_fixed, uint64_t num_instance,
+                                        uint64_t num_advice, uint64_t num_challenges, uint64_t num_constants,
+                                        uint64_t rotation_scale, uint64_t row_start, uint64_t row_end);
+/* evaluation.rs:1466-1490 ; quotient.cu:309-440 -- host columns and host output */
+RustError _halo2_quotient(const FFITraitObject* fixed, uint64_t num_fixed, const FFITraitObject* instance,
+                          uint64_t num_instance, const FFITraitObject* advices, uint64_t num_advice,
+                          FFITraitObject challenges, uint64_t num_challenges, FFITraitObject constants,
+                          uint64_t num_constants, FFITraitObject expr_constants, const uint64_t* rules,
+                          uint64_t num_rules, const uint64_t* value_part_rules, uint64_t num_vp_rules,
+                          FFITraitObject quotient_poly, uint64_t num_quotient, uint64_t rotation_scale,
+                          uint64_t row_start, uint64_t row_end, void* scratch, uint64_t scratch_bytes,
+                          h2b_stream_t stream);
+/* evaluation.rs:1498-1522 ; quotient.cu:570-710 -- device column pointers, device output */
+RustError _halo2_quotient_device_columns_device_out(
+    const void* const* fixed_d_ptrs, uint64_t num_fixed, const void* const* instance_d_ptrs, uint64_t num_instance,
+    const void* const* advice_d_ptrs, uint64_t num_advice, FFITraitObject challenges, uint64_t num_challenges,
+    FFITraitObject constants, uint64_t num_constants, FFITraitObject expr_constants, const uint64_t* rules,
+    uint64_t num_rules, const uint64_t* value_part_rules, uint64_t num_vp_rules, void* quotient_poly_device_ptr,
+    uint64_t num_quotient, const void* prev_values_device_ptr, uint64_t rotation_scale, uint64_t row_start,
+    uint64_t row_end, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* evaluation.rs:1536-1559 ; quotient.cu:450-568 -- device column pointers, host output */
+RustError _halo2_quotient_device_columns(const void* const* fixed_d_ptrs, uint64_t num_fixed,
+                                         const void* const* instance_d_ptrs, uint64_t num_instance,
+                                         const void* const* advice_d_ptrs, uint64_t num_advice,
+                                         FFITraitObject challenges, uint64_t num_challenges,
+                                         FFITraitObject constants, uint64_t num_constants,
+                                         FFITraitObject expr_constants, const uint64_t* rules, uint64_t num_rules,
+                                         const uint64_t* value_part_rules, uint64_t num_vp_rules,
+                                         FFITraitObject quotient_poly, uint64_t num_quotient,
+                                         uint64_t rotation_scale, uint64_t row_start, uint64_t row_end,
+                                         void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:603-617 ; quotient_lookups.cu:16-53 -- all device pointers */
+RustError _halo2_quotient_lookups(void* values, const void* table_values, const void* product_coset,
+                                  const void* permuted_input_coset, const void* permuted_table_coset, const void* l0,
+                                  const void* l_last, const void* l_active_row, const void* beta, const void* gamma,
+                                  const void* y, uint64_t poly_length, h2b_stream_t stream);
+/* culib.rs:622-650 ; permutation_quotient.cu:23-93 -- device buffers / pointer tables, host scalars */
+RustError _halo2_quotient_permutation(void* values, const void* l0, const void* l_last, const void* l_active_row,
+                                      const void* perm_prod_cosets, const void* perm_cosets, const void* column_values,
+                                      const void* beta, const void* gamma, const void* y, const void* delta,
+                                      const void* delta_start, const void* current_extended_omega, const void* omega,
+                                      uint64_t n_sets, uint64_t chunk_len, uint64_t n_perm_cols, int32_t last_rotation,
+                                      int32_t rot_scale, int32_t isize_, uint64_t poly_length, h2b_stream_t stream);
+
+/* ------------------------------------------- additions of this library --- */
+/* No counterpart in the reference.  Device-output, sync-free forms used by the
+ * batched and served provers, plus tuning hooks. */
+
+/* Same as _halo2_multiexp_device_scalars_device_bases but writes the 96-byte
+ * result to d_out on `stream` without synchronising. */
+RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out, uint64_t length, void* scratch,
+                         uint64_t scratch_bytes, h2b_stream_t stream);
+/* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
+void h2b_msm_set_tuning(int window_bits, int chunk);
+/* Batch inversion whose CTAs share a single inversion through scratch
+ * (h2b_batch_invert_workspace_size bytes); same semantics as _halo2_batch_invert. */
+uint64_t h2b_batch_invert_workspace_size(uint64_t length);
+RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_t length, void* scratch, uint64_t scratch_bytes,
+                           h2b_stream_t stream);
+/* Radix-2 stages per shared-memory NTT pass (1..10). */
+void h2b_ntt_set_pass_stages(int stages);
+int h2b_ntt_get_pass_stages(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HALO2_GPU_H */

@@ -1,0 +1,79 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol the
+public header declares, and the pure-host preflights / argument checks behave
+like the reference's (no device work is issued by any call here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = []
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names += re.findall(r"\b((?:_halo2|h2b)_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_declares_reference_entry_points():
+    names = declared_symbols()
+    for must in ("_halo2_multiexp", "_halo2_fft_normal", "_halo2_batch_invert", "_halo2_grand_product",
+                 "_halo2_permute_expression_pair", "_halo2_quotient_device_columns_device_out",
+                 "_halo2_quotient_permutation", "_halo2_quotient_lookups", "_halo2_commit_product_device_inputs"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    missing = [n for n in declared_symbols() if not hasattr(built_lib, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_python_mirror_binds_every_declared_symbol(h2b, built_lib):
+    bound = set(h2b._SIGS)
+    missing = [n for n in declared_symbols() if n not in bound]
+    assert not missing, f"python mirror lacks: {missing}"
+
+
+def test_workspace_preflights_are_pure_host(h2b, built_lib):
+    L = built_lib
+    for k in (1, 10, 16, 22):
+        a = L._halo2_fft_normal_workspace_size(1, k, k)
+        b = L._halo2_fft_normal_to_device_workspace_size(1, k, k)
+        assert a > b > 0
+        assert L._halo2_fft_many_workspace_size(3, k, k + 2) >= (32 << (k + 2))
+    assert L._halo2_multiexp_workspace_size(1 << 16) > L._halo2_multiexp_device_bases_workspace_size(1 << 16)
+    assert L._halo2_msm_max_length(1 << 40) == 1 << 28
+    assert L._halo2_msm_max_length(1 << 20) < (1 << 20)
+    assert L._halo2_fft_normal_check_memory(1, None, 10, 10)
+    assert L._halo2_fft_many_check_memory(1, 10, 10)
+    assert L._halo2_get_fft_split_radix(1, 20, 20, 1 << 40) == 0
+    assert L._halo2_get_fft_split_radix(1, 20, 20, 1) == -1
+    assert L._halo2_grand_product_max_len(1 << 20, 1 << 40) == 1 << 20
+    assert L._halo2_commit_product_max_len(1 << 20, 1 << 10) < (1 << 20)
+
+
+def test_argument_errors_match_reference(h2b, built_lib):
+    import numpy as np
+    z = np.zeros(4, np.uint64)
+    # iFFT_cosetFFT is rejected with -1 before any device work (ntt.cu:74,93-94)
+    e = built_lib._halo2_fft_normal(5, 4, z.ctypes.data, z.ctypes.data, z.ctypes.data, z.ctypes.data, None, 0, None)
+    assert e.code == -1
+    # log_n == 0 -> cudaErrorInvalidValue (1)
+    e = built_lib._halo2_fft_normal(1, 0, z.ctypes.data, z.ctypes.data, z.ctypes.data, z.ctypes.data, None, 0, None)
+    assert e.code == 1
+    # icosetFFT is refused by the many-FFT entries with code 2 (ntt.cu:837)
+    e = built_lib._halo2_fft_many(4, 1, 4, 4, None, None, None, None, None, 0, None)
+    assert e.code == 2
+    # bad field type / empty batch invert
+    assert built_lib._halo2_batch_invert(None, 7, 8, None).code == 1
+    assert built_lib._halo2_batch_invert(None, 0, 0, None).code == 1
+    # scratch too small is an error code, not a trap
+    e = built_lib._halo2_fft_normal_to_device(1, 10, None, None, None, z.ctypes.data, None, 0, None)
+    assert e.code == 1
+    with pytest.raises(h2b.Halo2GpuError):
+        h2b.check(built_lib._halo2_batch_invert(None, 9, 8, None), "batch_invert")

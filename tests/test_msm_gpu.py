@@ -1,0 +1,128 @@
+"""MSM parity against the oracle (bit-exact 96-byte Jacobian images), the
+reference's edge-case families (halo2_proofs/tests/multiexp_dense_bucket_edge_equivalence.rs:104-280,
+halo2_proofs/src/cuda/tests.rs:390-585) and the KZG property
+MSM(s, [tau^i]G) = [sum s_i tau^i] G at the full 2^22 size."""
+import numpy as np
+import pytest
+
+from conftest import assert_limbs_equal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def srs_small(h2b, orc):
+    tau = h2b.fields.fr_mont_limbs([0x1234567890ABCDEF1234567890ABCDEF])
+    return tau, orc.srs(tau, 1 << 12)
+
+
+def all_variants(h2b, sc, bases):
+    n = sc.shape[0]
+    out = [h2b.multiexp_gpu(sc, bases)]
+    d_b = h2b.to_dev(bases)
+    out.append(h2b.multiexp_gpu_device_bases(sc, d_b))
+    d_s = h2b.to_dev(sc)
+    out.append(h2b.multiexp_gpu_device_scalars_device_bases(d_s, d_b, n))
+    assert_limbs_equal(h2b.to_host(d_s), sc, "device scalars must not be mutated")
+    return out
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 20, 100, 1000, 4096])
+def test_msm_uniform_small(h2b, orc, cuda, srs_small, n):
+    _, srs = srs_small
+    bases = srs[:n]
+    sc = orc.chacha_fr(500 + n, n)
+    want = orc.msm(sc, bases)
+    for got in all_variants(h2b, sc, bases):
+        assert_limbs_equal(got, want, f"msm n={n}")
+
+
+def test_msm_edge_cases(h2b, orc, cuda, srs_small):
+    _, srs = srs_small
+    n = 2048
+    bases = srs[:n].copy()
+    sc = orc.chacha_fr(77, n)
+    # zero scalars and infinity bases
+    sc[::5] = 0
+    bases[::7] = 0
+    want = orc.msm(sc, bases)
+    for got in all_variants(h2b, sc, bases):
+        assert_limbs_equal(got, want, "zeros / infinity")
+    # all zero -> (0, 1, 0)
+    z = np.zeros((n, 4), np.uint64)
+    got = h2b.multiexp_gpu(z, srs[:n])
+    assert not got[0:4].any() and not got[8:12].any()
+    assert_limbs_equal(got, orc.msm(z, srs[:n]), "all zero")
+    # dense buckets: the first half share one constant scalar (reference's K)
+    K = h2b.fields.fr_mont_limbs([0x022B5F6A3C1D0E8F94D049BB133111EBBF58476D1CE4E5B99E3779B97F4A7C15])
+    sc2 = orc.chacha_fr(78, n)
+    sc2[: n // 2] = K
+    assert_limbs_equal(h2b.multiexp_gpu(sc2, srs[:n]), orc.msm(sc2, srs[:n]), "dense constant")
+    # every scalar 1 and every scalar -1 (one bucket per window, all points)
+    ones = h2b.fields.fr_mont_limbs([1] * n)
+    assert_limbs_equal(h2b.multiexp_gpu(ones, srs[:n]), orc.msm(ones, srs[:n]), "all ones")
+    negs = h2b.fields.fr_mont_limbs([h2b.fields.R_MOD - 1] * n)
+    assert_limbs_equal(h2b.multiexp_gpu(negs, srs[:n]), orc.msm(negs, srs[:n]), "all minus one")
+    # P + (-P) cancellation inside a bucket
+    b3 = srs[:n].copy()
+    b3[1::2] = b3[0::2]
+    sc3 = np.tile(h2b.fields.fr_mont_limbs([5, h2b.fields.R_MOD - 5]), (n // 2, 1))
+    got = h2b.multiexp_gpu(sc3, b3)
+    assert not got[8:12].any(), "sum must be infinity"
+
+
+def test_msm_all_bases_generator(h2b, orc, cuda):
+    n = 1 << 14
+    g = orc.g1_generator()
+    bases = np.tile(g, (n, 1))
+    sc = orc.chacha_fr(3, n)
+    total = h2b.fields.fr_mont_limbs([sum(h2b.fields.fr_from_mont_limbs(sc)) % h2b.fields.R_MOD])
+    want = orc.g1_mul(total, g)
+    assert_limbs_equal(h2b.multiexp_gpu(sc, bases), want, "(sum s) G")
+
+
+def test_msm_config1_k16_and_mix(h2b, orc, cuda):
+    n = 1 << 16
+    tau = h2b.fields.fr_mont_limbs([0xC0FFEE])
+    srs = h2b.to_host(h2b.srs_device(0xC0FFEE, n), (n, 8))
+    # device SRS generator agrees with the oracle at sampled indices
+    for i in (0, 1, 2, 777, n - 1):
+        p = orc.g1_mul(h2b.fields.fr_mont_limbs([pow(0xC0FFEE, i, h2b.fields.R_MOD)]), orc.g1_generator())
+        assert_limbs_equal(srs[i], p[:8], f"srs[{i}]")
+    del tau
+    for mix in (0, 1):
+        sc = h2b.to_host(h2b.random_fr_device(n, 42 + mix, mix))
+        want = orc.msm(sc, srs)
+        assert_limbs_equal(h2b.multiexp_gpu_device_bases(sc, h2b.to_dev(srs)), want, f"k=16 mix={mix}")
+
+
+def test_msm_n65540_ten_dense_buckets(h2b, orc, cuda):
+    """n = 65540 with ten distinct constants each on 10% of the rows
+    (the reference's ten-dense-buckets-per-window case)."""
+    n = 65540
+    srs = h2b.to_host(h2b.srs_device(99, n), (n, 8))
+    sc = orc.chacha_fr(11, n)
+    ks = orc.chacha_fr(12, 10)
+    for j in range(10):
+        sc[j * (n // 10):(j + 1) * (n // 10)] = ks[j]
+    assert_limbs_equal(h2b.multiexp_gpu(sc, srs), orc.msm(sc, srs), "ten dense")
+
+
+def test_msm_kzg_property_k22(h2b, orc, cuda):
+    """MSM over [tau^i]G with the 50/30/20 scalar mix at n = 2^22 equals
+    [f(tau)] G with f(tau) = sum s_i tau^i computed on the CPU."""
+    f = h2b.fields
+    n = 1 << 22
+    tau = 0x2A2B2C2D2E2F
+    d_srs = h2b.srs_device(tau, n)
+    d_sc = h2b.random_fr_device(n, 2022, 1)
+    got = h2b.multiexp_gpu_device_scalars_device_bases(d_sc, d_srs, n)
+    sc = h2b.to_host(d_sc)
+    ft = orc.fr_eval(sc, f.fr_mont_limbs([tau]))
+    want = orc.g1_mul(ft, orc.g1_generator())
+    assert_limbs_equal(got, want, "KZG property at 2^22")
+    # the device SRS agrees with the oracle at sampled indices
+    srs = h2b.to_host(d_srs[: 64 * 4], (4, 8))
+    for i in range(4):
+        p = orc.g1_mul(f.fr_mont_limbs([pow(tau, i, f.R_MOD)]), orc.g1_generator())
+        assert_limbs_equal(srs[i], p[:8], f"srs[{i}]")
