@@ -179,6 +179,44 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """One kernel family at 2^log_n, warmup + steps, nothing else (for ncu)."""
+    import torch
+    torch.cuda.set_device(0)
+    h2b = load_pkg()
+    L = h2b.lib()
+    f = h2b.fields
+    sh = h2b.stream_handle()
+    n = 1 << args.log_n
+    if args.case == "msm":
+        d_srs = h2b.srs_device(0x5EED, n)
+        d_sc = h2b.random_fr_device(n, 1000, 1)
+        d_out = h2b.dev_empty(96)
+        ws = h2b.msm_workspace(n)
+        fn = lambda: h2b.call("h2b_msm_device", h2b.ptr(d_sc), h2b.ptr(d_srs), h2b.ptr(d_out), n, h2b.ptr(ws),
+                              ws.numel(), sh)
+    elif args.case == "ntt":
+        dom = f.EvaluationDomain(5, args.log_n)
+        ek = dom.extended_k
+        d_in = h2b.random_fr_device(n, 2000, 0)
+        d_ext = h2b.dev_empty(32 << ek)
+        ws = h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(3, args.log_n, ek))
+        d_om = h2b.to_dev(f.fr_mont_limbs([dom.extended_omega]))
+        one = f.fr_mont_limbs([1])
+        one_ffi = h2b.host_ffi(one)
+        ins, outs = h2b.ffi_array([d_in.data_ptr()]), h2b.ffi_array([d_ext.data_ptr()])
+        fn = lambda: h2b.call("_halo2_fft_many_to_device", 3, 1, args.log_n, ek, ins, outs, h2b.ptr(d_om),
+                              ctypes.byref(one_ffi), True, h2b.ptr(ws), ws.numel(), sh)
+    else:
+        d = h2b.random_fr_device(n, 3000, 0)
+        ws = h2b.dev_empty(L.h2b_batch_invert_workspace_size(n))
+        fn = lambda: h2b.call("h2b_batch_invert", h2b.ptr(d), 0, n, h2b.ptr(ws), ws.numel(), sh)
+    for _ in range(args.warmup + args.steps):
+        fn()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "log_n": args.log_n, "runs": args.warmup + args.steps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -187,7 +225,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", choices=["msm", "ntt", "bi"], help="run one kernel family only (profiling runs)")
+    ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

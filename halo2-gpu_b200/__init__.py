@@ -449,3 +449,80 @@ def srs_device(tau, n, stream=None):
     out = dev_empty(64 * n)
     call("h2b_srs_from_powers", ptr(out), ptr(pw), n, ptr(table), stream_handle(stream))
     return out
+
+
+# --- quotient (halo2_proofs/src/plonk/evaluation.rs:916-1054) -----------------
+
+def _expr_constants(y):
+    f = fields
+    yv = y if isinstance(y, int) else f.fr_from_mont_limbs(np.asarray(y).reshape(1, 4))[0]
+    return f.fr_mont_limbs([0, 1, f.R_MOD - 1, 2, yv])
+
+
+def _ptr_table(tensors):
+    arr = (ctypes.c_void_p * max(len(tensors), 1))()
+    for i, t in enumerate(tensors):
+        arr[i] = t.data_ptr()
+    return arr
+
+
+def quotient_device(d_fixed, d_instance, d_advice, challenges, constants, y, rules, vp_rules, num_quotient,
+                    rot_scale, row_start, row_end, d_out, d_prev=None, stream=None):
+    """_halo2_quotient_device_columns_device_out: device columns in, device rows out."""
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 4) if len(challenges) else \
+        np.zeros((1, 4), np.uint64)
+    cs = np.ascontiguousarray(constants, dtype=np.uint64).reshape(-1, 4)
+    ec = _expr_constants(y)
+    r = np.ascontiguousarray(rules, dtype=np.uint64)
+    vp = np.ascontiguousarray(vp_rules, dtype=np.uint64)
+    nf, ni, na = len(d_fixed), len(d_instance), len(d_advice)
+    ws = dev_empty(lib()._halo2_quotient_workspace_size(r.ctypes.data, len(r) // 2, len(vp), num_quotient, nf, ni,
+                                                        na, len(challenges), cs.shape[0], rot_scale, row_start,
+                                                        row_end))
+    call("_halo2_quotient_device_columns_device_out", _ptr_table(d_fixed), nf, _ptr_table(d_instance), ni,
+         _ptr_table(d_advice), na, host_ffi(ch), len(challenges), host_ffi(cs), cs.shape[0], host_ffi(ec),
+         r.ctypes.data, len(r) // 2, vp.ctypes.data, len(vp), ptr(d_out), num_quotient,
+         ptr(d_prev) if d_prev is not None else None, rot_scale, row_start, row_end, ptr(ws), ws.numel(),
+         stream_handle(stream))
+    return d_out
+
+
+def quotient_host(fixed, instance, advice, challenges, constants, y, rules, vp_rules, num_quotient, rot_scale,
+                  row_start, row_end, stream=None):
+    """_halo2_quotient: host columns in, host rows out."""
+    fx = [np.ascontiguousarray(c, dtype=np.uint64) for c in fixed]
+    ins = [np.ascontiguousarray(c, dtype=np.uint64) for c in instance]
+    adv = [np.ascontiguousarray(c, dtype=np.uint64) for c in advice]
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 4) if len(challenges) else \
+        np.zeros((1, 4), np.uint64)
+    cs = np.ascontiguousarray(constants, dtype=np.uint64).reshape(-1, 4)
+    ec = _expr_constants(y)
+    r = np.ascontiguousarray(rules, dtype=np.uint64)
+    vp = np.ascontiguousarray(vp_rules, dtype=np.uint64)
+    out = np.zeros((row_end - row_start, 4), dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_quotient_workspace_size(r.ctypes.data, len(r) // 2, len(vp), num_quotient, len(fx),
+                                                        len(ins), len(adv), len(challenges), cs.shape[0], rot_scale,
+                                                        row_start, row_end))
+    call("_halo2_quotient", ffi_array([a.ctypes.data for a in fx]), len(fx), ffi_array([a.ctypes.data for a in ins]),
+         len(ins), ffi_array([a.ctypes.data for a in adv]), len(adv), host_ffi(ch), len(challenges), host_ffi(cs),
+         cs.shape[0], host_ffi(ec), r.ctypes.data, len(r) // 2, vp.ctypes.data, len(vp), host_ffi(out),
+         num_quotient, rot_scale, row_start, row_end, ptr(ws), ws.numel(), stream_handle(stream))
+    return out
+
+
+def quotient_lookups_device(d_values, d_table, d_z, d_pin, d_ptab, d_l0, d_llast, d_lactive, d_beta, d_gamma, d_y,
+                            n, stream=None):
+    call("_halo2_quotient_lookups", *[ptr(t) for t in (d_values, d_table, d_z, d_pin, d_ptab, d_l0, d_llast,
+                                                       d_lactive, d_beta, d_gamma, d_y)], n, stream_handle(stream))
+
+
+def quotient_permutation_device(d_values, d_l0, d_llast, d_lactive, d_prods, d_perms, d_cols, beta, gamma, y, delta,
+                                delta_start, ext_omega, omega, chunk_len, last_rotation, rot_scale, isize, n,
+                                stream=None):
+    tabs = [to_dev(np.array([t.data_ptr() for t in lst], dtype=np.uint64)) for lst in (d_prods, d_perms, d_cols)]
+    scal = [_scalar_bytes(x) for x in (beta, gamma, y, delta, delta_start, ext_omega, omega)]
+    call("_halo2_quotient_permutation", ptr(d_values), ptr(d_l0), ptr(d_llast), ptr(d_lactive), ptr(tabs[0]),
+         ptr(tabs[1]), ptr(tabs[2]), *[s.ctypes.data for s in scal], len(d_prods), chunk_len, len(d_cols),
+         last_rotation, rot_scale, isize, n, stream_handle(stream))
+    torch = _torch()
+    torch.cuda.current_stream().synchronize()

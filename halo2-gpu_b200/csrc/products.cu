@@ -209,6 +209,7 @@ __global__ void __launch_bounds__(GP_T) k_gp_up(Fr* __restrict__ d, uint64_t cou
     for (int j = 0; j < GP_E; j++) {
         uint64_t m = m0 + j;
         Fr x = (m < count) ? ld(&d[gp_pos(m, stride)]) : Fr::one();
+        if (m == 0 && prefix != nullptr) x = ld(prefix) * x;  // out[i] = prefix * prod_{j<=i} in[j]
         acc = (j == 0) ? x : acc * x;
         q[j] = acc;
     }
@@ -223,13 +224,10 @@ __global__ void __launch_bounds__(GP_T) k_gp_up(Fr* __restrict__ d, uint64_t cou
         __syncthreads();
     }
     Fr ex = (t > 0) ? tot[t - 1] : Fr::one();
-    bool first = (blockIdx.x == 0 && t == 0 && prefix != nullptr);
-    if (first) ex = ld(prefix);
-    bool apply = (t > 0) || first;
 #pragma unroll
     for (int j = 0; j < GP_E; j++) {
         uint64_t m = m0 + j;
-        if (m < count) st(&d[gp_pos(m, stride)], apply ? ex * q[j] : q[j]);
+        if (m < count) st(&d[gp_pos(m, stride)], t > 0 ? ex * q[j] : q[j]);
     }
 }
 

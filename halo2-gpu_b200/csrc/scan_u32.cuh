@@ -41,7 +41,7 @@ __device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t* to
     return res;
 }
 
-__global__ void k_scan_tile_sums(const uint32_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ tile_sums)
+static __global__ void k_scan_tile_sums(const uint32_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ tile_sums)
 {
     uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
     uint32_t s = 0;
@@ -55,7 +55,7 @@ __global__ void k_scan_tile_sums(const uint32_t* __restrict__ in, uint64_t n, ui
 }
 
 // One CTA of 256 threads: exclusive scan of tile_sums in place (any length).
-__global__ void k_scan_tile_sums_single(uint32_t* __restrict__ tile_sums, uint64_t ntiles)
+static __global__ void k_scan_tile_sums_single(uint32_t* __restrict__ tile_sums, uint64_t ntiles)
 {
     __shared__ uint32_t carry_s;
     __shared__ uint32_t tot;
@@ -73,7 +73,7 @@ __global__ void k_scan_tile_sums_single(uint32_t* __restrict__ tile_sums, uint64
     }
 }
 
-__global__ void k_scan_apply(const uint32_t* __restrict__ in, uint64_t n, const uint32_t* __restrict__ tile_offsets,
+static __global__ void k_scan_apply(const uint32_t* __restrict__ in, uint64_t n, const uint32_t* __restrict__ tile_offsets,
                              uint32_t* __restrict__ out, uint64_t ntiles)
 {
     uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * (SCAN_TILE / 256);
@@ -99,7 +99,7 @@ __global__ void k_scan_apply(const uint32_t* __restrict__ in, uint64_t n, const 
 inline uint64_t scan_u32_tiles(uint64_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE; }
 
 // out[0..n] = exclusive scan of in[0..n); tile_tmp needs scan_u32_tiles(n) words.
-inline cudaError_t scan_u32(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* tile_tmp, cudaStream_t st)
+static inline cudaError_t scan_u32(const uint32_t* in, uint64_t n, uint32_t* out, uint32_t* tile_tmp, cudaStream_t st)
 {
     uint64_t nt = scan_u32_tiles(n);
     if (nt == 0) {

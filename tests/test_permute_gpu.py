@@ -1,0 +1,68 @@
+"""Lookup permute-sort parity with permute_expression_pair_seq
+(halo2_proofs/src/plonk/lookup/prover.rs:787-880; GPU-vs-seq test at
+halo2_proofs/src/cuda/tests.rs:2340)."""
+import numpy as np
+import pytest
+
+from conftest import assert_limbs_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def make_lookup(orc, n, usable, table_size, seed, skew=False):
+    rng = np.random.default_rng(seed)
+    tvals = orc.chacha_fr(seed, table_size)
+    table = tvals[np.arange(usable) % table_size]
+    if skew:
+        idx = np.minimum(rng.geometric(0.3, usable) - 1, table_size - 1)
+    else:
+        idx = rng.integers(0, table_size, usable)
+    inp = tvals[idx]
+    pad = np.zeros((n - usable, 4), np.uint64)
+    return np.concatenate([inp, pad]), np.concatenate([table, pad])
+
+
+def run(h2b, orc, inp, table, n, usable):
+    want_a, want_s = orc.permute_pair(inp, table, n, usable)
+    d_in, d_tab = h2b.to_dev(inp), h2b.to_dev(table)
+    d_pa, d_ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+    h2b.permute_expression_pair_device(d_in, d_tab, d_pa, d_ps, n, usable)
+    assert_limbs_equal(h2b.to_host(d_pa), want_a, "A'")
+    assert_limbs_equal(h2b.to_host(d_ps), want_s, "S'")
+
+
+@pytest.mark.parametrize("k,table_size", [(4, 3), (8, 16), (12, 256), (16, 256), (16, 60000)])
+def test_permute_uniform(h2b, orc, cuda, k, table_size):
+    n = 1 << k
+    usable = n - 7
+    table_size = min(table_size, usable)
+    inp, table = make_lookup(orc, n, usable, table_size, 100 + k)
+    run(h2b, orc, inp, table, n, usable)
+
+
+def test_permute_skewed_and_constant(h2b, orc, cuda):
+    n = 1 << 14
+    usable = n - 5
+    inp, table = make_lookup(orc, n, usable, 256, 7, skew=True)
+    run(h2b, orc, inp, table, n, usable)
+    # every input row the same value
+    inp2 = inp.copy()
+    inp2[:usable] = table[3]
+    run(h2b, orc, inp2, table, n, usable)
+
+
+def test_permute_config3_size(h2b, orc, cuda):
+    n = 1 << 20
+    usable = n - 7
+    inp, table = make_lookup(orc, n, usable, 256, 20)
+    run(h2b, orc, inp, table, n, usable)
+
+
+def test_permute_missing_value_is_an_error(h2b, orc, cuda):
+    n = 1 << 10
+    usable = n - 3
+    inp, table = make_lookup(orc, n, usable, 64, 9)
+    inp[5] = orc.chacha_fr(12345, 1)[0]
+    d_pa, d_ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+    with pytest.raises(h2b.Halo2GpuError):
+        h2b.permute_expression_pair_device(h2b.to_dev(inp), h2b.to_dev(table), d_pa, d_ps, n, usable)
