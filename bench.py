@@ -359,7 +359,7 @@ def main():
             "modmul_probe_per_s": probe["h2b_probe_modmul"]}
     imad["frac"] = imad["achieved_imad_ops_per_s"] / imad_peak
     ntt_kernel_ms = nttp_ms / max(nttp_cnt, 1)
-    ntt_modmul = (n_ext // 2) * K_EXT
+    ntt_modmul = (n_ext // 2) * K_NTT   # the first K_EXT - K_NTT stages are broadcasts
     bi_kernel_ms = bik_ms / max(bik_cnt, 1)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -120,6 +120,7 @@ _SIGS = {
     "h2b_prof_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
     "h2b_probe_imad": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "h2b_probe_modmul": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "h2b_probe_imad_form": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "h2b_launch_count": (_u64, []),
     "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_msm_window_bits": (ctypes.c_int, [_u64]),

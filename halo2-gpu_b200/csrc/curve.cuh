@@ -12,6 +12,7 @@
 // halo2_proofs/cuda/include/curve/jacobian_t.hpp:64-83).
 #pragma once
 #include "field.cuh"
+#include "inverse.cuh"
 
 namespace h2b {
 
@@ -176,7 +177,7 @@ H2B_DEV G1Jac xyzz_to_jac_affine(const G1Xyzz& p)
         r.X = Fq::zero(); r.Y = Fq::one(); r.Z = Fq::zero();
         return r;
     }
-    Fq inv = finv(p.ZZ * p.ZZZ);      // 1 / (ZZ * ZZZ)
+    Fq inv = finv_fast(p.ZZ * p.ZZZ); // 1 / (ZZ * ZZZ)
     Fq izz = inv * p.ZZZ;             // 1 / ZZ
     Fq izzz = inv * p.ZZ;             // 1 / ZZZ
     r.X = p.X * izz;

@@ -163,7 +163,7 @@ H2B_DEV void cond_sub(uint32_t (&r)[8], const uint32_t (&t)[8])
 }
 
 template <class C>
-H2B_DEV Fp<C> operator*(const Fp<C>& a, const Fp<C>& b)
+H2B_DEV Fp<C> mont_mul_inline(const Fp<C>& a, const Fp<C>& b)
 {
     uint32_t t[9];
 #pragma unroll
@@ -176,6 +176,30 @@ H2B_DEV Fp<C> operator*(const Fp<C>& a, const Fp<C>& b)
     for (int i = 0; i < 8; i++) lo[i] = t[i];
     cond_sub<C>(r.v, lo);
     return r;
+}
+
+// One out-of-line body per field: kernels that chain many products (curve
+// formulas, the quotient interpreter) otherwise inline ~300 instructions per
+// product and starve on instruction fetch.  H2B_INLINE_MUL=1 restores full
+// inlining for kernels that want it.
+#ifndef H2B_INLINE_MUL
+#define H2B_INLINE_MUL 0
+#endif
+
+template <class C>
+__device__ __noinline__ Fp<C> mont_mul_outline(const Fp<C> a, const Fp<C> b)
+{
+    return mont_mul_inline<C>(a, b);
+}
+
+template <class C>
+H2B_DEV Fp<C> operator*(const Fp<C>& a, const Fp<C>& b)
+{
+#if H2B_INLINE_MUL
+    return mont_mul_inline<C>(a, b);
+#else
+    return mont_mul_outline<C>(a, b);
+#endif
 }
 
 template <class C>

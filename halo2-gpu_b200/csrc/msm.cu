@@ -5,10 +5,15 @@
 // halo2_proofs/src/cuda/culib.rs:30-70).
 //
 // Pipeline (all stream-ordered, no host round trip until the 96-byte result):
-//  1. canon:   scalars leave Montgomery form (one modmul each) into scratch;
-//              the caller's scalars are never mutated.
+//  1. split:   each scalar leaves Montgomery form and is split by the GLV
+//              endomorphism into two signed halves below 2^127 (glv.cuh), so
+//              n points become 2n virtual points P_i, phi(P_i) with 128-bit
+//              scalars: half the windows, half the buckets and half the
+//              final doubling chain of a 254-bit Pippenger.  The caller's
+//              scalars are never mutated.
 //  2. digits:  signed c-bit windows, digits in [-(2^(c-1)-1), 2^(c-1)], so a
-//              window needs 2^(c-1) buckets; a negative digit adds -P.
+//              window needs 2^(c-1) buckets; a negative digit (or a negative
+//              half) adds -P.
 //  3. sort:    counting sort of (window, bucket) keys -- warp-aggregated
 //              histogram, exclusive scan to bucket offsets, warp-aggregated
 //              scatter of point indices (sign in bit 31).
@@ -28,13 +33,17 @@
 #include "curve.cuh"
 #include "msm.cuh"
 #include "prof.cuh"
+#include "glv.cuh"
 #include "scan_u32.cuh"
 
 namespace h2b {
 
-static constexpr int SCALAR_BITS = 254;
+static constexpr int GLV_BITS = 127;
+// 32-bit sorted-entry offsets: 2 halves x 8 windows x n < 2^32
+static constexpr uint64_t MSM_MAX_LENGTH = 1ull << 27;
 static constexpr uint32_t SIGN_BIT = 0x80000000u;
 static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed serially in fixup
+static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
 
 static int g_msm_window_override = 0;
 static int g_msm_chunk_override = 0;
@@ -60,17 +69,24 @@ MsmPlan msm_plan(uint64_t n)
     else if (lg >= 10) c = 10;
     else c = 7;
     p.c = c;
-    p.W = (SCALAR_BITS + c - 1) / c + ((SCALAR_BITS % c) == 0 ? 1 : 0);
+    // GLV halves: magnitudes < 2^GLV_BITS; the top window must leave room
+    // for the signed-digit carry (its width <= c - 1).
+    p.W = (GLV_BITS + c - 1) / c;
+    if (GLV_BITS - c * (p.W - 1) > c - 1) p.W++;
     p.H = 1u << (c - 1);
     p.NB = (uint64_t)p.W * p.H;
-    p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 64u;
-    p.max_entries = n * (uint64_t)p.W;
+    p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 128u;
+    p.nv = 2 * n;
+    p.max_entries = p.nv * (uint64_t)p.W;
     p.max_chunks = (p.max_entries + p.K - 1) / p.K + 1;
-    // segments per window for the running-sum reduction
-    uint32_t L = p.H >= 4096 ? 16u : (p.H >= 256 ? 8u : 4u);
-    if (L > p.H) L = p.H;
+    // segments per window for the running-sum reduction (L buckets each)
+    uint32_t L = p.H >= 256 ? 8u : (p.H >= 4 ? 4u : 1u);
     p.L = L;
+    p.LOGL = 31 - __builtin_clz(L);
     p.S = p.H / L;
+    p.NBITS = p.S > 1 ? 31 - __builtin_clz(p.S) : 0;
+    // a bucket spanning more than DENSE_LIMIT chunks holds > DENSE_LIMIT*K entries
+    p.max_dense = p.max_entries / ((uint64_t)DENSE_LIMIT * p.K) + 1;
     return p;
 }
 
@@ -86,8 +102,11 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
     sp.add_n<uint32_t>(p.max_entries);                // sorted entries
     sp.add_n<G1Xyzz>(p.NB);                           // bucket sums
     sp.add_n<G1Xyzz>(p.max_chunks);                   // chunk head partials
-    sp.add_n<uint32_t>(p.NB + 1);                     // dense list + count
-    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment sums
+    sp.add_n<uint32_t>(p.max_dense + 1);              // dense list + count
+    sp.add_n<G1Xyzz>(p.max_dense * DENSE_PIECES);     // dense pieces
+    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment weighted sums
+    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment plain sums
+    sp.add_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));  // per-bit sums
     sp.add_n<G1Xyzz>(p.W);                            // window sums
     sp.add_n<G1Jac>(1);                               // result
 }
@@ -105,8 +124,11 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
     s.sorted = ar.take_n<uint32_t>(p.max_entries);
     s.buckets = ar.take_n<G1Xyzz>(p.NB);
     s.heads = ar.take_n<G1Xyzz>(p.max_chunks);
-    s.dense = ar.take_n<uint32_t>(p.NB + 1);
-    s.segs = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
+    s.dense = ar.take_n<uint32_t>(p.max_dense + 1);
+    s.pieces = ar.take_n<G1Xyzz>(p.max_dense * DENSE_PIECES);
+    s.segacc = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
+    s.segrun = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
+    s.bits = ar.take_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));
     s.wins = ar.take_n<G1Xyzz>(p.W);
     s.result = ar.take_n<G1Jac>(1);
     return s;
@@ -116,24 +138,31 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
 // kernels
 // ---------------------------------------------------------------------------
 
-__global__ void k_msm_canon(const Fr* __restrict__ sc, Fr* __restrict__ canon, uint64_t n)
+// Virtual scalars: vs[2i] = k1, vs[2i+1] = k2 of the GLV split of scalar i
+// (128-bit magnitudes, sign in bit 127), so entry v stands for point i = v/2,
+// taken as P_i (v even) or phi(P_i) (v odd).
+__global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t n)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        st(&canon[i], from_mont(ldg(&sc[i])));
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint4 a, b;
+        glv::decompose(from_mont(ldg(&sc[i])), a, b);
+        vs[2 * i] = a;
+        vs[2 * i + 1] = b;
+    }
 }
 
-__device__ __forceinline__ uint32_t window_bits(const Fr& s, int bit, int c)
+__device__ __forceinline__ uint32_t window_bits(const uint4& s, int bit, int c)
 {
+    const uint32_t w[5] = {s.x, s.y, s.z, s.w & 0x7fffffffu, 0u};
     int li = bit >> 5, sh = bit & 31;
-    uint64_t lo = s.v[li];
-    uint64_t hi = (li + 1 < 8) ? s.v[li + 1] : 0u;
-    uint64_t v = (lo | (hi << 32)) >> sh;
+    uint64_t v = ((uint64_t)w[li] | ((uint64_t)w[li + 1] << 32)) >> sh;
     return (uint32_t)(v & ((1ull << c) - 1));
 }
 
-// For each digit: key = w*H + |d| - 1 (or ~0 for zero digits), neg = d < 0.
+// For each digit: key = w*H + |d| - 1 (or ~0 for zero digits); the entry's
+// sign is the digit's sign flipped by the virtual scalar's sign.
 template <bool SCATTER>
-__global__ void k_msm_sort(const Fr* __restrict__ canon, uint64_t n, int c, int W, uint32_t H,
+__global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int W, uint32_t H,
                            uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted)
 {
     const unsigned lane = threadIdx.x & 31;
@@ -141,7 +170,8 @@ __global__ void k_msm_sort(const Fr* __restrict__ canon, uint64_t n, int c, int 
     for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t i = base + threadIdx.x;
         bool valid = i < n;
-        Fr s = valid ? ldg(&canon[i]) : Fr::zero();
+        uint4 s = valid ? vsc[i] : make_uint4(0u, 0u, 0u, 0u);
+        const bool sneg = (s.w >> 31) != 0;
         uint32_t carry = 0;
         for (int w = 0; w < W; w++) {
             uint32_t v = window_bits(s, w * c, c) + carry;
@@ -160,7 +190,7 @@ __global__ void k_msm_sort(const Fr* __restrict__ canon, uint64_t n, int c, int 
                 b = __shfl_sync(0xffffffffu, b, leader);
                 if (key != 0xffffffffu) {
                     uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-                    sorted[b + rank] = (uint32_t)i | (d < 0 ? SIGN_BIT : 0u);
+                    sorted[b + rank] = (uint32_t)i | (((d < 0) != sneg) ? SIGN_BIT : 0u);
                 }
             }
         }
@@ -169,7 +199,9 @@ __global__ void k_msm_sort(const Fr* __restrict__ canon, uint64_t n, int c, int 
 
 __device__ __forceinline__ G1Affine load_signed_point(const G1Affine* __restrict__ bases, uint32_t e)
 {
-    G1Affine P = ld_affine(&bases[e & ~SIGN_BIT]);
+    const uint32_t v = e & ~SIGN_BIT;
+    G1Affine P = ld_affine(&bases[v >> 1]);
+    if (v & 1u) P.x = P.x * glv::beta();  // phi(P); (0, 0) stays infinity
     if (e & SIGN_BIT) P = affine_neg(P);
     return P;
 }
@@ -209,7 +241,7 @@ __global__ void __launch_bounds__(128) k_msm_accumulate(const uint32_t* __restri
 }
 
 __global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K, G1Xyzz* __restrict__ buckets,
-                            const G1Xyzz* __restrict__ heads, uint32_t* __restrict__ dense)
+                            const G1Xyzz* __restrict__ heads, uint32_t* __restrict__ dense, uint64_t max_dense)
 {
     for (uint64_t gb = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gb < NB; gb += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t s = offsets[gb], e = offsets[gb + 1];
@@ -217,8 +249,8 @@ __global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, u
         uint32_t t0 = s / K, t1 = (e - 1) / K;
         if (t1 == t0) continue;
         if (t1 - t0 > DENSE_LIMIT) {
-            uint32_t idx = atomicAdd(&dense[NB], 1u);
-            dense[idx] = (uint32_t)gb;
+            uint32_t idx = atomicAdd(&dense[max_dense], 1u);
+            if (idx < max_dense) dense[idx] = (uint32_t)gb;
             continue;
         }
         G1Xyzz acc = ld_xyzz(&buckets[gb]);
@@ -249,27 +281,63 @@ __device__ G1Xyzz block_sum_xyzz(uint64_t n, Get get)
     return r;
 }
 
-__global__ void __launch_bounds__(256) k_msm_dense(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
-                                                   G1Xyzz* __restrict__ buckets, const G1Xyzz* __restrict__ heads,
-                                                   const uint32_t* __restrict__ dense)
+// Dense buckets (spanning more than DENSE_LIMIT chunks): DENSE_PIECES CTAs
+// each tree-sum a slice of the bucket's chunk partials, then one warp per
+// bucket tree-sums the pieces into the bucket.
+__global__ void __launch_bounds__(256) k_msm_dense_pieces(const uint32_t* __restrict__ offsets, uint64_t NB,
+                                                          uint32_t K, const G1Xyzz* __restrict__ heads,
+                                                          const uint32_t* __restrict__ dense,
+                                                          G1Xyzz* __restrict__ pieces)
 {
-    const uint32_t cnt = dense[NB];
-    for (uint32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+    const uint32_t items = dense[NB] * DENSE_PIECES;
+    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
+        uint32_t i = it / DENSE_PIECES, p = it % DENSE_PIECES;
         uint32_t gb = dense[i];
         uint32_t t0 = offsets[gb] / K, t1 = (offsets[gb + 1] - 1) / K;
-        G1Xyzz r = block_sum_xyzz(t1 - t0, [&](uint64_t j) { return ld_xyzz(&heads[t0 + 1 + j]); });
+        uint64_t len = t1 - t0;  // heads t0+1 .. t1
+        uint64_t b0 = len * p / DENSE_PIECES, b1 = len * (p + 1) / DENSE_PIECES;
+        G1Xyzz r = block_sum_xyzz(b1 - b0, [&](uint64_t j) { return ld_xyzz(&heads[t0 + 1 + b0 + j]); });
+        if (threadIdx.x == 0) st_xyzz(&pieces[it], r);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(DENSE_PIECES) k_msm_dense_merge(const uint64_t NB, G1Xyzz* __restrict__ buckets,
+                                                                  const uint32_t* __restrict__ dense,
+                                                                  const G1Xyzz* __restrict__ pieces)
+{
+    __shared__ G1Xyzz red[DENSE_PIECES];
+    const uint32_t cnt = dense[NB];
+    for (uint32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+        red[threadIdx.x] = ld_xyzz(&pieces[(uint64_t)i * DENSE_PIECES + threadIdx.x]);
+        __syncthreads();
+        for (int h = DENSE_PIECES / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h) {
+                G1Xyzz a = red[threadIdx.x];
+                xyzz_add(a, red[threadIdx.x + h]);
+                red[threadIdx.x] = a;
+            }
+            __syncthreads();
+        }
         if (threadIdx.x == 0) {
+            uint32_t gb = dense[i];
             G1Xyzz acc = ld_xyzz(&buckets[gb]);
-            xyzz_add(acc, r);
+            xyzz_add(acc, red[0]);
             st_xyzz(&buckets[gb], acc);
         }
         __syncthreads();
     }
 }
 
-// Thread (w, s): sum_{j in segment s} (j + 1) * B_{w, j}, buckets j = s*L .. s*L+L-1.
-__global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__ buckets, int W, uint32_t H, uint32_t L,
-                                                      uint32_t S, G1Xyzz* __restrict__ segs)
+// Bucket reduction, W_w = sum_{j<H} (j+1) B_{w,j}, in three parallel steps.
+// 1. Thread (w, s), segment s = buckets s*L .. s*L+L-1:
+//      acc_s = sum_j (j - sL + 1) B_j      run_s = sum_j B_j
+// 2. CTA (w, k): k < NBITS: T_k = sum over s with bit k set of run_s;
+//                k = NBITS: T = sum_s acc_s.
+// 3. Thread w: W_w = T + L * sum_k 2^k T_k (Horner over the bits).
+__global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__ buckets, int W, uint32_t H,
+                                                      uint32_t L, uint32_t S, G1Xyzz* __restrict__ segacc,
+                                                      G1Xyzz* __restrict__ segrun)
 {
     uint64_t total = (uint64_t)W * S;
     for (uint64_t id = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; id < total;
@@ -281,18 +349,43 @@ __global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__
             xyzz_add(run, ld_xyzz(&B[j]));
             xyzz_add(acc, run);
         }
-        // acc = sum (j - sL + 1) B_j ; add (s*L) * run
-        G1Xyzz off = xyzz_mul_u32(run, (uint32_t)(s * L));
-        xyzz_add(acc, off);
-        st_xyzz(&segs[id], acc);
+        st_xyzz(&segacc[id], acc);
+        st_xyzz(&segrun[id], run);
     }
 }
 
-__global__ void __launch_bounds__(256) k_msm_windows(const G1Xyzz* __restrict__ segs, uint32_t S, G1Xyzz* __restrict__ wins)
+__global__ void __launch_bounds__(256) k_msm_bitsums(const G1Xyzz* __restrict__ segacc,
+                                                     const G1Xyzz* __restrict__ segrun, uint32_t S, int nbits,
+                                                     G1Xyzz* __restrict__ bits)
 {
-    uint32_t w = blockIdx.x;
-    G1Xyzz r = block_sum_xyzz(S, [&](uint64_t j) { return ld_xyzz(&segs[(uint64_t)w * S + j]); });
-    if (threadIdx.x == 0) st_xyzz(&wins[w], r);
+    const uint32_t w = blockIdx.x / (nbits + 1);
+    const int k = (int)(blockIdx.x % (nbits + 1));
+    // k == nbits: all S weighted sums; else the S/2 plain sums with bit k set,
+    // s = (hi << (k+1)) | (1 << k) | lo
+    const bool all = (k == nbits);
+    const uint64_t lo_mask = all ? 0 : (1ull << k) - 1;
+    G1Xyzz r = block_sum_xyzz(all ? S : S / 2, [&](uint64_t j) {
+        if (all) return ld_xyzz(&segacc[(uint64_t)w * S + j]);
+        uint64_t s = ((j & ~lo_mask) << 1) | (1ull << k) | (j & lo_mask);
+        return ld_xyzz(&segrun[(uint64_t)w * S + s]);
+    });
+    if (threadIdx.x == 0) st_xyzz(&bits[blockIdx.x], r);
+}
+
+__global__ void k_msm_wincombine(const G1Xyzz* __restrict__ bits, int W, int nbits, int log_l,
+                                 G1Xyzz* __restrict__ wins)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= W) return;
+    const G1Xyzz* T = bits + (uint64_t)w * (nbits + 1);
+    G1Xyzz r = xyzz_inf();
+    for (int k = nbits - 1; k >= 0; k--) {
+        r = xyzz_dbl(r);
+        xyzz_add(r, ld_xyzz(&T[k]));
+    }
+    for (int d = 0; d < log_l; d++) r = xyzz_dbl(r);
+    xyzz_add(r, ld_xyzz(&T[nbits]));
+    st_xyzz(&wins[w], r);
 }
 
 // 2^(c*w) * W_w in parallel over w, then the sum and the affine conversion.
@@ -335,15 +428,16 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     }
     const unsigned sm_cap = 148u * 16u;
     prof_begin(PROF_MSM_TOTAL, st);
-    k_msm_canon<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, s.canon, p.n);
-    H2B_LAUNCHED("k_msm_canon");
+    uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
+    k_msm_glv<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, p.n);
+    H2B_LAUNCHED("k_msm_glv");
     H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
-    H2B_CUDA(cudaMemsetAsync(s.dense + p.NB, 0, sizeof(uint32_t), st));
-    k_msm_sort<false><<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(s.canon, p.n, p.c, p.W, p.H, s.counts, nullptr);
+    H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
+    k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr);
     H2B_LAUNCHED("k_msm_sort<hist>");
     H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
     H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    k_msm_sort<true><<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(s.canon, p.n, p.c, p.W, p.H, s.cursor, s.sorted);
+    k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.cursor, s.sorted);
     H2B_LAUNCHED("k_msm_sort<scatter>");
     uint64_t chunks = (p.max_entries + p.K - 1) / p.K;
     prof_begin(PROF_MSM_ACCUMULATE, st);
@@ -351,15 +445,20 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
                                                                        s.buckets, s.heads);
     prof_end(PROF_MSM_ACCUMULATE, st);
     H2B_LAUNCHED("k_msm_accumulate");
-    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense);
+    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense,
+                                                            p.max_dense);
     H2B_LAUNCHED("k_msm_fixup");
-    k_msm_dense<<<148, 256, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense);
-    H2B_LAUNCHED("k_msm_dense");
+    k_msm_dense_pieces<<<148 * 4, 256, 0, st>>>(s.offsets, p.max_dense, p.K, s.heads, s.dense, s.pieces);
+    H2B_LAUNCHED("k_msm_dense_pieces");
+    k_msm_dense_merge<<<148, DENSE_PIECES, 0, st>>>(p.max_dense, s.buckets, s.dense, s.pieces);
+    H2B_LAUNCHED("k_msm_dense_merge");
     uint64_t nseg = (uint64_t)p.W * p.S;
-    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.W, p.H, p.L, p.S, s.segs);
+    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.W, p.H, p.L, p.S, s.segacc, s.segrun);
     H2B_LAUNCHED("k_msm_segments");
-    k_msm_windows<<<p.W, 256, 0, st>>>(s.segs, p.S, s.wins);
-    H2B_LAUNCHED("k_msm_windows");
+    k_msm_bitsums<<<p.W * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
+    H2B_LAUNCHED("k_msm_bitsums");
+    k_msm_wincombine<<<1, 64, 0, st>>>(s.bits, p.W, p.NBITS, p.LOGL, s.wins);
+    H2B_LAUNCHED("k_msm_wincombine");
     k_msm_final<<<1, 64, 0, st>>>(s.wins, p.W, p.c, s.result);
     prof_end(PROF_MSM_TOTAL, st);
     H2B_LAUNCHED("k_msm_final");
@@ -384,7 +483,7 @@ static uint64_t msm_ws(uint64_t length, bool scalar_host, bool bases_host)
 
 extern "C" uint64_t _halo2_msm_max_length(uint64_t free_bytes)
 {
-    for (int lg = 28; lg > 0; lg--) {
+    for (int lg = 27; lg > 0; lg--) {
         if (msm_ws(1ull << lg, true, true) < free_bytes) return 1ull << lg;
     }
     return 0;
@@ -400,7 +499,7 @@ extern "C" uint64_t _halo2_multiexp_device_scalars_device_bases_workspace_size(u
 static RustError msm_entry(const void* scalars, bool scalar_host, const void* bases, bool bases_host, void* h_out,
                            uint64_t length, void* scratch, uint64_t scratch_bytes, cudaStream_t st, const char* who)
 {
-    if (length > 0xffffffffull / 32) return err(cudaErrorInvalidValue, "MSM length too large for 32-bit entry ids");
+    if (length > MSM_MAX_LENGTH) return err(cudaErrorInvalidValue, "MSM length above 2^27 points");
     MsmPlan p = msm_plan(length);
     uint64_t need = msm_ws(length, scalar_host, bases_host);
     if (scratch_bytes < need) return scratch_too_small(who, scratch_bytes, need);
@@ -453,7 +552,7 @@ extern "C" RustError _halo2_multiexp_device_scalars_device_bases(const void* d_s
 extern "C" RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out, uint64_t length,
                                     void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
 {
-    if (length > 0xffffffffull / 32) return err(cudaErrorInvalidValue, "MSM length too large for 32-bit entry ids");
+    if (length > MSM_MAX_LENGTH) return err(cudaErrorInvalidValue, "MSM length above 2^27 points");
     MsmPlan p = msm_plan(length);
     uint64_t need = msm_ws(length, false, false);
     if (scratch_bytes < need) return scratch_too_small("h2b_msm_device", scratch_bytes, need);
@@ -476,13 +575,16 @@ __global__ void k_msm_count(const Fr* __restrict__ sc, uint64_t n, int c, int W,
     unsigned long long local = 0;
     const uint32_t full = 1u << c;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        Fr s = from_mont(ldg(&sc[i]));
-        uint32_t carry = 0;
-        for (int w = 0; w < W; w++) {
-            uint32_t v = window_bits(s, w * c, c) + carry;
-            int32_t d = (v > H) ? (int32_t)v - (int32_t)full : (int32_t)v;
-            carry = (v > H) ? 1u : 0u;
-            if (d != 0) local++;
+        uint4 half[2];
+        glv::decompose(from_mont(ldg(&sc[i])), half[0], half[1]);
+        for (int h = 0; h < 2; h++) {
+            uint32_t carry = 0;
+            for (int w = 0; w < W; w++) {
+                uint32_t v = window_bits(half[h], w * c, c) + carry;
+                int32_t d = (v > H) ? (int32_t)v - (int32_t)full : (int32_t)v;
+                carry = (v > H) ? 1u : 0u;
+                if (d != 0) local++;
+            }
         }
     }
     atomicAdd(cnt, local);

@@ -14,10 +14,14 @@ struct MsmPlan {
     uint32_t H;      // buckets per window = 2^(c-1)
     uint64_t NB;     // W * H
     uint32_t K;      // sorted entries per accumulation chunk
+    uint64_t nv;     // virtual (GLV half) scalars = 2n
     uint64_t max_entries;
     uint64_t max_chunks;
     uint32_t L;      // buckets per reduction segment
+    int LOGL;        // log2(L)
     uint32_t S;      // segments per window
+    int NBITS;       // log2(S)
+    uint64_t max_dense;  // capacity of the dense-bucket list
 };
 
 struct MsmScratch {
@@ -32,7 +36,10 @@ struct MsmScratch {
     G1Xyzz* buckets;
     G1Xyzz* heads;
     uint32_t* dense;
-    G1Xyzz* segs;
+    G1Xyzz* pieces;
+    G1Xyzz* segacc;
+    G1Xyzz* segrun;
+    G1Xyzz* bits;
     G1Xyzz* wins;
     G1Jac* result;
 };

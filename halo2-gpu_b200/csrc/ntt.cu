@@ -107,11 +107,28 @@ __global__ void k_twist_bitrev_scatter(const Fr* __restrict__ in, Fr* __restrict
             if (mode == 1) {
                 v = v * p;
                 p = p * c;
-            } else if (mode == 2) {
+            } else if (mode == 2 && i < n_in) {
                 v = v * z3.f[i % 3];
             }
             st(&out[bitrev(i, log_out)], v);
         }
+    }
+}
+
+// Coset extension from 2^k inputs to 2^(k+e) outputs (zero padding).  After
+// the bit reversal over k+e bits, input i lands at rev_k(i) << e and every
+// other slot of that aligned group of 2^e is zero, so the first e DIT stages
+// only copy the value across the group.  This writes the twisted input
+// a_i * zeta^(i mod 3) to all 2^e slots; the DIT passes then start at stage e.
+__global__ void k_coset_spread(const Fr* __restrict__ in, Fr* __restrict__ out, int log_in, int e, Zeta3 z3)
+{
+    uint64_t n_in = 1ull << log_in;
+    const uint64_t g = 1ull << e;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_in;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        Fr v = ldg(&in[i]) * z3.f[i % 3];
+        Fr* dst = out + (bitrev(i, log_in) << e);
+        for (uint64_t j = 0; j < g; j++) st(&dst[j], v);
     }
 }
 
@@ -273,12 +290,14 @@ void ntt_set_pass_stages(int b)
     if (b >= 1 && b <= 10) g_max_pass_stages = b;
 }
 
-static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_t st)
+// Runs radix-2 stages [first, logn) in passes of at most g_max_pass_stages.
+static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_t st, int first = 0)
 {
-    if (logn == 0) return ok();
-    int passes = (logn + g_max_pass_stages - 1) / g_max_pass_stages;
-    int base = logn / passes, extra = logn % passes;
-    int s0 = 0;
+    if (logn - first <= 0) return ok();
+    int todo = logn - first;
+    int passes = (todo + g_max_pass_stages - 1) / g_max_pass_stages;
+    int base = todo / passes, extra = todo % passes;
+    int s0 = first;
     prof_begin(PROF_NTT_PASSES, st);
     for (int p = 0; p < passes; p++) {
         int nst = base + (p < extra ? 1 : 0);
@@ -399,6 +418,12 @@ static RustError transform_one(int type, int log_n, int log_ext, const void* in,
         } else if (type == 3) {
             z3 = zeta_factors(fr_const(FR_ONE), false);
             mode = 2;
+        }
+        if (!alias && type == 3 && logt > log_n) {
+            int e = logt - log_n;
+            k_coset_spread<<<grid_for(nin, 256), 256, 0, st>>>(din, d_out, log_n, e, z3);
+            H2B_LAUNCHED("k_coset_spread");
+            return run_passes(d_out, s.tw, logt, true, st, e);
         }
         if (!alias) {
             uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);

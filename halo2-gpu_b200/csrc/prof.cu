@@ -80,6 +80,44 @@ __global__ void k_probe_imad(uint32_t* sink, int iters, uint32_t seed)
     if (x == 0x12345678u) sink[blockIdx.x] = x;
 }
 
+// Single-form throughput: mode 0 = mad.lo.u32, 1 = mad.hi.u32, 2 = mad.wide.u32
+// (16 independent instructions per iteration per thread).
+__global__ void k_probe_imad_form(uint32_t* sink, int iters, uint32_t seed, int mode)
+{
+    uint32_t a[16];
+    for (int j = 0; j < 16; j++) a[j] = seed * (threadIdx.x + 1) + j * 0x9e3779b9u;
+    const uint32_t m = seed | 1u;
+    if (mode == 0) {
+        for (int it = 0; it < iters; it++) {
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(m), "r"(a[(j + 5) & 15]));
+        }
+    } else if (mode == 1) {
+        for (int it = 0; it < iters; it++) {
+#pragma unroll
+            for (int j = 0; j < 16; j++)
+                asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[j]) : "r"(m), "r"(a[(j + 5) & 15]));
+        }
+    } else {
+        uint64_t w[8];
+        for (int j = 0; j < 8; j++) w[j] = ((uint64_t)a[j] << 32) | a[j + 8];
+        for (int it = 0; it < iters; it++) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                uint32_t lo = (uint32_t)w[j];
+                asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[j]) : "r"(lo), "r"(m));
+                lo = (uint32_t)w[(j + 3) & 7];
+                asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[j]) : "r"(lo), "r"(m));
+            }
+        }
+        for (int j = 0; j < 8; j++) a[j] = (uint32_t)(w[j] ^ (w[j] >> 32));
+    }
+    uint32_t x = 0;
+    for (int j = 0; j < 16; j++) x ^= a[j];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
+}
+
 __global__ void k_probe_modmul(uint32_t* sink, int iters)
 {
     Fr a = Fr::one(), b = Fr::r2(), c = Fr::one(), d = Fr::r2();
@@ -132,6 +170,14 @@ extern "C" RustError h2b_probe_imad(int blocks, int threads, int iters, void* d_
 {
     k_probe_imad<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters, 0x2545f491u);
     H2B_LAUNCHED("k_probe_imad");
+    return ok();
+}
+
+extern "C" RustError h2b_probe_imad_form(int blocks, int threads, int iters, int mode, void* d_sink,
+                                         cudaStream_t stream)
+{
+    k_probe_imad_form<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters, 0x2545f491u, mode);
+    H2B_LAUNCHED("k_probe_imad_form");
     return ok();
 }
 

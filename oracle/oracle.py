@@ -41,7 +41,7 @@ def lib():
         _lib.o_permute_pair.restype = ctypes.c_int
         _lib.o_permute_pair.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
                                         ctypes.c_void_p, ctypes.c_void_p]
-        _lib.o_quotient.argtypes = [ctypes.c_void_p] * 9 + [ctypes.c_uint64, ctypes.c_void_p] + \
+        _lib.o_quotient.argtypes = [ctypes.c_void_p] * 7 + [ctypes.c_uint64, ctypes.c_void_p] + \
             [ctypes.c_uint64] * 5 + [ctypes.c_void_p, ctypes.c_void_p]
         _lib.o_quotient_lookups.argtypes = [ctypes.c_void_p] * 11 + [ctypes.c_size_t]
         _lib.o_permutation_quotient.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int,

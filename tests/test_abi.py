@@ -47,7 +47,7 @@ def test_workspace_preflights_are_pure_host(h2b, built_lib):
         assert a > b > 0
         assert L._halo2_fft_many_workspace_size(3, k, k + 2) >= (32 << (k + 2))
     assert L._halo2_multiexp_workspace_size(1 << 16) > L._halo2_multiexp_device_bases_workspace_size(1 << 16)
-    assert L._halo2_msm_max_length(1 << 40) == 1 << 28
+    assert L._halo2_msm_max_length(1 << 40) == 1 << 27
     assert L._halo2_msm_max_length(1 << 20) < (1 << 20)
     assert L._halo2_fft_normal_check_memory(1, None, 10, 10)
     assert L._halo2_fft_many_check_memory(1, 10, 10)

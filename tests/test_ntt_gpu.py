@@ -54,6 +54,18 @@ def test_cosetfft_extension(h2b, orc, cuda, k, ek):
     assert_limbs_equal(got, want, "coset extension")
 
 
+@pytest.mark.parametrize("k,ek", [(3, 5), (10, 12), (13, 16)])
+def test_coset_extension_device_input(h2b, orc, cuda, k, ek):
+    """Device-input coeff_to_extended (the spread path that skips the first
+    ek-k broadcast stages) against the oracle."""
+    f = h2b.fields
+    we = pow(f.ROOT_OF_UNITY, 1 << (28 - ek), f.R_MOD)
+    a = orc.chacha_fr(40 + k, 1 << k)
+    d_out = h2b.dev_empty(32 << ek)
+    h2b.fft_many_to_device(3, k, ek, [h2b.to_dev(a)], [d_out], we, 1, input_on_device=True)
+    assert_limbs_equal(h2b.to_host(d_out), orc.ntt(3, k, ek, a, mont(h2b, we), mont(h2b, 1)), "spread coset")
+
+
 @pytest.mark.parametrize("k", [10, 14])
 def test_fft_many_host_and_device(h2b, orc, cuda, k):
     f = h2b.fields

@@ -165,3 +165,31 @@ def test_chacha_fr_is_canonical(orc, h2b):
     ints = h2b.fields.limbs_to_ints(xs)
     assert all(x < h2b.fields.R_MOD for x in ints)
     assert len(set(ints)) == 64
+
+
+def test_quotient_interpreter_matches_direct_gate_evaluation(orc, h2b):
+    """The oracle's rule interpreter, fed the reference's 128-bit encoding of
+    the config-3 gates, equals the gates evaluated directly with integers."""
+    import rules as R
+    f = h2b.fields
+    P = f.R_MOD
+    g = R.Graph()
+    parts = R.plonk_and_fibonacci(g)
+    nq, rs = 64, 2
+    fixed = [orc.chacha_fr(10 + i, nq) for i in range(3)]
+    inst = [orc.chacha_fr(20, nq)]
+    adv = [orc.chacha_fr(30 + i, nq) for i in range(4)]
+    chal = orc.chacha_fr(40, 1)
+    y = 987654321
+    ec = f.fr_mont_limbs([0, 1, P - 1, 2, y])
+    got = orc.quotient(fixed, inst, adv, chal, f.fr_mont_limbs(g.constants), ec, np.array(g.rules, np.uint64),
+                       np.array(parts, np.uint64), nq, rs, 0, nq)
+    I = lambda a: f.fr_from_mont_limbs(a)
+    F, IN, A, C = [I(c) for c in fixed], I(inst[0]), [I(c) for c in adv], I(chal)[0]
+    for r in range(nq):
+        at = lambda k: (r + k * rs) % nq
+        g1 = (A[0][r] * F[0][r] + A[1][r] * F[1][r] + A[0][r] * A[1][r] * F[2][r] + A[2][r] * 7 + 12345) % P
+        g2 = (A[3][at(2)] - A[3][at(1)] - A[3][r]) % P
+        g3 = IN[at(-1)] * C % P
+        want = ((g1 * y + g2) * y + g3) % P
+        assert I(got[r:r + 1])[0] == want, f"row {r}"

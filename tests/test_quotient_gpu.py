@@ -34,6 +34,10 @@ def run_both(h2b, orc, g, parts, nf, ni, na, nch, nq, rot_scale, row_start, row_
     h2b.quotient_device([h2b.to_dev(c) for c in fixed], [h2b.to_dev(c) for c in inst], [h2b.to_dev(c) for c in adv],
                         chal, consts, y, rules, vp, nq, rot_scale, row_start, row_end, d_out, d_prev)
     assert_limbs_equal(h2b.to_host(d_out), want, "device quotient")
+    # the host-column entry point has no prev seed (quotient.cu:309-440)
+    if prev is not None:
+        want = orc.quotient(fixed, inst, adv, chal if nch else np.zeros((1, 4), np.uint64), consts, ec, rules, vp,
+                            nq, rot_scale, row_start, row_end, None)
     got = h2b.quotient_host(fixed, inst, adv, chal, consts, y, rules, vp, nq, rot_scale, row_start, row_end)
     assert_limbs_equal(got, want, "host quotient")
 
@@ -104,6 +108,6 @@ def test_permutation_quotient(h2b, orc, cuda, ncols, chunk_len):
     d_vals = h2b.to_dev(values)
     h2b.quotient_permutation_device(d_vals, h2b.to_dev(l0), h2b.to_dev(ll), h2b.to_dev(la),
                                     [h2b.to_dev(p) for p in prods], [h2b.to_dev(p) for p in perms],
-                                    [h2b.to_dev(c) for c in cols], y, beta, gamma, delta, delta_start, ext_omega,
+                                    [h2b.to_dev(c) for c in cols], beta, gamma, y, delta, delta_start, ext_omega,
                                     omega, chunk_len, last_rotation, rot_scale, n, n)
     assert_limbs_equal(h2b.to_host(d_vals), want, "permutation quotient")
