@@ -124,6 +124,7 @@ _SIGS = {
     "h2b_launch_count": (_u64, []),
     "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_msm_window_bits": (ctypes.c_int, [_u64]),
+    "h2b_batch_invert_noalloc": (RustError, [_vp, _u32, _u64, _vp]),
 }
 
 PROF_MSM_ACCUMULATE, PROF_MSM_TOTAL, PROF_NTT_PASSES, PROF_BATCH_INVERT, PROF_QUOTIENT, PROF_PERMUTE_SORT = range(6)

@@ -20,6 +20,7 @@
 //    commitment/permutation_commit.cu:51-256): acc_r * prod_i (b*sigma_i+g+v_i)
 //    inverted, times prod_i (deltaomega*delta^i*w^r*b + g + v_i); deltaomega
 //    is advanced by delta^batch in place.
+#include <mutex>
 #include <vector>
 #include "abi.cuh"
 #include "field.cuh"
@@ -622,4 +623,65 @@ extern "C" RustError _halo2_permutation_product_device_inputs(
     k_advance_deltaomega<<<1, 32, 0, stream>>>((Fr*)deltaomega_device, (const Fr*)delta_device, batch);
     H2B_LAUNCHED("k_advance_deltaomega");
     return ok();
+}
+
+// ---------------------------------------------------------------------------
+// Batch inversion without any allocation
+// ---------------------------------------------------------------------------
+// For callers that cannot allocate device memory: code that must keep the
+// reference's scratch-free `_halo2_batch_invert(d, field, len, stream)` call
+// shape (its Rust call sites own every device buffer and have no workspace to
+// hand over), code whose device memory is entirely pre-reserved by an arena
+// or pool it does not control, and code that must not trigger the
+// synchronisation cudaMalloc implies.  They still get the single-inversion
+// multi-level algorithm of h2b_batch_invert, with its per-tile totals kept
+// in a fixed array that lives in this library's device image.
+//
+// Limits and rules of use:
+//  * length <= 2^26 elements; larger inputs are rejected with an error.
+//  * The array (1.5 MiB) is reserved on every GPU that loads this library and
+//    stays reserved until the process exits.
+//  * All calls share the one array: calls whose work overlaps on the GPU
+//    (different streams without ordering, or several host threads) race and
+//    corrupt each other's results.  Serialise them on one stream.
+//  * The array keeps the previous call's contents; nothing in it needs to
+//    start at zero (every tile total is written before it is read).
+//  * The first call on each device looks up the array's device address
+//    (cudaGetSymbolAddress, with that device current); make that first call
+//    before any stream capture.  No call allocates or frees memory.
+namespace h2b {
+constexpr uint64_t NOALLOC_SCRATCH_BYTES = 1536ull << 10;
+constexpr uint64_t NOALLOC_MAX_LENGTH = 1ull << 26;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+} // namespace h2b
+
+extern "C" RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type, uint64_t length, cudaStream_t stream)
+{
+    if (field_type != 0 && field_type != 1) return err(cudaErrorInvalidValue, "Invalid scalar type");
+    if (length == 0) return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length must be >= 1");
+    if (length > NOALLOC_MAX_LENGTH)
+        return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length exceeds the 2^26-element maximum");
+    uint64_t need = h2b_batch_invert_workspace_size(length);
+    if (need > NOALLOC_SCRATCH_BYTES)
+        return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length needs more than the fixed scratch");
+    int dev = 0;
+    H2B_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: device id");
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (g_noalloc_addr[dev] == nullptr) {
+            void* p = nullptr;
+            cudaError_t c = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (c != cudaSuccess) return cuda_err(c, "cudaGetSymbolAddress(no-allocation scratch)");
+            g_noalloc_addr[dev] = p;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    ScratchArena ar(base, NOALLOC_SCRATCH_BYTES);
+    if (field_type == 0) return batch_invert_levels<FrCfg>((Fr*)d_data, length, ar, stream);
+    return batch_invert_levels<FqCfg>((Fq*)d_data, length, ar, stream);
 }

@@ -272,6 +272,16 @@ RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_t length, v
 void h2b_ntt_set_pass_stages(int stages);
 int h2b_ntt_get_pass_stages(void);
 
+/* No counterpart in the reference.  Batch inversion with the semantics of
+ * _halo2_batch_invert (in place, zeros stay zero, field_type 0 = Fr, 1 = Fq)
+ * for callers that cannot allocate device memory: it keeps the scratch-free
+ * call shape and uses a fixed 1.5 MiB array inside the library instead of a
+ * workspace, so it allocates and frees nothing.  length <= 2^26 (larger is
+ * an error).  All calls share that array: calls that overlap on the GPU
+ * race, so serialise them on one stream.  The first call on each device
+ * looks up the array's address; make it before any stream capture. */
+RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type, uint64_t length, h2b_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
