@@ -91,6 +91,15 @@ _SIGS = {
     "_halo2_fft_many_to_device": (RustError, [_u32, _u32, _u32, _u32, _ffi, _ffi, _vp, _ffi, _b, _vp, _u64, _vp]),
     "_halo2_fft_many_check_memory": (_b, [_u32, _u32, _u32]),
     "_halo2_get_fft_split_radix": (_i32, [_u32, _u32, _u32, _u64]),
+    "_halo2_power_of_omega_workspace_size": (_u64, [_u32]),
+    "_halo2_power_of_omega": (RustError, [_ffi, _ffi, _ffi, _u32, _u32, _vp, _u64, _vp]),
+    "_halo2_generate_omega_powers_workspace_size": (_u64, [_u32]),
+    "_halo2_generate_omega_powers": (RustError, [_vp, _vp, _u32, _vp, _u64, _vp]),
+    "_halo2_generate_omega_lut_workspace_size": (_u64, [_u32]),
+    "_halo2_generate_omega_lut": (RustError, [_ffi, _ffi, _u32, _vp, _u64, _vp]),
+    "_halo2_generate_omegadelta_workspace_size": (_u64, [_u32, _u32, _u32, _u32, _u32]),
+    "_halo2_generate_omegadelta": (RustError, [_vp, _vp, _vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp, _u64, _vp]),
+    "_halo2_quotient_decode": (None, [_vp, _u64, _u64, _u64, _u64, _u64]),
     "_halo2_evaluate_h_max_rows": (_u64, [_vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64,
                                           _u64]),
     "_halo2_quotient_workspace_size": (_u64, [_vp, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64, _u64,
@@ -121,6 +130,8 @@ _SIGS = {
     "h2b_probe_imad": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "h2b_probe_modmul": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "h2b_probe_imad_form": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "h2b_probe_modmul_impl": (RustError, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "h2b_fr_mul_batch": (RustError, [ctypes.c_int, _vp, _vp, _vp, _u64, _vp]),
     "h2b_launch_count": (_u64, []),
     "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_msm_window_bits": (ctypes.c_int, [_u64]),
@@ -317,6 +328,50 @@ def cosetfft(log_n, extend_log_n, values, extended_omega, stream=None):
     call("_halo2_cosetfft", NTT_COSET, log_n, extend_log_n, inp.ctypes.data, out.ctypes.data, om.ctypes.data,
          one.ctypes.data, ptr(ws), ws.numel(), stream_handle(stream))
     return out
+
+
+# --- twiddle tables (halo2_proofs/src/cuda/funcs/omega.rs) -----------------------
+
+def power_of_omega_gpu(omega, log_n, pow_, stream=None):
+    """power_of_omega_gpu (omega.rs:15-49): returns (omega^pow, log table of log_n + 1 limbs)."""
+    om = _scalar_bytes(omega)
+    res = np.zeros((1, 4), dtype=np.uint64)
+    lut = np.zeros((log_n + 1, 4), dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_power_of_omega_workspace_size(log_n))
+    call("_halo2_power_of_omega", ctypes.byref(host_ffi(res)), ctypes.byref(host_ffi(lut)),
+         ctypes.byref(host_ffi(om)), log_n, pow_, ptr(ws), ws.numel(), stream_handle(stream))
+    return res, lut
+
+
+def generate_omega_powers_gpu(omega, log_n, output_num=None, stream=None):
+    """generate_omega_powers_gpu (omega.rs:51-103): first output_num of omega^i, i < 2^log_n, to host."""
+    torch = _torch()
+    d_om = to_dev(_scalar_bytes(omega))
+    d_out = dev_empty(32 << log_n)
+    ws = dev_empty(lib()._halo2_generate_omega_powers_workspace_size(log_n))
+    call("_halo2_generate_omega_powers", ptr(d_out), ptr(d_om), log_n, ptr(ws), ws.numel(), stream_handle(stream))
+    torch.cuda.synchronize()
+    out = to_host(d_out)
+    return out if output_num is None else out[:output_num]
+
+
+def generate_omega_lut_gpu(omega, log_n, stream=None):
+    """generate_omega_lut_gpu (omega.rs:105-136): the 2^10 + 2^(log_n-10) two-level table."""
+    om = _scalar_bytes(omega)
+    out = np.zeros(((1 << 10) + (1 << (log_n - 10)), 4), dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_generate_omega_lut_workspace_size(log_n))
+    call("_halo2_generate_omega_lut", ctypes.byref(host_ffi(out)), ctypes.byref(host_ffi(om)), log_n, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    return out
+
+
+def generate_omegadelta_device(d_out, d_mapping, omega, delta, log_n, start, end, colnum, coloffset=0, stream=None):
+    """_halo2_generate_omegadelta: d_out[i] = omega^row * delta^col over mapping[start..=end]."""
+    om, de = _scalar_bytes(omega), _scalar_bytes(delta)
+    ws = dev_empty(lib()._halo2_generate_omegadelta_workspace_size(log_n, start, end, colnum, coloffset))
+    call("_halo2_generate_omegadelta", ptr(d_out), ptr(d_mapping), om.ctypes.data, de.ctypes.data, log_n, start,
+         end, colnum, coloffset, ptr(ws), ws.numel(), stream_handle(stream))
+    return d_out
 
 
 def fft_many(ntt_type, log_n, extend_log_n, polys, omega, divisor, stream=None):

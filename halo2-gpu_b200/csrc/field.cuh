@@ -178,6 +178,52 @@ H2B_DEV Fp<C> mont_mul_inline(const Fp<C>& a, const Fp<C>& b)
     return r;
 }
 
+// Same CIOS recurrence with each limb product formed by one 32x32->64
+// multiply-add (mad.wide.u32) and the 32-bit carry folded in with integer
+// adds: on sm_100a mad.hi issues at half the rate of mad.lo, so a lo/hi pair
+// costs three issue slots of the multiply pipe where one mad.wide costs about
+// 1.5, and the adds go to the ALU pipe.  Every intermediate fits its word:
+// a_j*b_i + t_j + c <= (2^32-1)^2 + 2(2^32-1) = 2^64 - 1.
+template <class C>
+H2B_DEV Fp<C> mont_mul_wide(const Fp<C>& a, const Fp<C>& b)
+{
+    const uint32_t P[8] = {C::M0, C::M1, C::M2, C::M3, C::M4, C::M5, C::M6, C::M7};
+    uint32_t t[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) t[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint32_t bi = b.v[i];
+        uint32_t c = 0;
+        uint64_t w;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            w = (uint64_t)a.v[j] * bi + t[j] + c;
+            t[j] = (uint32_t)w;
+            c = (uint32_t)(w >> 32);
+        }
+        t[8] += c;                         // t < 2p + p 2^32 < 2^287: no carry out
+        const uint32_t m = t[0] * C::N0;
+        w = (uint64_t)m * P[0] + t[0];     // low word becomes zero
+        c = (uint32_t)(w >> 32);
+#pragma unroll
+        for (int j = 1; j < 8; j++) {
+            w = (uint64_t)m * P[j] + t[j] + c;
+            t[j - 1] = (uint32_t)w;
+            c = (uint32_t)(w >> 32);
+        }
+        w = (uint64_t)t[8] + c;
+        t[7] = (uint32_t)w;
+        t[8] = (uint32_t)(w >> 32);        // zero: t < 2p after the shift
+    }
+    Fp<C> r;
+    uint32_t lo[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) lo[i] = t[i];
+    cond_sub<C>(r.v, lo);
+    return r;
+}
+
 // One out-of-line body per field: kernels that chain many products (curve
 // formulas, the quotient interpreter) otherwise inline ~300 instructions per
 // product and starve on instruction fetch.  H2B_INLINE_MUL=1 restores full

@@ -118,6 +118,37 @@ __global__ void k_probe_imad_form(uint32_t* sink, int iters, uint32_t seed, int 
     if (x == 0x12345678u) sink[blockIdx.x] = x;
 }
 
+template <int IMPL>
+__device__ __forceinline__ Fr mul_impl(const Fr& a, const Fr& b)
+{
+    return IMPL == 0 ? mont_mul_inline<FrCfg>(a, b) : mont_mul_wide<FrCfg>(a, b);
+}
+
+template <int IMPL>
+__global__ void k_probe_modmul_impl(uint32_t* sink, int iters)
+{
+    Fr a = Fr::one(), b = Fr::r2(), c = Fr::one(), d = Fr::r2();
+    a.v[0] ^= threadIdx.x;
+    c.v[1] ^= blockIdx.x;
+    Fr m = Fr::r2();
+    m.v[2] ^= blockIdx.x;  // not a compile-time constant
+    for (int it = 0; it < iters; it++) {
+        a = mul_impl<IMPL>(a, m);
+        b = mul_impl<IMPL>(b, m);
+        c = mul_impl<IMPL>(c, m);
+        d = mul_impl<IMPL>(d, m);
+    }
+    uint32_t x = a.v[0] ^ b.v[1] ^ c.v[2] ^ d.v[3];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
+}
+
+template <int IMPL>
+__global__ void k_fr_mul_batch(const Fr* __restrict__ a, const Fr* __restrict__ b, Fr* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        st(&out[i], mul_impl<IMPL>(ld(&a[i]), ld(&b[i])));
+}
+
 __global__ void k_probe_modmul(uint32_t* sink, int iters)
 {
     Fr a = Fr::one(), b = Fr::r2(), c = Fr::one(), d = Fr::r2();
@@ -178,6 +209,30 @@ extern "C" RustError h2b_probe_imad_form(int blocks, int threads, int iters, int
 {
     k_probe_imad_form<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters, 0x2545f491u, mode);
     H2B_LAUNCHED("k_probe_imad_form");
+    return ok();
+}
+
+// Montgomery-product throughput of one implementation (0 = mad.lo/mad.hi
+// carry chains, 1 = mad.wide), four independent products per iteration.
+extern "C" RustError h2b_probe_modmul_impl(int impl, int blocks, int threads, int iters, void* d_sink,
+                                           cudaStream_t stream)
+{
+    if (impl == 0) k_probe_modmul_impl<0><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    else k_probe_modmul_impl<1><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    H2B_LAUNCHED("k_probe_modmul_impl");
+    return ok();
+}
+
+// out[i] = a[i] * b[i] in Fr with the chosen product implementation (tests).
+extern "C" RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b, void* d_out, uint64_t n,
+                                      cudaStream_t stream)
+{
+    if (n == 0) return ok();
+    if (impl == 0)
+        k_fr_mul_batch<0><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    else
+        k_fr_mul_batch<1><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    H2B_LAUNCHED("k_fr_mul_batch");
     return ok();
 }
 

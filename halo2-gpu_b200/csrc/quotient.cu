@@ -478,6 +478,23 @@ extern "C" uint64_t _halo2_quotient_workspace_size(const uint64_t* rules, uint64
     return quotient_ws(num_rules, num_vp_rules, ncols, num_constants, num_challenges, rows, num_quotient, true);
 }
 
+// The reference's rule decoder hook (quotient.cu:334-345): it decodes the
+// rotation range of every value source for the row window and returns
+// nothing, and no caller reads a result.  Kept for link compatibility; it
+// walks the same encoding and has no effect.
+extern "C" void _halo2_quotient_decode(uint64_t* rules, uint64_t num_rules, uint64_t num_quotient,
+                                       uint64_t rotation_scale, uint64_t row_start, uint64_t row_end)
+{
+    (void)num_quotient; (void)row_start; (void)row_end;
+    int64_t lo = 0, hi = 0;
+    for (uint64_t i = 0; rules && i < 2 * num_rules; i++) {
+        int64_t r = (int64_t)decode_rot(rules[i]) * (int64_t)rotation_scale;
+        lo = std::min(lo, r);
+        hi = std::max(hi, r);
+    }
+    (void)lo; (void)hi;
+}
+
 extern "C" uint64_t _halo2_evaluate_h_max_rows(const uint64_t* rules, uint64_t num_rules, uint64_t num_vp_rules,
                                                uint64_t num_quotient, uint64_t num_fixed, uint64_t num_instance,
                                                uint64_t num_advice, uint64_t num_challenges, uint64_t num_constants,

@@ -199,7 +199,48 @@ bool _halo2_fft_many_check_memory(uint32_t ntt_type, uint32_t log_n, uint32_t ex
 /* culib.rs:596-601 ; ntt.cu:676-690 */
 int32_t _halo2_get_fft_split_radix(uint32_t ntt_type, uint32_t log_n, uint32_t extend_log_n, uint64_t free_bytes);
 
+/* ------------------------------------------------------------ twiddles --- */
+/* culib.rs:428 declares `cuda_omega_lut(res, log_n)`, but the reference's
+ * CUDA sources define no such symbol (nothing can call it); it has no
+ * counterpart here either. */
+
+/* culib.rs:430 ; polynomial/omega.cu:15-20 ; 0 when log_n >= 32 */
+uint64_t _halo2_power_of_omega_workspace_size(uint32_t log_n);
+/* culib.rs:432-441 ; polynomial/omega.cu:29-67 -- host omega in; host res = omega^pow and host
+ * omega_lut[0..=log_n] = [1, omega, omega^2, omega^4, ...]; synchronises.  Code 1 when
+ * log_n >= 32 or pow >= 2^log_n. */
+RustError _halo2_power_of_omega(const FFITraitObject* res, const FFITraitObject* omega_lut,
+                                const FFITraitObject* omega, uint32_t log_n, uint32_t pow, void* scratch,
+                                uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:443 ; polynomial/omega.cu:72-75 */
+uint64_t _halo2_generate_omega_powers_workspace_size(uint32_t log_n);
+/* culib.rs:449-456 ; polynomial/omega.cu:77-94 -- device out[i] = omega^i, i < 2^log_n, from a
+ * device omega; does not synchronise */
+RustError _halo2_generate_omega_powers(void* d_omega_powers, const void* d_omega, uint32_t log_n, void* scratch,
+                                       uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:458 ; polynomial/omega.cu:99-105 ; 0 outside [10, 42) */
+uint64_t _halo2_generate_omega_lut_workspace_size(uint32_t log_n);
+/* culib.rs:460-467 ; polynomial/omega.cu:107-150 -- host omega in; host table
+ * [omega^i, i < 2^10] ++ [(omega^1024)^i, i < 2^(log_n-10)]; synchronises.  Code 1 outside
+ * 10 <= log_n < 42. */
+RustError _halo2_generate_omega_lut(const FFITraitObject* sparse_twiddle, const FFITraitObject* omega,
+                                    uint32_t log_n, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:469-475 ; polynomial/omega.cu:153-161 */
+uint64_t _halo2_generate_omegadelta_workspace_size(uint32_t log_n, uint32_t omega_start, uint32_t omega_end,
+                                                   uint32_t colunm_num, uint32_t colunm_offset);
+/* culib.rs:477-490 ; polynomial/omega.cu:163-200 -- device res[i] = omega^row * delta^col for the
+ * u32 pairs (col, row) = mapping[2 (omega_start + i) .. +1], i <= omega_end - omega_start; host
+ * omega and delta; colunm_offset is unused (as in the reference kernel); does not synchronise. */
+RustError _halo2_generate_omegadelta(void* res, const void* mapping, const void* omega, const void* delta,
+                                     uint32_t log_n, uint32_t omega_start, uint32_t omega_end, uint32_t colunm_num,
+                                     uint32_t colunm_offset, void* scratch, uint64_t scratch_bytes,
+                                     h2b_stream_t stream);
+
 /* ------------------------------------------------------------ quotient --- */
+
+/* quotient.cu:334-345 -- rule decoding hook with no outputs (no Rust caller) */
+void _halo2_quotient_decode(uint64_t* rules, uint64_t num_rules, uint64_t num_quotient, uint64_t rotation_scale,
+                            uint64_t row_start, uint64_t row_end);
 
 /* evaluation.rs:1435-1449 ; quotient.cu:190-222 */
 uint64_t _halo2_evaluate_h_max_rows(const uint64_t* rules, uint64_t num_rules, uint64_t num_vp_rules,

@@ -77,3 +77,28 @@ def test_argument_errors_match_reference(h2b, built_lib):
     assert e.code == 1
     with pytest.raises(h2b.Halo2GpuError):
         h2b.check(built_lib._halo2_batch_invert(None, 9, 8, None), "batch_invert")
+
+
+def test_twiddle_preflights_and_argument_errors(h2b, built_lib):
+    import numpy as np
+    L = built_lib
+    assert L._halo2_power_of_omega_workspace_size(31) >= 32 * 34
+    assert L._halo2_power_of_omega_workspace_size(32) == 0
+    assert L._halo2_generate_omega_powers_workspace_size(22) > 0
+    assert L._halo2_generate_omega_lut_workspace_size(9) == 0
+    assert L._halo2_generate_omega_lut_workspace_size(20) >= 32 * ((1 << 10) + (1 << 10))
+    assert L._halo2_generate_omegadelta_workspace_size(20, 0, 100, 5, 0) > 0
+    z = np.zeros(4, np.uint64)
+    o = h2b.host_ffi(z)
+    # pow >= 2^log_n and log_n >= 32 are refused before any device work (omega.cu:40-43)
+    assert L._halo2_power_of_omega(ctypes.byref(o), ctypes.byref(o), ctypes.byref(o), 4, 16, None, 0, None).code == 1
+    assert L._halo2_power_of_omega(ctypes.byref(o), ctypes.byref(o), ctypes.byref(o), 32, 1, None, 0, None).code == 1
+    # log_n outside [DENSE_POWER_DEGREE, DENSE_POWER_DEGREE + 32) (omega.cu:118-120,181-183)
+    assert L._halo2_generate_omega_lut(ctypes.byref(o), ctypes.byref(o), 9, None, 0, None).code == 1
+    assert L._halo2_generate_omegadelta(None, None, z.ctypes.data, z.ctypes.data, 42, 0, 1, 1, 0, None, 0,
+                                        None).code == 1
+    # undersized scratch is an error code
+    assert L._halo2_power_of_omega(ctypes.byref(o), ctypes.byref(o), ctypes.byref(o), 4, 3, None, 0, None).code == 1
+    # the decode hook has no outputs and accepts any rule list
+    rules = np.zeros(4, np.uint64)
+    L._halo2_quotient_decode(rules.ctypes.data, 2, 1 << 10, 1, 0, 1 << 10)
