@@ -154,6 +154,141 @@ H2B_DEV void xyzz_add(G1Xyzz& acc, const G1Xyzz& q)
     acc.ZZZ = acc.ZZZ * q.ZZZ * PPP;
 }
 
+// ---- XYZZ in 29-bit limb form (MSM bucket accumulation) -------------------
+// Same madd-2008-s formula over Fl<FqCfg>: coordinates stay below 2p in limb
+// form between products, so a bucket addition converts only the loaded point
+// (and the accumulator when it is stored).
+
+typedef Fl<FqCfg> FqL;
+
+struct G1XyzzL {
+    FqL X, Y, ZZ, ZZZ;
+};
+
+H2B_DEV G1XyzzL xyzzl_inf()
+{
+    G1XyzzL r;
+    r.X = fl_zero<FqCfg>(); r.Y = fl_zero<FqCfg>(); r.ZZ = fl_zero<FqCfg>(); r.ZZZ = fl_zero<FqCfg>();
+    return r;
+}
+
+H2B_DEV bool is_inf(const G1XyzzL& p) { return fl_is_zero(p.ZZ); }
+
+H2B_DEV G1XyzzL xyzzl_from(const G1Xyzz& p)
+{
+    G1XyzzL r;
+    r.X = to_l(p.X); r.Y = to_l(p.Y); r.ZZ = to_l(p.ZZ); r.ZZZ = to_l(p.ZZZ);
+    return r;
+}
+
+// Canonical XYZZ (infinity keeps ZZ = 0).
+H2B_DEV G1Xyzz xyzzl_to(const G1XyzzL& p)
+{
+    G1Xyzz r;
+    r.X = from_l(p.X); r.Y = from_l(p.Y); r.ZZ = from_l(p.ZZ); r.ZZZ = from_l(p.ZZZ);
+    return r;
+}
+
+// Product helpers by call structure: MODE 0 pairs two independent products
+// per out-of-line call, MODE 1 inlines every product, MODE 2 makes one
+// out-of-line call per product.
+template <int MODE>
+H2B_DEV Fl2<FqCfg> xl_mul2(const FqL& a0, const FqL& b0, const FqL& a1, const FqL& b1)
+{
+    if (MODE == 0) return fl_mul2(a0, b0, a1, b1);
+    Fl2<FqCfg> r;
+    if (MODE == 1) { r.a = mul29(a0, b0); r.b = mul29(a1, b1); }
+    else { r.a = fl_mul(a0, b0); r.b = fl_mul(a1, b1); }
+    return r;
+}
+
+template <int MODE>
+H2B_DEV Fl2<FqCfg> xl_sqr2(const FqL& a0, const FqL& a1)
+{
+    if (MODE == 0) return fl_sqr2(a0, a1);
+    Fl2<FqCfg> r;
+    if (MODE == 1) { r.a = sqr29(a0); r.b = sqr29(a1); }
+    else { r.a = fl_sqr(a0); r.b = fl_sqr(a1); }
+    return r;
+}
+
+// madd-2008-s: acc += (qx, qy), an affine point that is not infinity.
+template <int MODE = 0>
+H2B_DEV void xyzzl_madd(G1XyzzL& acc, const FqL& qx, const FqL& qy)
+{
+    if (is_inf(acc)) {
+        acc.X = qx; acc.Y = qy; acc.ZZ = to_l(Fq::one()); acc.ZZZ = acc.ZZ;
+        return;
+    }
+    // products grouped in independent pairs: 8M + 2S in five pairs
+    const Fl2<FqCfg> us = xl_mul2<MODE>(qx, acc.ZZ, qy, acc.ZZZ);     // U2, S2
+    const FqL P = fl_sub(us.a, acc.X);
+    const FqL R = fl_sub(us.b, acc.Y);
+    if (fl_is_zero_mod(P)) {
+        G1Affine q;
+        q.x = from_l(qx); q.y = from_l(qy);
+        acc = fl_is_zero_mod(R) ? xyzzl_from(xyzz_dbl_affine(q)) : xyzzl_inf();
+        return;
+    }
+    const Fl2<FqCfg> sq = xl_sqr2<MODE>(P, R);                        // PP, R^2
+    const Fl2<FqCfg> pq = xl_mul2<MODE>(P, sq.a, acc.X, sq.a);        // PPP, Q
+    const FqL X3 = fl_sub(fl_sub(sq.b, pq.a), fl_add(pq.b, pq.b));
+    const Fl2<FqCfg> yy = xl_mul2<MODE>(R, fl_sub(pq.b, X3), acc.Y, pq.a);
+    const Fl2<FqCfg> zz = xl_mul2<MODE>(acc.ZZ, sq.a, acc.ZZZ, pq.a); // ZZ*PP, ZZZ*PPP
+    acc.Y = fl_sub(yy.a, yy.b);
+    acc.X = X3;
+    acc.ZZ = zz.a;
+    acc.ZZZ = zz.b;
+}
+
+// dbl-2008-s-1 and add-2008-s in limb form with the products inlined, for
+// the single-thread tails of the MSM (window combination, final doubling
+// chain) where latency, not throughput, sets the time: independent products
+// of one formula overlap.
+H2B_DEV G1XyzzL xyzzl_dbl(const G1XyzzL& p)
+{
+    if (is_inf(p) || fl_is_zero_mod(p.Y)) return xyzzl_inf();
+    const FqL U = fl_add(p.Y, p.Y);
+    const FqL V = sqr29(U);
+    const FqL xx = sqr29(p.X);
+    const FqL W = mul29(U, V);
+    const FqL S = mul29(p.X, V);
+    const FqL M = fl_add(fl_add(xx, xx), xx);
+    G1XyzzL r;
+    r.ZZ = mul29(V, p.ZZ);
+    r.ZZZ = mul29(W, p.ZZZ);
+    r.X = fl_sub(sqr29(M), fl_add(S, S));
+    r.Y = fl_sub(mul29(M, fl_sub(S, r.X)), mul29(W, p.Y));
+    return r;
+}
+
+H2B_DEV void xyzzl_add(G1XyzzL& acc, const G1XyzzL& q)
+{
+    if (is_inf(q)) return;
+    if (is_inf(acc)) { acc = q; return; }
+    const FqL U1 = mul29(acc.X, q.ZZ);
+    const FqL U2 = mul29(q.X, acc.ZZ);
+    const FqL S1 = mul29(acc.Y, q.ZZZ);
+    const FqL S2 = mul29(q.Y, acc.ZZZ);
+    const FqL P = fl_sub(U2, U1);
+    const FqL R = fl_sub(S2, S1);
+    if (fl_is_zero_mod(P)) {
+        acc = fl_is_zero_mod(R) ? xyzzl_dbl(acc) : xyzzl_inf();
+        return;
+    }
+    const FqL PP = sqr29(P);
+    const FqL RR = sqr29(R);
+    const FqL zz = mul29(acc.ZZ, q.ZZ);
+    const FqL zzz = mul29(acc.ZZZ, q.ZZZ);
+    const FqL PPP = mul29(P, PP);
+    const FqL Q = mul29(U1, PP);
+    const FqL X3 = fl_sub(fl_sub(RR, PPP), fl_add(Q, Q));
+    acc.Y = fl_sub(mul29(R, fl_sub(Q, X3)), mul29(S1, PPP));
+    acc.X = X3;
+    acc.ZZ = mul29(zz, PP);
+    acc.ZZZ = mul29(zzz, PPP);
+}
+
 H2B_DEV G1Affine affine_neg(const G1Affine& p)
 {
     G1Affine r;

@@ -46,6 +46,7 @@ static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed seri
 static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
 
 static int g_msm_window_override = 0;
+static int g_msm_acc_variant = 0;  // call structure of the accumulation kernel (0, 1, 2)
 static int g_msm_chunk_override = 0;
 
 void msm_set_tuning(int window_bits, int chunk)
@@ -197,17 +198,10 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int
     }
 }
 
-__device__ __forceinline__ G1Affine load_signed_point(const G1Affine* __restrict__ bases, uint32_t e)
-{
-    const uint32_t v = e & ~SIGN_BIT;
-    G1Affine P = ld_affine(&bases[v >> 1]);
-    if (v & 1u) P.x = P.x * glv::beta();  // phi(P); (0, 0) stays infinity
-    if (e & SIGN_BIT) P = affine_neg(P);
-    return P;
-}
-
-// One thread per chunk of K sorted entries.
-__global__ void __launch_bounds__(128) k_msm_accumulate(const uint32_t* __restrict__ sorted,
+// One thread per chunk of K sorted entries; the running bucket sum stays in
+// 29-bit limb form and is packed to the canonical 8 x 32 image when stored.
+template <int MODE>
+__global__ void __launch_bounds__(128, MODE == 1 ? 2 : 3) k_msm_accumulate(const uint32_t* __restrict__ sorted,
                                                         const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
                                                         const G1Affine* __restrict__ bases, G1Xyzz* __restrict__ buckets,
                                                         G1Xyzz* __restrict__ heads)
@@ -226,17 +220,24 @@ __global__ void __launch_bounds__(128) k_msm_accumulate(const uint32_t* __restri
         uint64_t b = lo;
         uint32_t next = offsets[b + 1];
         bool head = offsets[b] < start;
-        G1Xyzz acc = xyzz_inf();
+        G1XyzzL acc = xyzzl_inf();
         for (uint32_t e = start; e < end; e++) {
             if (e == next) {
-                if (head) st_xyzz(&heads[t], acc); else st_xyzz(&buckets[b], acc);
-                acc = xyzz_inf();
+                if (head) st_xyzz(&heads[t], xyzzl_to(acc)); else st_xyzz(&buckets[b], xyzzl_to(acc));
+                acc = xyzzl_inf();
                 head = false;
                 do { b++; next = offsets[b + 1]; } while (next == e);
             }
-            xyzz_madd(acc, load_signed_point(bases, sorted[e]));
+            const uint32_t ent = sorted[e];
+            const uint32_t v = ent & ~SIGN_BIT;
+            G1Affine P = ld_affine(&bases[v >> 1]);
+            if (is_inf(P)) continue;
+            if (ent & SIGN_BIT) P.y = fneg(P.y);
+            FqL qx = to_l(P.x);
+            if (v & 1u) qx = fl_mul(qx, to_l(glv::beta()));  // phi(P)
+            xyzzl_madd<MODE>(acc, qx, to_l(P.y));
         }
-        if (head) st_xyzz(&heads[t], acc); else st_xyzz(&buckets[b], acc);
+        if (head) st_xyzz(&heads[t], xyzzl_to(acc)); else st_xyzz(&buckets[b], xyzzl_to(acc));
     }
 }
 
@@ -378,14 +379,14 @@ __global__ void k_msm_wincombine(const G1Xyzz* __restrict__ bits, int W, int nbi
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= W) return;
     const G1Xyzz* T = bits + (uint64_t)w * (nbits + 1);
-    G1Xyzz r = xyzz_inf();
+    G1XyzzL r = xyzzl_inf();
     for (int k = nbits - 1; k >= 0; k--) {
-        r = xyzz_dbl(r);
-        xyzz_add(r, ld_xyzz(&T[k]));
+        r = xyzzl_dbl(r);
+        xyzzl_add(r, xyzzl_from(ld_xyzz(&T[k])));
     }
-    for (int d = 0; d < log_l; d++) r = xyzz_dbl(r);
-    xyzz_add(r, ld_xyzz(&T[nbits]));
-    st_xyzz(&wins[w], r);
+    for (int d = 0; d < log_l; d++) r = xyzzl_dbl(r);
+    xyzzl_add(r, xyzzl_from(ld_xyzz(&T[nbits])));
+    st_xyzz(&wins[w], xyzzl_to(r));
 }
 
 // 2^(c*w) * W_w in parallel over w, then the sum and the affine conversion.
@@ -394,9 +395,9 @@ __global__ void k_msm_final(const G1Xyzz* __restrict__ wins, int W, int c, G1Jac
     __shared__ G1Xyzz sh[64];
     int w = threadIdx.x;
     if (w < W) {
-        G1Xyzz x = ld_xyzz(&wins[w]);
-        for (int d = 0; d < c * w; d++) x = xyzz_dbl(x);
-        sh[w] = x;
+        G1XyzzL x = xyzzl_from(ld_xyzz(&wins[w]));
+        for (int d = 0; d < c * w; d++) x = xyzzl_dbl(x);
+        sh[w] = xyzzl_to(x);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -441,8 +442,13 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_LAUNCHED("k_msm_sort<scatter>");
     uint64_t chunks = (p.max_entries + p.K - 1) / p.K;
     prof_begin(PROF_MSM_ACCUMULATE, st);
-    k_msm_accumulate<<<grid_for(chunks, 128, 148u * 32u), 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases,
-                                                                       s.buckets, s.heads);
+    const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
+    if (g_msm_acc_variant == 1)
+        k_msm_accumulate<1><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
+    else if (g_msm_acc_variant == 2)
+        k_msm_accumulate<2><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
+    else
+        k_msm_accumulate<0><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
     prof_end(PROF_MSM_ACCUMULATE, st);
     H2B_LAUNCHED("k_msm_accumulate");
     k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense,
@@ -564,6 +570,14 @@ extern "C" RustError h2b_msm_device(const void* d_scalar, const void* d_bases, v
 }
 
 extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(window_bits, chunk); }
+
+// Call structure of the bucket-accumulation kernel: 0 = two products per
+// out-of-line call (default), 1 = all products inline, 2 = one product per
+// call.  Results are identical; only speed differs.
+extern "C" void h2b_msm_set_accumulate_variant(int v)
+{
+    if (v >= 0 && v <= 2) g_msm_acc_variant = v;
+}
 
 // Number of nonzero signed window digits (= sorted entries = bucket
 // additions) the MSM of these scalars performs; written to *d_count (u64).

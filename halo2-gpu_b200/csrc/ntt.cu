@@ -19,6 +19,8 @@
 // bit-reversed out) serves the inverse ones, followed by a fused
 // bit-reversal+scale(+untwist) pass.  Twiddles w^e, e < n/2, are generated
 // into caller scratch once per call (once per batch for the *_many entries).
+// Few product sites per kernel here: inline them (full product throughput).
+#define H2B_INLINE_MUL 1
 #include <algorithm>
 #include <cstring>
 #include "abi.cuh"
@@ -186,95 +188,78 @@ __global__ void k_bitrev_inplace(Fr* __restrict__ a, int k, bool scale, Zeta3 z3
 //   DIF: stage s pairs (i, i + n/2^(s+1)), twiddle w^((i mod n/2^(s+1)) * 2^s),
 //        groups: stride S = n / 2^(s0+nst).
 // A CTA owns G = TILE >> nst consecutive groups (G * 2^nst = TILE elements).
-constexpr int NTT_TILE = 1024;
+constexpr int NTT_LOG_TILE = 10;
+constexpr int NTT_TILE = 1 << NTT_LOG_TILE;
 constexpr int NTT_THREADS = 512;
 
+// One pass: nst consecutive stages on groups of 2^nst elements at stride
+// S = 2^lS (the group's elements are g-th residue class mod S inside a block
+// of S * 2^nst).  A CTA owns G = 2^lG consecutive groups.  Every size is a
+// power of two, so all index arithmetic is shifts and masks on 32 bits
+// (n <= 2^31).
 template <bool DIT>
 __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(Fr* __restrict__ a, const Fr* __restrict__ tw, int logn,
-                                                          int s0, int nst)
+                                                          int s0, int nst, int lS, int lG)
 {
     extern __shared__ uint4 smem_raw[];
     Fr* sm = reinterpret_cast<Fr*>(smem_raw);
-    const uint64_t n = 1ull << logn;
-    const int gsize = 1 << nst;
-    const uint64_t S = DIT ? (1ull << s0) : (n >> (s0 + nst));
-    const uint64_t BS = S << nst;
-    const uint64_t ngroups = n >> nst;
-    uint64_t G = (uint64_t)NTT_TILE >> nst;
-    if (G > ngroups) G = ngroups;
-    const uint64_t g0 = blockIdx.x * G;
-    if (g0 >= ngroups) return;
-    const uint64_t elems = G << nst;
-    const bool wide = S >= G;   // the G groups share one block, consecutive r
+    const uint32_t Smask = (1u << lS) - 1;
+    const uint32_t g0 = blockIdx.x << lG;
+    const uint32_t elems = 1u << (lG + nst);
+    const bool wide = lS >= lG;   // the G groups of a CTA are consecutive residues
 
-    // load
-    for (uint64_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        uint64_t gl, j, addr;
+    // element idx of the tile <-> (group gl, position j) and its address
+    auto locate = [&](uint32_t idx, uint32_t& slot) -> uint32_t {
         if (wide) {
-            gl = idx % G;
-            j = idx / G;
-            uint64_t g = g0 + gl;
-            addr = (g / S) * BS + j * S + (g % S);
-        } else {
-            uint64_t base = (g0 / S) * BS;
-            uint64_t bl = idx / BS, rem = idx % BS;
-            j = rem / S;
-            gl = bl * S + (rem % S);
-            addr = base + idx;
+            const uint32_t gl = idx & ((1u << lG) - 1), j = idx >> lG;
+            const uint32_t g = g0 + gl;
+            slot = (gl << nst) + j;
+            return ((g >> lS) << (lS + nst)) + (j << lS) + (g & Smask);
         }
-        sm[gl * gsize + j] = ld(&a[addr]);
+        const uint32_t bl = idx >> (lS + nst), rem = idx & ((1u << (lS + nst)) - 1);
+        const uint32_t j = rem >> lS, gl = (bl << lS) + (rem & Smask);
+        slot = (gl << nst) + j;
+        return ((g0 >> lS) << (lS + nst)) + idx;
+    };
+
+    for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint32_t slot;
+        const uint32_t addr = locate(idx, slot);
+        sm[slot] = ld(&a[addr]);
     }
     __syncthreads();
 
-    const uint64_t nbf = G << (nst - 1);
+    const uint32_t nbf = 1u << (lG + nst - 1);
+    const uint32_t mmask = (1u << (nst - 1)) - 1;
     for (int t = 0; t < nst; t++) {
         const int s = s0 + t;
-        for (uint64_t u = threadIdx.x; u < nbf; u += blockDim.x) {
-            uint64_t gl = u >> (nst - 1);
-            uint64_t m = u & ((1ull << (nst - 1)) - 1);
-            uint64_t g = g0 + gl;
-            uint64_t r = g % S;
+        for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
+            const uint32_t gl = u >> (nst - 1), m = u & mmask;
+            const uint32_t r = (g0 + gl) & Smask;
+            const int h = DIT ? t : nst - t - 1;
+            const uint32_t lowm = m & ((1u << h) - 1);
+            const uint32_t q = ((m >> h) << (h + 1)) | lowm;
+            Fr* px = &sm[(gl << nst) + q];
+            Fr* py = px + (1u << h);
+            const Fr x = *px, y = *py;
             if (DIT) {
-                uint64_t lowm = m & ((1ull << t) - 1);
-                uint64_t q = ((m >> t) << (t + 1)) | lowm;
-                uint64_t e = (lowm * S + r) * (n >> (s + 1));
-                Fr* px = &sm[gl * gsize + q];
-                Fr* py = px + (1ull << t);
-                Fr x = *px;
-                Fr y = *py * ldg(&tw[e]);
-                *px = x + y;
-                *py = x - y;
+                const Fr w = ldg(&tw[((lowm << lS) + r) << (logn - s - 1)]);
+                const Fr yw = y * w;
+                *px = x + yw;
+                *py = x - yw;
             } else {
-                int h = nst - t - 1;
-                uint64_t lowm = m & ((1ull << h) - 1);
-                uint64_t q = ((m >> h) << (h + 1)) | lowm;
-                uint64_t e = (lowm * S + r) << s;
-                Fr* px = &sm[gl * gsize + q];
-                Fr* py = px + (1ull << h);
-                Fr x = *px, y = *py;
+                const Fr w = ldg(&tw[((lowm << lS) + r) << s]);
                 *px = x + y;
-                *py = (x - y) * ldg(&tw[e]);
+                *py = (x - y) * w;
             }
         }
         __syncthreads();
     }
 
-    // store
-    for (uint64_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
-        uint64_t gl, j, addr;
-        if (wide) {
-            gl = idx % G;
-            j = idx / G;
-            uint64_t g = g0 + gl;
-            addr = (g / S) * BS + j * S + (g % S);
-        } else {
-            uint64_t base = (g0 / S) * BS;
-            uint64_t bl = idx / BS, rem = idx % BS;
-            j = rem / S;
-            gl = bl * S + (rem % S);
-            addr = base + idx;
-        }
-        st(&a[addr], sm[gl * gsize + j]);
+    for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint32_t slot;
+        const uint32_t addr = locate(idx, slot);
+        st(&a[addr], sm[slot]);
     }
 }
 
@@ -301,17 +286,15 @@ static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_
     prof_begin(PROF_NTT_PASSES, st);
     for (int p = 0; p < passes; p++) {
         int nst = base + (p < extra ? 1 : 0);
-        uint64_t n = 1ull << logn;
-        uint64_t G = (uint64_t)NTT_TILE >> nst;
-        uint64_t ngroups = n >> nst;
-        if (G > ngroups) G = ngroups;
-        uint64_t blocks = (ngroups + G - 1) / G;
-        size_t smem = (size_t)(G << nst) * sizeof(Fr);
-        int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, G << (nst - 1)));
+        const int lS = dit ? s0 : logn - s0 - nst;
+        const int lG = std::min(NTT_LOG_TILE - nst, logn - nst);
+        const uint64_t blocks = 1ull << (logn - nst - lG);
+        size_t smem = (size_t)(1ull << (lG + nst)) * sizeof(Fr);
+        int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 1)));
         if (dit)
-            k_ntt_pass<true><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst);
+            k_ntt_pass<true><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst, lS, lG);
         else
-            k_ntt_pass<false><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst);
+            k_ntt_pass<false><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst, lS, lG);
         H2B_LAUNCHED("k_ntt_pass");
         s0 += nst;
     }

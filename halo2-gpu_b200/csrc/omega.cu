@@ -19,6 +19,8 @@
 // steps by x^T, so each warp stores 32 consecutive elements per step.
 // Products are exact Montgomery products, so the tables are bit-identical to
 // the reference's (whose kernels use a different multiplication order).
+// Few product sites per kernel here: inline them (full product throughput).
+#define H2B_INLINE_MUL 1
 #include <algorithm>
 #include <cstdio>
 #include "abi.cuh"

@@ -7,6 +7,8 @@
 //   elementwise multiply, fill with one, multiply-add, short subtractions.
 // All are HBM-bound streaming kernels: one 32-byte load/store per operand,
 // grid sized to a few waves of the 148 SMs.
+// Few product sites per kernel here: inline them (full product throughput).
+#define H2B_INLINE_MUL 1
 #include "abi.cuh"
 #include "field.cuh"
 

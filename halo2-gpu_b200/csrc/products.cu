@@ -20,6 +20,8 @@
 //    commitment/permutation_commit.cu:51-256): acc_r * prod_i (b*sigma_i+g+v_i)
 //    inverted, times prod_i (deltaomega*delta^i*w^r*b + g + v_i); deltaomega
 //    is advanced by delta^batch in place.
+// Few product sites per kernel here: inline them (full product throughput).
+#define H2B_INLINE_MUL 1
 #include <mutex>
 #include <vector>
 #include "abi.cuh"

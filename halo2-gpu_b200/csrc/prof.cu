@@ -121,7 +121,36 @@ __global__ void k_probe_imad_form(uint32_t* sink, int iters, uint32_t seed, int 
 template <int IMPL>
 __device__ __forceinline__ Fr mul_impl(const Fr& a, const Fr& b)
 {
-    return IMPL == 0 ? mont_mul_inline<FrCfg>(a, b) : mont_mul_wide<FrCfg>(a, b);
+    if (IMPL == 0) return mont_mul_inline<FrCfg>(a, b);
+    if (IMPL == 1) return mont_mul_wide<FrCfg>(a, b);
+    if (IMPL == 3) return mont_sqr_29<FrCfg>(a);
+    return mont_mul_29<FrCfg>(a, b);
+}
+
+// Fq products through the 29-bit column form (IMPL 4: a*b, 5: a^2).
+template <int IMPL>
+__global__ void k_fq_mul_batch(const Fq* __restrict__ a, const Fq* __restrict__ b, Fq* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        st(&out[i], IMPL == 4 ? mont_mul_29<FqCfg>(ld(&a[i]), ld(&b[i])) : mont_sqr_29<FqCfg>(ld(&a[i])));
+}
+
+// Four independent chains of 29-bit-limb products that stay in limb form.
+__global__ void k_probe_mul29_chain(uint32_t* sink, int iters)
+{
+    Fr a0 = Fr::one(), b0 = Fr::r2();
+    a0.v[0] ^= threadIdx.x;
+    Fr m0 = Fr::r2();
+    m0.v[2] ^= blockIdx.x;
+    Fl<FrCfg> a = to_l(a0), b = to_l(b0), c = to_l(m0), d = to_l(a0), m = to_l(m0);
+    for (int it = 0; it < iters; it++) {
+        a = mul29(a, m);
+        b = mul29(b, m);
+        c = mul29(c, m);
+        d = mul29(d, m);
+    }
+    uint32_t x = a.l[0] ^ b.l[1] ^ c.l[2] ^ d.l[3];
+    if (x == 0x12345678u) sink[blockIdx.x] = x;
 }
 
 template <int IMPL>
@@ -213,25 +242,39 @@ extern "C" RustError h2b_probe_imad_form(int blocks, int threads, int iters, int
 }
 
 // Montgomery-product throughput of one implementation (0 = mad.lo/mad.hi
-// carry chains, 1 = mad.wide), four independent products per iteration.
+// carry chains, 1 = mad.wide CIOS, 2 = 29-bit limbs with conversion from and
+// to 8 x 32 per product, 3 = 29-bit limbs kept between products), four
+// independent products per iteration.
 extern "C" RustError h2b_probe_modmul_impl(int impl, int blocks, int threads, int iters, void* d_sink,
                                            cudaStream_t stream)
 {
     if (impl == 0) k_probe_modmul_impl<0><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
-    else k_probe_modmul_impl<1><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    else if (impl == 1) k_probe_modmul_impl<1><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    else if (impl == 2) k_probe_modmul_impl<2><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    else k_probe_mul29_chain<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
     H2B_LAUNCHED("k_probe_modmul_impl");
     return ok();
 }
 
-// out[i] = a[i] * b[i] in Fr with the chosen product implementation (tests).
+// out[i] = a[i] * b[i] with the chosen product implementation (tests):
+// 0-2 Fr products (CIOS lo/hi, CIOS wide, 29-bit), 3 Fr square (29-bit),
+// 4 Fq product, 5 Fq square (29-bit).
 extern "C" RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b, void* d_out, uint64_t n,
                                       cudaStream_t stream)
 {
     if (n == 0) return ok();
     if (impl == 0)
         k_fr_mul_batch<0><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
-    else
+    else if (impl == 1)
         k_fr_mul_batch<1><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    else if (impl == 2)
+        k_fr_mul_batch<2><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    else if (impl == 3)
+        k_fr_mul_batch<3><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    else if (impl == 4)
+        k_fq_mul_batch<4><<<grid_for(n, 256), 256, 0, stream>>>((const Fq*)d_a, (const Fq*)d_b, (Fq*)d_out, n);
+    else
+        k_fq_mul_batch<5><<<grid_for(n, 256), 256, 0, stream>>>((const Fq*)d_a, (const Fq*)d_b, (Fq*)d_out, n);
     H2B_LAUNCHED("k_fr_mul_batch");
     return ok();
 }

@@ -304,6 +304,9 @@ RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out,
                          uint64_t scratch_bytes, h2b_stream_t stream);
 /* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
+/* Call structure of the MSM bucket-accumulation kernel: 0 = two field products per out-of-line call
+ * (default), 1 = all products inline, 2 = one product per call.  Same results; tuning only. */
+void h2b_msm_set_accumulate_variant(int variant);
 /* Batch inversion whose CTAs share a single inversion through scratch
  * (h2b_batch_invert_workspace_size bytes); same semantics as _halo2_batch_invert. */
 uint64_t h2b_batch_invert_workspace_size(uint64_t length);

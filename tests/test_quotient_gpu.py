@@ -111,3 +111,34 @@ def test_permutation_quotient(h2b, orc, cuda, ncols, chunk_len):
                                     [h2b.to_dev(c) for c in cols], beta, gamma, y, delta, delta_start, ext_omega,
                                     omega, chunk_len, last_rotation, rot_scale, n, n)
     assert_limbs_equal(h2b.to_host(d_vals), want, "permutation quotient")
+
+
+def test_compress_expressions(h2b, orc, cuda):
+    """Lookup compression (compress_expressions_in_place_device,
+    halo2_proofs/src/plonk/evaluation.rs:1722-1856) runs through the same
+    evaluator: value parts are the lookup expressions and the Horner factor is
+    theta, giving sum_i theta^(m-1-i) expr_i per row.  Checked against a direct
+    Python evaluation."""
+    f = h2b.fields
+    p = f.R_MOD
+    nq = 1 << 9
+    g = R.Graph()
+    e0 = g.add("store", R.vs(R.ADVICE, 0, 0))
+    e1 = g.add("mul", R.vs(R.FIXED, 0, 0), R.vs(R.ADVICE, 1, 1))
+    e2 = g.add("add", R.vs(R.ADVICE, 2, -1), g.const(5))
+    parts = [e0, e1, e2]
+    fixed = columns(orc, 500, 1, nq)
+    adv = columns(orc, 600, 3, nq)
+    theta = 0xABCDEF0123456789
+    consts = f.fr_mont_limbs(g.constants)
+    d_out = h2b.dev_empty(32 * nq)
+    h2b.quotient_device([h2b.to_dev(c) for c in fixed], [], [h2b.to_dev(c) for c in adv], np.zeros((0, 4), np.uint64),
+                        consts, theta, np.array(g.rules, dtype=np.uint64), np.array(parts, dtype=np.uint64), nq, 1, 0,
+                        nq, d_out, None)
+    got = [f.from_mont(x) for x in f.limbs_to_ints(h2b.to_host(d_out))]
+    F = [[f.from_mont(x) for x in f.limbs_to_ints(c)] for c in fixed]
+    A = [[f.from_mont(x) for x in f.limbs_to_ints(c)] for c in adv]
+    for r in range(nq):
+        ex = [A[0][r], F[0][r] * A[1][(r + 1) % nq] % p, (A[2][(r - 1) % nq] + 5) % p]
+        want = (ex[0] * theta * theta + ex[1] * theta + ex[2]) % p
+        assert got[r] == want, r
