@@ -119,6 +119,7 @@ _SIGS = {
     "h2b_msm_device": (RustError, [_vp, _vp, _vp, _u64, _vp, _u64, _vp]),
     "h2b_msm_set_tuning": (None, [ctypes.c_int, ctypes.c_int]),
     "h2b_msm_set_accumulate_variant": (None, [ctypes.c_int]),
+    "h2b_msm_set_pair_rounds": (None, [ctypes.c_int]),
     "h2b_batch_invert_workspace_size": (_u64, [_u64]),
     "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
     "h2b_ntt_set_pass_stages": (None, [ctypes.c_int]),

@@ -241,24 +241,25 @@ H2B_DEV void xyzzl_madd(G1XyzzL& acc, const FqL& qx, const FqL& qy)
     acc.ZZZ = zz.b;
 }
 
-// dbl-2008-s-1 and add-2008-s in limb form with the products inlined, for
-// the single-thread tails of the MSM (window combination, final doubling
-// chain) where latency, not throughput, sets the time: independent products
-// of one formula overlap.
+// dbl-2008-s-1 and add-2008-s in limb form with out-of-line latency-oriented
+// products, for the single-thread tails of the MSM (window combination, final
+// doubling chain): one warp runs them, so latency sets the time; each
+// product's own critical path is short and the formula's code stays small
+// (fully inlined formulas measured twice as slow there).
 H2B_DEV G1XyzzL xyzzl_dbl(const G1XyzzL& p)
 {
     if (is_inf(p) || fl_is_zero_mod(p.Y)) return xyzzl_inf();
     const FqL U = fl_add(p.Y, p.Y);
-    const FqL V = sqr29(U);
-    const FqL xx = sqr29(p.X);
-    const FqL W = mul29(U, V);
-    const FqL S = mul29(p.X, V);
+    const FqL V = fl_sqr_ilp(U);
+    const FqL xx = fl_sqr_ilp(p.X);
+    const FqL W = fl_mul_ilp(U, V);
+    const FqL S = fl_mul_ilp(p.X, V);
     const FqL M = fl_add(fl_add(xx, xx), xx);
     G1XyzzL r;
-    r.ZZ = mul29(V, p.ZZ);
-    r.ZZZ = mul29(W, p.ZZZ);
-    r.X = fl_sub(sqr29(M), fl_add(S, S));
-    r.Y = fl_sub(mul29(M, fl_sub(S, r.X)), mul29(W, p.Y));
+    r.ZZ = fl_mul_ilp(V, p.ZZ);
+    r.ZZZ = fl_mul_ilp(W, p.ZZZ);
+    r.X = fl_sub(fl_sqr_ilp(M), fl_add(S, S));
+    r.Y = fl_sub(fl_mul_ilp(M, fl_sub(S, r.X)), fl_mul_ilp(W, p.Y));
     return r;
 }
 
@@ -266,27 +267,27 @@ H2B_DEV void xyzzl_add(G1XyzzL& acc, const G1XyzzL& q)
 {
     if (is_inf(q)) return;
     if (is_inf(acc)) { acc = q; return; }
-    const FqL U1 = mul29(acc.X, q.ZZ);
-    const FqL U2 = mul29(q.X, acc.ZZ);
-    const FqL S1 = mul29(acc.Y, q.ZZZ);
-    const FqL S2 = mul29(q.Y, acc.ZZZ);
+    const FqL U1 = fl_mul_ilp(acc.X, q.ZZ);
+    const FqL U2 = fl_mul_ilp(q.X, acc.ZZ);
+    const FqL S1 = fl_mul_ilp(acc.Y, q.ZZZ);
+    const FqL S2 = fl_mul_ilp(q.Y, acc.ZZZ);
     const FqL P = fl_sub(U2, U1);
     const FqL R = fl_sub(S2, S1);
     if (fl_is_zero_mod(P)) {
         acc = fl_is_zero_mod(R) ? xyzzl_dbl(acc) : xyzzl_inf();
         return;
     }
-    const FqL PP = sqr29(P);
-    const FqL RR = sqr29(R);
-    const FqL zz = mul29(acc.ZZ, q.ZZ);
-    const FqL zzz = mul29(acc.ZZZ, q.ZZZ);
-    const FqL PPP = mul29(P, PP);
-    const FqL Q = mul29(U1, PP);
+    const FqL PP = fl_sqr_ilp(P);
+    const FqL RR = fl_sqr_ilp(R);
+    const FqL zz = fl_mul_ilp(acc.ZZ, q.ZZ);
+    const FqL zzz = fl_mul_ilp(acc.ZZZ, q.ZZZ);
+    const FqL PPP = fl_mul_ilp(P, PP);
+    const FqL Q = fl_mul_ilp(U1, PP);
     const FqL X3 = fl_sub(fl_sub(RR, PPP), fl_add(Q, Q));
-    acc.Y = fl_sub(mul29(R, fl_sub(Q, X3)), mul29(S1, PPP));
+    acc.Y = fl_sub(fl_mul_ilp(R, fl_sub(Q, X3)), fl_mul_ilp(S1, PPP));
     acc.X = X3;
-    acc.ZZ = mul29(zz, PP);
-    acc.ZZZ = mul29(zzz, PPP);
+    acc.ZZ = fl_mul_ilp(zz, PP);
+    acc.ZZZ = fl_mul_ilp(zzz, PPP);
 }
 
 H2B_DEV G1Affine affine_neg(const G1Affine& p)

@@ -47,6 +47,18 @@ static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
 
 static int g_msm_window_override = 0;
 static int g_msm_acc_variant = 0;  // call structure of the accumulation kernel (0, 1, 2)
+static int g_msm_pair_rounds = 0;  // batch-affine pairing rounds before the XYZZ accumulation (0..3)
+constexpr int PR_T = 128;          // pairing rounds: threads per CTA
+constexpr int PR_E = 8;            // pairing rounds: input entries per thread (at most 4 additions)
+static uint64_t pr_ctas(uint64_t entries) { return (entries + (uint64_t)PR_T * PR_E - 1) / ((uint64_t)PR_T * PR_E); }
+
+uint64_t fq_batch_invert_scratch(uint64_t n);
+RustError fq_batch_invert(Fq* d, uint64_t n, void* scratch, uint64_t scratch_bytes, cudaStream_t st);
+
+void msm_set_pair_rounds(int rounds)
+{
+    if (rounds >= 0 && rounds <= 3) g_msm_pair_rounds = rounds;
+}
 static int g_msm_chunk_override = 0;
 
 void msm_set_tuning(int window_bits, int chunk)
@@ -79,7 +91,13 @@ MsmPlan msm_plan(uint64_t n)
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 128u;
     p.nv = 2 * n;
     p.max_entries = p.nv * (uint64_t)p.W;
-    p.max_chunks = (p.max_entries + p.K - 1) / p.K + 1;
+    // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
+    p.R = g_msm_pair_rounds;
+    p.cap[0] = p.max_entries;
+    for (int r = 1; r <= 3; r++) p.cap[r] = p.cap[r - 1] / 2 + p.NB / 2 + 1;
+    p.Kf = p.R > 0 ? std::max<uint32_t>(8u, p.K >> p.R) : p.K;
+    const uint64_t final_entries = p.cap[p.R];
+    p.max_chunks = (final_entries + p.Kf - 1) / p.Kf + 1;
     // segments per window for the running-sum reduction (L buckets each)
     uint32_t L = p.H >= 256 ? 8u : (p.H >= 4 ? 4u : 1u);
     p.L = L;
@@ -87,7 +105,7 @@ MsmPlan msm_plan(uint64_t n)
     p.S = p.H / L;
     p.NBITS = p.S > 1 ? 31 - __builtin_clz(p.S) : 0;
     // a bucket spanning more than DENSE_LIMIT chunks holds > DENSE_LIMIT*K entries
-    p.max_dense = p.max_entries / ((uint64_t)DENSE_LIMIT * p.K) + 1;
+    p.max_dense = final_entries / ((uint64_t)DENSE_LIMIT * p.Kf) + 1;
     return p;
 }
 
@@ -110,6 +128,18 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
     sp.add_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));  // per-bit sums
     sp.add_n<G1Xyzz>(p.W);                            // window sums
     sp.add_n<G1Jac>(1);                               // result
+    if (p.R >= 1) sp.add_n<G1Affine>(p.cap[1]);       // round outputs 1, 3
+    if (p.R >= 2) sp.add_n<G1Affine>(p.cap[2]);       // round output 2
+    for (int r = 0; r < p.R; r++) sp.add_n<uint32_t>(p.NB + 1);  // round offsets
+    if (p.R >= 1) {                                   // sized for round 1, reused by later rounds
+        const uint64_t ctas = pr_ctas(p.cap[0]);
+        sp.add_n<Fq>(ctas * PR_T * 4);                // denominator prefixes
+        sp.add_n<uint2>(ctas * PR_T * 4);             // jobs
+        sp.add_n<uint32_t>(ctas * PR_T);              // jobs per thread
+        sp.add_n<Fq>(ctas * 2 * PR_T);                // product trees
+        sp.add_n<Fq>(ctas);                           // CTA totals
+        sp.add(fq_batch_invert_scratch(ctas));
+    }
 }
 
 MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host)
@@ -132,6 +162,21 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
     s.bits = ar.take_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));
     s.wins = ar.take_n<G1Xyzz>(p.W);
     s.result = ar.take_n<G1Jac>(1);
+    s.pts[0] = p.R >= 1 ? ar.take_n<G1Affine>(p.cap[1]) : nullptr;
+    s.pts[1] = p.R >= 2 ? ar.take_n<G1Affine>(p.cap[2]) : nullptr;
+    for (int r = 0; r < 3; r++) s.roff[r] = r < p.R ? ar.take_n<uint32_t>(p.NB + 1) : nullptr;
+    s.pr_pref = nullptr; s.pr_job = nullptr; s.pr_nj = nullptr; s.pr_tree = nullptr; s.pr_tot = nullptr;
+    s.pr_inv_scratch = nullptr; s.pr_inv_bytes = 0;
+    if (p.R >= 1) {
+        const uint64_t ctas = pr_ctas(p.cap[0]);
+        s.pr_pref = ar.take_n<Fq>(ctas * PR_T * 4);
+        s.pr_job = ar.take_n<uint2>(ctas * PR_T * 4);
+        s.pr_nj = ar.take_n<uint32_t>(ctas * PR_T);
+        s.pr_tree = ar.take_n<Fq>(ctas * 2 * PR_T);
+        s.pr_tot = ar.take_n<Fq>(ctas);
+        s.pr_inv_bytes = fq_batch_invert_scratch(ctas);
+        s.pr_inv_scratch = ar.take(s.pr_inv_bytes);
+    }
     return s;
 }
 
@@ -200,7 +245,9 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int
 
 // One thread per chunk of K sorted entries; the running bucket sum stays in
 // 29-bit limb form and is packed to the canonical 8 x 32 image when stored.
-template <int MODE>
+// PTS: the entries are the affine points themselves (bases[e]), as left by
+// the pairing rounds, instead of signed (GLV) indices into the bases.
+template <int MODE, bool PTS>
 __global__ void __launch_bounds__(128, MODE == 1 ? 2 : 3) k_msm_accumulate(const uint32_t* __restrict__ sorted,
                                                         const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
                                                         const G1Affine* __restrict__ bases, G1Xyzz* __restrict__ buckets,
@@ -228,6 +275,12 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : 3) k_msm_accumulate(const
                 head = false;
                 do { b++; next = offsets[b + 1]; } while (next == e);
             }
+            if (PTS) {  // contiguous affine points left by the pairing rounds
+                const G1Affine P = ld_affine(&bases[e]);
+                if (is_inf(P)) continue;
+                xyzzl_madd<MODE>(acc, to_l(P.x), to_l(P.y));
+                continue;
+            }
             const uint32_t ent = sorted[e];
             const uint32_t v = ent & ~SIGN_BIT;
             G1Affine P = ld_affine(&bases[v >> 1]);
@@ -239,6 +292,192 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : 3) k_msm_accumulate(const
         }
         if (head) st_xyzz(&heads[t], xyzzl_to(acc)); else st_xyzz(&buckets[b], xyzzl_to(acc));
     }
+}
+
+// ---- pairing rounds (batch-affine bucket additions) -----------------------
+// Round r adds the points of every bucket pairwise in affine coordinates:
+// entries (2j, 2j+1) of a bucket become output point j (an odd last entry is
+// copied), so each round halves every bucket.  lambda = (y2 - y1) / (x2 - x1)
+// (or 3 x1^2 / (2 y1) for equal points) needs one inversion per addition; all
+// denominators share inversions through Montgomery's trick, so an addition
+// costs about 6 products against 10 for an XYZZ mixed addition, and the
+// additions of a thread are independent of each other.  Infinity inputs pass
+// the other point through; P + (-P) gives infinity, written as (0, 0) like an
+// input base.  A round is three launches: forward products with a product
+// tree per CTA, one batch inversion of all CTA totals, backward pass.  (An
+// inversion inside each CTA would put a long serial binary GCD behind every
+// 512 additions.)
+
+__device__ __forceinline__ void st_affine(G1Affine* p, const G1Affine& a)
+{
+    st(&p->x, a.x);
+    st(&p->y, a.y);
+}
+
+template <bool FIRST>
+__device__ __forceinline__ G1Affine pr_load(const uint32_t* __restrict__ sorted, const G1Affine* __restrict__ src,
+                                            uint32_t e)
+{
+    if (!FIRST) return ld_affine(&src[e]);
+    const uint32_t ent = sorted[e];
+    const uint32_t v = ent & ~SIGN_BIT;
+    G1Affine P = ld_affine(&src[v >> 1]);
+    if (is_inf(P)) return P;
+    if (v & 1u) P.x = P.x * glv::beta();  // phi(P)
+    if (ent & SIGN_BIT) P.y = fneg(P.y);
+    return P;
+}
+
+// Denominator and numerator of lambda for P1 + P2 (both finite, P2 != -P1).
+__device__ __forceinline__ void pr_slope_terms(const G1Affine& P1, const G1Affine& P2, FqL& d, FqL& num)
+{
+    const FqL x1 = to_l(P1.x), y1 = to_l(P1.y);
+    if (P1.x != P2.x) {
+        d = fl_sub(to_l(P2.x), x1);
+        num = fl_sub(to_l(P2.y), y1);
+    } else {
+        d = fl_add(y1, y1);
+        const FqL xx = fl_sqr(x1);
+        num = fl_add(fl_add(xx, xx), xx);
+    }
+}
+
+// Forward half.  A thread owns PR_E input entries; every entry at an even
+// position of its bucket starts an addition with the next entry (at most 4
+// per thread).  Running products of the denominators go to g_pref, the jobs
+// to g_job / g_nj, the CTA's product tree over the thread totals to g_tree
+// (nodes 1 .. 2T-1) and its root to g_tot[cta].  CTAs past the last entry
+// only set g_tot[cta] = 1.
+template <bool FIRST>
+__global__ void __launch_bounds__(PR_T) k_msm_pair_fwd(const uint32_t* __restrict__ sorted,
+                                                       const G1Affine* __restrict__ src,
+                                                       const uint32_t* __restrict__ in_off, uint64_t NB,
+                                                       const uint32_t* __restrict__ out_off,
+                                                       G1Affine* __restrict__ out_pts, Fq* __restrict__ g_pref,
+                                                       uint2* __restrict__ g_job, uint32_t* __restrict__ g_nj,
+                                                       Fq* __restrict__ g_tree, Fq* __restrict__ g_tot)
+{
+    __shared__ FqL tree[2 * PR_T];
+    const int t = threadIdx.x;
+    const uint32_t M = in_off[NB];
+    const uint64_t cta = blockIdx.x;
+    const uint64_t cta_start = cta * PR_T * PR_E;
+    if (cta_start >= M) {
+        if (t == 0) st(&g_tot[cta], Fq::one());
+        return;  // the whole CTA leaves before any barrier
+    }
+    const uint64_t gt = cta * PR_T + t;
+    const uint64_t s64 = cta_start + (uint64_t)t * PR_E;
+    uint32_t nj = 0;
+    FqL acc = to_l(Fq::one());
+    if (s64 < M) {
+        const uint32_t s = (uint32_t)s64;
+        const uint32_t end = (s64 + PR_E < M) ? s + PR_E : M;
+        uint64_t lo = 0, hi = NB;  // in_off[lo] <= s < in_off[hi]
+        while (hi - lo > 1) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (in_off[mid] <= s) lo = mid; else hi = mid;
+        }
+        uint64_t b = lo;
+        uint32_t bstart = in_off[b], bnext = in_off[b + 1];
+        for (uint32_t e = s; e < end; e++) {
+            while (e >= bnext) { b++; bstart = bnext; bnext = in_off[b + 1]; }
+            const uint32_t local = e - bstart;
+            if (local & 1u) continue;
+            const uint32_t o = out_off[b] + (local >> 1);
+            const G1Affine P1 = pr_load<FIRST>(sorted, src, e);
+            if (e + 1 >= bnext) { st_affine(&out_pts[o], P1); continue; }
+            const G1Affine P2 = pr_load<FIRST>(sorted, src, e + 1);
+            if (is_inf(P1) || is_inf(P2)) { st_affine(&out_pts[o], is_inf(P1) ? P2 : P1); continue; }
+            if (P1.x == P2.x && P1.y != P2.y) {  // P2 = -P1
+                G1Affine z;
+                z.x = Fq::zero(); z.y = Fq::zero();
+                st_affine(&out_pts[o], z);
+                continue;
+            }
+            FqL d, num;
+            pr_slope_terms(P1, P2, d, num);
+            acc = nj == 0 ? d : fl_mul(acc, d);
+            st(&g_pref[gt * 4 + nj], from_l(acc));
+            g_job[gt * 4 + nj] = make_uint2(e, o);
+            nj++;
+        }
+    }
+    g_nj[gt] = nj;
+    tree[PR_T + t] = acc;
+    __syncthreads();
+    for (int w = PR_T / 2; w >= 1; w >>= 1) {
+        if (t < w) tree[w + t] = fl_mul(tree[2 * (w + t)], tree[2 * (w + t) + 1]);
+        __syncthreads();
+    }
+    for (int i = t + 1; i < 2 * PR_T; i += PR_T) st(&g_tree[cta * 2 * PR_T + i], from_l(tree[i]));
+    if (t == 0) st(&g_tot[cta], from_l(tree[1]));
+}
+
+// Backward half: the inverted CTA total (g_tot[cta]) goes down the stored
+// tree to every thread, which walks its jobs in reverse, recovers each
+// denominator's inverse from its prefix, and writes P1 + P2.
+template <bool FIRST>
+__global__ void __launch_bounds__(PR_T) k_msm_pair_bwd(const uint32_t* __restrict__ sorted,
+                                                       const G1Affine* __restrict__ src,
+                                                       const uint32_t* __restrict__ in_off, uint64_t NB,
+                                                       G1Affine* __restrict__ out_pts, const Fq* __restrict__ g_pref,
+                                                       const uint2* __restrict__ g_job,
+                                                       const uint32_t* __restrict__ g_nj,
+                                                       const Fq* __restrict__ g_tree, const Fq* __restrict__ g_tot)
+{
+    __shared__ FqL tree[2 * PR_T];
+    const int t = threadIdx.x;
+    const uint32_t M = in_off[NB];
+    const uint64_t cta = blockIdx.x;
+    if (cta * PR_T * PR_E >= M) return;  // the whole CTA
+    const uint64_t gt = cta * PR_T + t;
+    for (int i = t + 1; i < 2 * PR_T; i += PR_T) tree[i] = to_l(ld(&g_tree[cta * 2 * PR_T + i]));
+    __syncthreads();
+    if (t == 0) tree[1] = to_l(ld(&g_tot[cta]));
+    __syncthreads();
+    for (int w = 1; w < PR_T; w <<= 1) {
+        if (t < w) {
+            const int k = w + t;
+            const FqL inv = tree[k], l = tree[2 * k], r = tree[2 * k + 1];
+            const Fl2<FqCfg> lr = fl_mul2(inv, r, inv, l);
+            tree[2 * k] = lr.a;
+            tree[2 * k + 1] = lr.b;
+        }
+        __syncthreads();
+    }
+    FqL inv = tree[PR_T + t];
+    const int nj = (int)g_nj[gt];
+    for (int k = nj - 1; k >= 0; k--) {
+        const uint2 job = g_job[gt * 4 + k];
+        const G1Affine P1 = pr_load<FIRST>(sorted, src, job.x);
+        const G1Affine P2 = pr_load<FIRST>(sorted, src, job.x + 1);
+        FqL d, num;
+        pr_slope_terms(P1, P2, d, num);
+        FqL inv_d;
+        if (k > 0) {
+            const Fl2<FqCfg> r = fl_mul2(inv, to_l(ld(&g_pref[gt * 4 + k - 1])), inv, d);
+            inv_d = r.a;
+            inv = r.b;
+        } else {
+            inv_d = inv;
+        }
+        const FqL x1 = to_l(P1.x), y1 = to_l(P1.y);
+        const FqL lam = fl_mul(num, inv_d);
+        const FqL x3 = fl_sub(fl_sub(fl_sqr(lam), x1), to_l(P2.x));
+        const FqL y3 = fl_sub(fl_mul(lam, fl_sub(x1, x3)), y1);
+        G1Affine R;
+        R.x = from_l(x3);
+        R.y = from_l(y3);
+        st_affine(&out_pts[job.y], R);
+    }
+}
+
+// Per-bucket entry counts after a pairing round: ceil(count / 2).
+__global__ void k_msm_half_counts(const uint32_t* __restrict__ in_off, uint64_t NB, uint32_t* __restrict__ out_cnt)
+{
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < NB; b += (uint64_t)gridDim.x * blockDim.x)
+        out_cnt[b] = (in_off[b + 1] - in_off[b] + 1) >> 1;
 }
 
 __global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K, G1Xyzz* __restrict__ buckets,
@@ -440,21 +679,51 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.cursor, s.sorted);
     H2B_LAUNCHED("k_msm_sort<scatter>");
-    uint64_t chunks = (p.max_entries + p.K - 1) / p.K;
     prof_begin(PROF_MSM_ACCUMULATE, st);
+    // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
+    const uint32_t* off = s.offsets;
+    const G1Affine* src = d_bases;
+    for (int r = 1; r <= p.R; r++) {
+        k_msm_half_counts<<<grid_for(p.NB, 256, sm_cap), 256, 0, st>>>(off, p.NB, s.counts);
+        H2B_LAUNCHED("k_msm_half_counts");
+        H2B_CUDA(scan_u32(s.counts, p.NB, s.roff[r - 1], s.scan_tmp, st));
+        G1Affine* dst = s.pts[(r - 1) & 1];
+        const uint64_t ctas = pr_ctas(p.cap[r - 1]);
+        const uint32_t* srt = r == 1 ? s.sorted : nullptr;
+        if (r == 1)
+            k_msm_pair_fwd<true><<<(unsigned)ctas, PR_T, 0, st>>>(srt, src, off, p.NB, s.roff[0], dst, s.pr_pref,
+                                                                  s.pr_job, s.pr_nj, s.pr_tree, s.pr_tot);
+        else
+            k_msm_pair_fwd<false><<<(unsigned)ctas, PR_T, 0, st>>>(srt, src, off, p.NB, s.roff[r - 1], dst,
+                                                                   s.pr_pref, s.pr_job, s.pr_nj, s.pr_tree, s.pr_tot);
+        H2B_LAUNCHED("k_msm_pair_fwd");
+        H2B_TRY(fq_batch_invert(s.pr_tot, ctas, s.pr_inv_scratch, s.pr_inv_bytes, st));
+        if (r == 1)
+            k_msm_pair_bwd<true><<<(unsigned)ctas, PR_T, 0, st>>>(srt, src, off, p.NB, dst, s.pr_pref, s.pr_job,
+                                                                  s.pr_nj, s.pr_tree, s.pr_tot);
+        else
+            k_msm_pair_bwd<false><<<(unsigned)ctas, PR_T, 0, st>>>(srt, src, off, p.NB, dst, s.pr_pref, s.pr_job,
+                                                                   s.pr_nj, s.pr_tree, s.pr_tot);
+        H2B_LAUNCHED("k_msm_pair_bwd");
+        off = s.roff[r - 1];
+        src = dst;
+    }
+    const uint64_t chunks = (p.cap[p.R] + p.Kf - 1) / p.Kf;
     const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
-    if (g_msm_acc_variant == 1)
-        k_msm_accumulate<1><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
+    if (p.R > 0)
+        k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
+    else if (g_msm_acc_variant == 1)
+        k_msm_accumulate<1, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 2)
-        k_msm_accumulate<2><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
+        k_msm_accumulate<2, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else
-        k_msm_accumulate<0><<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.K, d_bases, s.buckets, s.heads);
+        k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     prof_end(PROF_MSM_ACCUMULATE, st);
     H2B_LAUNCHED("k_msm_accumulate");
-    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.K, s.buckets, s.heads, s.dense,
+    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(off, p.NB, p.Kf, s.buckets, s.heads, s.dense,
                                                             p.max_dense);
     H2B_LAUNCHED("k_msm_fixup");
-    k_msm_dense_pieces<<<148 * 4, 256, 0, st>>>(s.offsets, p.max_dense, p.K, s.heads, s.dense, s.pieces);
+    k_msm_dense_pieces<<<148 * 4, 256, 0, st>>>(off, p.max_dense, p.Kf, s.heads, s.dense, s.pieces);
     H2B_LAUNCHED("k_msm_dense_pieces");
     k_msm_dense_merge<<<148, DENSE_PIECES, 0, st>>>(p.max_dense, s.buckets, s.dense, s.pieces);
     H2B_LAUNCHED("k_msm_dense_merge");
@@ -578,6 +847,14 @@ extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
     if (v >= 0 && v <= 2) g_msm_acc_variant = v;
 }
+
+// Batch-affine pairing rounds run before the XYZZ bucket accumulation
+// (0..3).  Default 0: on B200 a pairing addition (forward pass, shared
+// inversion, backward pass) measured about 0.5 ns per addition against
+// 0.3 ns for an XYZZ mixed addition (2^20 points, witness scalar mix).
+// Results are identical; speed and the workspace size differ (the
+// workspace-size queries follow this setting).
+extern "C" void h2b_msm_set_pair_rounds(int rounds) { msm_set_pair_rounds(rounds); }
 
 // Number of nonzero signed window digits (= sorted entries = bucket
 // additions) the MSM of these scalars performs; written to *d_count (u64).

@@ -22,6 +22,9 @@ struct MsmPlan {
     uint32_t S;      // segments per window
     int NBITS;       // log2(S)
     uint64_t max_dense;  // capacity of the dense-bucket list
+    int R;               // pairing rounds before the XYZZ accumulation
+    uint64_t cap[4];     // entry capacity after round r (cap[0] = max_entries)
+    uint32_t Kf;         // entries per XYZZ accumulation chunk after the rounds
 };
 
 struct MsmScratch {
@@ -42,6 +45,15 @@ struct MsmScratch {
     G1Xyzz* bits;
     G1Xyzz* wins;
     G1Jac* result;
+    G1Affine* pts[2];    // pairing-round outputs (ping-pong)
+    uint32_t* roff[3];   // per-round bucket offsets (NB + 1 each)
+    Fq* pr_pref;         // pairing rounds: per-job denominator prefixes
+    uint2* pr_job;       // pairing rounds: per-job (input entry, output slot)
+    uint32_t* pr_nj;     // pairing rounds: jobs per thread
+    Fq* pr_tree;         // pairing rounds: per-CTA product trees
+    Fq* pr_tot;          // pairing rounds: per-CTA totals (inverted in place)
+    void* pr_inv_scratch;
+    uint64_t pr_inv_bytes;
 };
 
 MsmPlan msm_plan(uint64_t n);
@@ -50,5 +62,6 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
 RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases,
                   cudaStream_t st);
 void msm_set_tuning(int window_bits, int chunk);
+void msm_set_pair_rounds(int rounds);
 
 } // namespace h2b

@@ -174,7 +174,7 @@ static void plan_batch_invert(ScratchPlan& p, uint64_t n)
 
 // Multi-level: tile totals -> recurse -> apply with the inverted totals.
 template <class C>
-static RustError batch_invert_levels(Fp<C>* d, uint64_t n, ScratchArena& ar, cudaStream_t st)
+static RustError batch_invert_levels(Fp<C>* d, uint64_t n, ScratchArena& ar, cudaStream_t st, bool prof = true)
 {
     if (n <= BI_TILE) return batch_invert_local<C>(d, n, st);
     uint64_t nt = tiles_of(n);
@@ -182,13 +182,28 @@ static RustError batch_invert_levels(Fp<C>* d, uint64_t n, ScratchArena& ar, cud
     if (!ar.good()) return err(cudaErrorInvalidValue, "batch_invert: scratch too small");
     k_tile_product<C><<<(unsigned)nt, BI_T, 0, st>>>(d, n, tot);
     H2B_LAUNCHED("k_tile_product");
-    H2B_TRY(batch_invert_levels<C>(tot, nt, ar, st));
+    H2B_TRY(batch_invert_levels<C>(tot, nt, ar, st, prof));
     enable_big_smem(k_batch_invert<C>);
-    prof_begin(PROF_BATCH_INVERT, st);
+    if (prof) prof_begin(PROF_BATCH_INVERT, st);
     k_batch_invert<C><<<(unsigned)nt, BI_T, BI_SMEM, st>>>(d, n, tot);
-    prof_end(PROF_BATCH_INVERT, st);
+    if (prof) prof_end(PROF_BATCH_INVERT, st);
     H2B_LAUNCHED("k_batch_invert");
     return ok();
+}
+
+// In-place Fq batch inversion for other kernels of this library (the MSM's
+// pairing rounds): zeros stay zero; scratch from fq_batch_invert_scratch().
+uint64_t fq_batch_invert_scratch(uint64_t n)
+{
+    ScratchPlan p;
+    plan_batch_invert(p, n);
+    return p.used;
+}
+
+RustError fq_batch_invert(Fq* d, uint64_t n, void* scratch, uint64_t scratch_bytes, cudaStream_t st)
+{
+    ScratchArena ar(scratch, scratch_bytes);
+    return batch_invert_levels<FqCfg>(d, n, ar, st, false);
 }
 
 // ---------------------------------------------------------------------------

@@ -307,6 +307,9 @@ void h2b_msm_set_tuning(int window_bits, int chunk);
 /* Call structure of the MSM bucket-accumulation kernel: 0 = two field products per out-of-line call
  * (default), 1 = all products inline, 2 = one product per call.  Same results; tuning only. */
 void h2b_msm_set_accumulate_variant(int variant);
+/* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
+ * MSM workspace-size queries depend on it (set it before sizing scratch). */
+void h2b_msm_set_pair_rounds(int rounds);
 /* Batch inversion whose CTAs share a single inversion through scratch
  * (h2b_batch_invert_workspace_size bytes); same semantics as _halo2_batch_invert. */
 uint64_t h2b_batch_invert_workspace_size(uint64_t length);
