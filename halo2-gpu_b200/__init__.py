@@ -33,6 +33,11 @@ class FFITraitObject(ctypes.Structure):
     _fields_ = [("ptr", ctypes.c_void_p)]
 
 
+class AssignedLayout(ctypes.Structure):
+    """Byte layout of the Rust Assigned<F> records (culib.rs:22-26)."""
+    _fields_ = [("stride_bytes", ctypes.c_uint32), ("num_offset", ctypes.c_uint32), ("denom_offset", ctypes.c_uint32)]
+
+
 class Halo2GpuError(RuntimeError):
     def __init__(self, code, message, who):
         super().__init__(f"{who}: code {code}: {message}")
@@ -79,6 +84,19 @@ _SIGS = {
     "_halo2_poly_sub_scalar_at_zero": (RustError, [_vp, _vp, _vp]),
     "_halo2_extended_from_lagrange_vec_device": (RustError, [_vp, _vp, _u32, _u64, _vp]),
     "_halo2_distribute_powers_zeta": (RustError, [_vp, _vp, _u32, _u64, _vp]),
+    "_halo2_eval_polynomial_workspace_size": (_u64, [_u64]),
+    "_halo2_eval_polynomial": (RustError, [_vp, _ffi, ctypes.POINTER(ctypes.c_void_p), _u64, _vp, _u64, _vp]),
+    "_halo2_eval_poly_batch_max_len": (_u64, [_u64, _u64, _u64]),
+    "_halo2_eval_polynomial_batch_workspace_size": (_u64, [_u64, _u64]),
+    "_halo2_eval_polynomial_batch": (RustError, [_ffi, _ffi, _ffi, _u64, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_kate_division_workspace_size": (_u64, [_u64]),
+    "_halo2_kate_division_device": (RustError, [_vp, _vp, _vp, _u64, _vp, _u64, _vp]),
+    "_halo2_kate_division_device_padded": (RustError, [_vp, _vp, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "_halo2_multiopen_poly_max_len": (_u64, [_u64, _u64, _u64]),
+    "_halo2_multiopen_poly_calculation_workspace_size": (_u64, [_u64, _u64]),
+    "_halo2_multiopen_poly_calculation": (RustError, [_ffi, _ffi, _u64, _u64, _u64, _ffi, _ffi, _ffi, _vp, _u64,
+                                                      _vp]),
+    "_halo2_decode_assigned": (RustError, [_vp, _vp, _vp, _u64, AssignedLayout, _vp]),
     "_halo2_fft_normal_workspace_size": (_u64, [_u32, _u32, _u32]),
     "_halo2_fft_normal": (RustError, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _u64, _vp]),
     "_halo2_fft_normal_check_memory": (_b, [_u32, _vp, _u32, _u32]),
@@ -330,6 +348,67 @@ def cosetfft(log_n, extend_log_n, values, extended_omega, stream=None):
     call("_halo2_cosetfft", NTT_COSET, log_n, extend_log_n, inp.ctypes.data, out.ctypes.data, om.ctypes.data,
          one.ctypes.data, ptr(ws), ws.numel(), stream_handle(stream))
     return out
+
+
+# --- opening-phase polynomials (halo2_proofs/src/cuda/funcs/polynomial_ops.rs) ----
+
+def eval_polynomial_device(d_poly, n, point, stream=None):
+    """eval_polynomial_device (polynomial_ops.rs:441-480): sum_i poly[i] point^i, result read back."""
+    torch = _torch()
+    pt = _scalar_bytes(point)
+    ws = dev_empty(lib()._halo2_eval_polynomial_workspace_size(n))
+    res = ctypes.c_void_p()
+    call("_halo2_eval_polynomial", ptr(d_poly), ctypes.byref(host_ffi(pt)), ctypes.byref(res), n, ptr(ws),
+         ws.numel(), stream_handle(stream))
+    out = np.zeros(4, dtype=np.uint64)
+    torch.cuda.synchronize()
+    base = ws.data_ptr()
+    off = res.value - base
+    assert 0 <= off <= ws.numel() - 32, "result must lie inside the scratch"
+    out[:] = ws[off:off + 32].cpu().numpy().view(np.uint64)
+    return out
+
+
+def batch_eval_polynomial_gpu(polys, points, poly_offset, poly_length, stream=None):
+    """basic_batch_eval_polynomial_gpu (polynomial_ops.rs:32-70): host polys, chunk-local exponents."""
+    ps = [np.ascontiguousarray(p, dtype=np.uint64) for p in polys]
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.uint64).reshape(-1, 4))
+    res = np.zeros((len(ps), 4), dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_eval_polynomial_batch_workspace_size(poly_length, len(ps)))
+    call("_halo2_eval_polynomial_batch", ffi_array([p.ctypes.data for p in ps]), ctypes.byref(host_ffi(pts)),
+         ctypes.byref(host_ffi(res)), poly_offset, poly_length, len(ps), ptr(ws), ws.numel(), stream_handle(stream))
+    return res
+
+
+def kate_division_device(d_a, d_q, d_u, n, out_len=None, stream=None):
+    """kate_division_device (polynomial_ops.rs:541-583); out_len selects the padded entry."""
+    ws = dev_empty(lib()._halo2_kate_division_workspace_size(n))
+    if out_len is None:
+        call("_halo2_kate_division_device", ptr(d_a), ptr(d_q), ptr(d_u), n, ptr(ws), ws.numel(),
+             stream_handle(stream))
+    else:
+        call("_halo2_kate_division_device_padded", ptr(d_a), ptr(d_q), ptr(d_u), n, out_len, ptr(ws), ws.numel(),
+             stream_handle(stream))
+    return d_q
+
+
+def multiopen_poly_calculation(polys, acc, challenges, points, poly_offset, poly_length, stream=None):
+    """_halo2_multiopen_poly_calculation: evaluations of each chunk, and acc chunk = sum c_i * chunk_i."""
+    ps = [np.ascontiguousarray(p, dtype=np.uint64) for p in polys]
+    ch = np.ascontiguousarray(np.asarray(challenges, dtype=np.uint64).reshape(-1, 4))
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.uint64).reshape(-1, 4))
+    res = np.zeros((len(ps), 4), dtype=np.uint64)
+    ws = dev_empty(lib()._halo2_multiopen_poly_calculation_workspace_size(poly_length, len(ps)))
+    call("_halo2_multiopen_poly_calculation", ffi_array([p.ctypes.data for p in ps]), ctypes.byref(host_ffi(acc)),
+         poly_offset, poly_length, len(ps), ctypes.byref(host_ffi(ch)), ctypes.byref(host_ffi(pts)),
+         ctypes.byref(host_ffi(res)), ptr(ws), ws.numel(), stream_handle(stream))
+    return res
+
+
+def decode_assigned_device(d_nums, d_denoms, d_raw, n, stride_bytes, num_offset, denom_offset, stream=None):
+    """decode_assigned_to_num_denom_device (polynomial_ops.rs): Assigned<F> records -> (nums, denoms)."""
+    call("_halo2_decode_assigned", ptr(d_nums), ptr(d_denoms), ptr(d_raw), n,
+         AssignedLayout(stride_bytes, num_offset, denom_offset), stream_handle(stream))
 
 
 # --- twiddle tables (halo2_proofs/src/cuda/funcs/omega.rs) -----------------------

@@ -160,6 +160,55 @@ RustError _halo2_extended_from_lagrange_vec_device(void* d_out, const void* d_pa
 RustError _halo2_distribute_powers_zeta(void* d_a, const void* d_coset_powers, uint32_t coset_powers_len,
                                        uint64_t n, h2b_stream_t stream);
 
+/* ------------------------------------------------- opening and witness --- */
+
+/* culib.rs:231 ; polynomial/polynomial.cu:62-66 */
+uint64_t _halo2_eval_polynomial_workspace_size(uint64_t length);
+/* culib.rs:235-243 ; polynomial/polynomial.cu:68-90 -- sum_i d_poly[i] * point^i; host point; *d_result_out =
+ * device address of the 32-byte result (inside scratch); does not synchronise */
+RustError _halo2_eval_polynomial(const void* d_poly, const FFITraitObject* point, void** d_result_out,
+                                 uint64_t length, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:245-249 ; polynomial/polynomial.cu:135-146 */
+uint64_t _halo2_eval_poly_batch_max_len(uint64_t poly_length, uint64_t batch_size, uint64_t free_bytes);
+/* culib.rs:251 ; polynomial/polynomial.cu:148-154 */
+uint64_t _halo2_eval_polynomial_batch_workspace_size(uint64_t poly_length, uint64_t batch_size);
+/* culib.rs:254-264 ; polynomial/polynomial.cu:156-245 -- host polys (chunk [offset, offset + length), exponents
+ * counted from the chunk start), host points, host results; synchronises */
+RustError _halo2_eval_polynomial_batch(const FFITraitObject* poly_in_many, const FFITraitObject* eval_points,
+                                       const FFITraitObject* eval_result, uint64_t poly_offset, uint64_t poly_length,
+                                       uint64_t batch_size, void* scratch, uint64_t scratch_bytes,
+                                       h2b_stream_t stream);
+/* culib.rs:319 ; polynomial/kate_division.cu:27-36 */
+uint64_t _halo2_kate_division_workspace_size(uint64_t n);
+/* culib.rs:325-333 ; polynomial/kate_division.cu:47-125 -- d_q (n - 1) = (d_a - d_a(u)) / (X - u), all device */
+RustError _halo2_kate_division_device(const void* d_a, void* d_q, const void* d_u, uint64_t n, void* scratch,
+                                      uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:339-348 ; polynomial/kate_division.cu:127-250 -- quotient then zeros up to out_len */
+RustError _halo2_kate_division_device_padded(const void* d_a, void* d_q, const void* d_u, uint64_t n,
+                                             uint64_t out_len, void* scratch, uint64_t scratch_bytes,
+                                             h2b_stream_t stream);
+/* culib.rs:401-405 ; multiopen.cu:30-45 */
+uint64_t _halo2_multiopen_poly_max_len(uint64_t poly_length, uint64_t batch_size, uint64_t free_bytes);
+/* culib.rs:407-410 ; multiopen.cu:47-53 */
+uint64_t _halo2_multiopen_poly_calculation_workspace_size(uint64_t poly_length, uint64_t batch_size);
+/* culib.rs:414-426 ; multiopen.cu:76-175 -- host polys; evaluate_result[i] = chunk i at evaluate_point[i];
+ * host poly_acc chunk = sum_i challenge_point[i] * chunk i (overwritten); synchronises */
+RustError _halo2_multiopen_poly_calculation(const FFITraitObject* poly_in_many, const FFITraitObject* poly_acc,
+                                            uint64_t poly_offset, uint64_t poly_length, uint64_t batch_size,
+                                            const FFITraitObject* challenge_point,
+                                            const FFITraitObject* evaluate_point,
+                                            const FFITraitObject* evaluate_result, void* scratch,
+                                            uint64_t scratch_bytes, h2b_stream_t stream);
+/* culib.rs:22-26 -- the Rust-side layout of Assigned<F> records */
+typedef struct AssignedLayout {
+    uint32_t stride_bytes;
+    uint32_t num_offset;
+    uint32_t denom_offset;
+} AssignedLayout;
+/* culib.rs:301-308 ; polynomial/decode_assigned.cu:28-60 -- tag byte 0 Zero, 1 Trivial, 2 Rational */
+RustError _halo2_decode_assigned(void* d_nums, void* d_denoms, const void* d_raw, uint64_t n, AssignedLayout layout,
+                                 h2b_stream_t stream);
+
 /* ------------------------------------------------------------------ NTT --- */
 /* ntt_type: 1 FFT, 2 iFFT, 3 cosetFFT, 4 icosetFFT, 5 unsupported, 6 CosetFFT_Part (ntt.cu:21-28);
  * for CosetFFT_Part the divisor slot carries the coset factor zeta * w_ext^j (domain.rs:527-540). */

@@ -126,3 +126,41 @@ def test_msm_kzg_property_k22(h2b, orc, cuda):
     for i in range(4):
         p = orc.g1_mul(f.fr_mont_limbs([pow(tau, i, f.R_MOD)]), orc.g1_generator())
         assert_limbs_equal(srs[i], p[:8], f"srs[{i}]")
+
+
+@pytest.mark.parametrize("rounds", [1, 2, 3])
+def test_msm_pairing_rounds(h2b, orc, cuda, srs_small, rounds):
+    """The batch-affine pairing rounds (h2b_msm_set_pair_rounds, off by
+    default) give the same bytes: uniform scalars, zeros, infinity bases,
+    equal points in a bucket (doubling), P + (-P), a dense constant and the
+    witness-like mix."""
+    f = h2b.fields
+    _, srs = srs_small
+    n = 4096
+    L = h2b.lib()
+    L.h2b_msm_set_pair_rounds(rounds)
+    try:
+        cases = []
+        sc = orc.chacha_fr(90 + rounds, n)
+        b = srs[:n].copy()
+        sc[::5] = 0
+        b[::7] = 0
+        cases.append((sc, b))
+        b2 = srs[:n].copy()
+        b2[1::2] = b2[0::2]                      # equal points -> doubling in the pair formula
+        cases.append((np.tile(f.fr_mont_limbs([5, 5]), (n // 2, 1)), b2))
+        cases.append((np.tile(f.fr_mont_limbs([5, f.R_MOD - 5]), (n // 2, 1)), b2))  # P + (-P)
+        sc4 = orc.chacha_fr(95, n)
+        sc4[: n // 2] = f.fr_mont_limbs([0x022B5F6A3C1D0E8F94D049BB133111EBBF58476D1CE4E5B99E3779B97F4A7C15])
+        cases.append((sc4, srs[:n]))
+        mix = f.fr_mont_limbs([v % f.R_MOD for v in ([0x1F2E3D4C5B6A7988 * (i + 1) for i in range(n // 4)] +
+                                                     [i % 2 for i in range(n // 4)] +
+                                                     [f.limbs_to_ints(orc.chacha_fr(96, n // 2))[i] for i in
+                                                      range(n // 2)])])
+        cases.append((mix, srs[:n]))
+        for sc_, b_ in cases:
+            want = orc.msm(sc_, b_)
+            for got in all_variants(h2b, sc_, b_):
+                assert_limbs_equal(got, want, f"pairing rounds {rounds}")
+    finally:
+        L.h2b_msm_set_pair_rounds(0)

@@ -1,0 +1,142 @@
+"""Opening-phase kernels against the oracle and Python integers: Horner
+evaluation (halo2_proofs/src/poly/domain.rs eval tests, polynomial_ops.rs
+eval_polynomial_gpu), Kate division q = (a - a(u)) / (X - u)
+(kate_division.cu; checked directly for small n and by the identity
+q(x)(x - u) = a(x) - a(u) at a random x for large n), the multiopen
+calculation (multiopen.cu) and the Assigned<F> decode (decode_assigned.cu)."""
+import numpy as np
+import pytest
+
+from conftest import assert_limbs_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def _ints(f, limbs):
+    return [f.from_mont(x) for x in f.limbs_to_ints(limbs)]
+
+
+def _synthetic_division(a, u, p):
+    """q_{n-2} = a_{n-1}; q_{j-1} = a_j + u q_j (Python integers)."""
+    n = len(a)
+    q = [0] * (n - 1)
+    acc = 0
+    for j in range(n - 1, 0, -1):
+        acc = (a[j] + u * acc) % p
+        q[j - 1] = acc
+    return q
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 4095, 4096, 4097, 100003, 1 << 20])
+def test_eval_polynomial(h2b, orc, cuda, n):
+    f = h2b.fields
+    a = orc.chacha_fr(700 + n % 97, n)
+    for z in (0, 1, 0x1234567890ABCDEF1122334455667788):
+        zl = f.fr_mont_limbs([z])
+        got = h2b.eval_polynomial_device(h2b.to_dev(a), n, zl)
+        assert_limbs_equal(got.reshape(1, 4), orc.fr_eval(a, zl), f"eval n={n} z={z}")
+
+
+def test_eval_polynomial_batch_chunks(h2b, orc, cuda):
+    f = h2b.fields
+    n = 5000
+    polys = [orc.chacha_fr(800 + i, n) for i in range(3)]
+    pts = f.fr_mont_limbs([3, 0xDEADBEEF, f.R_MOD - 2])
+    for off, ln in ((0, n), (1000, 2345), (4999, 1)):
+        got = h2b.batch_eval_polynomial_gpu(polys, pts, off, ln)
+        for i in range(3):
+            assert_limbs_equal(got[i:i + 1], orc.fr_eval(polys[i][off:off + ln], pts[i:i + 1]), f"batch {off},{ln}")
+
+
+@pytest.mark.parametrize("n", [2, 3, 9, 2048, 2049, 2050, 5001])
+def test_kate_division_small(h2b, orc, cuda, n):
+    f = h2b.fields
+    p = f.R_MOD
+    a = orc.chacha_fr(900 + n, n)
+    for u in (0, 5, 0xABCDEF0123456789ABCDEF):
+        want = _synthetic_division(_ints(f, a), u, p)
+        d_q = h2b.dev_empty(32 * (n - 1))
+        h2b.kate_division_device(h2b.to_dev(a), d_q, h2b.to_dev(f.fr_mont_limbs([u])), n)
+        assert _ints(f, h2b.to_host(d_q)) == want, f"kate n={n} u={u}"
+
+
+def test_kate_division_padded(h2b, orc, cuda):
+    f = h2b.fields
+    p = f.R_MOD
+    n = 3000
+    a = orc.chacha_fr(950, n)
+    u = 77
+    want = _synthetic_division(_ints(f, a), u, p)
+    for out_len in (n - 1, n + 500, 1000):
+        d_q = h2b.to_dev(np.full((out_len, 4), 0xFFFFFFFFFFFFFFFF, np.uint64))
+        h2b.kate_division_device(h2b.to_dev(a), d_q, h2b.to_dev(f.fr_mont_limbs([u])), n, out_len=out_len)
+        got = _ints(f, h2b.to_host(d_q))
+        k = min(n - 1, out_len)
+        assert got[:k] == want[:k] and all(x == 0 for x in got[k:]), f"padded out_len={out_len}"
+    # n < 2: zeros only
+    d_q = h2b.to_dev(np.full((8, 4), 0xFFFFFFFFFFFFFFFF, np.uint64))
+    h2b.kate_division_device(h2b.to_dev(a[:1]), d_q, h2b.to_dev(f.fr_mont_limbs([u])), 1, out_len=8)
+    assert not h2b.to_host(d_q).any()
+
+
+@pytest.mark.parametrize("n", [1 << 20, (1 << 22) + 5])
+def test_kate_division_identity_large(h2b, orc, cuda, n):
+    """Two and three scan levels: q(x)(x - u) = a(x) - a(u) at a random x."""
+    f = h2b.fields
+    p = f.R_MOD
+    a = orc.chacha_fr(990, n)
+    u, x = 0x5EED5EED5EED, 0xC0FFEE1234567
+    d_q = h2b.dev_empty(32 * (n - 1))
+    h2b.kate_division_device(h2b.to_dev(a), d_q, h2b.to_dev(f.fr_mont_limbs([u])), n)
+    q = h2b.to_host(d_q)
+    xl, ul = f.fr_mont_limbs([x]), f.fr_mont_limbs([u])
+    qx = _ints(f, orc.fr_eval(q, xl))[0]
+    ax, au = _ints(f, orc.fr_eval(a, xl))[0], _ints(f, orc.fr_eval(a, ul))[0]
+    assert qx * (x - u) % p == (ax - au) % p
+
+
+def test_multiopen_poly_calculation(h2b, orc, cuda):
+    f = h2b.fields
+    p = f.R_MOD
+    n, batch = 4000, 4
+    polys = [orc.chacha_fr(1100 + i, n) for i in range(batch)]
+    ch = f.fr_mont_limbs([2, 3, p - 1, 0x123456789])
+    pts = f.fr_mont_limbs([7, 11, 13, 0xFEDCBA])
+    for off, ln in ((0, n), (1500, 1200)):
+        acc = np.full((n, 4), 0x55, np.uint64)
+        acc_before = acc.copy()
+        res = h2b.multiopen_poly_calculation(polys, acc, ch, pts, off, ln)
+        for i in range(batch):
+            assert_limbs_equal(res[i:i + 1], orc.fr_eval(polys[i][off:off + ln], pts[i:i + 1]), "multiopen eval")
+        ci = _ints(f, ch)
+        P = [_ints(f, q[off:off + ln]) for q in polys]
+        want = [sum(ci[i] * P[i][k] for i in range(batch)) % p for k in range(ln)]
+        assert _ints(f, acc[off:off + ln]) == want, "multiopen accumulator"
+        # only the chunk is written
+        assert (acc[:off] == acc_before[:off]).all() and (acc[off + ln:] == acc_before[off + ln:]).all()
+
+
+def test_decode_assigned(h2b, orc, cuda):
+    """Assigned<F> as the Rust side lays it out: tag byte, then the payloads
+    at 8-byte-aligned offsets (stride 72 = 8 + 32 + 32)."""
+    f = h2b.fields
+    n = 3001
+    stride, no, do = 72, 8, 40
+    nums = orc.chacha_fr(1200, n)
+    dens = orc.chacha_fr(1201, n)
+    tags = np.arange(n) % 3
+    raw = np.zeros(n * stride, np.uint8)
+    for i in range(n):
+        raw[i * stride] = tags[i]
+        raw[i * stride + 1:i * stride + 8] = 0xAB   # padding bytes are ignored
+        if tags[i] >= 1:
+            raw[i * stride + no:i * stride + no + 32] = nums[i].view(np.uint8)
+        if tags[i] == 2:
+            raw[i * stride + do:i * stride + do + 32] = dens[i].view(np.uint8)
+    d_n, d_d = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+    h2b.decode_assigned_device(d_n, d_d, h2b.to_dev(raw), n, stride, no, do)
+    one = f.fr_mont_limbs([1])[0]
+    want_n = np.where((tags >= 1)[:, None], nums, 0).astype(np.uint64)
+    want_d = np.where((tags == 2)[:, None], dens, one).astype(np.uint64)
+    assert_limbs_equal(h2b.to_host(d_n), want_n, "numerators")
+    assert_limbs_equal(h2b.to_host(d_d), want_d, "denominators")
