@@ -248,7 +248,7 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int
 // PTS: the entries are the affine points themselves (bases[e]), as left by
 // the pairing rounds, instead of signed (GLV) indices into the bases.
 template <int MODE, bool PTS>
-__global__ void __launch_bounds__(128, MODE == 1 ? 2 : 3) k_msm_accumulate(const uint32_t* __restrict__ sorted,
+__global__ void __launch_bounds__(128, MODE == 1 ? 2 : (MODE >= 3 ? MODE + 1 : 3)) k_msm_accumulate(const uint32_t* __restrict__ sorted,
                                                         const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K,
                                                         const G1Affine* __restrict__ bases, G1Xyzz* __restrict__ buckets,
                                                         G1Xyzz* __restrict__ heads)
@@ -716,6 +716,10 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
         k_msm_accumulate<1, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 2)
         k_msm_accumulate<2, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
+    else if (g_msm_acc_variant == 3)
+        k_msm_accumulate<3, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
+    else if (g_msm_acc_variant == 4)
+        k_msm_accumulate<4, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else
         k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     prof_end(PROF_MSM_ACCUMULATE, st);
@@ -840,12 +844,14 @@ extern "C" RustError h2b_msm_device(const void* d_scalar, const void* d_bases, v
 
 extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(window_bits, chunk); }
 
-// Call structure of the bucket-accumulation kernel: 0 = two products per
-// out-of-line call (default), 1 = all products inline, 2 = one product per
-// call.  Results are identical; only speed differs.
+// Call structure and occupancy of the bucket-accumulation kernel: 0 = two
+// products per out-of-line call (default), 1 = all products inline, 2 = one
+// product per call, 3 and 4 = one product per call with at most 128 / 96
+// registers (4 / 5 CTAs of 128 threads per SM).  Results are identical; only
+// speed differs.
 extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
-    if (v >= 0 && v <= 2) g_msm_acc_variant = v;
+    if (v >= 0 && v <= 4) g_msm_acc_variant = v;
 }
 
 // Batch-affine pairing rounds run before the XYZZ bucket accumulation

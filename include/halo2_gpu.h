@@ -354,7 +354,8 @@ RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out,
 /* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
 /* Call structure of the MSM bucket-accumulation kernel: 0 = two field products per out-of-line call
- * (default), 1 = all products inline, 2 = one product per call.  Same results; tuning only. */
+ * (default), 1 = all products inline, 2 = one product per call, 3 / 4 = one per call with 4 / 5 CTAs
+ * per SM.  Same results; tuning only. */
 void h2b_msm_set_accumulate_variant(int variant);
 /* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
  * MSM workspace-size queries depend on it (set it before sizing scratch). */
