@@ -38,6 +38,12 @@ class AssignedLayout(ctypes.Structure):
     _fields_ = [("stride_bytes", ctypes.c_uint32), ("num_offset", ctypes.c_uint32), ("denom_offset", ctypes.c_uint32)]
 
 
+class MsmJob(ctypes.Structure):
+    """One job of h2b_msm_batch (device scalars, device bases, device 96-byte output, length)."""
+    _fields_ = [("d_scalars", ctypes.c_void_p), ("d_bases", ctypes.c_void_p), ("d_out", ctypes.c_void_p),
+                ("n", ctypes.c_uint64)]
+
+
 class Halo2GpuError(RuntimeError):
     def __init__(self, code, message, who):
         super().__init__(f"{who}: code {code}: {message}")
@@ -138,6 +144,14 @@ _SIGS = {
     "h2b_msm_set_tuning": (None, [ctypes.c_int, ctypes.c_int]),
     "h2b_msm_set_accumulate_variant": (None, [ctypes.c_int]),
     "h2b_msm_set_pair_rounds": (None, [ctypes.c_int]),
+    "h2b_exec_fork": (RustError, [_vp, _u32, ctypes.POINTER(ctypes.c_void_p)]),
+    "h2b_exec_join": (RustError, [_vp, _u32]),
+    "h2b_graph_begin": (RustError, [_vp]),
+    "h2b_graph_end": (RustError, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
+    "h2b_graph_launch": (RustError, [_vp, _vp]),
+    "h2b_graph_destroy": (None, [_vp]),
+    "h2b_msm_batch_workspace_size": (_u64, [ctypes.POINTER(_u64), _u64, _u32]),
+    "h2b_msm_batch": (RustError, [ctypes.POINTER(MsmJob), _u64, _u32, _vp, _u64, _vp]),
     "h2b_batch_invert_workspace_size": (_u64, [_u64]),
     "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
     "h2b_ntt_set_pass_stages": (None, [ctypes.c_int]),
@@ -218,6 +232,11 @@ def _torch():
 
 
 def stream_handle(stream=None):
+    """cudaStream_t of a torch stream (current stream by default), or a raw handle (c_void_p / int)."""
+    if isinstance(stream, ctypes.c_void_p):
+        return stream
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
     torch = _torch()
     s = stream if stream is not None else torch.cuda.current_stream()
     return ctypes.c_void_p(s.cuda_stream)
@@ -313,6 +332,62 @@ def msm_device(d_scalars, d_bases, d_out, n, ws, stream=None):
 
 def msm_workspace(n):
     return dev_empty(lib()._halo2_multiexp_device_scalars_device_bases_workspace_size(n))
+
+
+# --- batch execution (no reference counterpart) ---------------------------------
+
+def msm_batch_jobs(d_scalars, d_bases, d_outs, lengths):
+    jobs = (MsmJob * max(len(lengths), 1))()
+    for i, n in enumerate(lengths):
+        jobs[i].d_scalars = d_scalars[i].data_ptr()
+        jobs[i].d_bases = d_bases[i].data_ptr()
+        jobs[i].d_out = d_outs[i].data_ptr()
+        jobs[i].n = int(n)
+    return jobs
+
+
+def msm_batch_workspace(lengths, streams):
+    arr = (ctypes.c_uint64 * max(len(lengths), 1))(*[int(n) for n in lengths])
+    return dev_empty(lib().h2b_msm_batch_workspace_size(arr, len(lengths), streams))
+
+
+def msm_batch(jobs, count, streams, ws, stream=None):
+    """h2b_msm_batch: count device MSMs overlapped on `streams` forked streams."""
+    call("h2b_msm_batch", jobs, count, streams, ptr(ws), ws.numel(), stream_handle(stream))
+
+
+def exec_fork(n, stream=None):
+    out = (ctypes.c_void_p * n)()
+    call("h2b_exec_fork", stream_handle(stream), n, out)
+    return [ctypes.c_void_p(out[i]) for i in range(n)]
+
+
+def exec_join(n, stream=None):
+    call("h2b_exec_join", stream_handle(stream), n)
+
+
+class Graph:
+    """A CUDA graph captured from everything issued on `stream` between begin() and end()."""
+
+    def __init__(self, stream=None):
+        self.stream = stream
+        self.handle = None
+
+    def begin(self):
+        call("h2b_graph_begin", stream_handle(self.stream))
+
+    def end(self):
+        h = ctypes.c_void_p()
+        call("h2b_graph_end", stream_handle(self.stream), ctypes.byref(h))
+        self.handle = h
+
+    def launch(self, stream=None):
+        call("h2b_graph_launch", self.handle, stream_handle(stream if stream is not None else self.stream))
+
+    def close(self):
+        if self.handle is not None:
+            lib().h2b_graph_destroy(self.handle)
+            self.handle = None
 
 
 # --- NTT (halo2_proofs/src/cuda/funcs/ntt.rs, poly/domain.rs) ----------------------

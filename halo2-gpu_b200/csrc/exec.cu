@@ -1,0 +1,193 @@
+// Batch execution helpers for serving many independent jobs of uneven size
+// (many MSMs, NTTs and quotient evaluations of k = 14..22) on one GPU.  No
+// counterpart in the reference, which runs one launcher at a time on one
+// stream.
+//
+//  * h2b_exec_fork / h2b_exec_join: N internal non-blocking streams ordered
+//    after / before the caller's stream through events, so jobs issued on
+//    them overlap on the device while the caller keeps one stream of record.
+//    The streams and events are created once per device (first fork on that
+//    device) and live until process exit.
+//  * h2b_graph_begin / h2b_graph_end / h2b_graph_launch / h2b_graph_destroy:
+//    capture everything issued on the caller's stream (and on streams forked
+//    from it) into a CUDA graph and replay it; the pointers and sizes of the
+//    captured calls are baked in.  Only entry points that issue no host
+//    copies and no synchronisation can be captured (the device-resident MSM,
+//    NTT types 1-4 and the device-column quotient are such).
+//  * h2b_msm_batch: `count` device-resident MSMs spread over `streams`
+//    forked streams, longest job first onto the least-loaded stream, each
+//    stream with its own slice of the caller's scratch.
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <vector>
+#include "abi.cuh"
+#include "curve.cuh"
+#include "msm.cuh"
+
+namespace h2b {
+
+namespace {
+constexpr uint32_t EXEC_MAX_STREAMS = 32;
+
+struct DevExec {
+    std::vector<cudaStream_t> streams;
+    cudaEvent_t fork_ev = nullptr;
+    std::vector<cudaEvent_t> join_ev;
+};
+std::mutex g_exec_mu;
+std::map<int, DevExec> g_exec;
+
+// Streams and events of the current device, created on first use.
+RustError exec_get(uint32_t n, DevExec** out)
+{
+    if (n == 0 || n > EXEC_MAX_STREAMS) return err((int)cudaErrorInvalidValue, "exec: streams must be in 1..32");
+    int dev = 0;
+    H2B_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_exec_mu);
+    DevExec& d = g_exec[dev];
+    if (!d.fork_ev) H2B_CUDA(cudaEventCreateWithFlags(&d.fork_ev, cudaEventDisableTiming));
+    while (d.streams.size() < n) {
+        cudaStream_t s;
+        H2B_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        d.streams.push_back(s);
+        cudaEvent_t e;
+        H2B_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        d.join_ev.push_back(e);
+    }
+    *out = &d;
+    return ok();
+}
+
+struct GraphHandle {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+// Scratch of one MSM slot (device scalars and bases), 256-byte aligned.
+uint64_t msm_slot_bytes(uint64_t n)
+{
+    MsmPlan p = msm_plan(n);
+    ScratchPlan sp;
+    msm_plan_scratch(p, sp, false, false);
+    return align_up(sp.used);
+}
+} // namespace
+
+} // namespace h2b
+
+using namespace h2b;
+
+extern "C" RustError h2b_exec_fork(cudaStream_t parent, uint32_t n, cudaStream_t* out)
+{
+    DevExec* d = nullptr;
+    H2B_TRY(exec_get(n, &d));
+    H2B_CUDA(cudaEventRecord(d->fork_ev, parent));
+    for (uint32_t i = 0; i < n; i++) {
+        H2B_CUDA(cudaStreamWaitEvent(d->streams[i], d->fork_ev, 0));
+        out[i] = d->streams[i];
+    }
+    return ok();
+}
+
+extern "C" RustError h2b_exec_join(cudaStream_t parent, uint32_t n)
+{
+    DevExec* d = nullptr;
+    H2B_TRY(exec_get(n, &d));
+    for (uint32_t i = 0; i < n; i++) {
+        H2B_CUDA(cudaEventRecord(d->join_ev[i], d->streams[i]));
+        H2B_CUDA(cudaStreamWaitEvent(parent, d->join_ev[i], 0));
+    }
+    return ok();
+}
+
+extern "C" RustError h2b_graph_begin(cudaStream_t s)
+{
+    H2B_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    return ok();
+}
+
+extern "C" RustError h2b_graph_end(cudaStream_t s, void** handle)
+{
+    GraphHandle* g = new GraphHandle;
+    cudaError_t e = cudaStreamEndCapture(s, &g->graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e != cudaSuccess) {
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        return cuda_err(e, "h2b_graph_end");
+    }
+    *handle = g;
+    return ok();
+}
+
+extern "C" RustError h2b_graph_launch(void* handle, cudaStream_t s)
+{
+    if (!handle) return err((int)cudaErrorInvalidValue, "h2b_graph_launch: null handle");
+    H2B_CUDA(cudaGraphLaunch(static_cast<GraphHandle*>(handle)->exec, s));
+    return ok();
+}
+
+extern "C" void h2b_graph_destroy(void* handle)
+{
+    GraphHandle* g = static_cast<GraphHandle*>(handle);
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
+// ---- batched MSM --------------------------------------------------------------
+
+typedef struct h2b_msm_job {
+    const void* d_scalars;  // n Montgomery Fr (device)
+    const void* d_bases;    // n affine G1 (device)
+    void* d_out;            // 96-byte Jacobian image (device)
+    uint64_t n;
+} h2b_msm_job;
+
+// One scratch slot per stream, each sized for the longest job.
+extern "C" uint64_t h2b_msm_batch_workspace_size(const uint64_t* lengths, uint64_t count, uint32_t streams)
+{
+    if (streams == 0 || streams > EXEC_MAX_STREAMS) return 0;
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < count; i++) mx = std::max(mx, lengths[i]);
+    return (uint64_t)streams * msm_slot_bytes(mx);
+}
+
+extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
+                                   uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (count == 0) return ok();
+    if (streams == 0 || streams > EXEC_MAX_STREAMS)
+        return err((int)cudaErrorInvalidValue, "h2b_msm_batch: streams must be in 1..32");
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < count; i++) {
+        if (jobs[i].n > 0 && (!jobs[i].d_scalars || !jobs[i].d_bases))
+            return err((int)cudaErrorInvalidValue, "h2b_msm_batch: null input pointer");
+        if (!jobs[i].d_out) return err((int)cudaErrorInvalidValue, "h2b_msm_batch: null output pointer");
+        mx = std::max(mx, jobs[i].n);
+    }
+    const uint64_t slot = msm_slot_bytes(mx);
+    if (scratch_bytes < slot * streams || !scratch)
+        return scratch_too_small("h2b_msm_batch", scratch_bytes, slot * streams);
+    // longest job first onto the least-loaded stream
+    std::vector<uint64_t> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return jobs[a].n > jobs[b].n; });
+    std::vector<uint64_t> load(streams, 0);
+    cudaStream_t sub[EXEC_MAX_STREAMS];
+    H2B_TRY(h2b_exec_fork(stream, streams, sub));
+    for (uint64_t j : order) {
+        const uint32_t k = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += jobs[j].n + 4096;  // fixed cost per job: launch and tail latency
+        const MsmPlan p = msm_plan(jobs[j].n);
+        ScratchArena ar((uint8_t*)scratch + (uint64_t)k * slot, slot);
+        const MsmScratch s = msm_carve(p, ar, false, false);
+        if (!ar.good()) return err((int)cudaErrorInvalidValue, "h2b_msm_batch: slot carving failed");
+        H2B_TRY(msm_run(p, s, (const Fr*)jobs[j].d_scalars, (const G1Affine*)jobs[j].d_bases, sub[k]));
+        H2B_CUDA(cudaMemcpyAsync(jobs[j].d_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToDevice, sub[k]));
+    }
+    return h2b_exec_join(stream, streams);
+}

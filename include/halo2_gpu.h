@@ -360,6 +360,29 @@ void h2b_msm_set_accumulate_variant(int variant);
 /* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
  * MSM workspace-size queries depend on it (set it before sizing scratch). */
 void h2b_msm_set_pair_rounds(int rounds);
+
+/* Batch execution (no counterpart in the reference, which runs one launcher at a time on one stream).
+ * h2b_exec_fork: `n` (1..32) internal non-blocking streams of the current device, ordered after `parent`;
+ * created on the first fork on that device and kept until exit.  h2b_exec_join: `parent` waits for them. */
+RustError h2b_exec_fork(h2b_stream_t parent, uint32_t n, h2b_stream_t* out_streams);
+RustError h2b_exec_join(h2b_stream_t parent, uint32_t n);
+/* Capture what is issued on `s` (and on streams forked from it) into a CUDA graph; replay it with
+ * h2b_graph_launch.  Only calls without host copies or synchronisation can be captured. */
+RustError h2b_graph_begin(h2b_stream_t s);
+RustError h2b_graph_end(h2b_stream_t s, void** handle);
+RustError h2b_graph_launch(void* handle, h2b_stream_t s);
+void h2b_graph_destroy(void* handle);
+/* `count` device-resident MSMs overlapped on `streams` forked streams (longest first onto the least-loaded
+ * stream); each result is the 96-byte Jacobian image at d_out.  Scratch: h2b_msm_batch_workspace_size. */
+typedef struct h2b_msm_job {
+    const void* d_scalars;
+    const void* d_bases;
+    void* d_out;
+    uint64_t n;
+} h2b_msm_job;
+uint64_t h2b_msm_batch_workspace_size(const uint64_t* lengths, uint64_t count, uint32_t streams);
+RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
+                        uint64_t scratch_bytes, h2b_stream_t stream);
 /* Batch inversion whose CTAs share a single inversion through scratch
  * (h2b_batch_invert_workspace_size bytes); same semantics as _halo2_batch_invert. */
 uint64_t h2b_batch_invert_workspace_size(uint64_t length);
