@@ -179,6 +179,100 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def batch_section(h2b, torch, n_jobs=64, streams=8, reps=3, seed=4):
+    """Batched jobs of uneven size: n_jobs jobs with k drawn from {14, 16, 18,
+    20} (weights .4/.3/.2/.1, seeded), each one MSM with uniform scalars
+    against a shared 2^20 SRS and one coset extension 2^k -> 2^(k+2).  Plain:
+    one job after another through h2b_msm_device and _halo2_fft_many_to_device
+    on one stream.  Batched: the same calls spread over `streams` forked
+    streams (h2b_exec_fork / h2b_msm_batch), captured once into a CUDA graph
+    and replayed.  Outputs of both must be identical; times are CUDA events."""
+    import random
+    f = h2b.fields
+    L = h2b.lib()
+    rng = random.Random(seed)
+    ks = rng.choices([14, 16, 18, 20], weights=[4, 3, 2, 1], k=n_jobs)
+    srs = h2b.srs_device(0x5EED20, 1 << 20)
+    d_sc = [h2b.random_fr_device(1 << k, 5000 + i, 0) for i, k in enumerate(ks)]
+    d_in = [h2b.random_fr_device(1 << k, 6000 + i, 0) for i, k in enumerate(ks)]
+    d_ext = [h2b.dev_empty(32 << (k + 2)) for k in ks]
+    d_ext_plain = [h2b.dev_empty(32 << (k + 2)) for k in ks]
+    d_msm = [h2b.dev_empty(96) for _ in ks]
+    d_msm_plain = [h2b.dev_empty(96) for _ in ks]
+    doms = {k: f.EvaluationDomain(3, k) for k in set(ks)}
+    d_om = {k: h2b.to_dev(f.fr_mont_limbs([doms[k].extended_omega])) for k in doms}
+    one = f.fr_mont_limbs([1])
+    one_ffi = h2b.host_ffi(one)
+    kmax = max(ks)
+    ntt_ws = [h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(3, kmax, kmax + 2)) for _ in range(streams)]
+    msm_ws = h2b.msm_workspace(1 << kmax)
+    tabs = [(h2b.ffi_array([d_in[i].data_ptr()]), h2b.ffi_array([d_ext[i].data_ptr()]),
+             h2b.ffi_array([d_ext_plain[i].data_ptr()])) for i in range(n_jobs)]
+
+    def coset(i, out_tab, ws, st):
+        k = ks[i]
+        h2b.call("_halo2_fft_many_to_device", 3, 1, k, k + 2, tabs[i][0], out_tab, h2b.ptr(d_om[k]),
+                 ctypes.byref(one_ffi), True, h2b.ptr(ws), ws.numel(), h2b.stream_handle(st))
+
+    side = torch.cuda.Stream()
+
+    def plain():
+        for i, k in enumerate(ks):
+            h2b.call("h2b_msm_device", h2b.ptr(d_sc[i]), h2b.ptr(srs), h2b.ptr(d_msm_plain[i]), 1 << k,
+                     h2b.ptr(msm_ws), msm_ws.numel(), h2b.stream_handle(side))
+            coset(i, tabs[i][2], ntt_ws[0], side)
+
+    jobs = h2b.msm_batch_jobs(d_sc, [srs] * n_jobs, d_msm, [1 << k for k in ks])
+    bws = h2b.msm_batch_workspace(jobs, n_jobs, streams)
+    order = sorted(range(n_jobs), key=lambda i: -ks[i])
+
+    def batched():
+        # coset jobs go onto the forked streams, longest first onto the least
+        # loaded; the MSM batch forks the same streams again without a join in
+        # between, so MSMs queue behind each stream's NTTs and the two kinds
+        # overlap across streams; its join covers both
+        subs = h2b.exec_fork(streams, side)
+        load = [0] * streams
+        for i in order:
+            s = load.index(min(load))
+            load[s] += 1 << ks[i]
+            coset(i, tabs[i][1], ntt_ws[s], subs[s])
+        h2b.msm_batch(jobs, n_jobs, streams, bws, stream=side)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(side)
+        for _ in range(reps):
+            fn()
+        e1.record(side)
+        side.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    plain()
+    batched()  # warm-up: creates the forked streams, loads every kernel
+    side.synchronize()
+    t_plain = timed(plain)
+    t_batched_streams = timed(batched)
+    g = h2b.Graph(side)
+    g.begin()
+    batched()
+    g.end()
+    try:
+        g.launch(side)
+        side.synchronize()
+        t_graph = timed(lambda: g.launch(side))
+    finally:
+        g.close()
+    same = all(d_msm[i].cpu().numpy().tobytes() == d_msm_plain[i].cpu().numpy().tobytes() and
+               d_ext[i].cpu().numpy().tobytes() == d_ext_plain[i].cpu().numpy().tobytes() for i in range(n_jobs))
+    return {"workload": f"{n_jobs} jobs, k in {{14,16,18,20}} w .4/.3/.2/.1 (seed {seed}): MSM vs shared 2^20 SRS "
+                        f"+ coset extension x4", "k_counts": {k: ks.count(k) for k in sorted(set(ks))},
+            "msm_points": sum(1 << k for k in ks), "streams": streams,
+            "plain_ms": t_plain, "batched_streams_ms": t_batched_streams, "batched_graph_ms": t_graph,
+            "plain_jobs_per_s": n_jobs / (t_plain * 1e-3), "batched_jobs_per_s": n_jobs / (t_graph * 1e-3),
+            "speedup": t_plain / t_graph, "identical_outputs": same}
+
+
 def run_case(args):
     """One kernel family at 2^log_n, warmup + steps, nothing else (for ncu)."""
     import torch
@@ -225,6 +319,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--case", choices=["msm", "ntt", "bi"], help="run one kernel family only (profiling runs)")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     args = ap.parse_args()
@@ -428,6 +523,8 @@ def main():
                        "api": "_halo2_multiexp_device_bases (host scalars), _halo2_cosetfft (host in/out), "
                               "h2b_batch_invert with pinned H2D/D2H"}
 
+    if not args.no_batch:
+        line["batch"] = batch_section(h2b, torch)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_msm()
     if rank == 0:

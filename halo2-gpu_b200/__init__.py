@@ -41,7 +41,7 @@ class AssignedLayout(ctypes.Structure):
 class MsmJob(ctypes.Structure):
     """One job of h2b_msm_batch (device scalars, device bases, device 96-byte output, length)."""
     _fields_ = [("d_scalars", ctypes.c_void_p), ("d_bases", ctypes.c_void_p), ("d_out", ctypes.c_void_p),
-                ("n", ctypes.c_uint64)]
+                ("n", ctypes.c_uint64), ("table_n", ctypes.c_uint64)]
 
 
 class Halo2GpuError(RuntimeError):
@@ -150,7 +150,12 @@ _SIGS = {
     "h2b_graph_end": (RustError, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "h2b_graph_launch": (RustError, [_vp, _vp]),
     "h2b_graph_destroy": (None, [_vp]),
-    "h2b_msm_batch_workspace_size": (_u64, [ctypes.POINTER(_u64), _u64, _u32]),
+    "h2b_msm_batch_workspace_size": (_u64, [ctypes.POINTER(MsmJob), _u64, _u32]),
+    "h2b_msm_table_points": (_u64, [_u64]),
+    "h2b_msm_table_precompute_workspace_size": (_u64, [_u64]),
+    "h2b_msm_table_precompute": (RustError, [_vp, _u64, _vp, _vp, _u64, _vp]),
+    "h2b_msm_table_workspace_size": (_u64, [_u64, _u64]),
+    "h2b_msm_device_table": (RustError, [_vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp]),
     "h2b_msm_batch": (RustError, [ctypes.POINTER(MsmJob), _u64, _u32, _vp, _u64, _vp]),
     "h2b_batch_invert_workspace_size": (_u64, [_u64]),
     "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
@@ -336,19 +341,40 @@ def msm_workspace(n):
 
 # --- batch execution (no reference counterpart) ---------------------------------
 
-def msm_batch_jobs(d_scalars, d_bases, d_outs, lengths):
+def msm_batch_jobs(d_scalars, d_bases, d_outs, lengths, table_n=0):
+    """Job array for h2b_msm_batch; table_n > 0 when d_bases are window tables built for table_n bases."""
     jobs = (MsmJob * max(len(lengths), 1))()
     for i, n in enumerate(lengths):
         jobs[i].d_scalars = d_scalars[i].data_ptr()
         jobs[i].d_bases = d_bases[i].data_ptr()
         jobs[i].d_out = d_outs[i].data_ptr()
         jobs[i].n = int(n)
+        jobs[i].table_n = int(table_n)
     return jobs
 
 
-def msm_batch_workspace(lengths, streams):
-    arr = (ctypes.c_uint64 * max(len(lengths), 1))(*[int(n) for n in lengths])
-    return dev_empty(lib().h2b_msm_batch_workspace_size(arr, len(lengths), streams))
+def msm_batch_workspace(jobs, count, streams):
+    return dev_empty(lib().h2b_msm_batch_workspace_size(jobs, count, streams))
+
+
+def msm_table_precompute(d_bases, n, stream=None):
+    """Window table [2^(c w)] P_i for the n device bases (resident SRS form); returns the device table."""
+    pts = lib().h2b_msm_table_points(n)
+    if pts == 0:
+        raise ValueError(f"no window table for {n} bases")
+    table = dev_empty(64 * pts)
+    ws = dev_empty(lib().h2b_msm_table_precompute_workspace_size(n))
+    call("h2b_msm_table_precompute", ptr(d_bases), n, ptr(table), ptr(ws), ws.numel(), stream_handle(stream))
+    return table
+
+
+def msm_device_table(d_scalars, d_table, table_n, d_out, n, ws=None, stream=None):
+    need = lib().h2b_msm_table_workspace_size(n, table_n)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    call("h2b_msm_device_table", ptr(d_scalars), ptr(d_table), table_n, ptr(d_out), n, ptr(ws), ws.numel(),
+         stream_handle(stream))
+    return d_out
 
 
 def msm_batch(jobs, count, streams, ws, stream=None):

@@ -65,10 +65,13 @@ struct GraphHandle {
     cudaGraphExec_t exec = nullptr;
 };
 
+// Plan of one job: plain bases, or a precomputed window table of table_n points.
+MsmPlan job_plan(uint64_t n, uint64_t table_n) { return table_n ? msm_plan_table(n, table_n) : msm_plan(n); }
+
 // Scratch of one MSM slot (device scalars and bases), 256-byte aligned.
-uint64_t msm_slot_bytes(uint64_t n)
+uint64_t msm_slot_bytes(uint64_t n, uint64_t table_n)
 {
-    MsmPlan p = msm_plan(n);
+    MsmPlan p = job_plan(n, table_n);
     ScratchPlan sp;
     msm_plan_scratch(p, sp, false, false);
     return align_up(sp.used);
@@ -142,18 +145,24 @@ extern "C" void h2b_graph_destroy(void* handle)
 
 typedef struct h2b_msm_job {
     const void* d_scalars;  // n Montgomery Fr (device)
-    const void* d_bases;    // n affine G1 (device)
+    const void* d_bases;    // n affine G1, or a window table built for table_n bases (device)
     void* d_out;            // 96-byte Jacobian image (device)
     uint64_t n;
+    uint64_t table_n;       // 0: d_bases are plain bases
 } h2b_msm_job;
 
-// One scratch slot per stream, each sized for the longest job.
-extern "C" uint64_t h2b_msm_batch_workspace_size(const uint64_t* lengths, uint64_t count, uint32_t streams)
+static uint64_t batch_slot(const h2b_msm_job* jobs, uint64_t count)
+{
+    uint64_t mx = 0;
+    for (uint64_t i = 0; i < count; i++) mx = std::max(mx, msm_slot_bytes(jobs[i].n, jobs[i].table_n));
+    return mx;
+}
+
+// One scratch slot per stream, each sized for the largest job.
+extern "C" uint64_t h2b_msm_batch_workspace_size(const h2b_msm_job* jobs, uint64_t count, uint32_t streams)
 {
     if (streams == 0 || streams > EXEC_MAX_STREAMS) return 0;
-    uint64_t mx = 0;
-    for (uint64_t i = 0; i < count; i++) mx = std::max(mx, lengths[i]);
-    return (uint64_t)streams * msm_slot_bytes(mx);
+    return (uint64_t)streams * batch_slot(jobs, count);
 }
 
 extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
@@ -162,14 +171,14 @@ extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint
     if (count == 0) return ok();
     if (streams == 0 || streams > EXEC_MAX_STREAMS)
         return err((int)cudaErrorInvalidValue, "h2b_msm_batch: streams must be in 1..32");
-    uint64_t mx = 0;
     for (uint64_t i = 0; i < count; i++) {
         if (jobs[i].n > 0 && (!jobs[i].d_scalars || !jobs[i].d_bases))
             return err((int)cudaErrorInvalidValue, "h2b_msm_batch: null input pointer");
         if (!jobs[i].d_out) return err((int)cudaErrorInvalidValue, "h2b_msm_batch: null output pointer");
-        mx = std::max(mx, jobs[i].n);
+        if (jobs[i].table_n && jobs[i].n > jobs[i].table_n)
+            return err((int)cudaErrorInvalidValue, "h2b_msm_batch: job longer than its table");
     }
-    const uint64_t slot = msm_slot_bytes(mx);
+    const uint64_t slot = batch_slot(jobs, count);
     if (scratch_bytes < slot * streams || !scratch)
         return scratch_too_small("h2b_msm_batch", scratch_bytes, slot * streams);
     // longest job first onto the least-loaded stream
@@ -182,7 +191,7 @@ extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint
     for (uint64_t j : order) {
         const uint32_t k = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
         load[k] += jobs[j].n + 4096;  // fixed cost per job: launch and tail latency
-        const MsmPlan p = msm_plan(jobs[j].n);
+        const MsmPlan p = job_plan(jobs[j].n, jobs[j].table_n);
         ScratchArena ar((uint8_t*)scratch + (uint64_t)k * slot, slot);
         const MsmScratch s = msm_carve(p, ar, false, false);
         if (!ar.good()) return err((int)cudaErrorInvalidValue, "h2b_msm_batch: slot carving failed");

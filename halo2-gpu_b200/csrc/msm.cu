@@ -67,32 +67,39 @@ void msm_set_tuning(int window_bits, int chunk)
     g_msm_chunk_override = chunk;
 }
 
-MsmPlan msm_plan(uint64_t n)
+static int choose_c(uint64_t n)
+{
+    int lg = 0;
+    while ((1ull << (lg + 1)) <= n) lg++;
+    if (g_msm_window_override >= 4 && g_msm_window_override <= 20) return g_msm_window_override;
+    if (lg >= 21) return 16;
+    if (lg >= 19) return 15;
+    if (lg >= 17) return 13;
+    if (lg >= 14) return 12;
+    if (lg >= 10) return 10;
+    return 7;
+}
+
+// tn > 0: precomputed window table of tn points per window; all windows then
+// share one bucket set and the reduction has a single window.
+static MsmPlan plan_core(uint64_t n, int c, uint64_t tn)
 {
     MsmPlan p;
     p.n = n;
-    int lg = 0;
-    while ((1ull << (lg + 1)) <= n) lg++;
-    int c;
-    if (g_msm_window_override >= 4 && g_msm_window_override <= 20) c = g_msm_window_override;
-    else if (lg >= 21) c = 16;
-    else if (lg >= 19) c = 15;
-    else if (lg >= 17) c = 13;
-    else if (lg >= 14) c = 12;
-    else if (lg >= 10) c = 10;
-    else c = 7;
+    p.tn = tn;
     p.c = c;
     // GLV halves: magnitudes < 2^GLV_BITS; the top window must leave room
     // for the signed-digit carry (its width <= c - 1).
     p.W = (GLV_BITS + c - 1) / c;
     if (GLV_BITS - c * (p.W - 1) > c - 1) p.W++;
     p.H = 1u << (c - 1);
-    p.NB = (uint64_t)p.W * p.H;
+    p.Wr = tn ? 1 : p.W;
+    p.NB = (uint64_t)p.Wr * p.H;
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 128u;
     p.nv = 2 * n;
     p.max_entries = p.nv * (uint64_t)p.W;
     // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
-    p.R = g_msm_pair_rounds;
+    p.R = tn ? 0 : g_msm_pair_rounds;
     p.cap[0] = p.max_entries;
     for (int r = 1; r <= 3; r++) p.cap[r] = p.cap[r - 1] / 2 + p.NB / 2 + 1;
     p.Kf = p.R > 0 ? std::max<uint32_t>(8u, p.K >> p.R) : p.K;
@@ -109,6 +116,10 @@ MsmPlan msm_plan(uint64_t n)
     return p;
 }
 
+MsmPlan msm_plan(uint64_t n) { return plan_core(n, choose_c(n), 0); }
+
+MsmPlan msm_plan_table(uint64_t n, uint64_t tn) { return plan_core(n, choose_c(tn), tn); }
+
 void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host)
 {
     if (bases_host) sp.add(p.n * sizeof(G1Affine));
@@ -123,8 +134,8 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
     sp.add_n<G1Xyzz>(p.max_chunks);                   // chunk head partials
     sp.add_n<uint32_t>(p.max_dense + 1);              // dense list + count
     sp.add_n<G1Xyzz>(p.max_dense * DENSE_PIECES);     // dense pieces
-    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment weighted sums
-    sp.add_n<G1Xyzz>((uint64_t)p.W * p.S);            // segment plain sums
+    sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment weighted sums
+    sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment plain sums
     sp.add_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));  // per-bit sums
     sp.add_n<G1Xyzz>(p.W);                            // window sums
     sp.add_n<G1Jac>(1);                               // result
@@ -157,8 +168,8 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
     s.heads = ar.take_n<G1Xyzz>(p.max_chunks);
     s.dense = ar.take_n<uint32_t>(p.max_dense + 1);
     s.pieces = ar.take_n<G1Xyzz>(p.max_dense * DENSE_PIECES);
-    s.segacc = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
-    s.segrun = ar.take_n<G1Xyzz>((uint64_t)p.W * p.S);
+    s.segacc = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
+    s.segrun = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
     s.bits = ar.take_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));
     s.wins = ar.take_n<G1Xyzz>(p.W);
     s.result = ar.take_n<G1Jac>(1);
@@ -209,7 +220,7 @@ __device__ __forceinline__ uint32_t window_bits(const uint4& s, int bit, int c)
 // sign is the digit's sign flipped by the virtual scalar's sign.
 template <bool SCATTER>
 __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int W, uint32_t H,
-                           uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted)
+                           uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted, uint64_t tn)
 {
     const unsigned lane = threadIdx.x & 31;
     const uint32_t full = 1u << c;
@@ -225,7 +236,7 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int
             if (v > H) { d = (int32_t)v - (int32_t)full; carry = 1; }
             else { d = (int32_t)v; carry = 0; }
             uint32_t key = 0xffffffffu;
-            if (valid && d != 0) key = (uint32_t)w * H + (uint32_t)(d < 0 ? -d : d) - 1u;
+            if (valid && d != 0) key = (tn ? 0u : (uint32_t)w * H) + (uint32_t)(d < 0 ? -d : d) - 1u;
             unsigned peers = __match_any_sync(0xffffffffu, key);
             int leader = __ffs(peers) - 1;
             if (!SCATTER) {
@@ -236,7 +247,9 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int
                 b = __shfl_sync(0xffffffffu, b, leader);
                 if (key != 0xffffffffu) {
                     uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-                    sorted[b + rank] = (uint32_t)i | (((d < 0) != sneg) ? SIGN_BIT : 0u);
+                    // with a window table the entry names table point w * tn + i/2
+                    const uint32_t v = (uint32_t)(i + 2 * (uint64_t)w * tn);
+                    sorted[b + rank] = v | (((d < 0) != sneg) ? SIGN_BIT : 0u);
                 }
             }
         }
@@ -673,11 +686,13 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_LAUNCHED("k_msm_glv");
     H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
     H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
-    k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr);
+    k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr,
+                                                                     p.tn);
     H2B_LAUNCHED("k_msm_sort<hist>");
     H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
     H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.cursor, s.sorted);
+    k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.cursor, s.sorted,
+                                                                    p.tn);
     H2B_LAUNCHED("k_msm_sort<scatter>");
     prof_begin(PROF_MSM_ACCUMULATE, st);
     // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
@@ -731,14 +746,14 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_LAUNCHED("k_msm_dense_pieces");
     k_msm_dense_merge<<<148, DENSE_PIECES, 0, st>>>(p.max_dense, s.buckets, s.dense, s.pieces);
     H2B_LAUNCHED("k_msm_dense_merge");
-    uint64_t nseg = (uint64_t)p.W * p.S;
-    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.W, p.H, p.L, p.S, s.segacc, s.segrun);
+    uint64_t nseg = (uint64_t)p.Wr * p.S;
+    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.Wr, p.H, p.L, p.S, s.segacc, s.segrun);
     H2B_LAUNCHED("k_msm_segments");
-    k_msm_bitsums<<<p.W * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
+    k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
     H2B_LAUNCHED("k_msm_bitsums");
-    k_msm_wincombine<<<1, 64, 0, st>>>(s.bits, p.W, p.NBITS, p.LOGL, s.wins);
+    k_msm_wincombine<<<1, 64, 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
     H2B_LAUNCHED("k_msm_wincombine");
-    k_msm_final<<<1, 64, 0, st>>>(s.wins, p.W, p.c, s.result);
+    k_msm_final<<<1, 64, 0, st>>>(s.wins, p.Wr, p.c, s.result);
     prof_end(PROF_MSM_TOTAL, st);
     H2B_LAUNCHED("k_msm_final");
     return ok();
@@ -838,6 +853,130 @@ extern "C" RustError h2b_msm_device(const void* d_scalar, const void* d_bases, v
     ScratchArena ar(scratch, scratch_bytes);
     MsmScratch s = msm_carve(p, ar, false, false);
     H2B_TRY(msm_run(p, s, (const Fr*)d_scalar, (const G1Affine*)d_bases, stream));
+    H2B_CUDA(cudaMemcpyAsync(d_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToDevice, stream));
+    return ok();
+}
+
+// ---- precomputed window tables (SRS kept resident with its window multiples) --
+// A table for n bases holds W slices of n affine points, slice w being
+// [2^(c w)] P_i (c and W from the n-point plan).  An MSM over the table puts
+// the digits of every window into one bucket set, so the bucket reduction
+// covers one window and the final 2^(c w) doubling chain disappears; the
+// entry count (bucket additions) is unchanged.  Slice w + 1 is c doublings of
+// slice w, made affine with one batch inversion per slice.
+
+namespace h2b {
+
+__global__ void k_table_double(const G1Affine* __restrict__ prev, uint64_t n, int c, G1Xyzz* __restrict__ tmp,
+                               Fq* __restrict__ den)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const G1Affine P = ld_affine(&prev[i]);
+        if (is_inf(P)) {
+            st_xyzz(&tmp[i], xyzz_inf());
+            st(&den[i], Fq::zero());
+            continue;
+        }
+        G1Xyzz X = xyzz_dbl_affine(P);
+        for (int k = 1; k < c; k++) X = xyzz_dbl(X);
+        st_xyzz(&tmp[i], X);
+        st(&den[i], X.ZZ * X.ZZZ);
+    }
+}
+
+// den_inv[i] = 1 / (ZZ ZZZ): x = X ZZZ / (ZZ ZZZ), y = Y ZZ / (ZZ ZZZ); zero -> infinity (0, 0).
+__global__ void k_table_affine(const G1Xyzz* __restrict__ tmp, const Fq* __restrict__ den_inv, uint64_t n,
+                               G1Affine* __restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const Fq d = ld(&den_inv[i]);
+        G1Affine a;
+        if (d.is_zero()) {
+            a.x = Fq::zero();
+            a.y = Fq::zero();
+        } else {
+            const G1Xyzz X = ld_xyzz(&tmp[i]);
+            a.x = X.X * (d * X.ZZZ);
+            a.y = X.Y * (d * X.ZZ);
+        }
+        st(&out[i].x, a.x);
+        st(&out[i].y, a.y);
+    }
+}
+
+// Entries encode the table point as 2 (w tn + i) + half in 31 bits.
+static bool table_fits(uint64_t tn)
+{
+    const MsmPlan p = msm_plan(tn);
+    return tn > 0 && tn <= MSM_MAX_LENGTH && 2 * (uint64_t)p.W * tn < (1ull << 31);
+}
+
+} // namespace h2b
+
+extern "C" uint64_t h2b_msm_table_points(uint64_t n)
+{
+    if (!table_fits(n)) return 0;
+    return (uint64_t)msm_plan(n).W * n;
+}
+
+extern "C" uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n)
+{
+    if (!table_fits(n)) return 0;
+    ScratchPlan sp;
+    sp.add_n<G1Xyzz>(n);
+    sp.add_n<Fq>(n);
+    sp.add(fq_batch_invert_scratch(n));
+    return sp.used;
+}
+
+// d_table receives h2b_msm_table_points(n) affine points; d_bases is not modified.
+extern "C" RustError h2b_msm_table_precompute(const void* d_bases, uint64_t n, void* d_table, void* scratch,
+                                              uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (!table_fits(n)) return err(cudaErrorInvalidValue, "h2b_msm_table_precompute: n out of range");
+    const MsmPlan p = msm_plan(n);
+    ScratchArena ar(scratch, scratch_bytes);
+    G1Xyzz* tmp = ar.take_n<G1Xyzz>(n);
+    Fq* den = ar.take_n<Fq>(n);
+    const uint64_t inv_bytes = fq_batch_invert_scratch(n);
+    void* inv_scratch = ar.take(inv_bytes);
+    if (!ar.good())
+        return scratch_too_small("h2b_msm_table_precompute", scratch_bytes, h2b_msm_table_precompute_workspace_size(n));
+    G1Affine* table = (G1Affine*)d_table;
+    H2B_CUDA(cudaMemcpyAsync(table, d_bases, n * sizeof(G1Affine), cudaMemcpyDeviceToDevice, stream));
+    for (int w = 1; w < p.W; w++) {
+        k_table_double<<<grid_for(n, 128, 148u * 16u), 128, 0, stream>>>(table + (uint64_t)(w - 1) * n, n, p.c, tmp,
+                                                                         den);
+        H2B_LAUNCHED("k_table_double");
+        H2B_TRY(fq_batch_invert(den, n, inv_scratch, inv_bytes, stream));
+        k_table_affine<<<grid_for(n, 256), 256, 0, stream>>>(tmp, den, n, table + (uint64_t)w * n);
+        H2B_LAUNCHED("k_table_affine");
+    }
+    return ok();
+}
+
+extern "C" uint64_t h2b_msm_table_workspace_size(uint64_t n, uint64_t table_n)
+{
+    if (n > table_n || !table_fits(table_n)) return 0;
+    const MsmPlan p = msm_plan_table(n, table_n);
+    ScratchPlan sp;
+    msm_plan_scratch(p, sp, false, false);
+    return sp.used;
+}
+
+// MSM of n <= table_n device scalars over a table built for table_n bases
+// (its first n points of every slice are used); result to d_out (96 B, device).
+extern "C" RustError h2b_msm_device_table(const void* d_scalars, const void* d_table, uint64_t table_n, void* d_out,
+                                          uint64_t n, void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (n > table_n || !table_fits(table_n))
+        return err(cudaErrorInvalidValue, "h2b_msm_device_table: n above the table size, or table size out of range");
+    const MsmPlan p = msm_plan_table(n, table_n);
+    const uint64_t need = h2b_msm_table_workspace_size(n, table_n);
+    if (scratch_bytes < need) return scratch_too_small("h2b_msm_device_table", scratch_bytes, need);
+    ScratchArena ar(scratch, scratch_bytes);
+    MsmScratch s = msm_carve(p, ar, false, false);
+    H2B_TRY(msm_run(p, s, (const Fr*)d_scalars, (const G1Affine*)d_table, stream));
     H2B_CUDA(cudaMemcpyAsync(d_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToDevice, stream));
     return ok();
 }

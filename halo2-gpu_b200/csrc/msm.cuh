@@ -25,6 +25,8 @@ struct MsmPlan {
     int R;               // pairing rounds before the XYZZ accumulation
     uint64_t cap[4];     // entry capacity after round r (cap[0] = max_entries)
     uint32_t Kf;         // entries per XYZZ accumulation chunk after the rounds
+    uint64_t tn;         // points per window slice of a precomputed table (0: plain bases)
+    int Wr;              // windows in the bucket reduction (W, or 1 with a table)
 };
 
 struct MsmScratch {
@@ -57,6 +59,9 @@ struct MsmScratch {
 };
 
 MsmPlan msm_plan(uint64_t n);
+// Plan for an MSM of n <= tn points over a precomputed window table built for
+// tn points (window width chosen by tn; all windows share one bucket set).
+MsmPlan msm_plan_table(uint64_t n, uint64_t tn);
 void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host);
 MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host);
 RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases,

@@ -361,6 +361,18 @@ void h2b_msm_set_accumulate_variant(int variant);
  * MSM workspace-size queries depend on it (set it before sizing scratch). */
 void h2b_msm_set_pair_rounds(int rounds);
 
+/* Precomputed window tables (no counterpart in the reference): an SRS kept resident with its window
+ * multiples [2^(c w)] P_i, so an MSM over it reduces one bucket set and has no final doubling chain.
+ * h2b_msm_table_points: affine points in the table for n bases (0 if n is out of range). */
+uint64_t h2b_msm_table_points(uint64_t n);
+uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n);
+RustError h2b_msm_table_precompute(const void* d_bases, uint64_t n, void* d_table, void* scratch,
+                                   uint64_t scratch_bytes, h2b_stream_t stream);
+/* MSM of n <= table_n device scalars over a table built for table_n bases; 96-byte result at d_out (device). */
+uint64_t h2b_msm_table_workspace_size(uint64_t n, uint64_t table_n);
+RustError h2b_msm_device_table(const void* d_scalars, const void* d_table, uint64_t table_n, void* d_out, uint64_t n,
+                               void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+
 /* Batch execution (no counterpart in the reference, which runs one launcher at a time on one stream).
  * h2b_exec_fork: `n` (1..32) internal non-blocking streams of the current device, ordered after `parent`;
  * created on the first fork on that device and kept until exit.  h2b_exec_join: `parent` waits for them. */
@@ -376,11 +388,12 @@ void h2b_graph_destroy(void* handle);
  * stream); each result is the 96-byte Jacobian image at d_out.  Scratch: h2b_msm_batch_workspace_size. */
 typedef struct h2b_msm_job {
     const void* d_scalars;
-    const void* d_bases;
+    const void* d_bases;   /* plain bases, or a window table built for table_n bases */
     void* d_out;
     uint64_t n;
+    uint64_t table_n;      /* 0: plain bases */
 } h2b_msm_job;
-uint64_t h2b_msm_batch_workspace_size(const uint64_t* lengths, uint64_t count, uint32_t streams);
+uint64_t h2b_msm_batch_workspace_size(const h2b_msm_job* jobs, uint64_t count, uint32_t streams);
 RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
                         uint64_t scratch_bytes, h2b_stream_t stream);
 /* Batch inversion whose CTAs share a single inversion through scratch

@@ -33,7 +33,7 @@ def test_msm_batch_matches_single(h2b, cuda, msm_jobs, streams):
     lengths, d_sc, d_b, want = msm_jobs
     outs = [h2b.dev_empty(96) for _ in lengths]
     jobs = h2b.msm_batch_jobs(d_sc, d_b, outs, lengths)
-    ws = h2b.msm_batch_workspace(lengths, streams)
+    ws = h2b.msm_batch_workspace(jobs, len(lengths), streams)
     for _ in range(2):  # twice in a row: slots are reused
         for o in outs:
             o.zero_()
@@ -46,7 +46,7 @@ def test_msm_batch_argument_errors(h2b, cuda, msm_jobs):
     lengths, d_sc, d_b, _ = msm_jobs
     outs = [h2b.dev_empty(96) for _ in lengths]
     jobs = h2b.msm_batch_jobs(d_sc, d_b, outs, lengths)
-    ws = h2b.msm_batch_workspace(lengths, 2)
+    ws = h2b.msm_batch_workspace(jobs, len(lengths), 2)
     with pytest.raises(h2b.Halo2GpuError):
         h2b.msm_batch(jobs, len(lengths), 33, ws)
     small = h2b.dev_empty(1024)
@@ -73,7 +73,7 @@ def test_forked_streams_and_graph_replay(h2b, cuda, msm_jobs):
     ntt_ws = [h2b.dev_empty(h2b.lib()._halo2_fft_many_to_device_workspace_size(3, k, k + 2)) for k in logs]
     msm_outs = [h2b.dev_empty(96) for _ in lengths]
     jobs = h2b.msm_batch_jobs(d_sc, d_b, msm_outs, lengths)
-    msm_ws = h2b.msm_batch_workspace(lengths, 4)
+    msm_ws = h2b.msm_batch_workspace(jobs, len(lengths), 4)
 
     def reference():
         got_ntt = []

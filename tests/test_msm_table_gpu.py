@@ -1,0 +1,96 @@
+"""Precomputed window tables (SRS kept resident with [2^(c w)] P_i): the table
+entries against Python curve arithmetic, and MSMs over a table against the
+oracle and the plain MSM, including zero scalars, infinity bases, n below the
+table size, and batched jobs over a shared table."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import assert_limbs_equal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def table4k(h2b, orc, cuda):
+    tau = h2b.fields.fr_mont_limbs([0x7AB1E5])
+    srs = orc.srs(tau, 1 << 12)
+    srs[5] = 0                                   # an infinity base
+    d_srs = h2b.to_dev(srs)
+    table = h2b.msm_table_precompute(d_srs, 1 << 12)
+    torch.cuda.synchronize()
+    return srs, d_srs, table
+
+
+def test_table_entries(h2b, table4k):
+    f = h2b.fields
+    srs, _, table = table4k
+    tn = 1 << 12
+    pts = h2b.lib().h2b_msm_table_points(tn)
+    W = pts // tn
+    t = h2b.to_host(table, (pts, 8))
+    # the 2^12-point plan uses 10-bit windows: 13 of them cover the 127-bit GLV halves plus the digit carry
+    c = 10
+    assert W == 13
+    for i in (0, 1, 5, 77, tn - 1):
+        x = f.from_mont(f.limbs_to_ints(srs[i][:4].reshape(1, 4))[0], f.Q_MOD)
+        y = f.from_mont(f.limbs_to_ints(srs[i][4:].reshape(1, 4))[0], f.Q_MOD)
+        P = (x, y)
+        for w in (0, 1, W - 1):
+            got = t[w * tn + i]
+            if i == 5:
+                assert not got.any(), "infinity stays (0, 0)"
+                continue
+            want = f.g1_mul(P, 1 << (c * w))
+            assert f.limbs_to_ints(got[:4].reshape(1, 4))[0] == f.to_mont(want[0], f.Q_MOD)
+            assert f.limbs_to_ints(got[4:].reshape(1, 4))[0] == f.to_mont(want[1], f.Q_MOD)
+
+
+@pytest.mark.parametrize("n", [1, 2, 100, 3000, 4096])
+def test_msm_over_table(h2b, orc, cuda, table4k, n):
+    srs, d_srs, table = table4k
+    tn = 1 << 12
+    sc = orc.chacha_fr(300 + n, n)
+    sc[::7] = 0
+    want = orc.msm(sc, srs[:n])
+    d_sc = h2b.to_dev(sc)
+    out = h2b.dev_empty(96)
+    h2b.msm_device_table(d_sc, table, tn, out, n)
+    assert_limbs_equal(h2b.to_host(out, (12,)), want, f"table msm n={n}")
+    # the plain device MSM gives the same bytes
+    out2 = h2b.dev_empty(96)
+    ws = h2b.msm_workspace(n)
+    h2b.msm_device(d_sc, d_srs, out2, n, ws)
+    assert out.cpu().numpy().tobytes() == out2.cpu().numpy().tobytes()
+
+
+def test_msm_over_table_k16_mix_and_batch(h2b, orc, cuda):
+    """2^16 table, witness-like scalars; then 6 batched jobs over the shared
+    table next to the same jobs over plain bases."""
+    n = 1 << 16
+    d_srs = h2b.srs_device(0x7AB1E, n)
+    table = h2b.msm_table_precompute(d_srs, n)
+    d_sc = h2b.random_fr_device(n, 31, 1)
+    out_t, out_p = h2b.dev_empty(96), h2b.dev_empty(96)
+    h2b.msm_device_table(d_sc, table, n, out_t, n)
+    h2b.msm_device(d_sc, d_srs, out_p, n, h2b.msm_workspace(n))
+    torch.cuda.synchronize()
+    assert out_t.cpu().numpy().tobytes() == out_p.cpu().numpy().tobytes()
+    lengths = [n, 1 << 14, 1000, 1, 1 << 15, 77]
+    scs = [h2b.random_fr_device(m, 40 + i, i % 2) for i, m in enumerate(lengths)]
+    outs_t = [h2b.dev_empty(96) for _ in lengths]
+    outs_p = [h2b.dev_empty(96) for _ in lengths]
+    jt = h2b.msm_batch_jobs(scs, [table] * len(lengths), outs_t, lengths, table_n=n)
+    jp = h2b.msm_batch_jobs(scs, [d_srs] * len(lengths), outs_p, lengths)
+    h2b.msm_batch(jt, len(lengths), 4, h2b.msm_batch_workspace(jt, len(lengths), 4))
+    h2b.msm_batch(jp, len(lengths), 4, h2b.msm_batch_workspace(jp, len(lengths), 4))
+    torch.cuda.synchronize()
+    assert [o.cpu().numpy().tobytes() for o in outs_t] == [o.cpu().numpy().tobytes() for o in outs_p]
+
+
+def test_table_argument_errors(h2b, cuda, table4k):
+    _, _, table = table4k
+    d_sc = h2b.dev_empty(32 * 8192)
+    with pytest.raises(h2b.Halo2GpuError):   # n above the table size
+        h2b.msm_device_table(d_sc, table, 1 << 12, h2b.dev_empty(96), 8192, ws=h2b.dev_empty(1 << 20))
+    assert h2b.lib().h2b_msm_table_points(1 << 28) == 0
