@@ -179,6 +179,131 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def rows_section(h2b, torch, hbm_gbs, imad_peak, k=20, reps=5):
+    """Every other row of the hot path at the k = 20 proof size, timed with
+    CUDA events around the public entry point (as a caller would call it).
+    For each: ms per call, units/s, algorithmic GB/s and its fraction of the
+    measured HBM peak, and (where the product count per unit is fixed) the
+    fraction of the IMAD peak at 264 IMAD-class operations per product."""
+    import numpy as np
+    rules_mod = importlib.util.spec_from_file_location("h2b_rules", os.path.join(ROOT, "halo2-gpu_b200", "rules.py"))
+    R = importlib.util.module_from_spec(rules_mod)
+    rules_mod.loader.exec_module(R)
+    f = h2b.fields
+    L = h2b.lib()
+    n = 1 << k
+    side = torch.cuda.Stream()
+    rnd = lambda m, s: h2b.random_fr_device(m, s, 0)  # noqa: E731
+    out = {}
+
+    def timed(name, fn, units, unit, bytes_per_unit, products_per_unit=None):
+        with torch.cuda.stream(side):
+            fn()
+            side.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(side)
+            for _ in range(reps):
+                fn()
+            e1.record(side)
+        side.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = units * bytes_per_unit / (ms * 1e-3) / 1e9
+        r = {"ms": round(ms, 4), f"{unit}_per_s": units / (ms * 1e-3), "GB_per_s": round(gbs, 1),
+             "hbm_frac": round(gbs / hbm_gbs, 4)}
+        if products_per_unit:
+            r["imad_frac"] = round(units * products_per_unit * 264 / (ms * 1e-3) / imad_peak, 4)
+        out[name] = r
+
+    # a7: quotient evaluator, PLONK + Fibonacci gates over one extended part (rot_scale 4)
+    g = R.Graph()
+    parts = R.plonk_and_fibonacci(g)
+    rules = np.array(g.rules, dtype=np.uint64)
+    prods = sum(1 for i in range(0, len(rules), 2) if (int(rules[i]) >> 44) & 1) + len(parts)
+    fixed, inst, adv = [rnd(n, 10 + i) for i in range(3)], [rnd(n, 20)], [rnd(n, 30 + i) for i in range(4)]
+    ch = f.fr_mont_limbs([0xC4A1])
+    consts = f.fr_mont_limbs(g.constants)
+    vp = np.array(parts, dtype=np.uint64)
+    d_q = h2b.dev_empty(32 * n)
+    timed("quotient_plonk_fib", lambda: h2b.quotient_device(fixed, inst, adv, ch, consts, 0x1234, rules, vp, n, 4, 0,
+                                                            n, d_q, None, stream=side),
+          n, "rows", 9 * 32, prods)
+    # a8: permutation quotient (4 columns, chunk 2 -> 2 sets)
+    vals, l0, ll, la = (rnd(n, 40 + i) for i in range(4))
+    pprods, perms, cols = [rnd(n, 50 + i) for i in range(2)], [rnd(n, 60 + i) for i in range(4)], \
+        [rnd(n, 70 + i) for i in range(4)]
+    sc = lambda s: f.fr_mont_limbs([s])  # noqa: E731
+    dom = f.EvaluationDomain(4, k)
+    timed("permutation_quotient_4col", lambda: h2b.quotient_permutation_device(
+        vals, l0, ll, la, pprods, perms, cols, sc(3), sc(5), sc(7), f.fr_mont_limbs([f.DELTA]), sc(11),
+        f.fr_mont_limbs([pow(dom.extended_omega, 3, f.R_MOD)]), f.fr_mont_limbs([dom.extended_omega]), 2, -5, 4, n, n,
+        stream=side), n, "rows", 15 * 32)
+    # a9: lookup quotient
+    arrs = [rnd(n, 80 + i) for i in range(8)]
+    d_b, d_g, d_y = (h2b.to_dev(sc(s)) for s in (3, 5, 7))
+    timed("lookup_quotient", lambda: h2b.quotient_lookups_device(*arrs, d_b, d_g, d_y, n, stream=side), n, "rows",
+          9 * 32)
+    # a10: permutation grand product (4 columns)
+    mod = rnd(n, 90)
+    pv, pp = [rnd(n, 91 + i) for i in range(4)], [rnd(n, 95 + i) for i in range(4)]
+    d_delta, d_om, d_dw = h2b.to_dev(f.fr_mont_limbs([f.DELTA])), h2b.to_dev(f.fr_mont_limbs([dom.omega])), \
+        h2b.to_dev(sc(1))
+    timed("permutation_product_4col", lambda: h2b.permutation_product_device(
+        mod, pp, pv, d_b, d_g, d_delta, d_om, d_dw, n, stream=side), n, "rows", 9 * 32 + 32)
+    # a11: lookup grand product
+    lo = h2b.dev_empty(32 * n)
+    lk = [rnd(n, 100 + i) for i in range(4)]
+    timed("lookup_product", lambda: h2b.lookup_product_device(lo, *lk, d_b, d_g, n, stream=side), n, "rows", 5 * 32)
+    # grand product scan
+    gp = rnd(n, 110)
+    d_pre = h2b.to_dev(sc(1))
+    timed("grand_product", lambda: h2b.grand_product_device(gp, d_pre, n, stream=side), n, "elements", 64, 2)
+    # a12: batch inversion at the proof size
+    bi = rnd(n, 120)
+    bws = h2b.dev_empty(L.h2b_batch_invert_workspace_size(n))
+    timed("batch_invert", lambda: h2b.call("h2b_batch_invert", h2b.ptr(bi), 0, n, h2b.ptr(bws), bws.numel(),
+                                           h2b.stream_handle(side)), n, "elements", 64, 4)
+    # a13: lookup permute-sort, 2^8-entry table
+    tab = rnd(256, 130)
+    idx = torch.randint(0, 256, (n,), device="cuda")
+    d_in = tab.view(256, 32)[idx].reshape(-1).contiguous()
+    d_pa, d_ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+    d_tab = torch.zeros(32 * n, dtype=torch.uint8, device="cuda")
+    d_tab[: 32 * 256] = tab
+    timed("permute_pair_t256", lambda: h2b.permute_expression_pair_device(d_in, d_tab, d_pa, d_ps, n, n - 10,
+                                                                          stream=side), n, "rows", 4 * 32)
+    # a5: coset extension parts (CosetFFT_Part) for 8 polynomials, one part
+    polys = [rnd(n, 140 + i) for i in range(8)]
+    outs = [h2b.dev_empty(32 * n) for _ in polys]
+    cf = f.ZETA * dom.extended_omega % f.R_MOD
+    nws = h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(6, k, k))
+    timed("coset_part_ntt_x8", lambda: h2b.fft_many_to_device(6, k, k, polys, outs, dom.omega, cf, ws=nws,
+                                                              stream=side), 8 * n, "elements", 64, k / 2 + 1)
+    # a6: divide_by_vanishing over the extended domain (4 * 2^k)
+    ext = rnd(4 * n, 150)
+    d_t = h2b.to_dev(f.fr_mont_limbs(dom.t_evaluations))
+    timed("divide_by_vanishing_ext", lambda: h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(d_t),
+                                                      len(dom.t_evaluations), 4 * n, h2b.stream_handle(side)),
+          4 * n, "elements", 64, 1)
+    # opening: Kate division and Horner evaluation
+    a = rnd(n, 160)
+    dqq = h2b.dev_empty(32 * n)
+    d_u = h2b.to_dev(sc(0xABCDEF))
+    timed("kate_division", lambda: h2b.kate_division_device(a, dqq, d_u, n, stream=side), n, "coefficients", 64, 5)
+    ews = h2b.dev_empty(L._halo2_eval_polynomial_workspace_size(n))
+    pt = f.fr_mont_limbs([0x5A5A5A])
+    res = ctypes.c_void_p()
+    timed("eval_polynomial", lambda: h2b.call("_halo2_eval_polynomial", h2b.ptr(a), ctypes.byref(h2b.host_ffi(pt)),
+                                              ctypes.byref(res), n, h2b.ptr(ews), ews.numel(),
+                                              h2b.stream_handle(side)), n, "coefficients", 32, 1.5)
+    # twiddles: omega^i for i < 2^k
+    tw = h2b.dev_empty(32 * n)
+    d_w = h2b.to_dev(f.fr_mont_limbs([dom.omega]))
+    tws = h2b.dev_empty(L._halo2_generate_omega_powers_workspace_size(k))
+    timed("omega_powers", lambda: h2b.call("_halo2_generate_omega_powers", h2b.ptr(tw), h2b.ptr(d_w), k,
+                                           h2b.ptr(tws), tws.numel(), h2b.stream_handle(side)), n, "elements", 32)
+    return {"k": k, "rows": out}
+
+
 def table_section(h2b, torch, d_srs, d_sc, n, reps):
     """The same k=22 MSM over the SRS kept resident with its window multiples
     (h2b_msm_table_precompute once, then h2b_msm_device_table): one bucket
@@ -582,6 +707,7 @@ def main():
 
     if not args.no_batch:
         line["msm_table"] = table_section(h2b, torch, d_srs, d_sc, n_msm, args.steps)
+        line["rows_k20"] = rows_section(h2b, torch, hbm, imad_peak)
         line["batch"] = batch_section(h2b, torch)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_msm()
