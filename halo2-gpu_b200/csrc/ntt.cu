@@ -59,20 +59,20 @@ __device__ __forceinline__ Fr pow_from_lut(const Fr* __restrict__ lut, uint64_t 
     return r;
 }
 
-// tw[e] = w^e for e < half, using lut[i] = w^(2^i).
-constexpr int TW_CHUNK = 16;
-__global__ void k_twiddles(const Fr* __restrict__ lut, Fr* __restrict__ tw, uint64_t half)
+// tw[e] = w^e for e < half, using lut[i] = w^(2^i).  CTA b owns the tile
+// [b T K, (b + 1) T K); thread t starts at w^(b T K + t) and steps by w^T, so a
+// warp stores 32 consecutive twiddles per step (coalesced).
+constexpr int TW_T = 256, TW_LOGT = 8, TW_K = 16;
+__global__ void __launch_bounds__(TW_T) k_twiddles(const Fr* __restrict__ lut, Fr* __restrict__ tw, uint64_t half)
 {
-    uint64_t nthreads = (half + TW_CHUNK - 1) / TW_CHUNK;
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t e0 = t * TW_CHUNK;
-        Fr p = pow_from_lut(lut, e0);
-        Fr w = ldg(&lut[0]);
-        for (int j = 0; j < TW_CHUNK && e0 + j < half; j++) {
-            st(&tw[e0 + j], p);
-            p = p * w;
-        }
+    uint64_t e = blockIdx.x * (uint64_t)(TW_T * TW_K) + threadIdx.x;
+    if (e >= half) return;
+    Fr p = pow_from_lut(lut, e);
+    const Fr step = half > (uint64_t)TW_T ? ldg(&lut[TW_LOGT]) : Fr::one();  // lut covers bit 8 when half > 256
+#pragma unroll 1
+    for (int j = 0; j < TW_K && e < half; j++, e += TW_T) {
+        st(&tw[e], p);
+        p = p * step;
     }
 }
 
@@ -188,8 +188,7 @@ __global__ void k_bitrev_inplace(Fr* __restrict__ a, int k, bool scale, Zeta3 z3
 //   DIF: stage s pairs (i, i + n/2^(s+1)), twiddle w^((i mod n/2^(s+1)) * 2^s),
 //        groups: stride S = n / 2^(s0+nst).
 // A CTA owns G = TILE >> nst consecutive groups (G * 2^nst = TILE elements).
-constexpr int NTT_LOG_TILE = 10;
-constexpr int NTT_TILE = 1 << NTT_LOG_TILE;
+constexpr int NTT_LOG_TILE = 10;  // at most 2^10 elements per pass tile
 constexpr int NTT_THREADS = 512;
 
 // One pass: nst consecutive stages on groups of 2^nst elements at stride
@@ -341,8 +340,8 @@ static RustError make_twiddles(const Fr* d_omega, NttScratch& s, int logn, cudaS
     k_pow2_lut<<<1, 32, 0, st>>>(d_omega, s.lut_w, logn);
     H2B_LAUNCHED("k_pow2_lut");
     uint64_t half = 1ull << (logn - 1);
-    uint64_t nthreads = (half + TW_CHUNK - 1) / TW_CHUNK;
-    k_twiddles<<<grid_for(nthreads, 256), 256, 0, st>>>(s.lut_w, s.tw, half);
+    const uint64_t tile = (uint64_t)TW_T * TW_K;
+    k_twiddles<<<(unsigned)((half + tile - 1) / tile), TW_T, 0, st>>>(s.lut_w, s.tw, half);
     H2B_LAUNCHED("k_twiddles");
     return ok();
 }
