@@ -334,6 +334,35 @@ def table_section(h2b, torch, d_srs, d_sc, n, reps):
     return res
 
 
+def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9):
+    """The prover-shaped workload (halo2-gpu_b200/prover.py: per proof the
+    advice, lookup, permutation and quotient commitments, the per-part coset
+    NTTs and quotients, h, and the opening) served from one GPU.  A seeded
+    Poisson trace of `count` requests with k in {16, 18, 20, 22} (weights
+    .4/.3/.2/.1) arrives at 1.2x the rate the one-at-a-time prover sustains
+    (its mean service time measured first, one request per k, untimed
+    warm-up); the same trace is then run plain (one slot) and served (`slots`
+    worker streams under an HBM budget).  Reports proofs/s over the makespan
+    and p50/p99 latency (arrival to completion, host clock)."""
+    P = importlib.import_module(h2b.__name__ + ".prover")
+    res = P.Resident(h2b, kmax)
+    ks, weights = (16, 18, 20, 22), (0.4, 0.3, 0.2, 0.1)
+    plain = P.Server(res, 1, 96 << 30)
+    service = {}
+    for k in ks:
+        plain.serve([(0.0, k, 7 + k)])
+        r = plain.serve([(0.0, k, 8 + k)])
+        service[k] = float(r["latency_s"][0])
+    mean_s = sum(w * service[k] for k, w in zip(ks, weights))
+    rate = 1.2 / mean_s
+    reqs = P.requests(count, rate, seed, ks, weights)
+    out = {"requests": count, "arrival_rate_per_s": round(rate, 3), "slots": slots, "hbm_budget_GB": 96,
+           "service_ms_alone": {str(k): round(v * 1e3, 2) for k, v in service.items()}}
+    out["plain"] = P.summary(reqs, plain.serve(reqs))
+    out["served"] = P.summary(reqs, P.Server(res, slots, 96 << 30).serve(reqs))
+    return out
+
+
 def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
     """Batched jobs of uneven size: n_jobs jobs with k drawn from {14, 16, 18,
     20} (weights .4/.3/.2/.1, seeded), each one MSM with uniform scalars
@@ -502,9 +531,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
-    ap.add_argument("--case", choices=["msm", "ntt", "bi"], help="run one kernel family only (profiling runs)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
+    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve"],
+                    help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     args = ap.parse_args()
+    if args.case == "serve":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"case": "serve", "serving": serving_section(load_pkg(), torch)}))
+        return
     if args.case:
         run_case(args)
         return
@@ -709,6 +745,8 @@ def main():
         line["msm_table"] = table_section(h2b, torch, d_srs, d_sc, n_msm, args.steps)
         line["rows_k20"] = rows_section(h2b, torch, hbm, imad_peak)
         line["batch"] = batch_section(h2b, torch)
+    if world == 1 and not args.no_serve:
+        line["serving"] = serving_section(h2b, torch)
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline_msm()
     if rank == 0:

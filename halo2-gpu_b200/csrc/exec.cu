@@ -19,7 +19,6 @@
 //    stream with its own slice of the caller's scratch.
 #include <algorithm>
 #include <map>
-#include <mutex>
 #include <numeric>
 #include <vector>
 #include "abi.cuh"
@@ -36,17 +35,18 @@ struct DevExec {
     cudaEvent_t fork_ev = nullptr;
     std::vector<cudaEvent_t> join_ev;
 };
-std::mutex g_exec_mu;
-std::map<int, DevExec> g_exec;
+// Per calling thread: callers on different threads (one per served request,
+// say) never share forked streams or events, so their forks and joins cannot
+// interleave.
+thread_local std::map<int, DevExec> t_exec;
 
-// Streams and events of the current device, created on first use.
+// Streams and events of the current device and thread, created on first use.
 RustError exec_get(uint32_t n, DevExec** out)
 {
     if (n == 0 || n > EXEC_MAX_STREAMS) return err((int)cudaErrorInvalidValue, "exec: streams must be in 1..32");
     int dev = 0;
     H2B_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(g_exec_mu);
-    DevExec& d = g_exec[dev];
+    DevExec& d = t_exec[dev];
     if (!d.fork_ev) H2B_CUDA(cudaEventCreateWithFlags(&d.fork_ev, cudaEventDisableTiming));
     while (d.streams.size() < n) {
         cudaStream_t s;

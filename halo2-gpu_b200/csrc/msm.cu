@@ -44,6 +44,8 @@ static constexpr uint64_t MSM_MAX_LENGTH = 1ull << 27;
 static constexpr uint32_t SIGN_BIT = 0x80000000u;
 static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed serially in fixup
 static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
+static constexpr uint64_t ACC_TARGET_CHUNKS = 148ull * 3 * 128 * 4;  // accumulation threads x 4
+static constexpr uint64_t ACC_MIN_K = 16;       // smallest chunk of the default plan
 
 static int g_msm_window_override = 0;
 static int g_msm_acc_variant = 0;  // call structure of the accumulation kernel (0, 1, 2)
@@ -95,9 +97,16 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn)
     p.H = 1u << (c - 1);
     p.Wr = tn ? 1 : p.W;
     p.NB = (uint64_t)p.Wr * p.H;
-    p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override : 128u;
     p.nv = 2 * n;
     p.max_entries = p.nv * (uint64_t)p.W;
+    // Entries per accumulation chunk (one thread walks a chunk): 128 when the
+    // entries give at least ACC_TARGET_CHUNKS chunks (k >= 20 at every
+    // window size), fewer for small MSMs so that about ACC_TARGET_CHUNKS
+    // threads still run (148 SMs x 3 CTAs x 128 threads, 4 chunks each);
+    // a smaller K only adds chunk heads for the fixup to merge.
+    const uint64_t k_fit = p.max_entries / ACC_TARGET_CHUNKS;
+    p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override
+                                   : (uint32_t)std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
     // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
     p.R = tn ? 0 : g_msm_pair_rounds;
     p.cap[0] = p.max_entries;

@@ -81,6 +81,17 @@ __device__ __forceinline__ uint64_t bitrev(uint64_t x, int k)
     return k == 0 ? 0 : (__brevll(x) >> (64 - k));
 }
 
+// Pointers of up to NTT_MAX_BATCH transforms of one size run by the same
+// launches (blockIdx.y selects the transform): the polynomials of one
+// `_halo2_fft_many*` call share the twiddles, the divisor and every launch,
+// so small transforms fill the GPU together instead of one after another.
+// src[i] may equal dst[i] (in-place transforms).
+constexpr int NTT_MAX_BATCH = 32;
+struct NttBatch {
+    const Fr* src[NTT_MAX_BATCH];
+    Fr* dst[NTT_MAX_BATCH];
+};
+
 // Forward-path input stage: out[rev(i)] = in[i] * f(i) for i < n_out, where
 // in[i] = 0 for i >= n_in (zero padding) and f is
 //   mode 0: 1,   mode 1: c^i (lut_c[j] = c^(2^j)),   mode 2: z3[i mod 3].
@@ -89,9 +100,11 @@ constexpr int SC_CHUNK = 8;
 struct Zeta3 {
     Fr f[3];
 };
-__global__ void k_twist_bitrev_scatter(const Fr* __restrict__ in, Fr* __restrict__ out, uint64_t n_in, int log_out,
-                                       int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
+__global__ void k_twist_bitrev_scatter(NttBatch B, uint64_t n_in, int log_out, int mode,
+                                       const Fr* __restrict__ lut_c, Zeta3 z3)
 {
+    const Fr* __restrict__ in = B.src[blockIdx.y];
+    Fr* __restrict__ out = B.dst[blockIdx.y];
     uint64_t n_out = 1ull << log_out;
     uint64_t nthreads = n_out / SC_CHUNK + (n_out % SC_CHUNK ? 1 : 0);
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
@@ -122,8 +135,10 @@ __global__ void k_twist_bitrev_scatter(const Fr* __restrict__ in, Fr* __restrict
 // other slot of that aligned group of 2^e is zero, so the first e DIT stages
 // only copy the value across the group.  This writes the twisted input
 // a_i * zeta^(i mod 3) to all 2^e slots; the DIT passes then start at stage e.
-__global__ void k_coset_spread(const Fr* __restrict__ in, Fr* __restrict__ out, int log_in, int e, Zeta3 z3)
+__global__ void k_coset_spread(NttBatch B, int log_in, int e, Zeta3 z3)
 {
+    const Fr* __restrict__ in = B.src[blockIdx.y];
+    Fr* __restrict__ out = B.dst[blockIdx.y];
     uint64_t n_in = 1ull << log_in;
     const uint64_t g = 1ull << e;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_in;
@@ -135,8 +150,9 @@ __global__ void k_coset_spread(const Fr* __restrict__ in, Fr* __restrict__ out, 
 }
 
 // In-place a_i *= c^i (mode 1) or zeta^(i mod 3) factors (mode 2).
-__global__ void k_twist_inplace(Fr* __restrict__ a, uint64_t n, int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
+__global__ void k_twist_inplace(NttBatch B, uint64_t n, int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
 {
+    Fr* __restrict__ a = B.dst[blockIdx.y];
     uint64_t nthreads = n / SC_CHUNK + (n % SC_CHUNK ? 1 : 0);
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
          t += (uint64_t)gridDim.x * blockDim.x) {
@@ -162,8 +178,9 @@ __global__ void k_twist_inplace(Fr* __restrict__ a, uint64_t n, int mode, const 
 
 // In-place bit reversal; when `scale` each element landing at index i is
 // multiplied by z3.f[i mod 3] (used for divisor and divisor*zeta^-(i mod 3)).
-__global__ void k_bitrev_inplace(Fr* __restrict__ a, int k, bool scale, Zeta3 z3)
+__global__ void k_bitrev_inplace(NttBatch B, int k, bool scale, Zeta3 z3)
 {
+    Fr* __restrict__ a = B.dst[blockIdx.y];
     uint64_t n = 1ull << k;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t j = bitrev(i, k);
@@ -197,9 +214,11 @@ constexpr int NTT_THREADS = 512;
 // power of two, so all index arithmetic is shifts and masks on 32 bits
 // (n <= 2^31).
 template <bool DIT>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(Fr* __restrict__ a, const Fr* __restrict__ tw, int logn,
-                                                          int s0, int nst, int lS, int lG)
+__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
+                                                          int nst, int lS, int lG)
 {
+    const Fr* src = B.src[blockIdx.y];  // the first pass of an out-of-place transform reads here
+    Fr* a = B.dst[blockIdx.y];
     extern __shared__ uint4 smem_raw[];
     Fr* sm = reinterpret_cast<Fr*>(smem_raw);
     const uint32_t Smask = (1u << lS) - 1;
@@ -224,7 +243,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(Fr* __restrict__ a, co
     for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
         uint32_t slot;
         const uint32_t addr = locate(idx, slot);
-        sm[slot] = ld(&a[addr]);
+        sm[slot] = ld(&src[addr]);
     }
     __syncthreads();
 
@@ -274,8 +293,10 @@ void ntt_set_pass_stages(int b)
     if (b >= 1 && b <= 10) g_max_pass_stages = b;
 }
 
-// Runs radix-2 stages [first, logn) in passes of at most g_max_pass_stages.
-static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_t st, int first = 0)
+// Runs radix-2 stages [first, logn) of `count` transforms in passes of at
+// most g_max_pass_stages stages.  The first pass reads B.src and writes B.dst;
+// the later ones work in place on B.dst.
+static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool dit, cudaStream_t st, int first = 0)
 {
     if (logn - first <= 0) return ok();
     int todo = logn - first;
@@ -287,14 +308,15 @@ static RustError run_passes(Fr* a, const Fr* tw, int logn, bool dit, cudaStream_
         int nst = base + (p < extra ? 1 : 0);
         const int lS = dit ? s0 : logn - s0 - nst;
         const int lG = std::min(NTT_LOG_TILE - nst, logn - nst);
-        const uint64_t blocks = 1ull << (logn - nst - lG);
+        const dim3 grid((unsigned)(1ull << (logn - nst - lG)), (unsigned)count);
         size_t smem = (size_t)(1ull << (lG + nst)) * sizeof(Fr);
         int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 1)));
         if (dit)
-            k_ntt_pass<true><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst, lS, lG);
+            k_ntt_pass<true><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
         else
-            k_ntt_pass<false><<<(unsigned)blocks, threads, smem, st>>>(a, tw, logn, s0, nst, lS, lG);
+            k_ntt_pass<false><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
         H2B_LAUNCHED("k_ntt_pass");
+        for (int i = 0; i < count; i++) B.src[i] = B.dst[i];
         s0 += nst;
     }
     prof_end(PROF_NTT_PASSES, st);
@@ -367,12 +389,12 @@ static Zeta3 scale_factors(const host::Fr64& scale)
     return out;
 }
 
-// Core: one transform into `d_out` (device).  `in` may be host (in_host) or
-// device, and may alias d_out only when it is device memory.
+// Core: `count` (<= NTT_MAX_BATCH) transforms of one type and size, B.src[i]
+// -> B.dst[i], all on the device.  `alias`: every B.src[i] == B.dst[i].
 //   log_n   : input length (and transform size except for coset types)
 //   log_ext : transform size for cosetFFT / icosetFFT
-static RustError transform_one(int type, int log_n, int log_ext, const void* in, bool in_host, Fr* d_out,
-                               const host::Fr64* h_divisor, NttScratch& s, cudaStream_t st)
+static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, int count, bool alias,
+                                 const host::Fr64* h_divisor, NttScratch& s, cudaStream_t st)
 {
     using namespace host;
     const bool coset_full = (type == 3 || type == 4);
@@ -380,14 +402,9 @@ static RustError transform_one(int type, int log_n, int log_ext, const void* in,
     const uint64_t nt = 1ull << logt;
     const uint64_t nin = 1ull << log_n;
     Zeta3 none = scale_factors(fr_const(FR_ONE));
-
-    // Stage input on the device when it lives on the host.
-    const Fr* din = (const Fr*)in;
-    if (in_host) {
-        H2B_CUDA(cudaMemcpyAsync(d_out, in, nin * sizeof(Fr), cudaMemcpyHostToDevice, st));
-        din = d_out;
-    }
-    const bool alias = (din == d_out);
+    NttBatch D = B;  // in place on the outputs
+    for (int i = 0; i < count; i++) D.src[i] = D.dst[i];
+    auto grid = [&](uint64_t work) { return dim3(grid_for(work, 256), (unsigned)count); };
 
     if (type == 1 || type == 6 || type == 3) {
         int mode = 0;
@@ -403,44 +420,62 @@ static RustError transform_one(int type, int log_n, int log_ext, const void* in,
         }
         if (!alias && type == 3 && logt > log_n) {
             int e = logt - log_n;
-            k_coset_spread<<<grid_for(nin, 256), 256, 0, st>>>(din, d_out, log_n, e, z3);
+            k_coset_spread<<<grid(nin), 256, 0, st>>>(B, log_n, e, z3);
             H2B_LAUNCHED("k_coset_spread");
-            return run_passes(d_out, s.tw, logt, true, st, e);
+            return run_passes(D, count, s.tw, logt, true, st, e);
         }
+        const uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
         if (!alias) {
-            uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
-            k_twist_bitrev_scatter<<<grid_for(nthreads, 256), 256, 0, st>>>(din, d_out, type == 3 ? nin : nt,
-                                                                            logt, mode, s.lut_c, z3);
+            k_twist_bitrev_scatter<<<grid(nthreads), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.lut_c, z3);
             H2B_LAUNCHED("k_twist_bitrev_scatter");
         } else {
             if (type == 3 && nt != nin) {
                 // zero the padding in place, then twist + reverse
-                H2B_CUDA(cudaMemsetAsync(d_out + nin, 0, (nt - nin) * sizeof(Fr), st));
+                for (int i = 0; i < count; i++)
+                    H2B_CUDA(cudaMemsetAsync(D.dst[i] + nin, 0, (nt - nin) * sizeof(Fr), st));
             }
             if (mode != 0) {
-                uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
-                k_twist_inplace<<<grid_for(nthreads, 256), 256, 0, st>>>(d_out, nt, mode, s.lut_c, z3);
+                k_twist_inplace<<<grid(nthreads), 256, 0, st>>>(D, nt, mode, s.lut_c, z3);
                 H2B_LAUNCHED("k_twist_inplace");
             }
-            k_bitrev_inplace<<<grid_for(nt, 256), 256, 0, st>>>(d_out, logt, false, none);
+            k_bitrev_inplace<<<grid(nt), 256, 0, st>>>(D, logt, false, none);
             H2B_LAUNCHED("k_bitrev_inplace");
         }
-        return run_passes(d_out, s.tw, logt, true, st);
+        return run_passes(D, count, s.tw, logt, true, st);
     }
     if (type == 2 || type == 4) {
-        if (!alias) {
-            H2B_CUDA(cudaMemcpyAsync(d_out, din, nin * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
+        NttBatch P = alias ? D : B;  // the first DIF pass reads the inputs
+        if (type == 4) {
+            for (int i = 0; i < count; i++) {
+                if (!alias)
+                    H2B_CUDA(cudaMemcpyAsync(D.dst[i], B.src[i], nin * sizeof(Fr), cudaMemcpyDeviceToDevice, st));
+                if (nt != nin) H2B_CUDA(cudaMemsetAsync(D.dst[i] + nin, 0, (nt - nin) * sizeof(Fr), st));
+            }
+            P = D;
         }
-        if (type == 4 && nt != nin) {
-            H2B_CUDA(cudaMemsetAsync(d_out + nin, 0, (nt - nin) * sizeof(Fr), st));
-        }
-        H2B_TRY(run_passes(d_out, s.tw, logt, false, st));
+        H2B_TRY(run_passes(P, count, s.tw, logt, false, st));
         Zeta3 z3 = (type == 4) ? zeta_factors(*h_divisor, true) : scale_factors(*h_divisor);
-        k_bitrev_inplace<<<grid_for(nt, 256), 256, 0, st>>>(d_out, logt, true, z3);
+        k_bitrev_inplace<<<grid(nt), 256, 0, st>>>(D, logt, true, z3);
         H2B_LAUNCHED("k_bitrev_inplace");
         return ok();
     }
     return err(-1, "unsupported ntt_type");
+}
+
+// One transform into `d_out` (device).  `in` may be host (in_host) or device,
+// and may alias d_out only when it is device memory.
+static RustError transform_one(int type, int log_n, int log_ext, const void* in, bool in_host, Fr* d_out,
+                               const host::Fr64* h_divisor, NttScratch& s, cudaStream_t st)
+{
+    const Fr* din = (const Fr*)in;
+    if (in_host) {
+        H2B_CUDA(cudaMemcpyAsync(d_out, in, (sizeof(Fr) << log_n), cudaMemcpyHostToDevice, st));
+        din = d_out;
+    }
+    NttBatch B;
+    B.src[0] = din;
+    B.dst[0] = d_out;
+    return transform_group(type, log_n, log_ext, B, 1, din == d_out, h_divisor, s, st);
 }
 
 static RustError check_type(uint32_t t)
@@ -571,14 +606,55 @@ static RustError fft_many_impl(uint32_t ntt_type, uint32_t num_many, uint32_t lo
     NttScratch s = carve_ntt(ar, la, !out_on_device, la);
     H2B_TRY(make_twiddles((const Fr*)d_omega, s, la, stream));
     host::Fr64 div = (divisor && divisor->ptr) ? host::fr_from(divisor->ptr) : host::fr_const(host::FR_ONE);
-    for (uint32_t i = 0; i < num_many; i++) {
-        Fr* dst = out_on_device ? (Fr*)output[i].ptr : s.data;
-        H2B_TRY(transform_one(ntt_type, log_n, extend_log_n, input[i].ptr, !in_on_device, dst, &div, s, stream));
-        if (!out_on_device) {
+    if (!out_on_device) {
+        // one device slot: stage, transform and copy back one polynomial at a time
+        for (uint32_t i = 0; i < num_many; i++) {
+            H2B_TRY(transform_one(ntt_type, log_n, extend_log_n, input[i].ptr, !in_on_device, s.data, &div, s,
+                                  stream));
             H2B_CUDA(cudaMemcpyAsync(output[i].ptr, s.data, sizeof(Fr) << la, cudaMemcpyDeviceToHost, stream));
         }
+        H2B_CUDA(cudaStreamSynchronize(stream));
+        return ok();
     }
-    if (!out_on_device) H2B_CUDA(cudaStreamSynchronize(stream));
+    // An output that overlaps another polynomial's device input makes the
+    // result depend on the order of the transforms: run them one at a time.
+    bool cross = false;
+    if (in_on_device) {
+        const uint64_t out_b = sizeof(Fr) << la, in_b = sizeof(Fr) << log_n;
+        for (uint32_t i = 0; i < num_many && !cross; i++)
+            for (uint32_t j = 0; j < num_many && !cross; j++) {
+                const uintptr_t o = (uintptr_t)output[i].ptr, x = (uintptr_t)input[j].ptr;
+                cross = i != j && o < x + in_b && x < o + out_b;
+            }
+    }
+    if (cross) {
+        for (uint32_t i = 0; i < num_many; i++)
+            H2B_TRY(transform_one(ntt_type, log_n, extend_log_n, input[i].ptr, false, (Fr*)output[i].ptr, &div, s,
+                                  stream));
+        return ok();
+    }
+    // device outputs: host inputs are staged into their outputs, then the
+    // transforms run in groups (in-place ones and out-of-place ones apart)
+    NttBatch grp[2];
+    int cnt[2] = {0, 0};
+    for (uint32_t i = 0; i < num_many; i++) {
+        Fr* dst = (Fr*)output[i].ptr;
+        const Fr* src = (const Fr*)input[i].ptr;
+        if (!in_on_device) {
+            H2B_CUDA(cudaMemcpyAsync(dst, src, sizeof(Fr) << log_n, cudaMemcpyHostToDevice, stream));
+            src = dst;
+        }
+        const int g = src == dst ? 1 : 0;
+        grp[g].src[cnt[g]] = src;
+        grp[g].dst[cnt[g]] = dst;
+        if (++cnt[g] == NTT_MAX_BATCH || i + 1 == num_many) {
+            for (int h = 0; h < 2; h++) {
+                if (cnt[h] == 0 || (h != g && i + 1 != num_many)) continue;
+                H2B_TRY(transform_group(ntt_type, log_n, extend_log_n, grp[h], cnt[h], h == 1, &div, s, stream));
+                cnt[h] = 0;
+            }
+        }
+    }
     return ok();
 }
 

@@ -1,0 +1,349 @@
+"""Prover-shaped GPU workload and a serving loop around it.
+
+`ProofWorkload.run` issues, on one stream, the device work that `create_proof`
+(halo2_proofs/src/plonk/prover.rs:56-482) sends to the GPU for the config-3
+circuit family (4 advice, 3 fixed, 1 instance column; a standard-PLONK gate
+and a Fibonacci rotation gate; a 4-column copy permutation; one lookup into a
+2^8-entry table), through this library's entry points in the reference's
+order:
+
+  1. witness columns (seeded, generated on the device: synthesis stands in);
+  2. advice commitments (MSMs over the resident SRS window table);
+  3. lookup: permute-sort of the input against the table, A' and S' commits;
+  4. permutation grand products (2 sets of 2 columns) and lookup grand
+     product, and their commits;
+  5. lagrange_to_coeff of the per-proof polynomials (iNTT);
+  6. per extended part (4): coset-part NTTs of every polynomial, the gate
+     quotient (evaluate_h), the permutation and the lookup quotients;
+  7. h: the parts gathered and brought to coefficients on the extended
+     coset, and its 3 pieces committed;
+  8. opening: evaluations at x, Kate divisions, 2 commits.
+
+Challenges come from a seeded generator, not a transcript, and the witness
+does not satisfy the circuit, so the outputs are deterministic GPU work, not
+a proof: whole-proof parity needs the Rust transcript and serde.  What this
+measures is the served prover's device side: proofs/s and latency when
+requests of uneven k share one GPU.
+
+`Server` runs such requests with `slots` worker threads, each on its own
+stream (the GPU overlaps them), admitting a request when a slot is free and
+the HBM budget allows; `plain` runs them one at a time.
+"""
+import queue
+import threading
+import time
+
+import numpy as np
+
+from . import fields as F
+from . import rules as R
+
+_torch = None
+
+
+def _t():
+    global _torch
+    if _torch is None:
+        import torch
+        _torch = torch
+    return _torch
+
+
+def _bytes_per_proof(k):
+    """Device memory one in-flight proof of size 2^k holds besides its MSM
+    scratch (upper bound): 11 Lagrange and 11 coefficient polynomials, 21
+    coset parts, 4 quotient parts, 8 extended-domain vectors, 2 Kate
+    quotients, evaluation scratch and small tensors."""
+    n = 1 << k
+    return 64 * 32 * n + (64 << 20)
+
+
+class Resident:
+    """State kept on the device across requests: the SRS window table and,
+    per k, the proving-key polynomials (fixed, sigma, Lagrange selectors) in
+    coefficient form, the lookup table column and the domain constants."""
+
+    def __init__(self, h2b, kmax, seed=0x5EED):
+        self.h2b = h2b
+        self.kmax = kmax
+        self.srs = h2b.srs_device(seed, 1 << kmax)
+        self.table = h2b.msm_table_precompute(self.srs, 1 << kmax)
+        self.pk = {}
+        g = R.Graph()
+        self.parts = np.array(R.plonk_and_fibonacci(g), dtype=np.uint64)
+        self.rules = np.array(g.rules, dtype=np.uint64)
+        self.consts = F.fr_mont_limbs(g.constants)
+
+    def key(self, k):
+        if k not in self.pk:
+            h2b, n = self.h2b, 1 << k
+            dom = F.EvaluationDomain(4, k)
+            rnd = lambda s: h2b.random_fr_device(n, s, 0)  # noqa: E731
+            pk = {"dom": dom,
+                  "fixed": [rnd(1000 * k + i) for i in range(3)],
+                  "sigma": [rnd(1000 * k + 10 + i) for i in range(4)],
+                  "lag": [rnd(1000 * k + 20 + i) for i in range(3)],  # l0, l_last, l_active
+                  "table": h2b.random_fr_device(256, 1000 * k + 30, 0),
+                  "t_evals": h2b.to_dev(F.fr_mont_limbs(dom.t_evaluations))}
+            tab_col = _t().zeros(32 * n, dtype=_t().uint8, device="cuda")
+            tab_col[: 32 * 256] = pk["table"]
+            pk["table_col"] = tab_col
+            self.pk[k] = pk
+        return self.pk[k]
+
+
+def _slice(t, i, n):
+    """Elements [i n, (i + 1) n) of a device field vector."""
+    return t[32 * n * i: 32 * n * (i + 1)]
+
+
+class ProofWorkload:
+    """The device work of one proof of size 2^k (see the module docstring)."""
+
+    def __init__(self, res, k, seed):
+        self.res, self.k, self.seed = res, k, seed
+
+    def run(self, stream):
+        """Issues everything on `stream` (the calling thread blocks only where
+        an entry point synchronises: the permute-sort and the permutation
+        quotient); returns the commitments (96 B each) and evaluations (32 B
+        each) as device tensors, complete once `stream` is."""
+        torch, h2b, res = _t(), self.res.h2b, self.res
+        k, n, seed = self.k, 1 << self.k, self.seed
+        pk = res.key(k)
+        dom = pk["dom"]
+        tn = 1 << res.kmax
+        rng = np.random.default_rng(seed)
+        chal = lambda: int(rng.integers(1, 1 << 62))  # noqa: E731
+        sc = lambda v: F.fr_mont_limbs([v % F.R_MOD])  # noqa: E731
+        with torch.cuda.stream(stream):
+            commits, evals, pending = [], [], []
+            probe = h2b.dev_empty(32)
+            slots = h2b.msm_batch_jobs([probe] * 4, [res.table] * 4, [probe] * 4, [n] * 4, table_n=tn)
+            msm_ws = h2b.msm_batch_workspace(slots, 4, 4)
+
+            def commit(d, m=n):
+                out = h2b.dev_empty(96)
+                pending.append((d, out, m))
+                commits.append(out)
+
+            def flush():
+                """The commitments of one phase as one batch: each MSM on its own
+                forked stream, so their serial tails overlap."""
+                jobs = h2b.msm_batch_jobs([p[0] for p in pending], [res.table] * len(pending),
+                                          [p[1] for p in pending], [p[2] for p in pending], table_n=tn)
+                h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
+                pending.clear()
+
+            # 1-2. witness and advice commitments
+            adv = [h2b.random_fr_device(n, seed * 64 + i, 1, stream) for i in range(4)]
+            inst = h2b.random_fr_device(n, seed * 64 + 4, 0, stream)
+            for a in adv:
+                commit(a)
+            flush()
+            # 3. lookup: the input takes values of the table; permute-sort, commit A', S'
+            gen = torch.Generator(device="cuda")
+            gen.manual_seed(seed)
+            idx = torch.randint(0, 256, (n,), device="cuda", generator=gen)
+            lin = pk["table"].view(256, 32)[idx].reshape(-1)
+            pa, ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+            h2b.permute_expression_pair_device(lin, pk["table_col"], pa, ps, n, n - 10, stream=stream)
+            commit(pa)
+            commit(ps)
+            flush()
+            # 4. permutation grand products (2 sets of 2 columns), lookup grand product
+            beta, gamma = sc(chal()), sc(chal())
+            d_beta, d_gamma = h2b.to_dev(beta), h2b.to_dev(gamma)
+            d_delta, d_om = h2b.to_dev(F.fr_mont_limbs([F.DELTA])), h2b.to_dev(F.fr_mont_limbs([dom.omega]))
+            d_one = h2b.to_dev(sc(1))
+            zs = []
+            for s in range(2):
+                z = h2b.dev_empty(32 * n)
+                h2b.call("_halo2_poly_fill_one", h2b.ptr(z), n, h2b.stream_handle(stream))
+                d_dw = h2b.to_dev(sc(pow(F.DELTA, 2 * s, F.R_MOD)))
+                h2b.permutation_product_device(z, pk["sigma"][2 * s: 2 * s + 2], adv[2 * s: 2 * s + 2], d_beta,
+                                               d_gamma, d_delta, d_om, d_dw, n, stream=stream)
+                h2b.grand_product_device(z, d_one, n, stream=stream)
+                zs.append(z)
+                commit(z)
+            zl = h2b.dev_empty(32 * n)
+            h2b.lookup_product_device(zl, pa, ps, lin, pk["table_col"], d_beta, d_gamma, n, stream=stream)
+            h2b.grand_product_device(zl, d_one, n, stream=stream)
+            commit(zl)
+            flush()
+            # 5. lagrange_to_coeff of the per-proof polynomials
+            lag = adv + [inst] + zs + [zl, pa, ps, lin]
+            coef = [h2b.dev_empty(32 * n) for _ in lag]
+            h2b.fft_many_to_device(2, k, k, lag, coef, dom.omega_inv, dom.ifft_divisor, stream=stream)
+            del lag
+            # 6. per extended part: coset-part NTTs, gate / permutation / lookup quotients.
+            #    Columns: advice 0-3, instance 4, z 5-6, lookup z 7, A' 8, S' 9,
+            #    compressed input 10, fixed 11-13, sigma 14-17, l0 18, l_last 19, l_active 20.
+            y, theta = chal(), chal()
+            d_y = h2b.to_dev(sc(y))
+            keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
+            allc = coef + keyp
+            parts = [h2b.dev_empty(32 * n) for _ in allc]
+            hs = [h2b.dev_empty(32 * n) for _ in range(1 << (dom.extended_k - k))]
+            ext_w = dom.extended_omega
+            nws = h2b.dev_empty(h2b.lib()._halo2_fft_many_to_device_workspace_size(6, k, k))
+            beta_v = F.fr_from_mont_limbs(beta)[0]
+            for j, hj in enumerate(hs):
+                shift = pow(ext_w, j, F.R_MOD)
+                h2b.fft_many_to_device(6, k, k, allc, parts, dom.omega, F.ZETA * shift % F.R_MOD, ws=nws,
+                                       stream=stream)
+                h2b.quotient_device(parts[11:14], [parts[4]], parts[0:4], sc(theta), res.consts, y, res.rules,
+                                    res.parts, n, 1, 0, n, hj, None, stream=stream)
+                h2b.quotient_permutation_device(hj, parts[18], parts[19], parts[20], parts[5:7], parts[14:18],
+                                                parts[0:4], beta, gamma, sc(y), F.fr_mont_limbs([F.DELTA]),
+                                                sc(beta_v * F.ZETA), sc(shift), sc(dom.omega), 2, -3, 1, n, n,
+                                                stream=stream)
+                h2b.quotient_lookups_device(hj, parts[10], parts[7], parts[8], parts[9], parts[18], parts[19],
+                                            parts[20], d_beta, d_gamma, d_y, n, stream=stream)
+            del parts
+            # 7. h on the extended coset: gather the parts, divide by the vanishing
+            #    polynomial, back to coefficients (extended_to_coeff), commit its pieces
+            en = len(hs) * n
+            ext, hc = h2b.dev_empty(32 * en), h2b.dev_empty(32 * en)
+            tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64))
+            h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), len(hs), n,
+                     h2b.stream_handle(stream))
+            h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk["t_evals"]),
+                     len(dom.t_evaluations), en, h2b.stream_handle(stream))
+            h2b.fft_many_to_device(2, dom.extended_k, dom.extended_k, [ext], [hc], dom.extended_omega_inv,
+                                   dom.extended_ifft_divisor, stream=stream)
+            del ext, hs
+            zp = h2b.to_dev(F.fr_mont_limbs([dom.g_coset_inv, dom.g_coset]))
+            h2b.call("_halo2_distribute_powers_zeta", h2b.ptr(hc), h2b.ptr(zp), 2, en, h2b.stream_handle(stream))
+            for i in range(dom.quotient_poly_degree):
+                commit(_slice(hc, i, n))
+            flush()
+            # 8. opening: evaluations at x of every polynomial, two Kate divisions
+            #    (an advice column and the first h piece) and their commitments
+            x = sc(chal())
+            ews = [h2b.dev_empty(h2b.lib()._halo2_eval_polynomial_workspace_size(n)) for _ in range(len(allc) + 1)]
+            for p, ws in zip(allc + [_slice(hc, 0, n)], ews):
+                evals.append(_eval(h2b, p, x, n, ws, stream))
+            d_x = h2b.to_dev(x)
+            for p in (coef[0], _slice(hc, 0, n)):
+                q = h2b.dev_empty(32 * n)
+                h2b.kate_division_device(p, q, d_x, n, stream=stream)
+                commit(q, n - 1)
+            flush()
+        return commits, evals
+
+
+def _eval(h2b, d_poly, x, n, ws, stream):
+    """Horner evaluation left on the device: a 32-byte view into `ws`."""
+    import ctypes
+    res = ctypes.c_void_p()
+    h2b.call("_halo2_eval_polynomial", h2b.ptr(d_poly), ctypes.byref(h2b.host_ffi(x)), ctypes.byref(res), n,
+             h2b.ptr(ws), ws.numel(), h2b.stream_handle(stream))
+    off = res.value - ws.data_ptr()
+    return ws[off: off + 32]
+
+
+def requests(count, rate, seed, ks=(16, 18, 20, 22), weights=(0.4, 0.3, 0.2, 0.1)):
+    """A seeded open-loop request trace: Poisson arrivals at `rate` per second,
+    k drawn from `ks` with `weights`.  Returns [(arrival_s, k, seed)]."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=count) if rate > 0 else np.zeros(count)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    kk = rng.choice(np.asarray(ks), size=count, p=np.asarray(weights) / np.sum(weights))
+    return [(float(a), int(k), 1 + seed * 1000 + i) for i, (a, k) in enumerate(zip(arrivals, kk))]
+
+
+class Server:
+    """Runs proof requests with `slots` worker threads, each issuing on its
+    own CUDA stream, so that the GPU overlaps one request's kernels with
+    another's (and a small request is not stuck behind a large one).  A
+    request is admitted when a slot is free and the device memory it will
+    hold fits in `hbm_budget` bytes beside those in flight; `slots=1` is the
+    plain one-at-a-time prover.  Latency is arrival to completion of the
+    request's stream, measured on the host clock."""
+
+    def __init__(self, res, slots, hbm_budget):
+        self.res, self.slots, self.budget = res, slots, hbm_budget
+        self.in_use = 0
+        self.cv = threading.Condition()
+        self.streams = [_t().cuda.Stream() for _ in range(slots)]
+
+    def bytes_for(self, k):
+        """Device bytes a 2^k request holds while in flight (its polynomials
+        and the scratch of 4 concurrent MSMs)."""
+        n = 1 << k
+        return _bytes_per_proof(k) + 4 * int(self.res.h2b.lib().h2b_msm_table_workspace_size(n, 1 << self.res.kmax))
+
+    def serve(self, reqs, keep_outputs=False):
+        """Serves `reqs` (from `requests`) in arrival order; returns a dict of
+        latencies (s), the makespan and, if asked, each request's outputs."""
+        torch = _t()
+        for _, k, _ in reqs:
+            if self.bytes_for(k) > self.budget:
+                raise ValueError(f"a 2^{k} proof needs more than the {self.budget}-byte budget")
+            self.res.key(k)
+        torch.cuda.synchronize()
+        q = queue.Queue()
+        done = [None] * len(reqs)
+        outs = [None] * len(reqs)
+        errors = []
+        t0 = time.perf_counter()
+
+        def worker(slot):
+            st = self.streams[slot]
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                i, (arr, k, seed) = item
+                need = self.bytes_for(k)
+                with self.cv:
+                    while self.in_use + need > self.budget and self.in_use > 0:
+                        self.cv.wait()
+                    self.in_use += need
+                try:
+                    out = ProofWorkload(self.res, k, seed).run(st)
+                    st.synchronize()
+                    done[i] = time.perf_counter() - t0
+                    if keep_outputs:
+                        outs[i] = ([c.cpu() for c in out[0]], [e.cpu() for e in out[1]])
+                    del out
+                except Exception as e:  # surfaced after the join
+                    errors.append(e)
+                    done[i] = float("nan")
+                finally:
+                    with self.cv:
+                        self.in_use -= need
+                        self.cv.notify_all()
+
+        threads = [threading.Thread(target=worker, args=(s,), daemon=True) for s in range(self.slots)]
+        for th in threads:
+            th.start()
+        for i, r in enumerate(reqs):
+            wait = r[0] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            q.put((i, r))
+        for _ in threads:
+            q.put(None)
+        for th in threads:
+            th.join()
+        if errors:
+            raise errors[0]
+        lat = np.array([d - r[0] for d, r in zip(done, reqs)])
+        return {"latency_s": lat, "makespan_s": float(max(done)), "outputs": outs if keep_outputs else None}
+
+
+def summary(reqs, result):
+    """proofs/s over the makespan and latency percentiles, overall and per k."""
+    lat = result["latency_s"]
+    ks = np.array([k for _, k, _ in reqs])
+    out = {"requests": len(reqs), "proofs_per_s": round(len(reqs) / result["makespan_s"], 3),
+           "makespan_s": round(result["makespan_s"], 4),
+           "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+           "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2), "per_k": {}}
+    for k in sorted(set(ks.tolist())):
+        lk = lat[ks == k]
+        out["per_k"][str(k)] = {"count": int(lk.size), "p50_ms": round(float(np.percentile(lk, 50)) * 1e3, 2),
+                                "p99_ms": round(float(np.percentile(lk, 99)) * 1e3, 2)}
+    return out

@@ -374,8 +374,9 @@ RustError h2b_msm_device_table(const void* d_scalars, const void* d_table, uint6
                                void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
 
 /* Batch execution (no counterpart in the reference, which runs one launcher at a time on one stream).
- * h2b_exec_fork: `n` (1..32) internal non-blocking streams of the current device, ordered after `parent`;
- * created on the first fork on that device and kept until exit.  h2b_exec_join: `parent` waits for them. */
+ * h2b_exec_fork: `n` (1..32) internal non-blocking streams of the current device and calling thread, ordered
+ * after `parent`; created on the first fork by that thread on that device and kept until exit (threads never
+ * share them).  h2b_exec_join: `parent` waits for them; call it from the thread that forked. */
 RustError h2b_exec_fork(h2b_stream_t parent, uint32_t n, h2b_stream_t* out_streams);
 RustError h2b_exec_join(h2b_stream_t parent, uint32_t n);
 /* Capture what is issued on `s` (and on streams forked from it) into a CUDA graph; replay it with
