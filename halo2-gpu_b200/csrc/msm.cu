@@ -634,40 +634,45 @@ __global__ void __launch_bounds__(256) k_msm_bitsums(const G1Xyzz* __restrict__ 
     if (threadIdx.x == 0) st_xyzz(&bits[blockIdx.x], r);
 }
 
+// One warp per window (warps loop when there are more windows than warps),
+// the Horner steps on the lane-parallel formulas.
 __global__ void k_msm_wincombine(const G1Xyzz* __restrict__ bits, int W, int nbits, int log_l,
                                  G1Xyzz* __restrict__ wins)
 {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= W) return;
-    const G1Xyzz* T = bits + (uint64_t)w * (nbits + 1);
-    G1XyzzL r = xyzzl_inf();
-    for (int k = nbits - 1; k >= 0; k--) {
-        r = xyzzl_dbl(r);
-        xyzzl_add(r, xyzzl_from(ld_xyzz(&T[k])));
+    for (int w = (int)(threadIdx.x >> 5); w < W; w += (int)(blockDim.x >> 5)) {
+        const G1Xyzz* T = bits + (uint64_t)w * (nbits + 1);
+        G1XyzzL r = xyzzl_inf();
+        for (int k = nbits - 1; k >= 0; k--) {
+            r = xyzzw_dbl(r);
+            xyzzw_add(r, xyzzl_from(ld_xyzz(&T[k])));
+        }
+        for (int d = 0; d < log_l; d++) r = xyzzw_dbl(r);
+        xyzzw_add(r, xyzzl_from(ld_xyzz(&T[nbits])));
+        if ((threadIdx.x & 31) == 0) st_xyzz(&wins[w], xyzzl_to(r));
     }
-    for (int d = 0; d < log_l; d++) r = xyzzl_dbl(r);
-    xyzzl_add(r, xyzzl_from(ld_xyzz(&T[nbits])));
-    st_xyzz(&wins[w], xyzzl_to(r));
 }
 
-// 2^(c*w) * W_w in parallel over w, then the sum and the affine conversion.
+// 2^(c*w) * W_w with one warp per window (lane-parallel doublings), then the
+// sum over windows and the affine conversion by the first warp.
+constexpr int FINAL_MAX_W = 64;
 __global__ void k_msm_final(const G1Xyzz* __restrict__ wins, int W, int c, G1Jac* __restrict__ out)
 {
-    __shared__ G1Xyzz sh[64];
-    int w = threadIdx.x;
-    if (w < W) {
+    __shared__ G1Xyzz sh[FINAL_MAX_W];
+    for (int w = (int)(threadIdx.x >> 5); w < W; w += (int)(blockDim.x >> 5)) {
         G1XyzzL x = xyzzl_from(ld_xyzz(&wins[w]));
-        for (int d = 0; d < c * w; d++) x = xyzzl_dbl(x);
-        sh[w] = xyzzl_to(x);
+        for (int d = 0; d < c * w; d++) x = xyzzw_dbl(x);
+        if ((threadIdx.x & 31) == 0) sh[w] = xyzzl_to(x);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        G1Xyzz acc = xyzz_inf();
-        for (int i = 0; i < W; i++) xyzz_add(acc, sh[i]);
-        G1Jac j = xyzz_to_jac_affine(acc);
-        st(&out->X, j.X);
-        st(&out->Y, j.Y);
-        st(&out->Z, j.Z);
+    if (threadIdx.x < 32) {
+        G1XyzzL acc = xyzzl_inf();
+        for (int i = 0; i < W; i++) xyzzw_add(acc, xyzzl_from(sh[i]));
+        if (threadIdx.x == 0) {
+            G1Jac j = xyzz_to_jac_affine(xyzzl_to(acc));
+            st(&out->X, j.X);
+            st(&out->Y, j.Y);
+            st(&out->Z, j.Z);
+        }
     }
 }
 
@@ -760,9 +765,9 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_LAUNCHED("k_msm_segments");
     k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
     H2B_LAUNCHED("k_msm_bitsums");
-    k_msm_wincombine<<<1, 64, 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
+    k_msm_wincombine<<<1, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
     H2B_LAUNCHED("k_msm_wincombine");
-    k_msm_final<<<1, 64, 0, st>>>(s.wins, p.Wr, p.c, s.result);
+    k_msm_final<<<1, 32 * std::min(p.Wr, 8), 0, st>>>(s.wins, p.Wr, p.c, s.result);
     prof_end(PROF_MSM_TOTAL, st);
     H2B_LAUNCHED("k_msm_final");
     return ok();
