@@ -334,32 +334,43 @@ def table_section(h2b, torch, d_srs, d_sc, n, reps):
     return res
 
 
-def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9):
+def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 1.0, 1.5)):
     """The prover-shaped workload (halo2-gpu_b200/prover.py: per proof the
     advice, lookup, permutation and quotient commitments, the per-part coset
-    NTTs and quotients, h, and the opening) served from one GPU.  A seeded
-    Poisson trace of `count` requests with k in {16, 18, 20, 22} (weights
-    .4/.3/.2/.1) arrives at 1.2x the rate the one-at-a-time prover sustains
-    (its mean service time measured first, one request per k, untimed
-    warm-up); the same trace is then run plain (one slot) and served (`slots`
-    worker streams under an HBM budget).  Reports proofs/s over the makespan
-    and p50/p99 latency (arrival to completion, host clock)."""
+    NTTs and quotients, h, and the opening) served from one GPU.  The service
+    time of one request alone is measured first for each k (untimed warm-up
+    request before it); `prove_k20` is the k = 20 one as proofs/s.  Then, for
+    each load factor, a seeded Poisson trace of `count` requests with k in
+    {16, 18, 20, 22} (weights .4/.3/.2/.1) arrives at load x the rate the
+    one-at-a-time prover sustains, and runs plain (one slot) and served
+    (`slots` worker streams under an HBM budget).  Reports proofs/s over the
+    makespan, p50/p99 latency (arrival to completion, host clock) and the
+    device-memory high-water mark of the run."""
     P = importlib.import_module(h2b.__name__ + ".prover")
     res = P.Resident(h2b, kmax)
     ks, weights = (16, 18, 20, 22), (0.4, 0.3, 0.2, 0.1)
-    plain = P.Server(res, 1, 96 << 30)
+    budget = 96 << 30
+    plain, served = P.Server(res, 1, budget), P.Server(res, slots, budget)
     service = {}
     for k in ks:
         plain.serve([(0.0, k, 7 + k)])
+        torch.cuda.reset_peak_memory_stats()
         r = plain.serve([(0.0, k, 8 + k)])
-        service[k] = float(r["latency_s"][0])
-    mean_s = sum(w * service[k] for k, w in zip(ks, weights))
-    rate = 1.2 / mean_s
-    reqs = P.requests(count, rate, seed, ks, weights)
-    out = {"requests": count, "arrival_rate_per_s": round(rate, 3), "slots": slots, "hbm_budget_GB": 96,
-           "service_ms_alone": {str(k): round(v * 1e3, 2) for k, v in service.items()}}
-    out["plain"] = P.summary(reqs, plain.serve(reqs))
-    out["served"] = P.summary(reqs, P.Server(res, slots, 96 << 30).serve(reqs))
+        service[k] = (float(r["latency_s"][0]), torch.cuda.max_memory_allocated() / 1e9)
+    mean_s = sum(w * service[k][0] for k, w in zip(ks, weights))
+    out = {"requests": count, "slots": slots, "hbm_budget_GB": budget >> 30,
+           "service_ms_alone": {str(k): round(v[0] * 1e3, 2) for k, v in service.items()},
+           "prove_k20": {"proofs_per_s": round(1.0 / service[20][0], 3), "ms": round(service[20][0] * 1e3, 2),
+                         "hbm_peak_GB": round(service[20][1], 2)},
+           "capacity_plain_per_s": round(1.0 / mean_s, 3), "loads": {}}
+    for load in loads:
+        reqs = P.requests(count, load / mean_s, seed, ks, weights)
+        row = {"arrival_rate_per_s": round(load / mean_s, 3)}
+        for name, srv in (("plain", plain), ("served", served)):
+            torch.cuda.reset_peak_memory_stats()
+            row[name] = P.summary(reqs, srv.serve(reqs))
+            row[name]["hbm_peak_GB"] = round(torch.cuda.max_memory_allocated() / 1e9, 2)
+        out["loads"][str(load)] = row
     return out
 
 
@@ -660,13 +671,13 @@ def main():
     acc_avg_ms = acc_ms / max(acc_cnt, 1)
     acc_bytes = entries * (4 + 64) + (1 << 19) * 128          # sorted ids + affine points + bucket sums
     acc_modmul = entries * 10                                  # XYZZ mixed add 8M + 2S
-    roofline = {"bound": "hbm", "kernel": "k_msm_accumulate", "achieved": acc_bytes / (acc_avg_ms * 1e-3) / 1e9,
+    roofline = {"bound": "hbm", "kernel": "k_msm_accumulate_z", "achieved": acc_bytes / (acc_avg_ms * 1e-3) / 1e9,
                 "peak": hbm, "unit": "GB/s", "peak_source": f"{hbm_kind} MEASURED_PEAKS.json hbm_gbs",
-                "traffic": ncu_traffic("msm_accumulate_k22.md"),
+                "traffic": ncu_traffic("msm_accumulate_z_k22.md"),
                 "algorithmic_bytes_per_launch": acc_bytes, "launch_ms": acc_avg_ms}
     roofline["frac"] = roofline["achieved"] / roofline["peak"]
     imad_peak = probe["h2b_probe_imad"]
-    imad = {"kernel": "k_msm_accumulate", "modmul_per_launch": acc_modmul,
+    imad = {"kernel": "k_msm_accumulate_z", "modmul_per_launch": acc_modmul,
             "achieved_imad_ops_per_s": acc_modmul * 264 / (acc_avg_ms * 1e-3),
             "peak_imad_ops_per_s": imad_peak, "peak_source": "measured h2b_probe_imad (mad.lo/mad.hi chains)",
             "modmul_probe_per_s": probe["h2b_probe_modmul"]}

@@ -13,6 +13,7 @@
 #pragma once
 #include "field.cuh"
 #include "inverse.cuh"
+#include "lazy.cuh"
 
 namespace h2b {
 
@@ -288,6 +289,87 @@ H2B_DEV void xyzzl_add(G1XyzzL& acc, const G1XyzzL& q)
     acc.X = X3;
     acc.ZZ = fl_mul_ilp(zz, PP);
     acc.ZZZ = fl_mul_ilp(zzz, PPP);
+}
+
+// ---- XYZZ in the lazy form (R = 2^261), for the bucket accumulation -------
+// Bounds (multiples of p) that every step relies on are written beside it;
+// products follow (1 + 0.0059 a b) p (lazy.cuh).  The accumulator keeps
+// X < 5.39p, Y < 3.34p, ZZ and ZZZ < 2p from one addition to the next;
+// affine inputs are qx < 1.01p (canonical, or times beta) and qy < 2p
+// (canonical, or negated as 2p - y).
+
+typedef Fz<FqCfg> FqZ;
+
+struct G1XyzzZ {
+    FqZ X, Y, ZZ, ZZZ;
+};
+
+H2B_DEV G1XyzzZ xyzzz_inf()
+{
+    G1XyzzZ r;
+    r.X = fz_zero<FqCfg>(); r.Y = fz_zero<FqCfg>(); r.ZZ = fz_zero<FqCfg>(); r.ZZZ = fz_zero<FqCfg>();
+    return r;
+}
+
+// infinity is the explicit all-zero ZZ (no other path makes ZZ vanish)
+H2B_DEV bool is_inf(const G1XyzzZ& p) { return fz_is_zero(p.ZZ); }
+
+// 2 q for an affine q (qx < 1.01p, qy < 2p, qy != 0): dbl-2008-s-1 with Z = 1.
+H2B_DEV G1XyzzZ xyzzz_dbl_affine(const FqZ& qx, const FqZ& qy)
+{
+    const FqZ U = fz_add(qy, qy);                              // < 4p
+    const Fz2<FqCfg> vx = fz_sqr2(U, qx);                      // V < 1.094p, xx < 1.006p
+    const Fz2<FqCfg> ws = fz_mul2(U, vx.a, qx, vx.a);          // W < 1.026p, S < 1.0065p
+    const FqZ M = fz_add(fz_add(vx.b, vx.b), vx.b);            // < 3.02p
+    const Fz2<FqCfg> mm = fz_mul2(M, M, ws.a, qy);             // MM < 1.054p, W y < 1.012p
+    G1XyzzZ r;
+    r.X = fz_sub<FqCfg, 3>(mm.a, fz_add(ws.b, ws.b));          // 2S < 2.013p; X3 < 4.054p
+    const FqZ t1 = fz_mul_call(M, fz_sub<FqCfg, 5>(ws.b, r.X)); // S - X3 + 5p < 6.007p; t1 < 1.107p
+    r.Y = fz_sub<FqCfg, 2>(t1, mm.b);                          // < 3.107p
+    r.ZZ = vx.a;                                               // < 1.094p
+    r.ZZZ = ws.a;                                              // < 1.026p
+    return r;
+}
+
+// madd-2008-s: acc += (qx, qy), q affine and not infinity.  PP and R^2 are
+// formed before the equal-x test (PP == 0 mod p exactly when P is).
+H2B_DEV void xyzzz_madd(G1XyzzZ& acc, const FqZ& qx, const FqZ& qy, const FqZ& one)
+{
+    if (is_inf(acc)) {
+        acc.X = qx; acc.Y = qy; acc.ZZ = one; acc.ZZZ = one;
+        return;
+    }
+    const Fz2<FqCfg> us = fz_mul2(qx, acc.ZZ, qy, acc.ZZZ);   // U2 < 1.012p, S2 < 1.024p
+    const FqZ P = fz_sub<FqCfg, 6>(us.a, acc.X);               // X1 < 5.39p; P < 7.01p
+    const FqZ R = fz_sub<FqCfg, 4>(us.b, acc.Y);               // Y1 < 3.34p; R < 5.02p
+    const Fz2<FqCfg> sq = fz_sqr2(P, R);                       // PP < 1.29p, RR < 1.149p
+    if (fz_is_zero_mod(sq.a)) {
+        acc = fz_is_zero_mod(sq.b) ? xyzzz_dbl_affine(qx, qy) : xyzzz_inf();
+        return;
+    }
+    const Fz2<FqCfg> pq = fz_mul2(P, sq.a, acc.X, sq.a);       // PPP < 1.053p, Q < 1.041p
+    const FqZ X3 = fz_sub<FqCfg, 4>(sq.b, fz_add(pq.a, fz_add(pq.b, pq.b)));  // PPP + 2Q < 3.135p; X3 < 5.149p
+    const Fz2<FqCfg> yy = fz_mul2(R, fz_sub<FqCfg, 6>(pq.b, X3), acc.Y, pq.a); // Q - X3 + 6p < 7.041p;
+                                                                              // < 1.209p, < 1.021p
+    const Fz2<FqCfg> zz = fz_mul2(acc.ZZ, sq.a, acc.ZZZ, pq.a); // < 1.015p, < 1.012p
+    acc.Y = fz_sub<FqCfg, 2>(yy.a, yy.b);                     // < 3.209p
+    acc.X = X3;
+    acc.ZZ = zz.a;
+    acc.ZZZ = zz.b;
+}
+
+// Stores the canonical memory image of the accumulator (infinity stays
+// ZZ = 0): four products by 2^256 mod p through the shared out-of-line
+// product bodies, then the conditional subtractions.  Out of line itself, so
+// the rarely taken store path does not crowd the addition loop's code.
+static __device__ __noinline__ void st_xyzzz(G1Xyzz* dst, const G1XyzzZ p, const FqZ r256)
+{
+    const Fz2<FqCfg> a = fz_mul2(p.X, r256, p.Y, r256);    // X < 5.39p, Y < 3.34p: both < 1.032p
+    const Fz2<FqCfg> b = fz_mul2(p.ZZ, r256, p.ZZZ, r256);  // < 1.012p
+    G1Xyzz r;
+    r.X = fz_canonical(a.a); r.Y = fz_canonical(a.b);
+    r.ZZ = fz_canonical(b.a); r.ZZZ = fz_canonical(b.b);
+    st_xyzz(dst, r);
 }
 
 // ---- lane-parallel XYZZ formulas for one warp ------------------------------

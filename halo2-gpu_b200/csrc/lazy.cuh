@@ -1,0 +1,264 @@
+// Lazy 29-bit limb arithmetic for the MSM bucket accumulation.
+//
+// The accumulation runs one mixed XYZZ addition per sorted entry; in the
+// normalised limb form (field.cuh, R = 2^256) each of its seven additions and
+// subtractions needs two serial carry chains and a conditional correction,
+// which made the addition cost about 1.8x its ten products.  Here:
+//
+//  * R = 2^261 (nine full 29-bit reduction steps): p/R is 0.0059 for BN254
+//    Fq, so a product of two values below a*p and b*p is below
+//    (1 + 0.0059 a b) p.  Values may therefore sit well above p between
+//    products ("lazy"): every bound used by the formulas below is written
+//    next to the operation that relies on it.
+//  * a + b and a - b + K p are limb-wise, followed by ONE parallel carry step
+//    (each limb keeps its low 29 bits and adds the carry of the limb below),
+//    no conditional subtraction.  Limbs then stay below 2^29 + 8 ("almost
+//    normalised"), which the product's 64-bit column sums absorb: 18 terms
+//    below 2^58.01 each.
+//  * K p is added in a borrow-adjusted limb form (every limb below the top
+//    one raised by 2^30, the next one lowered by 2) so that a_i + L_i - b_i
+//    is never negative for an almost-normalised b below (K - 0.001) p.
+//
+// Values in this form are x * 2^261 mod p (plus multiples of p).  Affine
+// bases enter as canonical x * 2^261 mod p (converted once, k_to_r261); the
+// results leave through one product by 2^256 mod p, which yields the memory
+// image x * 2^256 mod p, then a final conditional subtraction.
+#pragma once
+#include "field.cuh"
+
+namespace h2b {
+
+template <class C>
+struct Fz {
+    uint32_t l[9];
+};
+
+// limb i (29-bit grid, normalised) of K * p
+template <class C>
+__host__ __device__ constexpr uint32_t kp29(int K, int i)
+{
+    uint64_t carry = 0, t = 0;
+    for (int j = 0; j <= i; j++) {
+        t = (uint64_t)K * p29<C>(j) + carry;
+        carry = t >> 29;
+        if (j < i) t &= M29;
+    }
+    return (uint32_t)(i < 8 ? (t & M29) : t);
+}
+
+// borrow-adjusted limb i of K * p: the same value, every limb below the top
+// one at least 2^30 - 2
+template <class C>
+__host__ __device__ constexpr uint32_t kp29_adj(int K, int i)
+{
+    return kp29<C>(K, i) + (i < 8 ? (1u << 30) : 0u) - (i > 0 ? 2u : 0u);
+}
+
+// One parallel carry step: limb i keeps its low 29 bits plus the carry of
+// limb i - 1; the top limb keeps everything.
+template <class C>
+H2B_DEV Fz<C> fz_carry(const uint32_t (&d)[9])
+{
+    Fz<C> r;
+    r.l[0] = d[0] & M29;
+#pragma unroll
+    for (int i = 1; i < 8; i++) r.l[i] = (d[i] & M29) + (d[i - 1] >> 29);
+    r.l[8] = d[8] + (d[7] >> 29);
+    return r;
+}
+
+template <class C>
+H2B_DEV Fz<C> fz_add(const Fz<C>& a, const Fz<C>& b)
+{
+    uint32_t d[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) d[i] = a.l[i] + b.l[i];
+    return fz_carry<C>(d);
+}
+
+// a - b + K p.  Every limb below the top one is non-negative for any
+// almost-normalised b; the top one is when b <= K p - 3 * 2^232 in value
+// (kp29(K, 8) >= K p / 2^232 - 1 and b's top limb <= b / 2^232), which holds
+// for every b below (K - 0.001) p.
+template <class C, int K>
+H2B_DEV Fz<C> fz_sub(const Fz<C>& a, const Fz<C>& b)
+{
+    uint32_t d[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) d[i] = a.l[i] + kp29_adj<C>(K, i) - b.l[i];
+    return fz_carry<C>(d);
+}
+
+// Montgomery product with R = 2^261: (a b + M p) / 2^261, M < 2^261 chosen
+// limb by limb.  Output limbs are normalised (the top one holds the rest).
+template <class C>
+H2B_DEV Fz<C> fz_mul(const Fz<C>& a, const Fz<C>& b)
+{
+    const uint32_t np = C::N0 & M29;
+    uint32_t m[9];
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+#pragma unroll
+        for (int i = 0; i <= k; i++) acc = madw(a.l[i], b.l[k - i], acc);
+#pragma unroll
+        for (int i = 0; i < k; i++) acc = madw(m[i], p29<C>(k - i), acc);
+        const uint32_t mk = ((uint32_t)acc * np) & M29;
+        m[k] = mk;
+        acc = madw(mk, p29<C>(0), acc);
+        acc >>= 29;
+    }
+    Fz<C> r;
+#pragma unroll
+    for (int k = 9; k < 17; k++) {
+#pragma unroll
+        for (int i = k - 8; i <= 8; i++) acc = madw(a.l[i], b.l[k - i], acc);
+#pragma unroll
+        for (int i = k - 8; i <= 8; i++) acc = madw(m[i], p29<C>(k - i), acc);
+        r.l[k - 9] = (uint32_t)acc & M29;
+        acc >>= 29;
+    }
+    r.l[8] = (uint32_t)acc;
+    return r;
+}
+
+// a^2: each cross product once, against the doubled limb (2 a_j < 2^30.1,
+// so a doubled term stays below 2^59.1 and a column below 2^62.4).
+template <class C>
+H2B_DEV Fz<C> fz_sqr(const Fz<C>& a)
+{
+    const uint32_t np = C::N0 & M29;
+    uint32_t d[9], m[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) d[i] = a.l[i] << 1;
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+#pragma unroll
+        for (int i = 0; 2 * i < k; i++) acc = madw(a.l[i], d[k - i], acc);
+        if ((k & 1) == 0) acc = madw(a.l[k / 2], a.l[k / 2], acc);
+#pragma unroll
+        for (int i = 0; i < k; i++) acc = madw(m[i], p29<C>(k - i), acc);
+        const uint32_t mk = ((uint32_t)acc * np) & M29;
+        m[k] = mk;
+        acc = madw(mk, p29<C>(0), acc);
+        acc >>= 29;
+    }
+    Fz<C> r;
+#pragma unroll
+    for (int k = 9; k < 17; k++) {
+#pragma unroll
+        for (int i = k - 8; 2 * i < k; i++) acc = madw(a.l[i], d[k - i], acc);
+        if ((k & 1) == 0) acc = madw(a.l[k / 2], a.l[k / 2], acc);
+#pragma unroll
+        for (int i = k - 8; i <= 8; i++) acc = madw(m[i], p29<C>(k - i), acc);
+        r.l[k - 9] = (uint32_t)acc & M29;
+        acc >>= 29;
+    }
+    r.l[8] = (uint32_t)acc;
+    return r;
+}
+
+template <class C>
+__device__ __noinline__ Fz<C> fz_mul_call(const Fz<C> a, const Fz<C> b)
+{
+    return fz_mul<C>(a, b);
+}
+
+template <class C>
+struct Fz2 {
+    Fz<C> a, b;
+};
+
+// two independent products per out-of-line call (two dependency chains for
+// the scheduler, one call overhead)
+template <class C>
+__device__ __noinline__ Fz2<C> fz_mul2(const Fz<C> a0, const Fz<C> b0, const Fz<C> a1, const Fz<C> b1)
+{
+    Fz2<C> r;
+    r.a = fz_mul<C>(a0, b0);
+    r.b = fz_mul<C>(a1, b1);
+    return r;
+}
+
+template <class C>
+__device__ __noinline__ Fz2<C> fz_sqr2(const Fz<C> a0, const Fz<C> a1)
+{
+    Fz2<C> r;
+    r.a = fz_sqr<C>(a0);
+    r.b = fz_sqr<C>(a1);
+    return r;
+}
+
+template <class C>
+H2B_DEV Fz<C> fz_zero()
+{
+    Fz<C> r;
+#pragma unroll
+    for (int i = 0; i < 9; i++) r.l[i] = 0;
+    return r;
+}
+
+template <class C>
+H2B_DEV bool fz_is_zero(const Fz<C>& a)
+{
+    uint32_t z = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) z |= a.l[i];
+    return z == 0;
+}
+
+// a == 0 (mod p) for a product output (normalised limbs, value < 2p): a is 0 or p
+template <class C>
+H2B_DEV bool fz_is_zero_mod(const Fz<C>& a)
+{
+    uint32_t z = 0, e = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        z |= a.l[i];
+        e |= a.l[i] ^ p29<C>(i);
+    }
+    return z == 0 || e == 0;
+}
+
+// bit-sliced view of a 256-bit word image (value < 2^256, normalised limbs)
+template <class C>
+H2B_DEV Fz<C> fz_from_words(const Fp<C>& a)
+{
+    Fl<C> t = to_l(a);
+    Fz<C> r;
+#pragma unroll
+    for (int i = 0; i < 9; i++) r.l[i] = t.l[i];
+    return r;
+}
+
+// 2^261 mod p as a canonical word image (= 2^256 mod p doubled five times)
+template <class C>
+H2B_DEV Fp<C> r261_words()
+{
+    Fp<C> c = Fp<C>::one();
+#pragma unroll 1
+    for (int i = 0; i < 5; i++) c = c + c;
+    return c;
+}
+
+// memory image x 2^256 mod p -> canonical x 2^261 mod p (word image)
+template <class C>
+H2B_DEV Fp<C> to_r261(const Fp<C>& x, const Fp<C>& r261)
+{
+    return x * r261;
+}
+
+// A product output (normalised limbs, value < 2p) packed to 8 x 32 and
+// reduced below p.  With a product by 2^256 mod p before it, a lazy
+// x 2^261 value (below 8p) becomes the memory image x 2^256 mod p.
+template <class C>
+H2B_DEV Fp<C> fz_canonical(const Fz<C>& t)
+{
+    Fl<C> u;
+#pragma unroll
+    for (int i = 0; i < 9; i++) u.l[i] = t.l[i];
+    return from_l(u);
+}
+
+} // namespace h2b

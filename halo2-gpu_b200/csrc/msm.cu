@@ -160,6 +160,7 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
         sp.add_n<Fq>(ctas);                           // CTA totals
         sp.add(fq_batch_invert_scratch(ctas));
     }
+    if (p.tn == 0 && p.R == 0) sp.add_n<G1Affine>(p.n);  // bases in the lazy form (x 2^261)
 }
 
 MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host)
@@ -197,6 +198,7 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
         s.pr_inv_bytes = fq_batch_invert_scratch(ctas);
         s.pr_inv_scratch = ar.take(s.pr_inv_bytes);
     }
+    s.rbases = (p.tn == 0 && p.R == 0) ? ar.take_n<G1Affine>(p.n) : nullptr;
     return s;
 }
 
@@ -313,6 +315,72 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : (MODE >= 3 ? MODE + 1 : 3
             xyzzl_madd<MODE>(acc, qx, to_l(P.y));
         }
         if (head) st_xyzz(&heads[t], xyzzl_to(acc)); else st_xyzz(&buckets[b], xyzzl_to(acc));
+    }
+}
+
+// Bases (affine, memory image x 2^256 mod p) -> canonical x 2^261 mod p, the
+// form the lazy accumulation reads; infinity (0, 0) stays (0, 0).
+__global__ void k_to_r261(const G1Affine* in, G1Affine* out, uint64_t n)  // in may equal out
+{
+    const Fq r261 = r261_words<FqCfg>();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const G1Affine a = ld_affine(&in[i]);
+        G1Affine r;
+        r.x = to_r261(a.x, r261);
+        r.y = to_r261(a.y, r261);
+        st(&out[i].x, r.x);
+        st(&out[i].y, r.y);
+    }
+}
+
+// The accumulation in the lazy form (curve.cuh, lazy.cuh): same chunking,
+// bucket boundaries and outputs as k_msm_accumulate, over bases in the
+// x 2^261 form.  The accumulator's additions and subtractions are one-step
+// carry passes with no conditional correction; results are converted back
+// to the canonical memory image when a bucket or chunk head is stored.
+__global__ void __launch_bounds__(128, 3) k_msm_accumulate_z(const uint32_t* __restrict__ sorted,
+                                                             const uint32_t* __restrict__ offsets, uint64_t NB,
+                                                             uint32_t K, const G1Affine* __restrict__ bases,
+                                                             G1Xyzz* __restrict__ buckets,
+                                                             G1Xyzz* __restrict__ heads)
+{
+    const Fq r261 = r261_words<FqCfg>();
+    const FqZ one = fz_from_words(r261);                          // 1 in the lazy form
+    const FqZ r256 = fz_from_words(Fq::one());                    // 2^256 mod p, for the stores
+    const FqZ beta = fz_from_words(to_r261(glv::beta(), r261));   // phi(x, y) = (beta x, y)
+    const uint32_t M = offsets[NB];
+    const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = (uint32_t)(t * K);
+        const uint32_t end = ((uint64_t)start + K < (uint64_t)M) ? start + K : M;
+        uint64_t lo = 0, hi = NB;  // offsets[lo] <= start < offsets[hi]
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= start) lo = mid; else hi = mid;
+        }
+        uint64_t b = lo;
+        uint32_t next = offsets[b + 1];
+        bool head = offsets[b] < start;
+        G1XyzzZ acc = xyzzz_inf();
+        for (uint32_t e = start; e < end; e++) {
+            if (e == next) {
+                st_xyzzz(head ? &heads[t] : &buckets[b], acc, r256);
+                acc = xyzzz_inf();
+                head = false;
+                do { b++; next = offsets[b + 1]; } while (next == e);
+            }
+            const uint32_t ent = sorted[e];
+            const uint32_t v = ent & ~SIGN_BIT;
+            const G1Affine P = ld_affine(&bases[v >> 1]);
+            if (is_inf(P)) continue;
+            FqZ qx = fz_from_words(P.x);                                   // < p
+            FqZ qy = fz_from_words(P.y);                                   // < p
+            if (ent & SIGN_BIT) qy = fz_sub<FqCfg, 2>(fz_zero<FqCfg>(), qy);  // 2p - y < 2p
+            if (v & 1u) qx = fz_mul_call(qx, beta);                        // < 1.006p
+            xyzzz_madd(acc, qx, qy, one);
+        }
+        st_xyzzz(head ? &heads[t] : &buckets[b], acc, r256);
     }
 }
 
@@ -698,6 +766,13 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
     k_msm_glv<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, p.n);
     H2B_LAUNCHED("k_msm_glv");
+    // the lazy accumulation (window tables are stored in its form; plain bases
+    // are converted here) unless pairing rounds or an older variant run
+    const bool lazy = p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0);
+    if (lazy && p.tn == 0) {
+        k_to_r261<<<grid_for(p.n, 256, 148u * 8u), 256, 0, st>>>(d_bases, s.rbases, p.n);
+        H2B_LAUNCHED("k_to_r261");
+    }
     H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
     H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
     k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr,
@@ -741,6 +816,11 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
     if (p.R > 0)
         k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
+    else if (lazy)
+        k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
+                                                     s.buckets, s.heads);
+    else if (g_msm_acc_variant == 5)
+        k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 1)
         k_msm_accumulate<1, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 2)
@@ -749,8 +829,6 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
         k_msm_accumulate<3, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 4)
         k_msm_accumulate<4, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
-    else
-        k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     prof_end(PROF_MSM_ACCUMULATE, st);
     H2B_LAUNCHED("k_msm_accumulate");
     k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(off, p.NB, p.Kf, s.buckets, s.heads, s.dense,
@@ -966,6 +1044,9 @@ extern "C" RustError h2b_msm_table_precompute(const void* d_bases, uint64_t n, v
         k_table_affine<<<grid_for(n, 256), 256, 0, stream>>>(tmp, den, n, table + (uint64_t)w * n);
         H2B_LAUNCHED("k_table_affine");
     }
+    // the accumulation reads the table in the lazy x 2^261 form
+    k_to_r261<<<grid_for((uint64_t)p.W * n, 256, 148u * 8u), 256, 0, stream>>>(table, table, (uint64_t)p.W * n);
+    H2B_LAUNCHED("k_to_r261");
     return ok();
 }
 
@@ -997,14 +1078,15 @@ extern "C" RustError h2b_msm_device_table(const void* d_scalars, const void* d_t
 
 extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(window_bits, chunk); }
 
-// Call structure and occupancy of the bucket-accumulation kernel: 0 = two
-// products per out-of-line call (default), 1 = all products inline, 2 = one
-// product per call, 3 and 4 = one product per call with at most 128 / 96
-// registers (4 / 5 CTAs of 128 threads per SM).  Results are identical; only
-// speed differs.
+// Form and call structure of the bucket-accumulation kernel: 0 = the lazy
+// R = 2^261 form with one-step carries (default; window tables always use
+// it); the normalised R = 2^256 limb form with 5 = two products per
+// out-of-line call, 1 = all products inline, 2 = one product per call, 3 and
+// 4 = one product per call with at most 128 / 96 registers (4 / 5 CTAs of 128
+// threads per SM).  Results are identical; only speed differs.
 extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
-    if (v >= 0 && v <= 4) g_msm_acc_variant = v;
+    if (v >= 0 && v <= 5) g_msm_acc_variant = v;
 }
 
 // Batch-affine pairing rounds run before the XYZZ bucket accumulation

@@ -353,9 +353,10 @@ RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out,
                          uint64_t scratch_bytes, h2b_stream_t stream);
 /* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
-/* Call structure of the MSM bucket-accumulation kernel: 0 = two field products per out-of-line call
- * (default), 1 = all products inline, 2 = one product per call, 3 / 4 = one per call with 4 / 5 CTAs
- * per SM.  Same results; tuning only. */
+/* Form of the MSM bucket-accumulation kernel: 0 = lazy R = 2^261 limbs with one-step carries (default;
+ * window-table MSMs always use it); normalised R = 2^256 limbs with 5 = two field products per
+ * out-of-line call, 1 = all products inline, 2 = one product per call, 3 / 4 = one per call with 4 / 5
+ * CTAs per SM.  Same results; tuning only. */
 void h2b_msm_set_accumulate_variant(int variant);
 /* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
  * MSM workspace-size queries depend on it (set it before sizing scratch). */
@@ -363,6 +364,8 @@ void h2b_msm_set_pair_rounds(int rounds);
 
 /* Precomputed window tables (no counterpart in the reference): an SRS kept resident with its window
  * multiples [2^(c w)] P_i, so an MSM over it reduces one bucket set and has no final doubling chain.
+ * The table is opaque to callers: its points are stored as x * 2^261 mod p images, the form the
+ * accumulation kernel reads.
  * h2b_msm_table_points: affine points in the table for n bases (0 if n is out of range). */
 uint64_t h2b_msm_table_points(uint64_t n);
 uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n);
