@@ -66,12 +66,15 @@ struct GraphHandle {
 };
 
 // Plan of one job: plain bases, or a precomputed window table of table_n points.
-MsmPlan job_plan(uint64_t n, uint64_t table_n) { return table_n ? msm_plan_table(n, table_n) : msm_plan(n); }
+MsmPlan job_plan(uint64_t n, uint64_t table_n, uint32_t concurrent)
+{
+    return msm_plan_shared(n, table_n, concurrent);
+}
 
 // Scratch of one MSM slot (device scalars and bases), 256-byte aligned.
-uint64_t msm_slot_bytes(uint64_t n, uint64_t table_n)
+uint64_t msm_slot_bytes(uint64_t n, uint64_t table_n, uint32_t concurrent)
 {
-    MsmPlan p = job_plan(n, table_n);
+    MsmPlan p = job_plan(n, table_n, concurrent);
     ScratchPlan sp;
     msm_plan_scratch(p, sp, false, false);
     return align_up(sp.used);
@@ -151,10 +154,16 @@ typedef struct h2b_msm_job {
     uint64_t table_n;       // 0: d_bases are plain bases
 } h2b_msm_job;
 
-static uint64_t batch_slot(const h2b_msm_job* jobs, uint64_t count)
+// MSMs of a batch that run at the same time: one per forked stream.
+static uint32_t batch_concurrency(uint64_t count, uint32_t streams)
+{
+    return (uint32_t)std::min<uint64_t>(count, streams);
+}
+
+static uint64_t batch_slot(const h2b_msm_job* jobs, uint64_t count, uint32_t concurrent)
 {
     uint64_t mx = 0;
-    for (uint64_t i = 0; i < count; i++) mx = std::max(mx, msm_slot_bytes(jobs[i].n, jobs[i].table_n));
+    for (uint64_t i = 0; i < count; i++) mx = std::max(mx, msm_slot_bytes(jobs[i].n, jobs[i].table_n, concurrent));
     return mx;
 }
 
@@ -162,7 +171,7 @@ static uint64_t batch_slot(const h2b_msm_job* jobs, uint64_t count)
 extern "C" uint64_t h2b_msm_batch_workspace_size(const h2b_msm_job* jobs, uint64_t count, uint32_t streams)
 {
     if (streams == 0 || streams > EXEC_MAX_STREAMS) return 0;
-    return (uint64_t)streams * batch_slot(jobs, count);
+    return (uint64_t)streams * batch_slot(jobs, count, batch_concurrency(count, streams));
 }
 
 extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
@@ -178,7 +187,8 @@ extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint
         if (jobs[i].table_n && jobs[i].n > jobs[i].table_n)
             return err((int)cudaErrorInvalidValue, "h2b_msm_batch: job longer than its table");
     }
-    const uint64_t slot = batch_slot(jobs, count);
+    const uint32_t conc = batch_concurrency(count, streams);
+    const uint64_t slot = batch_slot(jobs, count, conc);
     if (scratch_bytes < slot * streams || !scratch)
         return scratch_too_small("h2b_msm_batch", scratch_bytes, slot * streams);
     // longest job first onto the least-loaded stream
@@ -191,7 +201,7 @@ extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint
     for (uint64_t j : order) {
         const uint32_t k = (uint32_t)(std::min_element(load.begin(), load.end()) - load.begin());
         load[k] += jobs[j].n + 4096;  // fixed cost per job: launch and tail latency
-        const MsmPlan p = job_plan(jobs[j].n, jobs[j].table_n);
+        const MsmPlan p = job_plan(jobs[j].n, jobs[j].table_n, conc);
         ScratchArena ar((uint8_t*)scratch + (uint64_t)k * slot, slot);
         const MsmScratch s = msm_carve(p, ar, false, false);
         if (!ar.good()) return err((int)cudaErrorInvalidValue, "h2b_msm_batch: slot carving failed");

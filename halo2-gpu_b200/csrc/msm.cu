@@ -84,7 +84,7 @@ static int choose_c(uint64_t n)
 
 // tn > 0: precomputed window table of tn points per window; all windows then
 // share one bucket set and the reduction has a single window.
-static MsmPlan plan_core(uint64_t n, int c, uint64_t tn)
+static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1)
 {
     MsmPlan p;
     p.n = n;
@@ -101,10 +101,13 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn)
     p.max_entries = p.nv * (uint64_t)p.W;
     // Entries per accumulation chunk (one thread walks a chunk): 128 when the
     // entries give at least ACC_TARGET_CHUNKS chunks (k >= 20 at every
-    // window size), fewer for small MSMs so that about ACC_TARGET_CHUNKS
-    // threads still run (148 SMs x 3 CTAs x 128 threads, 4 chunks each);
-    // a smaller K only adds chunk heads for the fixup to merge.
-    const uint64_t k_fit = p.max_entries / ACC_TARGET_CHUNKS;
+    // window size), fewer for a small MSM so that about ACC_TARGET_CHUNKS
+    // threads still run (148 SMs x 3 CTAs x 128 threads, 4 chunks each).
+    // MSMs that run `concurrent` at a time share that target.  A smaller K
+    // adds chunk heads that the fixup sums serially per bucket, so K must
+    // not drop where buckets are long: on the 64-job batch (16 streams) a
+    // fixed K = 32 took 133 ms over a window table against 85 ms at 128.
+    const uint64_t k_fit = p.max_entries / std::max<uint64_t>(1, ACC_TARGET_CHUNKS / std::max(concurrent, 1u));
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override
                                    : (uint32_t)std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
     // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
@@ -128,6 +131,11 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn)
 MsmPlan msm_plan(uint64_t n) { return plan_core(n, choose_c(n), 0); }
 
 MsmPlan msm_plan_table(uint64_t n, uint64_t tn) { return plan_core(n, choose_c(tn), tn); }
+
+MsmPlan msm_plan_shared(uint64_t n, uint64_t tn, uint32_t concurrent)
+{
+    return tn ? plan_core(n, choose_c(tn), tn, concurrent) : plan_core(n, choose_c(n), 0, concurrent);
+}
 
 void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host)
 {

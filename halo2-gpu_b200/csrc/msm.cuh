@@ -59,6 +59,9 @@ struct MsmScratch {
     uint64_t pr_inv_bytes;
 };
 
+// Plan for an MSM that runs beside `concurrent` - 1 others (batches): same
+// results; the accumulation's chunk size assumes the others share the SMs.
+MsmPlan msm_plan_shared(uint64_t n, uint64_t tn, uint32_t concurrent);
 MsmPlan msm_plan(uint64_t n);
 // Plan for an MSM of n <= tn points over a precomputed window table built for
 // tn points (window width chosen by tn; all windows share one bucket set).

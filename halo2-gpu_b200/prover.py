@@ -259,20 +259,62 @@ class Server:
     another's (and a small request is not stuck behind a large one).  A
     request is admitted when a slot is free and the device memory it will
     hold fits in `hbm_budget` bytes beside those in flight; `slots=1` is the
-    plain one-at-a-time prover.  Latency is arrival to completion of the
-    request's stream, measured on the host clock."""
+    plain one-at-a-time prover.  The workers (and their streams, forked
+    streams and memory pools) persist across `serve` calls until `close`.
+    Latency is arrival to completion of the request's stream, measured on the
+    host clock."""
 
     def __init__(self, res, slots, hbm_budget):
         self.res, self.slots, self.budget = res, slots, hbm_budget
         self.in_use = 0
         self.cv = threading.Condition()
         self.streams = [_t().cuda.Stream() for _ in range(slots)]
+        self.q = queue.Queue()
+        self.threads = [threading.Thread(target=self._worker, args=(s,), daemon=True) for s in range(slots)]
+        for th in self.threads:
+            th.start()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def close(self):
+        for _ in self.threads:
+            self.q.put(None)
+        for th in self.threads:
+            th.join()
+        self.threads = []
 
     def bytes_for(self, k):
         """Device bytes a 2^k request holds while in flight (its polynomials
         and the scratch of 4 concurrent MSMs)."""
         n = 1 << k
         return _bytes_per_proof(k) + 4 * int(self.res.h2b.lib().h2b_msm_table_workspace_size(n, 1 << self.res.kmax))
+
+    def _worker(self, slot):
+        st = self.streams[slot]
+        while True:
+            job = self.q.get()
+            if job is None:
+                return
+            k, seed, finish = job
+            need = self.bytes_for(k)
+            with self.cv:
+                while self.in_use + need > self.budget and self.in_use > 0:
+                    self.cv.wait()
+                self.in_use += need
+            try:
+                out = ProofWorkload(self.res, k, seed).run(st)
+                st.synchronize()
+                finish(time.perf_counter(), out, None)
+            except Exception as e:  # handed to serve(), which raises it
+                finish(time.perf_counter(), None, e)
+            finally:
+                with self.cv:
+                    self.in_use -= need
+                    self.cv.notify_all()
 
     def serve(self, reqs, keep_outputs=False):
         """Serves `reqs` (from `requests`) in arrival order; returns a dict of
@@ -283,55 +325,40 @@ class Server:
                 raise ValueError(f"a 2^{k} proof needs more than the {self.budget}-byte budget")
             self.res.key(k)
         torch.cuda.synchronize()
-        q = queue.Queue()
         done = [None] * len(reqs)
         outs = [None] * len(reqs)
         errors = []
+        left = [len(reqs)]
+        lock = threading.Lock()
+        finished = threading.Event()
+        if not reqs:
+            finished.set()
         t0 = time.perf_counter()
 
-        def worker(slot):
-            st = self.streams[slot]
-            while True:
-                item = q.get()
-                if item is None:
-                    return
-                i, (arr, k, seed) = item
-                need = self.bytes_for(k)
-                with self.cv:
-                    while self.in_use + need > self.budget and self.in_use > 0:
-                        self.cv.wait()
-                    self.in_use += need
-                try:
-                    out = ProofWorkload(self.res, k, seed).run(st)
-                    st.synchronize()
-                    done[i] = time.perf_counter() - t0
-                    if keep_outputs:
-                        outs[i] = ([c.cpu() for c in out[0]], [e.cpu() for e in out[1]])
-                    del out
-                except Exception as e:  # surfaced after the join
-                    errors.append(e)
-                    done[i] = float("nan")
-                finally:
-                    with self.cv:
-                        self.in_use -= need
-                        self.cv.notify_all()
+        def finisher(i):
+            def finish(t, out, err):
+                done[i] = t - t0
+                if err is not None:
+                    errors.append(err)
+                elif keep_outputs:
+                    outs[i] = ([c.cpu() for c in out[0]], [e.cpu() for e in out[1]])
+                with lock:
+                    left[0] -= 1
+                    if left[0] == 0:
+                        finished.set()
+            return finish
 
-        threads = [threading.Thread(target=worker, args=(s,), daemon=True) for s in range(self.slots)]
-        for th in threads:
-            th.start()
-        for i, r in enumerate(reqs):
-            wait = r[0] - (time.perf_counter() - t0)
+        for i, (arr, k, seed) in enumerate(reqs):
+            wait = arr - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
-            q.put((i, r))
-        for _ in threads:
-            q.put(None)
-        for th in threads:
-            th.join()
+            self.q.put((k, seed, finisher(i)))
+        finished.wait()
         if errors:
             raise errors[0]
         lat = np.array([d - r[0] for d, r in zip(done, reqs)])
-        return {"latency_s": lat, "makespan_s": float(max(done)), "outputs": outs if keep_outputs else None}
+        return {"latency_s": lat, "makespan_s": float(max(done)) if done else 0.0,
+                "outputs": outs if keep_outputs else None}
 
 
 def summary(reqs, result):

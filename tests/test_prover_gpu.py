@@ -48,14 +48,18 @@ def test_served_outputs_match_alone(h2b):
     res = P.Resident(h2b, 12)
     reqs = [(0.0, 12, 11), (0.0, 10, 12), (0.0, 11, 13), (0.0, 10, 14), (0.0, 12, 15)]
     alone = []
-    for r in reqs:
-        out = P.Server(res, 1, 1 << 36).serve([r], keep_outputs=True)["outputs"][0]
-        alone.append(_bytes(out))
-    mixed = P.Server(res, 3, 1 << 36).serve(reqs, keep_outputs=True)["outputs"]
-    for a, m in zip(alone, mixed):
-        assert a == _bytes(m)
+    with P.Server(res, 1, 1 << 36) as one:
+        for r in reqs:
+            alone.append(_bytes(one.serve([r], keep_outputs=True)["outputs"][0]))
+        need12 = one.bytes_for(12)
+    with P.Server(res, 3, 1 << 36) as srv:
+        mixed = srv.serve(reqs, keep_outputs=True)["outputs"]
+        again = srv.serve(reqs, keep_outputs=True)["outputs"]   # workers persist across calls
+    for a, m, g in zip(alone, mixed, again):
+        assert a == _bytes(m) == _bytes(g)
     # a budget that admits one request at a time gives the same bytes too
-    tight = P.Server(res, 3, P.Server(res, 1, 1 << 36).bytes_for(12)).serve(reqs, keep_outputs=True)["outputs"]
+    with P.Server(res, 3, need12) as tight_srv:
+        tight = tight_srv.serve(reqs, keep_outputs=True)["outputs"]
     for a, m in zip(alone, tight):
         assert a == _bytes(m)
     # each request's outputs: 4 advice + A' + S' + 2 z + lookup z + 3 h pieces + 2 Kate quotients
@@ -76,5 +80,5 @@ def test_served_outputs_match_alone(h2b):
 def test_server_rejects_oversize(h2b):
     P = _prover(h2b)
     res = P.Resident(h2b, 10)
-    with pytest.raises(ValueError):
-        P.Server(res, 2, 1 << 20).serve([(0.0, 10, 1)])
+    with P.Server(res, 2, 1 << 20) as srv, pytest.raises(ValueError):
+        srv.serve([(0.0, 10, 1)])
