@@ -94,14 +94,14 @@ struct NttBatch {
 
 // Forward-path input stage: out[rev(i)] = in[i] * f(i) for i < n_out, where
 // in[i] = 0 for i >= n_in (zero padding) and f is
-//   mode 0: 1,   mode 1: c^i (lut_c[j] = c^(2^j)),   mode 2: z3[i mod 3].
+//   mode 0: 1,   mode 1: c^i (cpow[i] = c^i),   mode 2: z3[i mod 3].
 // `out` must not alias `in`.
 constexpr int SC_CHUNK = 8;
 struct Zeta3 {
     Fr f[3];
 };
 __global__ void k_twist_bitrev_scatter(NttBatch B, uint64_t n_in, int log_out, int mode,
-                                       const Fr* __restrict__ lut_c, Zeta3 z3)
+                                       const Fr* __restrict__ cpow, Zeta3 z3)
 {
     const Fr* __restrict__ in = B.src[blockIdx.y];
     Fr* __restrict__ out = B.dst[blockIdx.y];
@@ -110,18 +110,11 @@ __global__ void k_twist_bitrev_scatter(NttBatch B, uint64_t n_in, int log_out, i
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
          t += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t i0 = t * SC_CHUNK;
-        Fr p;
-        Fr c;
-        if (mode == 1) {
-            p = pow_from_lut(lut_c, i0);
-            c = ldg(&lut_c[0]);
-        }
         for (int j = 0; j < SC_CHUNK && i0 + j < n_out; j++) {
             uint64_t i = i0 + j;
             Fr v = (i < n_in) ? ldg(&in[i]) : Fr::zero();
             if (mode == 1) {
-                v = v * p;
-                p = p * c;
+                v = v * ldg(&cpow[i]);
             } else if (mode == 2 && i < n_in) {
                 v = v * z3.f[i % 3];
             }
@@ -149,28 +142,18 @@ __global__ void k_coset_spread(NttBatch B, int log_in, int e, Zeta3 z3)
     }
 }
 
-// In-place a_i *= c^i (mode 1) or zeta^(i mod 3) factors (mode 2).
-__global__ void k_twist_inplace(NttBatch B, uint64_t n, int mode, const Fr* __restrict__ lut_c, Zeta3 z3)
+// In-place a_i *= c^i (mode 1, cpow[i] = c^i) or zeta^(i mod 3) factors (mode 2).
+__global__ void k_twist_inplace(NttBatch B, uint64_t n, int mode, const Fr* __restrict__ cpow, Zeta3 z3)
 {
     Fr* __restrict__ a = B.dst[blockIdx.y];
     uint64_t nthreads = n / SC_CHUNK + (n % SC_CHUNK ? 1 : 0);
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
          t += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t i0 = t * SC_CHUNK;
-        Fr p, c;
-        if (mode == 1) {
-            p = pow_from_lut(lut_c, i0);
-            c = ldg(&lut_c[0]);
-        }
         for (int j = 0; j < SC_CHUNK && i0 + j < n; j++) {
             uint64_t i = i0 + j;
             Fr v = ld(&a[i]);
-            if (mode == 1) {
-                v = v * p;
-                p = p * c;
-            } else {
-                v = v * z3.f[i % 3];
-            }
+            v = v * (mode == 1 ? ldg(&cpow[i]) : z3.f[i % 3]);
             st(&a[i], v);
         }
     }
@@ -214,7 +197,7 @@ constexpr int NTT_THREADS = 512;
 // power of two, so all index arithmetic is shifts and masks on 32 bits
 // (n <= 2^31).
 template <bool DIT>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
+__global__ void __launch_bounds__(NTT_THREADS, 3) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
                                                           int nst, int lS, int lG)
 {
     const Fr* src = B.src[blockIdx.y];  // the first pass of an out-of-place transform reads here
@@ -251,10 +234,24 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* 
     const uint32_t mmask = (1u << (nst - 1)) - 1;
     for (int t = 0; t < nst; t++) {
         const int s = s0 + t;
+        const int h = DIT ? t : nst - t - 1;
+        if (DIT ? s == 0 : s == logn - 1) {
+            // the first DIT stage and the last DIF stage use only w^0 = 1
+            for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
+                const uint32_t gl = u >> (nst - 1), m = u & mmask;
+                const uint32_t q = ((m >> h) << (h + 1)) | (m & ((1u << h) - 1));
+                Fr* px = &sm[(gl << nst) + q];
+                Fr* py = px + (1u << h);
+                const Fr x = *px, y = *py;
+                *px = x + y;
+                *py = x - y;
+            }
+            __syncthreads();
+            continue;
+        }
         for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
             const uint32_t gl = u >> (nst - 1), m = u & mmask;
             const uint32_t r = (g0 + gl) & Smask;
-            const int h = DIT ? t : nst - t - 1;
             const uint32_t lowm = m & ((1u << h) - 1);
             const uint32_t q = ((m >> h) << (h + 1)) | lowm;
             Fr* px = &sm[(gl << nst) + q];
@@ -324,16 +321,18 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
 }
 
 // Scratch layout for one transform family: twiddles (n/2), lut_w (64), lut_c
-// (64), omega staging, then (host-input variants) one data slot.
+// (64), omega staging, (host-input variants) one data slot, then (coset
+// parts) the coset powers c^i, i < n.
 struct NttScratch {
     Fr* tw = nullptr;
     Fr* lut_w = nullptr;
     Fr* lut_c = nullptr;
     Fr* omega = nullptr;
     Fr* data = nullptr;
+    Fr* cpow = nullptr;
 };
 
-static void plan_ntt(ScratchPlan& p, int log_size, bool data_slot, int log_data)
+static void plan_ntt(ScratchPlan& p, int log_size, bool data_slot, int log_data, bool coset_powers)
 {
     uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
     p.add_n<Fr>(half);
@@ -341,9 +340,10 @@ static void plan_ntt(ScratchPlan& p, int log_size, bool data_slot, int log_data)
     p.add_n<Fr>(64);
     p.add_n<Fr>(1);
     if (data_slot) p.add_n<Fr>(1ull << log_data);
+    if (coset_powers) p.add_n<Fr>(1ull << log_size);
 }
 
-static NttScratch carve_ntt(ScratchArena& ar, int log_size, bool data_slot, int log_data)
+static NttScratch carve_ntt(ScratchArena& ar, int log_size, bool data_slot, int log_data, bool coset_powers)
 {
     NttScratch s;
     uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
@@ -352,6 +352,7 @@ static NttScratch carve_ntt(ScratchArena& ar, int log_size, bool data_slot, int 
     s.lut_c = ar.take_n<Fr>(64);
     s.omega = ar.take_n<Fr>(1);
     if (data_slot) s.data = ar.take_n<Fr>(1ull << log_data);
+    if (coset_powers) s.cpow = ar.take_n<Fr>(1ull << log_size);
     return s;
 }
 
@@ -410,9 +411,14 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
         int mode = 0;
         Zeta3 z3 = none;
         if (type == 6) {
+            // c^i for i < n once for the group (one product per element), so the
+            // twist costs each polynomial one product per element
             Fr64 lut[64];
             fr_pow2_lut(*h_divisor, logt, lut);
             H2B_CUDA(cudaMemcpyAsync(s.lut_c, lut, sizeof(Fr) * logt, cudaMemcpyHostToDevice, st));
+            const uint64_t tile = (uint64_t)TW_T * TW_K;
+            k_twiddles<<<(unsigned)((nt + tile - 1) / tile), TW_T, 0, st>>>(s.lut_c, s.cpow, nt);
+            H2B_LAUNCHED("k_twiddles");
             mode = 1;
         } else if (type == 3) {
             z3 = zeta_factors(fr_const(FR_ONE), false);
@@ -426,7 +432,7 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
         }
         const uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
         if (!alias) {
-            k_twist_bitrev_scatter<<<grid(nthreads), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.lut_c, z3);
+            k_twist_bitrev_scatter<<<grid(nthreads), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.cpow, z3);
             H2B_LAUNCHED("k_twist_bitrev_scatter");
         } else {
             if (type == 3 && nt != nin) {
@@ -435,7 +441,7 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
                     H2B_CUDA(cudaMemsetAsync(D.dst[i] + nin, 0, (nt - nin) * sizeof(Fr), st));
             }
             if (mode != 0) {
-                k_twist_inplace<<<grid(nthreads), 256, 0, st>>>(D, nt, mode, s.lut_c, z3);
+                k_twist_inplace<<<grid(nthreads), 256, 0, st>>>(D, nt, mode, s.cpow, z3);
                 H2B_LAUNCHED("k_twist_inplace");
             }
             k_bitrev_inplace<<<grid(nt), 256, 0, st>>>(D, logt, false, none);
@@ -499,7 +505,7 @@ extern "C" uint64_t _halo2_fft_normal_workspace_size(uint32_t ntt_type, uint32_t
 {
     ScratchPlan p;
     int la = active_log(ntt_type, log_n, extend_log_n);
-    plan_ntt(p, la, true, la);
+    plan_ntt(p, la, true, la, ntt_type == 6);
     return p.used;
 }
 
@@ -514,7 +520,7 @@ extern "C" RustError _halo2_fft_normal(uint32_t ntt_type, uint32_t log_n, const 
     uint64_t need = _halo2_fft_normal_workspace_size(ntt_type, log_n, log_n);
     if (scratch_bytes < need) return scratch_too_small("_halo2_fft_normal", scratch_bytes, need);
     ScratchArena ar(scratch, scratch_bytes);
-    NttScratch s = carve_ntt(ar, log_n, true, log_n);
+    NttScratch s = carve_ntt(ar, log_n, true, log_n, ntt_type == 6);
     if (!ar.good()) return scratch_too_small("_halo2_fft_normal", scratch_bytes, need);
     H2B_CUDA(cudaMemcpyAsync(s.omega, omega, sizeof(Fr), cudaMemcpyHostToDevice, stream));
     H2B_TRY(make_twiddles(s.omega, s, log_n, stream));
@@ -529,7 +535,7 @@ extern "C" uint64_t _halo2_fft_normal_to_device_workspace_size(uint32_t ntt_type
                                                                uint32_t extend_log_n)
 {
     ScratchPlan p;
-    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0);
+    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0, ntt_type == 6);
     return p.used;
 }
 
@@ -543,7 +549,7 @@ extern "C" RustError _halo2_fft_normal_to_device(uint32_t ntt_type, uint32_t log
     uint64_t need = _halo2_fft_normal_to_device_workspace_size(ntt_type, log_n, log_n);
     if (scratch_bytes < need) return scratch_too_small("_halo2_fft_normal_to_device", scratch_bytes, need);
     ScratchArena ar(scratch, scratch_bytes);
-    NttScratch s = carve_ntt(ar, log_n, false, 0);
+    NttScratch s = carve_ntt(ar, log_n, false, 0, ntt_type == 6);
     H2B_TRY(make_twiddles((const Fr*)d_omega, s, log_n, stream));
     host::Fr64 div = host::fr_from(h_divisor);
     return transform_one(ntt_type, log_n, log_n, d_input, false, (Fr*)d_output, &div, s, stream);
@@ -562,7 +568,7 @@ extern "C" RustError _halo2_cosetfft(uint32_t ntt_type, uint32_t log_n, uint32_t
     uint64_t need = _halo2_fft_normal_workspace_size(3, log_n, extend_log_n);
     if (scratch_bytes < need) return scratch_too_small("_halo2_cosetfft", scratch_bytes, need);
     ScratchArena ar(scratch, scratch_bytes);
-    NttScratch s = carve_ntt(ar, extend_log_n, true, extend_log_n);
+    NttScratch s = carve_ntt(ar, extend_log_n, true, extend_log_n, false);
     H2B_CUDA(cudaMemcpyAsync(s.omega, omega, sizeof(Fr), cudaMemcpyHostToDevice, stream));
     H2B_TRY(make_twiddles(s.omega, s, extend_log_n, stream));
     host::Fr64 one = host::fr_const(host::FR_ONE);
@@ -576,7 +582,7 @@ extern "C" uint64_t _halo2_fft_many_workspace_size(uint32_t ntt_type, uint32_t l
 {
     ScratchPlan p;
     int la = active_log(ntt_type, log_n, extend_log_n);
-    plan_ntt(p, la, true, la);
+    plan_ntt(p, la, true, la, ntt_type == 6);
     return p.used;
 }
 
@@ -584,7 +590,7 @@ extern "C" uint64_t _halo2_fft_many_to_device_workspace_size(uint32_t ntt_type, 
                                                              uint32_t extend_log_n)
 {
     ScratchPlan p;
-    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0);
+    plan_ntt(p, active_log(ntt_type, log_n, extend_log_n), false, 0, ntt_type == 6);
     return p.used;
 }
 
@@ -603,7 +609,7 @@ static RustError fft_many_impl(uint32_t ntt_type, uint32_t num_many, uint32_t lo
                                   : _halo2_fft_many_workspace_size(ntt_type, log_n, extend_log_n);
     if (scratch_bytes < need) return scratch_too_small(who, scratch_bytes, need);
     ScratchArena ar(scratch, scratch_bytes);
-    NttScratch s = carve_ntt(ar, la, !out_on_device, la);
+    NttScratch s = carve_ntt(ar, la, !out_on_device, la, ntt_type == 6);
     H2B_TRY(make_twiddles((const Fr*)d_omega, s, la, stream));
     host::Fr64 div = (divisor && divisor->ptr) ? host::fr_from(divisor->ptr) : host::fr_const(host::FR_ONE);
     if (!out_on_device) {
