@@ -20,7 +20,8 @@
 //    is never negative for an almost-normalised b below (K - 0.001) p.
 //
 // Values in this form are x * 2^261 mod p (plus multiples of p).  Affine
-// bases enter as canonical x * 2^261 mod p (converted once, k_to_r261); the
+// bases enter as canonical x * 2^261 mod p (converted once per MSM by a shift
+// and a reduction, to_r261, or stored that way in window tables); the
 // results leave through one product by 2^256 mod p, which yields the memory
 // image x * 2^256 mod p, then a final conditional subtraction.
 #pragma once
@@ -232,21 +233,34 @@ H2B_DEV Fz<C> fz_from_words(const Fp<C>& a)
     return r;
 }
 
-// 2^261 mod p as a canonical word image (= 2^256 mod p doubled five times)
+// memory image X = x 2^256 mod p -> canonical x 2^261 mod p = 32 X mod p:
+// a 5-bit shift and one subtraction of q p, with q = floor(32 X / p) taken
+// from the top 64 bits (q_est <= q <= q_est + 1 since p's top word M7 is
+// above 2^29), then one conditional subtraction.  No product.
 template <class C>
-H2B_DEV Fp<C> r261_words()
+H2B_DEV Fp<C> to_r261(const Fp<C>& x)
 {
-    Fp<C> c = Fp<C>::one();
-#pragma unroll 1
-    for (int i = 0; i < 5; i++) c = c + c;
-    return c;
-}
-
-// memory image x 2^256 mod p -> canonical x 2^261 mod p (word image)
-template <class C>
-H2B_DEV Fp<C> to_r261(const Fp<C>& x, const Fp<C>& r261)
-{
-    return x * r261;
+    uint32_t y[9];
+    y[0] = x.v[0] << 5;
+#pragma unroll
+    for (int i = 1; i < 8; i++) y[i] = (x.v[i] << 5) | (x.v[i - 1] >> 27);
+    y[8] = x.v[7] >> 27;
+    const uint64_t top = ((uint64_t)y[8] << 32) | y[7];
+    const uint32_t q = (uint32_t)(top / ((uint64_t)C::M7 + 1));
+    uint32_t r[8];
+    uint64_t carry = 0;
+    uint32_t borrow = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const uint64_t qp = (uint64_t)q * mword<C>(i) + carry;
+        carry = qp >> 32;
+        const uint64_t d = (uint64_t)y[i] - (uint32_t)qp - borrow;
+        r[i] = (uint32_t)d;
+        borrow = (uint32_t)(d >> 63);
+    }
+    Fp<C> out;
+    cond_sub<C>(out.v, r);
+    return out;
 }
 
 // A product output (normalised limbs, value < 2p) packed to 8 x 32 and

@@ -217,13 +217,21 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
 // Virtual scalars: vs[2i] = k1, vs[2i+1] = k2 of the GLV split of scalar i
 // (128-bit magnitudes, sign in bit 127), so entry v stands for point i = v/2,
 // taken as P_i (v even) or phi(P_i) (v odd).
-__global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t n)
+// GLV split of each scalar; with `rb` set, base i is also converted to the
+// lazy x 2^261 form the accumulation reads (same index space, one launch).
+__global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t n,
+                          const G1Affine* __restrict__ bases, G1Affine* __restrict__ rb)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint4 a, b;
         glv::decompose(from_mont(ldg(&sc[i])), a, b);
         vs[2 * i] = a;
         vs[2 * i + 1] = b;
+        if (rb) {
+            const G1Affine q = ld_affine(&bases[i]);
+            st(&rb[i].x, to_r261(q.x));
+            st(&rb[i].y, to_r261(q.y));
+        }
     }
 }
 
@@ -330,12 +338,11 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : (MODE >= 3 ? MODE + 1 : 3
 // form the lazy accumulation reads; infinity (0, 0) stays (0, 0).
 __global__ void k_to_r261(const G1Affine* in, G1Affine* out, uint64_t n)  // in may equal out
 {
-    const Fq r261 = r261_words<FqCfg>();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const G1Affine a = ld_affine(&in[i]);
         G1Affine r;
-        r.x = to_r261(a.x, r261);
-        r.y = to_r261(a.y, r261);
+        r.x = to_r261(a.x);
+        r.y = to_r261(a.y);
         st(&out[i].x, r.x);
         st(&out[i].y, r.y);
     }
@@ -352,10 +359,9 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_z(const uint32_t* __r
                                                              G1Xyzz* __restrict__ buckets,
                                                              G1Xyzz* __restrict__ heads)
 {
-    const Fq r261 = r261_words<FqCfg>();
-    const FqZ one = fz_from_words(r261);                          // 1 in the lazy form
+    const FqZ one = fz_from_words(to_r261(Fq::one()));           // 1 in the lazy form (2^261 mod p)
     const FqZ r256 = fz_from_words(Fq::one());                    // 2^256 mod p, for the stores
-    const FqZ beta = fz_from_words(to_r261(glv::beta(), r261));   // phi(x, y) = (beta x, y)
+    const FqZ beta = fz_from_words(to_r261(glv::beta()));         // phi(x, y) = (beta x, y)
     const uint32_t M = offsets[NB];
     const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
@@ -772,15 +778,12 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     const unsigned sm_cap = 148u * 16u;
     prof_begin(PROF_MSM_TOTAL, st);
     uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
-    k_msm_glv<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, p.n);
-    H2B_LAUNCHED("k_msm_glv");
     // the lazy accumulation (window tables are stored in its form; plain bases
-    // are converted here) unless pairing rounds or an older variant run
+    // are converted by the split kernel) unless pairing rounds or an older variant run
     const bool lazy = p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0);
-    if (lazy && p.tn == 0) {
-        k_to_r261<<<grid_for(p.n, 256, 148u * 8u), 256, 0, st>>>(d_bases, s.rbases, p.n);
-        H2B_LAUNCHED("k_to_r261");
-    }
+    k_msm_glv<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, p.n, d_bases,
+                                                         lazy && p.tn == 0 ? s.rbases : nullptr);
+    H2B_LAUNCHED("k_msm_glv");
     H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
     H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
     k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr,
