@@ -597,30 +597,32 @@ __global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, u
             if (idx < max_dense) dense[idx] = (uint32_t)gb;
             continue;
         }
-        G1Xyzz acc = ld_xyzz(&buckets[gb]);
-        for (uint32_t t = t0 + 1; t <= t1; t++) xyzz_add(acc, ld_xyzz(&heads[t]));
-        st_xyzz(&buckets[gb], acc);
+        G1XyzzL acc = xyzzl_from(ld_xyzz(&buckets[gb]));
+        for (uint32_t t = t0 + 1; t <= t1; t++) xyzzl_add(acc, xyzzl_from(ld_xyzz(&heads[t])));
+        st_xyzz(&buckets[gb], xyzzl_to(acc));
     }
 }
 
-// CTA-wide tree sum of n XYZZ values produced by get(i); result valid in thread 0.
+// CTA-wide tree sum of n XYZZ values produced by get(i); result valid in
+// thread 0.  The partial sums stay in 29-bit limb form (latency-oriented
+// products: every level of the tree is one dependent addition per thread).
 template <class Get>
 __device__ G1Xyzz block_sum_xyzz(uint64_t n, Get get)
 {
-    __shared__ G1Xyzz red[256];
-    G1Xyzz acc = xyzz_inf();
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) xyzz_add(acc, get(i));
+    __shared__ G1XyzzL red[256];
+    G1XyzzL acc = xyzzl_inf();
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) xyzzl_add(acc, xyzzl_from(get(i)));
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
         if ((int)threadIdx.x < h) {
-            G1Xyzz a = red[threadIdx.x];
-            xyzz_add(a, red[threadIdx.x + h]);
+            G1XyzzL a = red[threadIdx.x];
+            xyzzl_add(a, red[threadIdx.x + h]);
             red[threadIdx.x] = a;
         }
         __syncthreads();
     }
-    G1Xyzz r = red[0];
+    G1Xyzz r = xyzzl_to(red[0]);
     __syncthreads();
     return r;
 }
@@ -688,13 +690,13 @@ __global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__
          id += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t w = id / S, s = id % S;
         const G1Xyzz* B = buckets + w * H + s * L;
-        G1Xyzz run = xyzz_inf(), acc = xyzz_inf();
+        G1XyzzL run = xyzzl_inf(), acc = xyzzl_inf();
         for (int j = (int)L - 1; j >= 0; j--) {
-            xyzz_add(run, ld_xyzz(&B[j]));
-            xyzz_add(acc, run);
+            xyzzl_add(run, xyzzl_from(ld_xyzz(&B[j])));
+            xyzzl_add(acc, run);
         }
-        st_xyzz(&segacc[id], acc);
-        st_xyzz(&segrun[id], run);
+        st_xyzz(&segacc[id], xyzzl_to(acc));
+        st_xyzz(&segrun[id], xyzzl_to(run));
     }
 }
 
