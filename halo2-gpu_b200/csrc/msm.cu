@@ -36,6 +36,8 @@
 #include "glv.cuh"
 #include "scan_u32.cuh"
 
+extern "C" RustError h2b_exec_fork(cudaStream_t parent, uint32_t n, cudaStream_t* out);  // exec.cu
+
 namespace h2b {
 
 static constexpr int GLV_BITS = 127;
@@ -46,6 +48,8 @@ static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed seri
 static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
 static constexpr uint64_t ACC_TARGET_CHUNKS = 148ull * 3 * 128 * 4;  // accumulation threads x 4
 static constexpr uint64_t ACC_MIN_K = 16;       // smallest chunk of the default plan
+static constexpr uint64_t MSM_PIPE_MIN = 1ull << 18;  // host scalars from here on are copied in pieces
+static constexpr int MSM_PIPE_PIECES = 8;
 
 static int g_msm_window_override = 0;
 static int g_msm_acc_variant = 0;  // call structure of the accumulation kernel (0, 1, 2)
@@ -219,10 +223,11 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
 // taken as P_i (v even) or phi(P_i) (v odd).
 // GLV split of each scalar; with `rb` set, base i is also converted to the
 // lazy x 2^261 form the accumulation reads (same index space, one launch).
-__global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t n,
+__global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t lo, uint64_t hi,
                           const G1Affine* __restrict__ bases, G1Affine* __restrict__ rb)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t i = lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < hi;
+         i += (uint64_t)gridDim.x * blockDim.x) {
         uint4 a, b;
         glv::decompose(from_mont(ldg(&sc[i])), a, b);
         vs[2 * i] = a;
@@ -245,13 +250,14 @@ __device__ __forceinline__ uint32_t window_bits(const uint4& s, int bit, int c)
 
 // For each digit: key = w*H + |d| - 1 (or ~0 for zero digits); the entry's
 // sign is the digit's sign flipped by the virtual scalar's sign.
+// Virtual points v0 <= i < n.
 template <bool SCATTER>
-__global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t n, int c, int W, uint32_t H,
+__global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t n, int c, int W, uint32_t H,
                            uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted, uint64_t tn)
 {
     const unsigned lane = threadIdx.x & 31;
     const uint32_t full = 1u << c;
-    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t base = v0 + blockIdx.x * (uint64_t)blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t i = base + threadIdx.x;
         bool valid = i < n;
         uint4 s = valid ? vsc[i] : make_uint4(0u, 0u, 0u, 0u);
@@ -770,31 +776,47 @@ __global__ void k_write_inf(G1Jac* out)
 }
 
 // Runs steps 1-7 on device buffers; result (96 bytes) lands in s.result.
-RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases, cudaStream_t st)
+// The lazy accumulation (window tables are stored in its form; plain bases
+// are converted by the split kernel) unless pairing rounds or an older
+// variant run.
+static bool msm_lazy(const MsmPlan& p) { return p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0); }
+
+// Phases of one MSM on `st`: msm_begin clears the histogram, msm_split takes
+// points [lo, hi) through the GLV split (and base conversion) and the
+// histogram -- callers may feed the points in pieces as they arrive --, and
+// msm_finish sorts, accumulates and reduces.
+static RustError msm_begin(const MsmPlan& p, const MsmScratch& s, cudaStream_t st)
 {
-    if (p.n == 0) {
-        k_write_inf<<<1, 32, 0, st>>>(s.result);
-        H2B_LAUNCHED("k_write_inf");
-        return ok();
-    }
-    const unsigned sm_cap = 148u * 16u;
     prof_begin(PROF_MSM_TOTAL, st);
-    uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
-    // the lazy accumulation (window tables are stored in its form; plain bases
-    // are converted by the split kernel) unless pairing rounds or an older variant run
-    const bool lazy = p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0);
-    k_msm_glv<<<grid_for(p.n, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, p.n, d_bases,
-                                                         lazy && p.tn == 0 ? s.rbases : nullptr);
-    H2B_LAUNCHED("k_msm_glv");
     H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
     H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
-    k_msm_sort<false><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.counts, nullptr,
-                                                                     p.tn);
+    return ok();
+}
+
+static RustError msm_split(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases,
+                           uint64_t lo, uint64_t hi, cudaStream_t st)
+{
+    if (hi <= lo) return ok();
+    const unsigned sm_cap = 148u * 16u;
+    uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
+    k_msm_glv<<<grid_for(hi - lo, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, lo, hi, d_bases,
+                                                              msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr);
+    H2B_LAUNCHED("k_msm_glv");
+    k_msm_sort<false><<<grid_for(2 * (hi - lo), 256, sm_cap), 256, 0, st>>>(vsc, 2 * lo, 2 * hi, p.c, p.W, p.H,
+                                                                              s.counts, nullptr, p.tn);
     H2B_LAUNCHED("k_msm_sort<hist>");
+    return ok();
+}
+
+static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affine* d_bases, cudaStream_t st)
+{
+    const unsigned sm_cap = 148u * 16u;
+    const uint4* vsc = reinterpret_cast<const uint4*>(s.canon);
+    const bool lazy = msm_lazy(p);
     H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
     H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, p.nv, p.c, p.W, p.H, s.cursor, s.sorted,
-                                                                    p.tn);
+    k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, 0, p.nv, p.c, p.W, p.H, s.cursor,
+                                                                    s.sorted, p.tn);
     H2B_LAUNCHED("k_msm_sort<scatter>");
     prof_begin(PROF_MSM_ACCUMULATE, st);
     // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
@@ -864,6 +886,18 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     return ok();
 }
 
+RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases, cudaStream_t st)
+{
+    if (p.n == 0) {
+        k_write_inf<<<1, 32, 0, st>>>(s.result);
+        H2B_LAUNCHED("k_write_inf");
+        return ok();
+    }
+    H2B_TRY(msm_begin(p, s, st));
+    H2B_TRY(msm_split(p, s, d_scalars, d_bases, 0, p.n, st));
+    return msm_finish(p, s, d_bases, st);
+}
+
 } // namespace h2b
 
 using namespace h2b;
@@ -907,15 +941,36 @@ static RustError msm_entry(const void* scalars, bool scalar_host, const void* ba
     if (!ar.good()) return scratch_too_small(who, scratch_bytes, need);
     const Fr* d_sc = (const Fr*)scalars;
     const G1Affine* d_b = (const G1Affine*)bases;
-    if (length > 0 && scalar_host) {
-        H2B_CUDA(cudaMemcpyAsync(s.scalar_stage, scalars, length * sizeof(Fr), cudaMemcpyHostToDevice, st));
-        d_sc = s.scalar_stage;
-    }
     if (length > 0 && bases_host) {
         H2B_CUDA(cudaMemcpyAsync(s.bases_stage, bases, length * sizeof(G1Affine), cudaMemcpyHostToDevice, st));
         d_b = s.bases_stage;
     }
-    H2B_TRY(msm_run(p, s, d_sc, d_b, st));
+    if (length >= MSM_PIPE_MIN && scalar_host) {
+        // Host scalars arrive in MSM_PIPE_PIECES pieces on a forked copy stream;
+        // the split and histogram of each piece run while the next one copies.
+        cudaStream_t cs;
+        H2B_TRY(h2b_exec_fork(st, 1, &cs));
+        cudaEvent_t ev[MSM_PIPE_PIECES];
+        for (int i = 0; i < MSM_PIPE_PIECES; i++) H2B_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+        RustError e = msm_begin(p, s, st);
+        for (int i = 0; i < MSM_PIPE_PIECES && e.code == 0; i++) {
+            const uint64_t lo = length * i / MSM_PIPE_PIECES, hi = length * (i + 1) / MSM_PIPE_PIECES;
+            cudaError_t c = cudaMemcpyAsync(s.scalar_stage + lo, (const Fr*)scalars + lo, (hi - lo) * sizeof(Fr),
+                                            cudaMemcpyHostToDevice, cs);
+            if (c == cudaSuccess) c = cudaEventRecord(ev[i], cs);
+            if (c == cudaSuccess) c = cudaStreamWaitEvent(st, ev[i], 0);
+            e = c == cudaSuccess ? msm_split(p, s, s.scalar_stage, d_b, lo, hi, st) : cuda_err(c, who);
+        }
+        for (int i = 0; i < MSM_PIPE_PIECES; i++) cudaEventDestroy(ev[i]);
+        H2B_TRY(e);
+        H2B_TRY(msm_finish(p, s, d_b, st));
+    } else {
+        if (length > 0 && scalar_host) {
+            H2B_CUDA(cudaMemcpyAsync(s.scalar_stage, scalars, length * sizeof(Fr), cudaMemcpyHostToDevice, st));
+            d_sc = s.scalar_stage;
+        }
+        H2B_TRY(msm_run(p, s, d_sc, d_b, st));
+    }
     H2B_CUDA(cudaMemcpyAsync(h_out, s.result, sizeof(G1Jac), cudaMemcpyDeviceToHost, st));
     H2B_CUDA(cudaStreamSynchronize(st));
     return ok();

@@ -126,6 +126,19 @@ def test_msm_kzg_property_k22(h2b, orc, cuda):
     for i in range(4):
         p = orc.g1_mul(f.fr_mont_limbs([pow(tau, i, f.R_MOD)]), orc.g1_generator())
         assert_limbs_equal(srs[i], p[:8], f"srs[{i}]")
+    # host scalars (copied in pieces that overlap the split) give the same point
+    assert_limbs_equal(h2b.multiexp_gpu_device_bases(sc, d_srs, n), want, "host scalars at 2^22")
+
+
+@pytest.mark.parametrize("n", [(1 << 18) - 1, 1 << 18, (1 << 18) + 5, 300007])
+def test_msm_host_scalars_in_pieces(h2b, orc, cuda, n):
+    """_halo2_multiexp_device_bases copies host scalars in pieces from 2^18
+    points on; ragged piece boundaries against the device-scalar path."""
+    d_srs = h2b.srs_device(0x51CE5, n)
+    d_sc = h2b.random_fr_device(n, 77 + n, 1)
+    want = h2b.multiexp_gpu_device_scalars_device_bases(d_sc, d_srs, n)
+    got = h2b.multiexp_gpu_device_bases(h2b.to_host(d_sc), d_srs, n)
+    assert_limbs_equal(got, want, f"host scalars n={n}")
 
 
 @pytest.mark.parametrize("rounds", [1, 2, 3])
