@@ -1,0 +1,96 @@
+"""The value bounds behind the lazy accumulation form (csrc/lazy.cuh,
+csrc/curve.cuh xyzzz_madd / xyzzz_dbl_affine), re-derived with exact
+rational arithmetic: every subtraction a - b + K p must see b below
+(K - 0.001) p, every product input must keep the 64-bit column sums exact,
+and the accumulator bounds (X < 5.39p, Y < 3.34p, ZZ, ZZZ < 2p) must be
+stable from one addition to the next.  Also checks the borrow-adjusted K p
+limbs the kernels add."""
+from fractions import Fraction as Q
+
+P = 0x30644E72E131A029B85045B68181585D97816A916871CA8D3C208C16D87CFD47
+R = 1 << 261
+EPS = Q(P, R)                   # product of a p and b p is below (1 + EPS a b) p
+
+
+def mul(a, b):
+    return 1 + EPS * a * b
+
+
+def sub(a, b, K):
+    assert b < K - Q(1, 1000), f"subtrahend bound {float(b)} needs K > {float(b)}, got {K}"
+    return a + K
+
+
+def madd(X1, Y1, ZZ1, ZZZ1, qx, qy):
+    U2, S2 = mul(qx, ZZ1), mul(qy, ZZZ1)
+    P_ = sub(U2, X1, 6)
+    R_ = sub(S2, Y1, 4)
+    PP, RR = mul(P_, P_), mul(R_, R_)
+    PPP, Qv = mul(P_, PP), mul(X1, PP)
+    X3 = sub(RR, PPP + 2 * Qv, 4)
+    w = sub(Qv, X3, 6)
+    Y3 = sub(mul(R_, w), mul(Y1, PPP), 2)
+    return X3, Y3, mul(ZZ1, PP), mul(ZZZ1, PPP), (U2, S2, P_, R_, PP, RR, PPP, Qv, w)
+
+
+def dbl_affine(qx, qy):
+    U = qy + qy
+    V, xx = mul(U, U), mul(qx, qx)
+    W, S = mul(U, V), mul(qx, V)
+    M = 3 * xx
+    MM, Wy = mul(M, M), mul(W, qy)
+    X3 = sub(MM, 2 * S, 3)
+    Y3 = sub(mul(M, sub(S, X3, 5)), Wy, 2)
+    return X3, Y3, V, W
+
+
+def test_madd_bounds_are_stable():
+    qx, qy = Q(101, 100), Q(2)          # canonical or times beta; canonical or negated (2p - y)
+    X, Y, ZZ, ZZZ = Q(539, 100), Q(334, 100), Q(2), Q(2)
+    X3, Y3, ZZ3, ZZZ3, inner = madd(X, Y, ZZ, ZZZ, qx, qy)
+    assert X3 <= X and Y3 <= Y and ZZ3 <= ZZ and ZZZ3 <= ZZZ
+    # the infinity start (acc = q, ZZ = ZZZ = 1 < p) is inside the same bounds
+    assert qx <= X and qy <= Y
+    # every product input stays well inside the column-sum budget (values below 16 p)
+    assert max(inner) < 16
+
+
+def test_doubling_path_bounds():
+    X3, Y3, ZZ3, ZZZ3 = dbl_affine(Q(101, 100), Q(2))
+    assert X3 < Q(539, 100) and Y3 < Q(334, 100) and ZZ3 < 2 and ZZZ3 < 2
+
+
+def test_store_product_below_2p():
+    # the store multiplies each coordinate by 2^256 mod p (< p): result < 2p
+    for bound in (Q(539, 100), Q(334, 100), Q(2)):
+        assert mul(bound, 1) < 2
+
+
+def _p29(i):
+    return (P >> (29 * i)) & ((1 << 29) - 1) if i < 8 else P >> 232
+
+
+def _kp29(K, i):
+    v = K * P
+    return (v >> (29 * i)) & ((1 << 29) - 1) if i < 8 else v >> 232
+
+
+def test_borrow_adjusted_limbs():
+    for K in (2, 3, 4, 5, 6):
+        limbs = [_kp29(K, i) + ((1 << 30) if i < 8 else 0) - (2 if i > 0 else 0) for i in range(9)]
+        assert sum(l << (29 * i) for i, l in enumerate(limbs)) == K * P
+        assert all(l >= (1 << 30) - 2 for l in limbs[:8])
+        assert all(l < (1 << 32) for l in limbs)
+        # an almost-normalised b < (K - 0.001) p keeps the top limb difference non-negative
+        b_top_max = (K * P - P // 1000) >> 232
+        assert limbs[8] >= b_top_max
+        # a + L - b stays below 2^32 per limb for a, b limbs below 2^29 + 8
+        assert max(limbs[:8]) + (1 << 29) + 8 < (1 << 32)
+
+
+def test_column_sums_fit_64_bits():
+    lim = (1 << 29) + 8                 # almost-normalised limb
+    assert 9 * lim * lim + 9 * ((1 << 29) - 1) ** 2 + (1 << 35) < 1 << 64
+    # squares use doubled limbs (2 a_j < 2^30.1)
+    assert 5 * lim * (2 * lim) + lim * lim + 9 * ((1 << 29) - 1) ** 2 + (1 << 35) < 1 << 64
+    assert _p29(8) < (1 << 29)
