@@ -92,34 +92,39 @@ struct NttBatch {
     Fr* dst[NTT_MAX_BATCH];
 };
 
-// Forward-path input stage: out[rev(i)] = in[i] * f(i) for i < n_out, where
-// in[i] = 0 for i >= n_in (zero padding) and f is
-//   mode 0: 1,   mode 1: c^i (cpow[i] = c^i),   mode 2: z3[i mod 3].
-// `out` must not alias `in`.
+// Forward-path input stage fused with the first DIT stage (whose twiddle is
+// w^0 = 1): with a_i = in[i] * f(i) (in[i] = 0 for i >= n_in) and f
+//   mode 0: 1,   mode 1: c^i (cpow[i] = c^i),   mode 2: z3[i mod 3],
+// output pair (2m, 2m + 1) of the bit-reversed array holds inputs
+// i0 = rev(2m) and i1 = i0 + n/2, and becomes (a_i0 + a_i1, a_i0 - a_i1).
+// Threads walk the output pairs in order: stores are contiguous, the
+// 32-byte input loads are scattered.  `out` must not alias `in`.
 constexpr int SC_CHUNK = 8;
 struct Zeta3 {
     Fr f[3];
 };
-__global__ void k_twist_bitrev_scatter(NttBatch B, uint64_t n_in, int log_out, int mode,
-                                       const Fr* __restrict__ cpow, Zeta3 z3)
+__device__ __forceinline__ Fr twist_in(const Fr* __restrict__ in, uint64_t i, uint64_t n_in, int mode,
+                                       const Fr* __restrict__ cpow, const Zeta3& z3)
+{
+    if (i >= n_in) return Fr::zero();
+    const Fr v = ldg(&in[i]);
+    if (mode == 1) return v * ldg(&cpow[i]);
+    if (mode == 2) return v * z3.f[i % 3];
+    return v;
+}
+__global__ void k_twist_bitrev_stage0(NttBatch B, uint64_t n_in, int log_out, int mode,
+                                      const Fr* __restrict__ cpow, Zeta3 z3)
 {
     const Fr* __restrict__ in = B.src[blockIdx.y];
     Fr* __restrict__ out = B.dst[blockIdx.y];
-    uint64_t n_out = 1ull << log_out;
-    uint64_t nthreads = n_out / SC_CHUNK + (n_out % SC_CHUNK ? 1 : 0);
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t i0 = t * SC_CHUNK;
-        for (int j = 0; j < SC_CHUNK && i0 + j < n_out; j++) {
-            uint64_t i = i0 + j;
-            Fr v = (i < n_in) ? ldg(&in[i]) : Fr::zero();
-            if (mode == 1) {
-                v = v * ldg(&cpow[i]);
-            } else if (mode == 2 && i < n_in) {
-                v = v * z3.f[i % 3];
-            }
-            st(&out[bitrev(i, log_out)], v);
-        }
+    const uint64_t half = 1ull << (log_out - 1);
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < half;
+         m += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i0 = bitrev(m, log_out - 1);   // rev(2m) over log_out bits
+        const Fr a = twist_in(in, i0, n_in, mode, cpow, z3);
+        const Fr b = twist_in(in, i0 + half, n_in, mode, cpow, z3);
+        st(&out[2 * m], a + b);
+        st(&out[2 * m + 1], a - b);
     }
 }
 
@@ -128,16 +133,20 @@ __global__ void k_twist_bitrev_scatter(NttBatch B, uint64_t n_in, int log_out, i
 // other slot of that aligned group of 2^e is zero, so the first e DIT stages
 // only copy the value across the group.  This writes the twisted input
 // a_i * zeta^(i mod 3) to all 2^e slots; the DIT passes then start at stage e.
+// Threads walk the OUTPUT groups in order (group r holds input bitrev(r)), so
+// a warp's stores form one contiguous run and only the 32-byte input loads
+// are scattered.
 __global__ void k_coset_spread(NttBatch B, int log_in, int e, Zeta3 z3)
 {
     const Fr* __restrict__ in = B.src[blockIdx.y];
     Fr* __restrict__ out = B.dst[blockIdx.y];
     uint64_t n_in = 1ull << log_in;
     const uint64_t g = 1ull << e;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_in;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n_in;
+         r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = bitrev(r, log_in);
         Fr v = ldg(&in[i]) * z3.f[i % 3];
-        Fr* dst = out + (bitrev(i, log_in) << e);
+        Fr* dst = out + (r << e);
         for (uint64_t j = 0; j < g; j++) st(&dst[j], v);
     }
 }
@@ -197,7 +206,7 @@ constexpr int NTT_THREADS = 512;
 // power of two, so all index arithmetic is shifts and masks on 32 bits
 // (n <= 2^31).
 template <bool DIT>
-__global__ void __launch_bounds__(NTT_THREADS, 3) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
+__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
                                                           int nst, int lS, int lG)
 {
     const Fr* src = B.src[blockIdx.y];  // the first pass of an out-of-place transform reads here
@@ -234,24 +243,10 @@ __global__ void __launch_bounds__(NTT_THREADS, 3) k_ntt_pass(NttBatch B, const F
     const uint32_t mmask = (1u << (nst - 1)) - 1;
     for (int t = 0; t < nst; t++) {
         const int s = s0 + t;
-        const int h = DIT ? t : nst - t - 1;
-        if (DIT ? s == 0 : s == logn - 1) {
-            // the first DIT stage and the last DIF stage use only w^0 = 1
-            for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
-                const uint32_t gl = u >> (nst - 1), m = u & mmask;
-                const uint32_t q = ((m >> h) << (h + 1)) | (m & ((1u << h) - 1));
-                Fr* px = &sm[(gl << nst) + q];
-                Fr* py = px + (1u << h);
-                const Fr x = *px, y = *py;
-                *px = x + y;
-                *py = x - y;
-            }
-            __syncthreads();
-            continue;
-        }
         for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
             const uint32_t gl = u >> (nst - 1), m = u & mmask;
             const uint32_t r = (g0 + gl) & Smask;
+            const int h = DIT ? t : nst - t - 1;
             const uint32_t lowm = m & ((1u << h) - 1);
             const uint32_t q = ((m >> h) << (h + 1)) | lowm;
             Fr* px = &sm[(gl << nst) + q];
@@ -432,8 +427,10 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
         }
         const uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
         if (!alias) {
-            k_twist_bitrev_scatter<<<grid(nthreads), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.cpow, z3);
-            H2B_LAUNCHED("k_twist_bitrev_scatter");
+            // the fused input stage also runs DIT stage 0
+            k_twist_bitrev_stage0<<<grid(nt / 2), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.cpow, z3);
+            H2B_LAUNCHED("k_twist_bitrev_stage0");
+            return run_passes(D, count, s.tw, logt, true, st, 1);
         } else {
             if (type == 3 && nt != nin) {
                 // zero the padding in place, then twist + reverse
