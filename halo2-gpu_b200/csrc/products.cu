@@ -191,6 +191,96 @@ static RustError batch_invert_levels(Fp<C>* d, uint64_t n, ScratchArena& ar, cud
     return ok();
 }
 
+// Group form of the Montgomery trick, for the scratch entry point.  Group t
+// of a level owns BI_E elements of the 1024-element tile t / 128, at stride
+// 128 (bi_index), so every step of a warp touches 32 consecutive elements and
+// a CTA stays inside one tile.  Up: the group product
+// (zero counts as one) goes to totals[t]; the totals are inverted by the same
+// scheme one level down; down: the group walks its elements backwards with
+// the inverted total, two products per element, after recomputing its
+// prefix products in registers.  No shared memory and no block-wide trees:
+// every level is a fully parallel pass of independent threads.
+constexpr int BI_GT = 128;                          // groups per tile
+__device__ __forceinline__ uint64_t bi_index(uint64_t t, int j)
+{
+    return (t / BI_GT) * (BI_GT * BI_E) + (uint64_t)j * BI_GT + (t % BI_GT);
+}
+
+template <class C>
+__global__ void __launch_bounds__(128) k_bi_up(const Fp<C>* __restrict__ d, uint64_t n, uint64_t nt,
+                                               Fp<C>* __restrict__ totals)
+{
+    using F = Fp<C>;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt; t += (uint64_t)gridDim.x * blockDim.x) {
+        F acc = F::one();
+#pragma unroll 1
+        for (int j = 0; j < BI_E; j++) {
+            const uint64_t i = bi_index(t, j);
+            if (i < n) {
+                const F x = ld(&d[i]);
+                if (!x.is_zero()) acc = acc * x;
+            }
+        }
+        st(&totals[t], acc);
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(128) k_bi_down(Fp<C>* __restrict__ d, uint64_t n, uint64_t nt,
+                                                 const Fp<C>* __restrict__ inv_totals)
+{
+    using F = Fp<C>;
+    __shared__ F pre[BI_E][128];                           // per thread: product of the nonzero elements before j
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt; t += (uint64_t)gridDim.x * blockDim.x) {
+        F acc = F::one();
+#pragma unroll 1
+        for (int j = 0; j < BI_E; j++) {
+            const uint64_t i = bi_index(t, j);
+            const F x = i < n ? ld(&d[i]) : F::zero();
+            pre[j][threadIdx.x] = acc;
+            if (!x.is_zero()) acc = acc * x;
+        }
+        F inv = ld(&inv_totals[t]);                        // (product of all nonzero elements)^-1
+#pragma unroll 1
+        for (int j = BI_E - 1; j >= 0; j--) {
+            const uint64_t i = bi_index(t, j);
+            if (i >= n) continue;
+            const F x = ld(&d[i]);                         // read again (still the input: i is written last)
+            if (x.is_zero()) continue;                     // zero stays zero
+            const F out = inv * pre[j][threadIdx.x];
+            inv = inv * x;
+            st(&d[i], out);
+        }
+    }
+}
+
+static uint64_t groups_of(uint64_t n) { return (n + BI_GT * BI_E - 1) / (BI_GT * BI_E) * BI_GT; }
+
+static void plan_batch_invert_groups(ScratchPlan& p, uint64_t n)
+{
+    while (n > BI_TILE) {
+        n = groups_of(n);
+        p.add(n * 32);
+    }
+}
+
+template <class C>
+static RustError batch_invert_groups(Fp<C>* d, uint64_t n, ScratchArena& ar, cudaStream_t st, bool top = true)
+{
+    if (n <= BI_TILE) return batch_invert_local<C>(d, n, st);
+    const uint64_t nt = groups_of(n);
+    Fp<C>* tot = ar.take_n<Fp<C>>(nt);
+    if (!ar.good()) return err(cudaErrorInvalidValue, "batch_invert: scratch too small");
+    k_bi_up<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot);
+    H2B_LAUNCHED("k_bi_up");
+    H2B_TRY(batch_invert_groups<C>(tot, nt, ar, st, false));
+    if (top) prof_begin(PROF_BATCH_INVERT, st);
+    k_bi_down<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot);
+    if (top) prof_end(PROF_BATCH_INVERT, st);
+    H2B_LAUNCHED("k_bi_down");
+    return ok();
+}
+
 // In-place Fq batch inversion for other kernels of this library (the MSM's
 // pairing rounds): zeros stay zero; scratch from fq_batch_invert_scratch().
 uint64_t fq_batch_invert_scratch(uint64_t n)
@@ -430,7 +520,7 @@ extern "C" RustError _halo2_batch_invert(void* d_data, uint32_t field_type, uint
 extern "C" uint64_t h2b_batch_invert_workspace_size(uint64_t length)
 {
     ScratchPlan p;
-    plan_batch_invert(p, length);
+    plan_batch_invert_groups(p, length);
     return p.used;
 }
 
@@ -442,8 +532,8 @@ extern "C" RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_
     uint64_t need = h2b_batch_invert_workspace_size(length);
     if (scratch_bytes < need) return scratch_too_small("h2b_batch_invert", scratch_bytes, need);
     ScratchArena ar(scratch, scratch_bytes);
-    if (field_type == 0) return batch_invert_levels<FrCfg>((Fr*)d_data, length, ar, stream);
-    return batch_invert_levels<FqCfg>((Fq*)d_data, length, ar, stream);
+    if (field_type == 0) return batch_invert_groups<FrCfg>((Fr*)d_data, length, ar, stream);
+    return batch_invert_groups<FqCfg>((Fq*)d_data, length, ar, stream);
 }
 
 // grand product ---------------------------------------------------------------
@@ -681,7 +771,9 @@ extern "C" RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type,
     if (length == 0) return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length must be >= 1");
     if (length > NOALLOC_MAX_LENGTH)
         return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length exceeds the 2^26-element maximum");
-    uint64_t need = h2b_batch_invert_workspace_size(length);
+    ScratchPlan plan;                                  // the tile levels (small totals arrays)
+    plan_batch_invert(plan, length);
+    const uint64_t need = plan.used;
     if (need > NOALLOC_SCRATCH_BYTES)
         return err(cudaErrorInvalidValue, "h2b_batch_invert_noalloc: length needs more than the fixed scratch");
     int dev = 0;
