@@ -17,7 +17,8 @@ order:
      quotient (evaluate_h), the permutation and the lookup quotients;
   7. h: the parts gathered and brought to coefficients on the extended
      coset, and its 3 pieces committed;
-  8. opening: evaluations at x, Kate divisions, 2 commits.
+  8. opening: SHPLONK over the committed polynomials at x and their
+     rotations (shplonk.py), 2 commits.
 
 Challenges come from a seeded generator, not a transcript, and the witness
 does not satisfy the circuit, so the outputs are deterministic GPU work, not
@@ -37,6 +38,7 @@ import numpy as np
 
 from . import fields as F
 from . import rules as R
+from . import shplonk
 
 _torch = None
 
@@ -90,6 +92,23 @@ class Resident:
             pk["table_col"] = tab_col
             self.pk[k] = pk
         return self.pk[k]
+
+    def keygen(self, k, stream=None):
+        """Verifying-key commitments of the 2^k key (keygen_vk's GPU part,
+        halo2_proofs/src/plonk/keygen.rs:265-290): the 3 fixed and 4
+        permutation polynomials, committed in one MSM batch over the resident
+        SRS table (coefficient form with monomial bases: the same points as
+        the Lagrange form with Lagrange bases).  Returns 96-byte device images."""
+        torch, h2b = _t(), self.h2b
+        pk, n, tn = self.key(k), 1 << k, 1 << self.kmax
+        polys = pk["fixed"] + pk["sigma"]
+        st = stream if stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(st):
+            outs = [h2b.dev_empty(96) for _ in polys]
+            jobs = h2b.msm_batch_jobs(polys, [self.table] * len(polys), outs, [n] * len(polys), table_n=tn)
+            ws = h2b.msm_batch_workspace(jobs, len(polys), len(polys))
+            h2b.msm_batch(jobs, len(polys), len(polys), ws, stream=st)
+        return outs
 
 
 def _slice(t, i, n):
@@ -218,29 +237,33 @@ class ProofWorkload:
             for i in range(dom.quotient_poly_degree):
                 commit(_slice(hc, i, n))
             flush()
-            # 8. opening: evaluations at x of every polynomial, two Kate divisions
-            #    (an advice column and the first h piece) and their commitments
-            x = sc(chal())
-            ews = [h2b.dev_empty(h2b.lib()._halo2_eval_polynomial_workspace_size(n)) for _ in range(len(allc) + 1)]
-            for p, ws in zip(allc + [_slice(hc, 0, n)], ews):
-                evals.append(_eval(h2b, p, x, n, ws, stream))
-            d_x = h2b.to_dev(x)
-            for p in (coef[0], _slice(hc, 0, n)):
-                q = h2b.dev_empty(32 * n)
-                h2b.kate_division_device(p, q, d_x, n, stream=stream)
-                commit(q, n - 1)
-            flush()
+            # 8. opening (SHPLONK): the committed polynomials at x and their
+            #    rotations -- advice 0 at x, x w^-1; advice 3 (Fibonacci) at x, x w,
+            #    x w^2; the permutation products at x, x w, x w^last; the lookup
+            #    product at x, x w; A' at x, x w^-1; the rest at x
+            x = chal()
+            w = dom.omega
+            at = lambda r: x * pow(w, r % n, F.R_MOD) % F.R_MOD  # noqa: E731
+            rots = {0: (0, -1), 3: (0, 1, 2), 5: (0, 1, -3), 6: (0, 1, -3), 7: (0, 1), 8: (0, -1)}
+            queries = []
+            for idx in (0, 1, 2, 3, 5, 6, 7, 8, 9):
+                queries += [(coef[idx], at(r)) for r in rots.get(idx, (0,))]
+            queries += [(c, at(0)) for c in pk["fixed"] + pk["sigma"]]
+            queries += [(_slice(hc, i, n), at(0)) for i in range(dom.quotient_poly_degree)]
+            cws = h2b.dev_empty(h2b.lib().h2b_msm_table_workspace_size(n, tn))
+
+            def commit_now(d):
+                out = h2b.dev_empty(96)
+                h2b.msm_device_table(d, res.table, tn, out, n, ws=cws, stream=stream)
+                commits.append(out)
+                return out
+
+            opened, _, l_at_u = shplonk.open_queries(h2b, queries, iter([chal(), chal(), chal()]), commit_now,
+                                                     stream=stream)
+            if l_at_u != 0:
+                raise RuntimeError("SHPLONK linearisation does not vanish at u")
+            evals.append(torch.from_numpy(np.ascontiguousarray(F.fr_mont_limbs(opened)).view(np.uint8).reshape(-1)))
         return commits, evals
-
-
-def _eval(h2b, d_poly, x, n, ws, stream):
-    """Horner evaluation left on the device: a 32-byte view into `ws`."""
-    import ctypes
-    res = ctypes.c_void_p()
-    h2b.call("_halo2_eval_polynomial", h2b.ptr(d_poly), ctypes.byref(h2b.host_ffi(x)), ctypes.byref(res), n,
-             h2b.ptr(ws), ws.numel(), h2b.stream_handle(stream))
-    off = res.value - ws.data_ptr()
-    return ws[off: off + 32]
 
 
 def requests(count, rate, seed, ks=(16, 18, 20, 22), weights=(0.4, 0.3, 0.2, 0.1)):

@@ -1,0 +1,167 @@
+"""SHPLONK multi-point opening on the device (the flow of
+halo2_proofs/src/poly/kzg/multiopen/shplonk/prover.rs:97-466, over this
+library's entry points).
+
+Queries are (device polynomial in coefficient form, length n; point).
+Polynomials queried at the same SET of points form a rotation set.  With
+challenges y, v, u (from a seeded generator here, not a transcript):
+
+  q_i(X) = sum_j y^j (p_ij(X) - r_ij(X)) / Z_{S_i}(X)   r_ij interpolates p_ij on S_i
+  h(X)   = sum_i v^i q_i(X)                             -> commitment W
+  L(X)   = sum_i v^i Z_{T \\ S_i}(u) sum_j y^j (p_ij(X) - r_ij(u)) - Z_T(u) h(X)
+  h'(X)  = L(X) / (X - u)                               -> commitment W'
+
+with T the union of all points.  L(u) = 0 whenever every evaluation is
+right, so the division is exact; `open_queries` returns it for checking.
+Device
+work: Horner evaluations (_halo2_eval_polynomial), linear combinations
+(_halo2_poly_multiply_add), the interpolant subtraction
+(_halo2_poly_sub_short_inplace, _halo2_poly_sub_scalar_at_zero), divisions by
+(X - s) (_halo2_kate_division_device_padded) and the two MSMs (the caller's
+`commit`).  Host work: the interpolants (at most a few points per set) and
+the scalar bookkeeping.
+"""
+import ctypes
+
+from . import fields as F
+
+P = F.R_MOD
+
+
+def _interpolate(points, values):
+    """Coefficients (low first) of the polynomial of degree < len(points)
+    through (points[k], values[k]), by Lagrange's formula mod r."""
+    m = len(points)
+    coeffs = [0] * m
+    for k in range(m):
+        basis = [1]                     # prod_{l != k} (X - x_l)
+        denom = 1
+        for l_ in range(m):
+            if l_ == k:
+                continue
+            basis = [(a - points[l_] * b) % P for a, b in zip([0] + basis, basis + [0])]
+            denom = denom * (points[k] - points[l_]) % P
+        scale = values[k] * pow(denom, -1, P) % P
+        for i in range(m):
+            coeffs[i] = (coeffs[i] + scale * basis[i]) % P
+    return coeffs
+
+
+def _eval_host(coeffs, x):
+    acc = 0
+    for c in reversed(coeffs):
+        acc = (acc * x + c) % P
+    return acc
+
+
+def _vanishing_at(points, u):
+    acc = 1
+    for s in points:
+        acc = acc * (u - s) % P
+    return acc
+
+
+class Shplonk:
+    """Device scratch and helpers for one opening of polynomials of length n."""
+
+    def __init__(self, h2b, n, stream=None):
+        self.h2b, self.n, self.stream = h2b, n, stream
+        self.sh = h2b.stream_handle(stream)
+        self.ews = h2b.dev_empty(h2b.lib()._halo2_eval_polynomial_workspace_size(n))
+        self.kws = h2b.dev_empty(h2b.lib()._halo2_kate_division_workspace_size(n))
+
+    def _scalar(self, v):
+        return self.h2b.to_dev(F.fr_mont_limbs([v % P]))
+
+    def eval(self, d_poly, x):
+        """p(x) as an int (synchronises the stream)."""
+        h2b = self.h2b
+        pt = F.fr_mont_limbs([x % P])
+        res = ctypes.c_void_p()
+        h2b.call("_halo2_eval_polynomial", h2b.ptr(d_poly), ctypes.byref(h2b.host_ffi(pt)), ctypes.byref(res),
+                 self.n, h2b.ptr(self.ews), self.ews.numel(), self.sh)
+        off = res.value - self.ews.data_ptr()
+        return F.fr_from_mont_limbs(h2b.to_host(self.ews[off:off + 32]))[0]
+
+    def madd(self, d_acc, d_in, c):
+        """acc += c * in over n coefficients."""
+        self.h2b.call("_halo2_poly_multiply_add", self.h2b.ptr(d_acc), self.h2b.ptr(d_in),
+                      self.h2b.ptr(self._scalar(c)), self.n, self.sh)
+
+    def sub_short(self, d_acc, coeffs):
+        d = self.h2b.to_dev(F.fr_mont_limbs([c % P for c in coeffs]))
+        self.h2b.call("_halo2_poly_sub_short_inplace", self.h2b.ptr(d_acc), self.h2b.ptr(d), len(coeffs), self.sh)
+
+    def div_linear(self, d_a, d_q, s):
+        """q = (a - a(s)) / (X - s), written with zeros up to n."""
+        self.h2b.call("_halo2_kate_division_device_padded", self.h2b.ptr(d_a), self.h2b.ptr(d_q),
+                      self.h2b.ptr(self._scalar(s)), self.n, self.n, self.h2b.ptr(self.kws), self.kws.numel(),
+                      self.sh)
+
+    def zeros(self):
+        t = self.h2b.dev_empty(32 * self.n)
+        t.zero_()
+        return t
+
+
+def open_queries(h2b, queries, challenges, commit, stream=None):
+    """SHPLONK opening of `queries` = [(device poly, point)] (all of length n).
+    `challenges` yields three ints (y, v, u); `commit(d_poly)` returns the
+    96-byte device commitment of a length-n polynomial.  Returns
+    (evaluations in query order, [W, W'], L(u)) with L(u) == 0 for a sound
+    opening."""
+    n = queries[0][0].numel() // 32
+    sp = Shplonk(h2b, n, stream)
+    # evaluations, and the point set of every polynomial (by identity)
+    evals, point_sets, polys = [], {}, {}
+    for d, x in queries:
+        e = sp.eval(d, x)
+        evals.append(e)
+        key = d.data_ptr()
+        polys[key] = d
+        point_sets.setdefault(key, {})[x % P] = e
+    # rotation sets: polynomials with the same point set, in first-query order
+    sets = {}
+    for key, pe in point_sets.items():
+        sets.setdefault(tuple(sorted(pe)), []).append(key)
+    y, v, u = (next(challenges) % P for _ in range(3))
+    super_points = sorted({x for s in sets for x in s})
+    # h = sum_i v^i (sum_j y^j (p_ij - r_ij)) / Z_{S_i}
+    h = sp.zeros()
+    bufs = [sp.zeros(), sp.zeros()]
+    lin_terms = []
+    for i, (pts, keys) in enumerate(sets.items()):
+        num = bufs[0]
+        num.zero_()
+        short = [0] * len(pts)
+        r_at_u = 0
+        for j, key in enumerate(keys):
+            yj = pow(y, j, P)
+            sp.madd(num, polys[key], yj)
+            r = _interpolate(list(pts), [point_sets[key][x] for x in pts])
+            short = [(a + yj * b) % P for a, b in zip(short, r)]
+            r_at_u = (r_at_u + yj * _eval_host(r, u)) % P
+        sp.sub_short(num, short)
+        cur, other = bufs
+        for pt in pts:                   # divide by (X - s) for every point of the set
+            sp.div_linear(cur, other, pt)
+            cur, other = other, cur
+        vi = pow(v, i, P)
+        sp.madd(h, cur, vi)
+        diff = [x for x in super_points if x not in pts]
+        lin_terms.append((keys, vi * _vanishing_at(diff, u) % P, r_at_u))
+    w = commit(h)
+    # L = sum_i v^i Z_{T\S_i}(u) sum_j y^j (p_ij - r_ij(u)) - Z_T(u) h
+    lx = sp.zeros()
+    const = 0
+    for keys, c_i, r_at_u in lin_terms:
+        for j, key in enumerate(keys):
+            sp.madd(lx, polys[key], c_i * pow(y, j, P))
+        const = (const + c_i * r_at_u) % P
+    h2b.call("_halo2_poly_sub_scalar_at_zero", h2b.ptr(lx), h2b.ptr(sp._scalar(const)), sp.sh)
+    sp.madd(lx, h, -_vanishing_at(super_points, u))
+    l_at_u = sp.eval(lx, u)
+    q = sp.zeros()
+    sp.div_linear(lx, q, u)
+    w2 = commit(q)
+    return evals, [w, w2], l_at_u

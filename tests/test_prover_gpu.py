@@ -62,9 +62,10 @@ def test_served_outputs_match_alone(h2b):
         tight = tight_srv.serve(reqs, keep_outputs=True)["outputs"]
     for a, m in zip(alone, tight):
         assert a == _bytes(m)
-    # each request's outputs: 4 advice + A' + S' + 2 z + lookup z + 3 h pieces + 2 Kate quotients
+    # each request's outputs: 4 advice + A' + S' + 2 z + lookup z + 3 h pieces + the 2 SHPLONK
+    # commitments, and the 28 opened evaluations
     c, e = alone[0]
-    assert len(c) == 96 * 14 and len(e) == 32 * 22
+    assert len(c) == 96 * 14 and len(e) == 32 * 28
     # the first commitment is the advice column's MSM over the plain SRS
     n = 1 << 12
     adv0 = h2b.random_fr_device(n, 11 * 64, 1)
@@ -82,3 +83,20 @@ def test_server_rejects_oversize(h2b):
     res = P.Resident(h2b, 10)
     with P.Server(res, 2, 1 << 20) as srv, pytest.raises(ValueError):
         srv.serve([(0.0, 10, 1)])
+
+
+@pytest.mark.gpu
+def test_keygen_commitments(h2b):
+    """The verifying-key commitments equal the plain MSM of each key polynomial."""
+    import torch
+    P = _prover(h2b)
+    res = P.Resident(h2b, 11)
+    k, n = 10, 1 << 10
+    vk = res.keygen(k)
+    torch.cuda.synchronize()
+    pk = res.key(k)
+    for poly, got in zip(pk["fixed"] + pk["sigma"], vk):
+        out = h2b.dev_empty(96)
+        h2b.msm_device(poly, res.srs, out, n, h2b.msm_workspace(n))
+        torch.cuda.synchronize()
+        assert out.cpu().numpy().tobytes() == got.cpu().numpy().tobytes()
