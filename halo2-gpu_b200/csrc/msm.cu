@@ -172,7 +172,7 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
         sp.add_n<Fq>(ctas);                           // CTA totals
         sp.add(fq_batch_invert_scratch(ctas));
     }
-    if (p.tn == 0 && p.R == 0) sp.add_n<G1Affine>(p.n);  // bases in the lazy form (x 2^261)
+    if (p.tn == 0 && p.R == 0) sp.add_n<G1Affine>(2 * p.n);  // P_i and phi(P_i) in the lazy form (x 2^261)
 }
 
 MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host)
@@ -210,7 +210,7 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
         s.pr_inv_bytes = fq_batch_invert_scratch(ctas);
         s.pr_inv_scratch = ar.take(s.pr_inv_bytes);
     }
-    s.rbases = (p.tn == 0 && p.R == 0) ? ar.take_n<G1Affine>(p.n) : nullptr;
+    s.rbases = (p.tn == 0 && p.R == 0) ? ar.take_n<G1Affine>(2 * p.n) : nullptr;
     return s;
 }
 
@@ -222,10 +222,13 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
 // (128-bit magnitudes, sign in bit 127), so entry v stands for point i = v/2,
 // taken as P_i (v even) or phi(P_i) (v odd).
 // GLV split of each scalar; with `rb` set, base i is also converted to the
-// lazy x 2^261 form the accumulation reads (same index space, one launch).
+// lazy x 2^261 form the accumulation reads (same index space, one launch):
+// rb[i] = P_i and rb[n + i] = phi(P_i) = (beta x, y), so the accumulation
+// multiplies by beta nowhere.
 __global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t lo, uint64_t hi,
-                          const G1Affine* __restrict__ bases, G1Affine* __restrict__ rb)
+                          const G1Affine* __restrict__ bases, G1Affine* __restrict__ rb, uint64_t n)
 {
+    const Fq beta = glv::beta();
     for (uint64_t i = lo + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < hi;
          i += (uint64_t)gridDim.x * blockDim.x) {
         uint4 a, b;
@@ -234,8 +237,11 @@ __global__ void k_msm_glv(const Fr* __restrict__ sc, uint4* __restrict__ vs, uin
         vs[2 * i + 1] = b;
         if (rb) {
             const G1Affine q = ld_affine(&bases[i]);
+            const Fq y = to_r261(q.y);
             st(&rb[i].x, to_r261(q.x));
-            st(&rb[i].y, to_r261(q.y));
+            st(&rb[i].y, y);
+            st(&rb[n + i].x, to_r261(q.x * beta));     // infinity (0, 0) stays (0, 0)
+            st(&rb[n + i].y, y);
         }
     }
 }
@@ -342,13 +348,18 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : (MODE >= 3 ? MODE + 1 : 3
 
 // Bases (affine, memory image x 2^256 mod p) -> canonical x 2^261 mod p, the
 // form the lazy accumulation reads; infinity (0, 0) stays (0, 0).
-__global__ void k_to_r261(const G1Affine* in, G1Affine* out, uint64_t n)  // in may equal out
+__global__ void k_to_r261(const G1Affine* in, G1Affine* out, uint64_t n, G1Affine* phi)  // in may equal out
 {
+    const Fq beta = glv::beta();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const G1Affine a = ld_affine(&in[i]);
         G1Affine r;
         r.x = to_r261(a.x);
         r.y = to_r261(a.y);
+        if (phi) {
+            st(&phi[i].x, to_r261(a.x * beta));   // phi(P) = (beta x, y); infinity stays (0, 0)
+            st(&phi[i].y, r.y);
+        }
         st(&out[i].x, r.x);
         st(&out[i].y, r.y);
     }
@@ -359,15 +370,16 @@ __global__ void k_to_r261(const G1Affine* in, G1Affine* out, uint64_t n)  // in 
 // x 2^261 form.  The accumulator's additions and subtractions are one-step
 // carry passes with no conditional correction; results are converted back
 // to the canonical memory image when a bucket or chunk head is stored.
+// phi(P) of the point at bases[j] is stored at bases[phi_off + j] (plain
+// bases: phi_off = n; window tables: W n, after all slices).
 __global__ void __launch_bounds__(128, 3) k_msm_accumulate_z(const uint32_t* __restrict__ sorted,
                                                              const uint32_t* __restrict__ offsets, uint64_t NB,
                                                              uint32_t K, const G1Affine* __restrict__ bases,
-                                                             G1Xyzz* __restrict__ buckets,
+                                                             uint64_t phi_off, G1Xyzz* __restrict__ buckets,
                                                              G1Xyzz* __restrict__ heads)
 {
     const FqZ one = fz_from_words(to_r261(Fq::one()));           // 1 in the lazy form (2^261 mod p)
     const FqZ r256 = fz_from_words(Fq::one());                    // 2^256 mod p, for the stores
-    const FqZ beta = fz_from_words(to_r261(glv::beta()));         // phi(x, y) = (beta x, y)
     const uint32_t M = offsets[NB];
     const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
@@ -392,12 +404,13 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_z(const uint32_t* __r
             }
             const uint32_t ent = sorted[e];
             const uint32_t v = ent & ~SIGN_BIT;
-            const G1Affine P = ld_affine(&bases[v >> 1]);
+            const bool phi = (v & 1u) != 0;
+            const G1Affine P = ld_affine(&bases[(v >> 1) + (phi ? phi_off : 0)]);    // phi(P) precomputed
             if (is_inf(P)) continue;
             FqZ qx = fz_from_words(P.x);                                   // < p
             FqZ qy = fz_from_words(P.y);                                   // < p
             if (ent & SIGN_BIT) qy = fz_sub<FqCfg, 2>(fz_zero<FqCfg>(), qy);  // 2p - y < 2p
-            if (v & 1u) qx = fz_mul_call(qx, beta);                        // < 1.006p
+
             xyzzz_madd(acc, qx, qy, one);
         }
         st_xyzzz(head ? &heads[t] : &buckets[b], acc, r256);
@@ -800,7 +813,7 @@ static RustError msm_split(const MsmPlan& p, const MsmScratch& s, const Fr* d_sc
     const unsigned sm_cap = 148u * 16u;
     uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
     k_msm_glv<<<grid_for(hi - lo, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, lo, hi, d_bases,
-                                                              msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr);
+                                                              msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr, p.n);
     H2B_LAUNCHED("k_msm_glv");
     k_msm_sort<false><<<grid_for(2 * (hi - lo), 256, sm_cap), 256, 0, st>>>(vsc, 2 * lo, 2 * hi, p.c, p.W, p.H,
                                                                               s.counts, nullptr, p.tn);
@@ -853,7 +866,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
         k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (lazy)
         k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
-                                                     s.buckets, s.heads);
+                                                     p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
     else if (g_msm_acc_variant == 5)
         k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 1)
@@ -1073,10 +1086,11 @@ static bool table_fits(uint64_t tn)
 
 } // namespace h2b
 
+// W window slices of n points, then the same W slices under phi (x -> beta x).
 extern "C" uint64_t h2b_msm_table_points(uint64_t n)
 {
     if (!table_fits(n)) return 0;
-    return (uint64_t)msm_plan(n).W * n;
+    return 2 * (uint64_t)msm_plan(n).W * n;
 }
 
 extern "C" uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n)
@@ -1112,8 +1126,10 @@ extern "C" RustError h2b_msm_table_precompute(const void* d_bases, uint64_t n, v
         k_table_affine<<<grid_for(n, 256), 256, 0, stream>>>(tmp, den, n, table + (uint64_t)w * n);
         H2B_LAUNCHED("k_table_affine");
     }
-    // the accumulation reads the table in the lazy x 2^261 form
-    k_to_r261<<<grid_for((uint64_t)p.W * n, 256, 148u * 8u), 256, 0, stream>>>(table, table, (uint64_t)p.W * n);
+    // the accumulation reads the table in the lazy x 2^261 form, with the
+    // phi images of all slices after them
+    const uint64_t pts = (uint64_t)p.W * n;
+    k_to_r261<<<grid_for(pts, 256, 148u * 8u), 256, 0, stream>>>(table, table, pts, table + pts);
     H2B_LAUNCHED("k_to_r261");
     return ok();
 }

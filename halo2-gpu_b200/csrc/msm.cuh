@@ -47,7 +47,7 @@ struct MsmScratch {
     G1Xyzz* bits;
     G1Xyzz* wins;
     G1Jac* result;
-    G1Affine* rbases;    // plain bases converted to the lazy x 2^261 form (no pairing rounds)
+    G1Affine* rbases;    // plain bases P_i, then phi(P_i), in the lazy x 2^261 form (no pairing rounds)
     G1Affine* pts[2];    // pairing-round outputs (ping-pong)
     uint32_t* roff[3];   // per-round bucket offsets (NB + 1 each)
     Fq* pr_pref;         // pairing rounds: per-job denominator prefixes

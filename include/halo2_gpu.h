@@ -365,7 +365,7 @@ void h2b_msm_set_pair_rounds(int rounds);
 /* Precomputed window tables (no counterpart in the reference): an SRS kept resident with its window
  * multiples [2^(c w)] P_i, so an MSM over it reduces one bucket set and has no final doubling chain.
  * The table is opaque to callers: its points are stored as x * 2^261 mod p images, the form the
- * accumulation kernel reads.
+ * accumulation kernel reads, with the endomorphism images (beta x, y) of all slices after them.
  * h2b_msm_table_points: affine points in the table for n bases (0 if n is out of range). */
 uint64_t h2b_msm_table_points(uint64_t n);
 uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n);

@@ -27,7 +27,7 @@ def test_table_entries(h2b, table4k):
     srs, _, table = table4k
     tn = 1 << 12
     pts = h2b.lib().h2b_msm_table_points(tn)
-    W = pts // tn
+    W = pts // (2 * tn)                          # W slices, then their phi images
     t = h2b.to_host(table, (pts, 8))
     # the 2^12-point plan uses 10-bit windows: 13 of them cover the 127-bit GLV halves plus the digit carry
     c = 10
@@ -39,13 +39,18 @@ def test_table_entries(h2b, table4k):
         for w in (0, 1, W - 1):
             got = t[w * tn + i]
             if i == 5:
-                assert not got.any(), "infinity stays (0, 0)"
+                assert not got.any() and not t[W * tn + w * tn + i].any(), "infinity stays (0, 0)"
                 continue
             want = f.g1_mul(P, 1 << (c * w))
             # stored as x * 2^261 mod p, the form the accumulation reads
             r261 = pow(2, 261, f.Q_MOD)
             assert f.limbs_to_ints(got[:4].reshape(1, 4))[0] == want[0] * r261 % f.Q_MOD
             assert f.limbs_to_ints(got[4:].reshape(1, 4))[0] == want[1] * r261 % f.Q_MOD
+            # phi image W tn points later: (beta x, y), beta a cube root of unity mod p
+            ph = t[W * tn + w * tn + i]
+            px = f.limbs_to_ints(ph[:4].reshape(1, 4))[0] * pow(r261, -1, f.Q_MOD) % f.Q_MOD
+            assert px != want[0] and pow(px * pow(want[0], -1, f.Q_MOD) % f.Q_MOD, 3, f.Q_MOD) == 1
+            assert f.limbs_to_ints(ph[4:].reshape(1, 4))[0] == want[1] * r261 % f.Q_MOD
 
 
 @pytest.mark.parametrize("n", [1, 2, 100, 3000, 4096])
