@@ -146,6 +146,7 @@ _SIGS = {
     "h2b_msm_set_pair_rounds": (None, [ctypes.c_int]),
     "h2b_exec_fork": (RustError, [_vp, _u32, ctypes.POINTER(ctypes.c_void_p)]),
     "h2b_exec_join": (RustError, [_vp, _u32]),
+    "h2b_upload": (RustError, [_vp, _vp, _u64, _vp]),
     "h2b_graph_begin": (RustError, [_vp]),
     "h2b_graph_end": (RustError, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "h2b_graph_launch": (RustError, [_vp, _vp]),
@@ -252,12 +253,22 @@ def dev_empty(nbytes):
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
 
 
-def to_dev(arr):
-    """numpy (any dtype) -> torch uint8 device tensor with the same bytes."""
+def to_dev(arr, stream=None):
+    """numpy (any dtype) -> torch uint8 device tensor with the same bytes.
+    With a `stream`, the copy is queued there (h2b_upload) without waiting for
+    the work already queued on it, and is ordered only with that stream's
+    later work.  Without one, it runs on the current stream and is complete
+    when this returns (usable from any stream)."""
     torch = _torch()
     a = np.ascontiguousarray(arr)
-    t = torch.from_numpy(a.view(np.uint8).reshape(-1))
-    return t.to("cuda")
+    nbytes = a.nbytes
+    t = torch.empty(max(nbytes, 1), dtype=torch.uint8, device="cuda")
+    if nbytes:
+        call("h2b_upload", ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(a.ctypes.data), nbytes,
+             stream_handle(stream))
+        if stream is None:
+            torch.cuda.current_stream().synchronize()
+    return t[:nbytes] if nbytes else t[:0]
 
 
 def to_host(t, shape=None):
@@ -430,7 +441,7 @@ def fft_normal(ntt_type, log_n, values, omega, divisor, stream=None):
 
 
 def fft_normal_to_device(ntt_type, log_n, d_in, d_out, omega, divisor, ws=None, stream=None):
-    d_om = to_dev(_scalar_bytes(omega))
+    d_om = to_dev(_scalar_bytes(omega), stream)
     dv = _scalar_bytes(divisor)
     need = lib()._halo2_fft_normal_to_device_workspace_size(ntt_type, log_n, log_n)
     if ws is None or ws.numel() < need:
@@ -528,7 +539,7 @@ def power_of_omega_gpu(omega, log_n, pow_, stream=None):
 def generate_omega_powers_gpu(omega, log_n, output_num=None, stream=None):
     """generate_omega_powers_gpu (omega.rs:51-103): first output_num of omega^i, i < 2^log_n, to host."""
     torch = _torch()
-    d_om = to_dev(_scalar_bytes(omega))
+    d_om = to_dev(_scalar_bytes(omega), stream)
     d_out = dev_empty(32 << log_n)
     ws = dev_empty(lib()._halo2_generate_omega_powers_workspace_size(log_n))
     call("_halo2_generate_omega_powers", ptr(d_out), ptr(d_om), log_n, ptr(ws), ws.numel(), stream_handle(stream))
@@ -561,7 +572,7 @@ def fft_many(ntt_type, log_n, extend_log_n, polys, omega, divisor, stream=None):
     ins = [np.ascontiguousarray(p, dtype=np.uint64) for p in polys]
     la = extend_log_n if ntt_type in (NTT_COSET, NTT_ICOSET) else log_n
     outs = [np.zeros((1 << la, 4), dtype=np.uint64) for _ in polys]
-    d_om = to_dev(_scalar_bytes(omega))
+    d_om = to_dev(_scalar_bytes(omega), stream)
     dv = _scalar_bytes(divisor)
     dvo = host_ffi(dv)
     ws = dev_empty(lib()._halo2_fft_many_workspace_size(ntt_type, log_n, extend_log_n))
@@ -573,7 +584,7 @@ def fft_many(ntt_type, log_n, extend_log_n, polys, omega, divisor, stream=None):
 
 def fft_many_to_device(ntt_type, log_n, extend_log_n, d_ins, d_outs, omega, divisor, input_on_device=True,
                        ws=None, stream=None):
-    d_om = to_dev(_scalar_bytes(omega))
+    d_om = to_dev(_scalar_bytes(omega), stream)
     dv = _scalar_bytes(divisor)
     dvo = host_ffi(dv)
     need = lib()._halo2_fft_many_to_device_workspace_size(ntt_type, log_n, extend_log_n)
@@ -623,7 +634,7 @@ def lookup_product(permuted_input, permuted_table, compressed_input, compressed_
             (permuted_input, permuted_table, compressed_input, compressed_table)]
     length = arrs[0].shape[0] - offset if length is None else length
     out = np.zeros_like(arrs[0])
-    d_b, d_g = to_dev(_scalar_bytes(beta)), to_dev(_scalar_bytes(gamma))
+    d_b, d_g = to_dev(_scalar_bytes(beta), stream), to_dev(_scalar_bytes(gamma), stream)
     ws = dev_empty(lib()._halo2_commit_product_workspace_size(length))
     objs = [host_ffi(out)] + [host_ffi(a) for a in arrs]
     call("_halo2_commit_product", *[ctypes.byref(o) for o in objs], ptr(d_b), ptr(d_g), length, offset, ptr(ws),
@@ -644,7 +655,7 @@ def permutation_product(modified_values, permutations, values, beta, gamma, delt
     perms = [np.ascontiguousarray(p, dtype=np.uint64) for p in permutations]
     vals = [np.ascontiguousarray(v, dtype=np.uint64) for v in values]
     length = mv.shape[0] if length is None else length
-    d_sc = [to_dev(_scalar_bytes(x)) for x in (beta, gamma, delta, omega, deltaomega)]
+    d_sc = [to_dev(_scalar_bytes(x), stream) for x in (beta, gamma, delta, omega, deltaomega)]
     ws = dev_empty(lib()._halo2_permutation_product_workspace_size(length))
     m = host_ffi(mv)
     call("_halo2_permutation_product", ctypes.byref(m), ffi_array([p.ctypes.data for p in perms]),
@@ -677,14 +688,14 @@ def random_fr_device(n, seed, mix=0, stream=None):
 
 def powers_device(x, n, stream=None):
     d = dev_empty(32 * n)
-    call("h2b_powers", ptr(d), n, ptr(to_dev(_scalar_bytes(x))), stream_handle(stream))
+    call("h2b_powers", ptr(d), n, ptr(to_dev(_scalar_bytes(x), stream)), stream_handle(stream))
     return d
 
 
 def srs_device(tau, n, stream=None):
     """[tau^i] G, i < n, as a device tensor of n affine points (64 bytes each)."""
     pw = powers_device(tau, n, stream)
-    table = to_dev(fields.g1_pow2_table(256))
+    table = to_dev(fields.g1_pow2_table(256), stream)
     out = dev_empty(64 * n)
     call("h2b_srs_from_powers", ptr(out), ptr(pw), n, ptr(table), stream_handle(stream))
     return out
@@ -758,10 +769,22 @@ def quotient_lookups_device(d_values, d_table, d_z, d_pin, d_ptab, d_l0, d_llast
 def quotient_permutation_device(d_values, d_l0, d_llast, d_lactive, d_prods, d_perms, d_cols, beta, gamma, y, delta,
                                 delta_start, ext_omega, omega, chunk_len, last_rotation, rot_scale, isize, n,
                                 stream=None):
-    tabs = [to_dev(np.array([t.data_ptr() for t in lst], dtype=np.uint64)) for lst in (d_prods, d_perms, d_cols)]
+    tabs = [to_dev(np.array([t.data_ptr() for t in lst], dtype=np.uint64), stream) for lst in (d_prods, d_perms, d_cols)]
     scal = [_scalar_bytes(x) for x in (beta, gamma, y, delta, delta_start, ext_omega, omega)]
     call("_halo2_quotient_permutation", ptr(d_values), ptr(d_l0), ptr(d_llast), ptr(d_lactive), ptr(tabs[0]),
          ptr(tabs[1]), ptr(tabs[2]), *[s.ctypes.data for s in scal], len(d_prods), chunk_len, len(d_cols),
          last_rotation, rot_scale, isize, n, stream_handle(stream))
+    _keep_until_done(tabs, stream)
+
+
+def _keep_until_done(tensors, stream):
+    """Device tensors that a kernel queued on `stream` reads must not be
+    reused before it ran: for a torch stream the caching allocator is told so
+    (record_stream); for a raw handle the call waits for the stream."""
     torch = _torch()
-    torch.cuda.current_stream().synchronize()
+    if stream is None or isinstance(stream, torch.cuda.Stream):
+        s = stream if stream is not None else torch.cuda.current_stream()
+        for t in tensors:
+            t.record_stream(s)
+    else:
+        torch.cuda.synchronize()

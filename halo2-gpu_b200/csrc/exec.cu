@@ -108,6 +108,17 @@ extern "C" RustError h2b_exec_join(cudaStream_t parent, uint32_t n)
     return ok();
 }
 
+// Stream-ordered upload of a small host buffer (pageable memory is staged by
+// the driver before this returns, so the source may be reused at once); unlike
+// a synchronous copy it does not wait for the work already queued on `s`.
+extern "C" RustError h2b_upload(void* d_dst, const void* h_src, uint64_t bytes, cudaStream_t s)
+{
+    if (bytes == 0) return ok();
+    if (!d_dst || !h_src) return err((int)cudaErrorInvalidValue, "h2b_upload: null pointer");
+    H2B_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, s));
+    return ok();
+}
+
 extern "C" RustError h2b_graph_begin(cudaStream_t s)
 {
     H2B_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));

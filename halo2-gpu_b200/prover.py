@@ -172,14 +172,15 @@ class ProofWorkload:
             flush()
             # 4. permutation grand products (2 sets of 2 columns), lookup grand product
             beta, gamma = sc(chal()), sc(chal())
-            d_beta, d_gamma = h2b.to_dev(beta), h2b.to_dev(gamma)
-            d_delta, d_om = h2b.to_dev(F.fr_mont_limbs([F.DELTA])), h2b.to_dev(F.fr_mont_limbs([dom.omega]))
-            d_one = h2b.to_dev(sc(1))
+            d_beta, d_gamma = h2b.to_dev(beta, stream), h2b.to_dev(gamma, stream)
+            d_delta = h2b.to_dev(F.fr_mont_limbs([F.DELTA]), stream)
+            d_om = h2b.to_dev(F.fr_mont_limbs([dom.omega]), stream)
+            d_one = h2b.to_dev(sc(1), stream)
             zs = []
             for s in range(2):
                 z = h2b.dev_empty(32 * n)
                 h2b.call("_halo2_poly_fill_one", h2b.ptr(z), n, h2b.stream_handle(stream))
-                d_dw = h2b.to_dev(sc(pow(F.DELTA, 2 * s, F.R_MOD)))
+                d_dw = h2b.to_dev(sc(pow(F.DELTA, 2 * s, F.R_MOD)), stream)
                 h2b.permutation_product_device(z, pk["sigma"][2 * s: 2 * s + 2], adv[2 * s: 2 * s + 2], d_beta,
                                                d_gamma, d_delta, d_om, d_dw, n, stream=stream)
                 h2b.grand_product_device(z, d_one, n, stream=stream)
@@ -199,7 +200,7 @@ class ProofWorkload:
             #    Columns: advice 0-3, instance 4, z 5-6, lookup z 7, A' 8, S' 9,
             #    compressed input 10, fixed 11-13, sigma 14-17, l0 18, l_last 19, l_active 20.
             y, theta = chal(), chal()
-            d_y = h2b.to_dev(sc(y))
+            d_y = h2b.to_dev(sc(y), stream)
             keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
             allc = coef + keyp
             parts = [h2b.dev_empty(32 * n) for _ in allc]
@@ -224,7 +225,7 @@ class ProofWorkload:
             #    polynomial, back to coefficients (extended_to_coeff), commit its pieces
             en = len(hs) * n
             ext, hc = h2b.dev_empty(32 * en), h2b.dev_empty(32 * en)
-            tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64))
+            tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64), stream)
             h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), len(hs), n,
                      h2b.stream_handle(stream))
             h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk["t_evals"]),
@@ -232,7 +233,7 @@ class ProofWorkload:
             h2b.fft_many_to_device(2, dom.extended_k, dom.extended_k, [ext], [hc], dom.extended_omega_inv,
                                    dom.extended_ifft_divisor, stream=stream)
             del ext, hs
-            zp = h2b.to_dev(F.fr_mont_limbs([dom.g_coset_inv, dom.g_coset]))
+            zp = h2b.to_dev(F.fr_mont_limbs([dom.g_coset_inv, dom.g_coset]), stream)
             h2b.call("_halo2_distribute_powers_zeta", h2b.ptr(hc), h2b.ptr(zp), 2, en, h2b.stream_handle(stream))
             for i in range(dom.quotient_poly_degree):
                 commit(_slice(hc, i, n))

@@ -66,22 +66,37 @@ class Shplonk:
 
     def __init__(self, h2b, n, stream=None):
         self.h2b, self.n, self.stream = h2b, n, stream
-        self.sh = h2b.stream_handle(stream)
+        self.st = stream if stream is not None else __import__("torch").cuda.current_stream()
+        self.sh = h2b.stream_handle(self.st)
         self.ews = h2b.dev_empty(h2b.lib()._halo2_eval_polynomial_workspace_size(n))
         self.kws = h2b.dev_empty(h2b.lib()._halo2_kate_division_workspace_size(n))
 
     def _scalar(self, v):
-        return self.h2b.to_dev(F.fr_mont_limbs([v % P]))
+        return self.h2b.to_dev(F.fr_mont_limbs([v % P]), self.st)
 
-    def eval(self, d_poly, x):
-        """p(x) as an int (synchronises the stream)."""
+    def eval_device(self, d_poly, x):
+        """p(x) left on the device (a 32-byte view into fresh scratch)."""
         h2b = self.h2b
+        ws = h2b.dev_empty(self.ews.numel())
         pt = F.fr_mont_limbs([x % P])
         res = ctypes.c_void_p()
         h2b.call("_halo2_eval_polynomial", h2b.ptr(d_poly), ctypes.byref(h2b.host_ffi(pt)), ctypes.byref(res),
-                 self.n, h2b.ptr(self.ews), self.ews.numel(), self.sh)
-        off = res.value - self.ews.data_ptr()
-        return F.fr_from_mont_limbs(h2b.to_host(self.ews[off:off + 32]))[0]
+                 self.n, h2b.ptr(ws), ws.numel(), self.sh)
+        off = res.value - ws.data_ptr()
+        return ws[off:off + 32]
+
+    def eval_many(self, items):
+        """[p(x) for (p, x) in items] as ints, with one synchronisation."""
+        if not items:
+            return []
+        views = [self.eval_device(d, x) for d, x in items]
+        torch = __import__("torch")
+        packed = torch.cat(views).cpu().numpy().view("<u8").reshape(-1, 4)
+        return F.fr_from_mont_limbs(packed)
+
+    def eval(self, d_poly, x):
+        """p(x) as an int (synchronises the stream)."""
+        return self.eval_many([(d_poly, x)])[0]
 
     def madd(self, d_acc, d_in, c):
         """acc += c * in over n coefficients."""
@@ -89,7 +104,7 @@ class Shplonk:
                       self.h2b.ptr(self._scalar(c)), self.n, self.sh)
 
     def sub_short(self, d_acc, coeffs):
-        d = self.h2b.to_dev(F.fr_mont_limbs([c % P for c in coeffs]))
+        d = self.h2b.to_dev(F.fr_mont_limbs([c % P for c in coeffs]), self.st)
         self.h2b.call("_halo2_poly_sub_short_inplace", self.h2b.ptr(d_acc), self.h2b.ptr(d), len(coeffs), self.sh)
 
     def div_linear(self, d_a, d_q, s):
@@ -113,10 +128,8 @@ def open_queries(h2b, queries, challenges, commit, stream=None):
     n = queries[0][0].numel() // 32
     sp = Shplonk(h2b, n, stream)
     # evaluations, and the point set of every polynomial (by identity)
-    evals, point_sets, polys = [], {}, {}
-    for d, x in queries:
-        e = sp.eval(d, x)
-        evals.append(e)
+    evals, point_sets, polys = sp.eval_many(queries), {}, {}
+    for (d, x), e in zip(queries, evals):
         key = d.data_ptr()
         polys[key] = d
         point_sets.setdefault(key, {})[x % P] = e

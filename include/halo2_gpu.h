@@ -382,6 +382,9 @@ RustError h2b_msm_device_table(const void* d_scalars, const void* d_table, uint6
  * share them).  h2b_exec_join: `parent` waits for them; call it from the thread that forked. */
 RustError h2b_exec_fork(h2b_stream_t parent, uint32_t n, h2b_stream_t* out_streams);
 RustError h2b_exec_join(h2b_stream_t parent, uint32_t n);
+/* Stream-ordered upload of `bytes` from host memory (pageable is staged before the call returns) without
+ * waiting for the work already queued on `stream` (scalars and small tables between kernels). */
+RustError h2b_upload(void* d_dst, const void* h_src, uint64_t bytes, h2b_stream_t stream);
 /* Capture what is issued on `s` (and on streams forked from it) into a CUDA graph; replay it with
  * h2b_graph_launch.  Only calls without host copies or synchronisation can be captured. */
 RustError h2b_graph_begin(h2b_stream_t s);
