@@ -98,10 +98,18 @@ H2B_DEV Fz<C> fz_mul(const Fz<C>& a, const Fz<C>& b)
     const uint32_t np = C::N0 & M29;
     uint32_t m[9];
     uint64_t acc = 0;
+#if H2B_MUL_KARATSUBA
+    uint64_t T[17];
+    kcols29(a.l, b.l, T);
+#endif
 #pragma unroll
     for (int k = 0; k < 9; k++) {
+#if H2B_MUL_KARATSUBA
+        acc += T[k];
+#else
 #pragma unroll
         for (int i = 0; i <= k; i++) acc = madw(a.l[i], b.l[k - i], acc);
+#endif
 #pragma unroll
         for (int i = 0; i < k; i++) acc = madw(m[i], p29<C>(k - i), acc);
         const uint32_t mk = ((uint32_t)acc * np) & M29;
@@ -112,8 +120,12 @@ H2B_DEV Fz<C> fz_mul(const Fz<C>& a, const Fz<C>& b)
     Fz<C> r;
 #pragma unroll
     for (int k = 9; k < 17; k++) {
+#if H2B_MUL_KARATSUBA
+        acc += T[k];
+#else
 #pragma unroll
         for (int i = k - 8; i <= 8; i++) acc = madw(a.l[i], b.l[k - i], acc);
+#endif
 #pragma unroll
         for (int i = k - 8; i <= 8; i++) acc = madw(m[i], p29<C>(k - i), acc);
         r.l[k - 9] = (uint32_t)acc & M29;
