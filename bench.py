@@ -51,6 +51,24 @@ def load_pkg():
     return mod
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings over all ranks (the slowest
+    rank sets every whole-job figure); values unchanged without a process
+    group."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_points_per_s(world, points_per_rank, ms):
+    """Weak scaling: every rank runs its own MSM of `points_per_rank` points;
+    the job's throughput is all points over the slowest rank's time."""
+    return world * points_per_rank / (ms * 1e-3)
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -662,13 +680,10 @@ def main():
     L.h2b_prof_enable(0)
 
     step_ms = total_ms / args.steps
-    if dist is not None:
-        t = torch.tensor([step_ms, msm_ms, ntt_ms, bi_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, msm_ms, ntt_ms, bi_ms = t.tolist()
+    step_ms, msm_ms, ntt_ms, bi_ms = max_over_ranks([step_ms, msm_ms, ntt_ms, bi_ms], dist, "cuda")
 
     ntt_bytes = 32 * n_ntt + 32 * n_ext
-    value = world * n_msm / (msm_ms * 1e-3)
+    value = whole_job_points_per_s(world, n_msm, msm_ms)
     hbm, hbm_kind = peaks()
     # dominant kernel: MSM bucket accumulation (one launch per MSM)
     acc_avg_ms = acc_ms / max(acc_cnt, 1)
@@ -745,11 +760,8 @@ def main():
         torch.cuda.synchronize()
         e_msm = sum(e[0].elapsed_time(e[1]) for e in eevs) / args.steps
         e_step = sum(e[0].elapsed_time(e[2]) for e in eevs) / args.steps
-        if dist is not None:
-            t = torch.tensor([e_msm, e_step], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_msm, e_step = t.tolist()
-        line["e2e"] = {"value": world * n_msm / (e_msm * 1e-3), "unit": UNIT,
+        e_msm, e_step = max_over_ranks([e_msm, e_step], dist, "cuda")
+        line["e2e"] = {"value": whole_job_points_per_s(world, n_msm, e_msm), "unit": UNIT,
                        "h2d_bytes_per_step": 32 * n_msm + 32 * n_ntt + 32 * n_bi,
                        "d2h_bytes_per_step": 96 + 32 * n_ext + 32 * n_bi, "step_ms": e_step,
                        "api": "_halo2_multiexp_device_bases (host scalars), _halo2_cosetfft (host in/out), "
