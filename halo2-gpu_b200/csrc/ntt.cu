@@ -206,7 +206,7 @@ constexpr int NTT_THREADS = 512;
 // power of two, so all index arithmetic is shifts and masks on 32 bits
 // (n <= 2^31).
 template <bool DIT>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
+__global__ void __launch_bounds__(NTT_THREADS, 3) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
                                                           int nst, int lS, int lG)
 {
     const Fr* src = B.src[blockIdx.y];  // the first pass of an out-of-place transform reads here
@@ -239,26 +239,35 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(NttBatch B, const Fr* 
     }
     __syncthreads();
 
+    // One butterfly per thread and stage (nbf <= blockDim.x: a tile holds at
+    // most 2^10 elements).  Everything that does not change with the stage is
+    // computed once; addresses are 32-bit byte offsets (shift and add), so the
+    // integer multiply pipe is left to the products.
     const uint32_t nbf = 1u << (lG + nst - 1);
-    const uint32_t mmask = (1u << (nst - 1)) - 1;
+    const uint32_t u = threadIdx.x;
+    const uint32_t m = u & ((1u << (nst - 1)) - 1);
+    const uint32_t gl = u >> (nst - 1);
+    const uint32_t r = (g0 + gl) & Smask;
+    char* const base = reinterpret_cast<char*>(sm) + ((gl << nst) << 5);
+    const char* const twb = reinterpret_cast<const char*>(tw);
     for (int t = 0; t < nst; t++) {
         const int s = s0 + t;
-        for (uint32_t u = threadIdx.x; u < nbf; u += blockDim.x) {
-            const uint32_t gl = u >> (nst - 1), m = u & mmask;
-            const uint32_t r = (g0 + gl) & Smask;
-            const int h = DIT ? t : nst - t - 1;
-            const uint32_t lowm = m & ((1u << h) - 1);
-            const uint32_t q = ((m >> h) << (h + 1)) | lowm;
-            Fr* px = &sm[(gl << nst) + q];
-            Fr* py = px + (1u << h);
+        const int h = DIT ? t : nst - t - 1;
+        const uint32_t lo = (1u << h) - 1;
+        const uint32_t lowm = m & lo;
+        const uint32_t q = m + (m & ~lo);                 // ((m >> h) << (h + 1)) | lowm
+        const int sh = DIT ? logn - s - 1 : s;            // twiddle w^(((lowm << lS) + r) << sh)
+        const uint32_t toff = (((lowm << lS) + r) << sh) << 5;
+        if (u < nbf) {
+            Fr* px = reinterpret_cast<Fr*>(base + (q << 5));
+            Fr* py = reinterpret_cast<Fr*>(base + ((q + (1u << h)) << 5));
             const Fr x = *px, y = *py;
+            const Fr w = ldg(reinterpret_cast<const Fr*>(twb + toff));
             if (DIT) {
-                const Fr w = ldg(&tw[((lowm << lS) + r) << (logn - s - 1)]);
                 const Fr yw = y * w;
                 *px = x + yw;
                 *py = x - yw;
             } else {
-                const Fr w = ldg(&tw[((lowm << lS) + r) << s]);
                 *px = x + y;
                 *py = (x - y) * w;
             }
