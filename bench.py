@@ -197,12 +197,13 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def rows_section(h2b, torch, hbm_gbs, imad_peak, k=20, reps=5):
+def rows_section(h2b, torch, hbm_gbs, product_peak, k=20, reps=5):
     """Every other row of the hot path at the k = 20 proof size, timed with
     CUDA events around the public entry point (as a caller would call it).
     For each: ms per call, units/s, algorithmic GB/s and its fraction of the
     measured HBM peak, and (where the product count per unit is fixed) the
-    fraction of the IMAD peak at 264 IMAD-class operations per product."""
+    fraction of the measured field-product throughput (register-resident
+    chains of the same operator*, h2b_probe_modmul)."""
     import numpy as np
     rules_mod = importlib.util.spec_from_file_location("h2b_rules", os.path.join(ROOT, "halo2-gpu_b200", "rules.py"))
     R = importlib.util.module_from_spec(rules_mod)
@@ -229,7 +230,7 @@ def rows_section(h2b, torch, hbm_gbs, imad_peak, k=20, reps=5):
         r = {"ms": round(ms, 4), f"{unit}_per_s": units / (ms * 1e-3), "GB_per_s": round(gbs, 1),
              "hbm_frac": round(gbs / hbm_gbs, 4)}
         if products_per_unit:
-            r["imad_frac"] = round(units * products_per_unit * 264 / (ms * 1e-3) / imad_peak, 4)
+            r["product_frac"] = round(units * products_per_unit / (ms * 1e-3) / product_peak, 4)
         out[name] = r
 
     # a7: quotient evaluator, PLONK + Fibonacci gates over one extended part (rot_scale 4)
@@ -713,7 +714,7 @@ def main():
                 "window_bits": L.h2b_msm_window_bits(n_msm)},
         "ntt": {"ms": ntt_ms, "GB_per_s": ntt_bytes / (ntt_ms * 1e-3) / 1e9,
                 "elements_per_s": n_ext / (ntt_ms * 1e-3), "pass_kernels_ms": ntt_kernel_ms,
-                "imad_frac_passes": ntt_modmul * 264 / (ntt_kernel_ms * 1e-3) / imad_peak},
+                "product_frac_passes": ntt_modmul / (ntt_kernel_ms * 1e-3) / probe["h2b_probe_modmul"]},
         "batch_invert": {"ms": bi_ms, "elements_per_s": n_bi / (bi_ms * 1e-3), "apply_kernel_ms": bi_kernel_ms},
         "roofline": roofline, "imad_roofline": imad, "clocks": clk, "gpu_launches": launches,
     }
@@ -769,7 +770,7 @@ def main():
 
     if not args.no_batch:
         line["msm_table"] = table_section(h2b, torch, d_srs, d_sc, n_msm, args.steps)
-        line["rows_k20"] = rows_section(h2b, torch, hbm, imad_peak)
+        line["rows_k20"] = rows_section(h2b, torch, hbm, probe["h2b_probe_modmul"])
         line["batch"] = batch_section(h2b, torch)
     if world == 1 and not args.no_serve:
         line["serving"] = serving_section(h2b, torch)

@@ -205,8 +205,15 @@ constexpr int NTT_THREADS = 512;
 // of S * 2^nst).  A CTA owns G = 2^lG consecutive groups.  Every size is a
 // power of two, so all index arithmetic is shifts and masks on 32 bits
 // (n <= 2^31).
+// Blocks per SM for the pass: the FP64 product needs more live registers.
+#if H2B_MUL_F64
+constexpr int NTT_MIN_BLOCKS = 2;
+#else
+constexpr int NTT_MIN_BLOCKS = 3;
+#endif
+
 template <bool DIT>
-__global__ void __launch_bounds__(NTT_THREADS, 3) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
+__global__ void __launch_bounds__(NTT_THREADS, NTT_MIN_BLOCKS) k_ntt_pass(NttBatch B, const Fr* __restrict__ tw, int logn, int s0,
                                                           int nst, int lS, int lG)
 {
     const Fr* src = B.src[blockIdx.y];  // the first pass of an out-of-place transform reads here

@@ -124,15 +124,18 @@ __device__ __forceinline__ Fr mul_impl(const Fr& a, const Fr& b)
     if (IMPL == 0) return mont_mul_inline<FrCfg>(a, b);
     if (IMPL == 1) return mont_mul_wide<FrCfg>(a, b);
     if (IMPL == 3) return mont_sqr_29<FrCfg>(a);
+    if (IMPL == 6) return mont_mul_f64<FrCfg>(a, b);
     return mont_mul_29<FrCfg>(a, b);
 }
 
-// Fq products through the 29-bit column form (IMPL 4: a*b, 5: a^2).
+// Fq products (IMPL 4: a*b 29-bit, 5: a^2 29-bit, 7: a*b FP64).
 template <int IMPL>
 __global__ void k_fq_mul_batch(const Fq* __restrict__ a, const Fq* __restrict__ b, Fq* __restrict__ out, uint64_t n)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        st(&out[i], IMPL == 4 ? mont_mul_29<FqCfg>(ld(&a[i]), ld(&b[i])) : mont_sqr_29<FqCfg>(ld(&a[i])));
+        st(&out[i], IMPL == 4   ? mont_mul_29<FqCfg>(ld(&a[i]), ld(&b[i]))
+                    : IMPL == 7 ? mont_mul_f64<FqCfg>(ld(&a[i]), ld(&b[i]))
+                                : mont_sqr_29<FqCfg>(ld(&a[i])));
 }
 
 // Four independent chains of 29-bit-limb products that stay in limb form.
@@ -243,14 +246,15 @@ extern "C" RustError h2b_probe_imad_form(int blocks, int threads, int iters, int
 
 // Montgomery-product throughput of one implementation (0 = mad.lo/mad.hi
 // carry chains, 1 = mad.wide CIOS, 2 = 29-bit limbs with conversion from and
-// to 8 x 32 per product, 3 = 29-bit limbs kept between products), four
-// independent products per iteration.
+// to 8 x 32 per product, 3 = 29-bit limbs kept between products, 4 = FP64
+// product over 52-bit limbs), four independent products per iteration.
 extern "C" RustError h2b_probe_modmul_impl(int impl, int blocks, int threads, int iters, void* d_sink,
                                            cudaStream_t stream)
 {
     if (impl == 0) k_probe_modmul_impl<0><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
     else if (impl == 1) k_probe_modmul_impl<1><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
     else if (impl == 2) k_probe_modmul_impl<2><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
+    else if (impl == 4) k_probe_modmul_impl<6><<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
     else k_probe_mul29_chain<<<blocks, threads, 0, stream>>>((uint32_t*)d_sink, iters);
     H2B_LAUNCHED("k_probe_modmul_impl");
     return ok();
@@ -258,7 +262,7 @@ extern "C" RustError h2b_probe_modmul_impl(int impl, int blocks, int threads, in
 
 // out[i] = a[i] * b[i] with the chosen product implementation (tests):
 // 0-2 Fr products (CIOS lo/hi, CIOS wide, 29-bit), 3 Fr square (29-bit),
-// 4 Fq product, 5 Fq square (29-bit).
+// 4 Fq product, 5 Fq square (29-bit), 6 Fr product, 7 Fq product (FP64).
 extern "C" RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b, void* d_out, uint64_t n,
                                       cudaStream_t stream)
 {
@@ -273,6 +277,10 @@ extern "C" RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b
         k_fr_mul_batch<3><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
     else if (impl == 4)
         k_fq_mul_batch<4><<<grid_for(n, 256), 256, 0, stream>>>((const Fq*)d_a, (const Fq*)d_b, (Fq*)d_out, n);
+    else if (impl == 6)
+        k_fr_mul_batch<6><<<grid_for(n, 256), 256, 0, stream>>>((const Fr*)d_a, (const Fr*)d_b, (Fr*)d_out, n);
+    else if (impl == 7)
+        k_fq_mul_batch<7><<<grid_for(n, 256), 256, 0, stream>>>((const Fq*)d_a, (const Fq*)d_b, (Fq*)d_out, n);
     else
         k_fq_mul_batch<5><<<grid_for(n, 256), 256, 0, stream>>>((const Fq*)d_a, (const Fq*)d_b, (Fq*)d_out, n);
     H2B_LAUNCHED("k_fr_mul_batch");

@@ -1,6 +1,6 @@
 """Montgomery product parity on the device: every product implementation
-(mad.lo/mad.hi CIOS, mad.wide CIOS, 29-bit column products and squares, for
-Fr and Fq) against Python integers, on random and boundary operands (the
+(mad.lo/mad.hi CIOS, mad.wide CIOS, 29-bit column products and squares, and
+the FP64 product over 52-bit limbs, for Fr and Fq) against Python integers, on random and boundary operands (the
 reference's field arithmetic is Montgomery multiplication with R = 2^256,
 halo2_proofs/cuda/include/field/alt_bn128.hpp:15-43)."""
 import numpy as np
@@ -17,10 +17,10 @@ def _edge_ints(p):
             (1 << 255) % p, ((1 << 254) - 1) % p, p - (1 << 32), (1 << 232) - 1, p - (1 << 232), (1 << 29) - 1]
 
 
-@pytest.mark.parametrize("impl", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("impl", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_product_impls(h2b, orc, cuda, impl):
     f = h2b.fields
-    p = f.Q_MOD if impl >= 4 else f.R_MOD
+    p = f.Q_MOD if impl in (4, 5, 7) else f.R_MOD
     square = impl in (3, 5)
     n = 1 << 16
     rng = np.random.default_rng(impl)
