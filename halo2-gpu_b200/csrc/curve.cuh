@@ -14,6 +14,7 @@
 #include "field.cuh"
 #include "inverse.cuh"
 #include "lazy.cuh"
+#include "lazy64.cuh"
 
 namespace h2b {
 
@@ -369,6 +370,83 @@ static __device__ __noinline__ void st_xyzzz(G1Xyzz* dst, const G1XyzzZ p, const
     G1Xyzz r;
     r.X = fz_canonical(a.a); r.Y = fz_canonical(a.b);
     r.ZZ = fz_canonical(b.a); r.ZZZ = fz_canonical(b.b);
+    st_xyzz(dst, r);
+}
+
+// ---- XYZZ in the FP64 lazy form (R' = 2^260), accumulate variant 6 -------
+// The same formulas as the R = 2^261 form above; products follow
+// (1 + 0.0118 a b) p, so the accumulator bounds are X < 5.4p, Y < 3.45p,
+// ZZ and ZZZ < 1.2p (stable from one addition to the next); affine inputs
+// are qx < p and qy < 2p.
+
+typedef Fd<FqCfg> FqD;
+
+struct G1XyzzD {
+    FqD X, Y, ZZ, ZZZ;
+};
+
+H2B_DEV G1XyzzD xyzzd_inf()
+{
+    G1XyzzD r;
+    r.X = fd_zero<FqCfg>(); r.Y = fd_zero<FqCfg>(); r.ZZ = fd_zero<FqCfg>(); r.ZZZ = fd_zero<FqCfg>();
+    return r;
+}
+
+H2B_DEV bool is_inf(const G1XyzzD& p) { return fd_is_zero(p.ZZ); }
+
+// 2 q for an affine q (qx < p, qy < 2p, qy != 0): dbl-2008-s-1 with Z = 1.
+H2B_DEV G1XyzzD xyzzd_dbl_affine(const FqD& qx, const FqD& qy)
+{
+    const FqD U = fd_add(qy, qy);                              // < 4p
+    const Fd2<FqCfg> vx = fd_mul2(U, U, qx, qx);               // V < 1.19p, xx < 1.012p
+    const Fd2<FqCfg> ws = fd_mul2(U, vx.a, qx, vx.a);          // W < 1.057p, S < 1.015p
+    const FqD M = fd_add(fd_add(vx.b, vx.b), vx.b);            // < 3.04p
+    const Fd2<FqCfg> mm = fd_mul2(M, M, ws.a, qy);             // MM < 1.11p, W y < 1.025p
+    G1XyzzD r;
+    r.X = fd_sub<FqCfg, 3>(mm.a, fd_add(ws.b, ws.b));          // 2S < 2.03p; X3 < 4.11p
+    const FqD t1 = fd_mul_call(M, fd_sub<FqCfg, 5>(ws.b, r.X)); // S - X3 + 5p < 6.02p; t1 < 1.22p
+    r.Y = fd_sub<FqCfg, 2>(t1, mm.b);                          // < 3.22p
+    r.ZZ = vx.a;                                               // < 1.19p
+    r.ZZZ = ws.a;                                              // < 1.057p
+    return r;
+}
+
+// madd-2008-s: acc += (qx, qy), q affine and not infinity.  PP == 0 mod p
+// exactly when P is, so the equal-x test reads the square.
+H2B_DEV void xyzzd_madd(G1XyzzD& acc, const FqD& qx, const FqD& qy, const FqD& one)
+{
+    if (is_inf(acc)) {
+        acc.X = qx; acc.Y = qy; acc.ZZ = one; acc.ZZZ = one;
+        return;
+    }
+    const Fd2<FqCfg> us = fd_mul2(qx, acc.ZZ, qy, acc.ZZZ);   // U2 < 1.015p, S2 < 1.03p
+    const FqD P = fd_sub<FqCfg, 6>(us.a, acc.X);               // X1 < 5.4p; P < 7.02p
+    const FqD R = fd_sub<FqCfg, 4>(us.b, acc.Y);               // Y1 < 3.45p; R < 5.03p
+    const Fd2<FqCfg> sq = fd_mul2(P, P, R, R);                 // PP < 1.59p, RR < 1.3p
+    if (fd_is_zero_mod(sq.a)) {
+        acc = fd_is_zero_mod(sq.b) ? xyzzd_dbl_affine(qx, qy) : xyzzd_inf();
+        return;
+    }
+    const Fd2<FqCfg> pq = fd_mul2(P, sq.a, acc.X, sq.a);       // PPP < 1.14p, Q < 1.11p
+    const FqD X3 = fd_sub<FqCfg, 4>(sq.b, fd_add(pq.a, fd_add(pq.b, pq.b)));  // PPP + 2Q < 3.36p; X3 < 5.3p
+    const Fd2<FqCfg> yy = fd_mul2(R, fd_sub<FqCfg, 6>(pq.b, X3), acc.Y, pq.a); // Q - X3 + 6p < 7.11p;
+                                                                              // < 1.43p, < 1.05p
+    const Fd2<FqCfg> zz = fd_mul2(acc.ZZ, sq.a, acc.ZZZ, pq.a); // < 1.03p, < 1.02p
+    acc.Y = fd_sub<FqCfg, 2>(yy.a, yy.b);                     // < 3.43p
+    acc.X = X3;
+    acc.ZZ = zz.a;
+    acc.ZZZ = zz.b;
+}
+
+// Canonical memory image of the accumulator (infinity stays ZZ = 0): four
+// products by 2^256 mod p (each below 1.07p), then conditional subtractions.
+static __device__ __noinline__ void st_xyzzd(G1Xyzz* dst, const G1XyzzD p, const FqD r256)
+{
+    const Fd2<FqCfg> a = fd_mul2(p.X, r256, p.Y, r256);
+    const Fd2<FqCfg> b = fd_mul2(p.ZZ, r256, p.ZZZ, r256);
+    G1Xyzz r;
+    r.X = fd_canonical(a.a); r.Y = fd_canonical(a.b);
+    r.ZZ = fd_canonical(b.a); r.ZZZ = fd_canonical(b.b);
     st_xyzz(dst, r);
 }
 

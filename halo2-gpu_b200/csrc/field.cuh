@@ -617,15 +617,14 @@ __host__ __device__ constexpr uint64_t bias(int k)
 }
 }  // namespace f64
 
+// The Montgomery core over 52-bit limbs: l = A B / 2^260 + (multiple of p
+// absorbed), limbs normalised below 2^52 except the top one, which holds the
+// rest.  A and B are limbs below 2^52 held exactly in doubles (any value
+// below 2^260); the result is below A B / 2^260 + p.
+namespace f64 {
 template <class C>
-H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
+H2B_DEV void mont52(const double (&A)[5], const double (&B)[5], uint64_t (&l)[5])
 {
-    using namespace f64;
-    double A[5], B[5];
-    A[0] = u52d(bits52<-4>(a.v)); A[1] = u52d(bits52<48>(a.v)); A[2] = u52d(bits52<100>(a.v));
-    A[3] = u52d(bits52<152>(a.v)); A[4] = u52d(bits52<204>(a.v));
-    B[0] = u52d(bits52<0>(b.v)); B[1] = u52d(bits52<52>(b.v)); B[2] = u52d(bits52<104>(b.v));
-    B[3] = u52d(bits52<156>(b.v)); B[4] = u52d(bits52<208>(b.v));
     uint64_t col[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) col[k] = 0 - bias(k);
@@ -635,8 +634,8 @@ H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
 #pragma unroll
         for (int j = 0; j < 5; j++) {
             const double h = __fma_rz(A[i], B[j], C104);
-            const double l = __fma_rn(A[i], B[j], __dsub_rn(C104_52, h));
-            col[i + j] = j == 0 ? col[i + j] + dbits(l) : col[i + j] + (dbits(l) + hp);
+            const double lo = __fma_rn(A[i], B[j], __dsub_rn(C104_52, h));
+            col[i + j] = j == 0 ? col[i + j] + dbits(lo) : col[i + j] + (dbits(lo) + hp);
             hp = dbits(h);
         }
         col[i + 5] += hp;
@@ -651,20 +650,34 @@ H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
         for (int j = 1; j < 5; j++) {
             const double pj = (double)p52<C>(j);
             const double h = __fma_rz(qd, pj, C104);
-            const double l = __fma_rn(qd, pj, __dsub_rn(C104_52, h));
-            col[i + j] = col[i + j] + (dbits(l) + hp);
+            const double lo = __fma_rn(qd, pj, __dsub_rn(C104_52, h));
+            col[i + j] = col[i + j] + (dbits(lo) + hp);
             hp = dbits(h);
         }
         col[i + 5] += hp;
     }
-    // columns 5..9 -> 52-bit limbs -> 8 x 32 words
-    uint64_t l[5], c = 0;
+    uint64_t c = 0;
 #pragma unroll
     for (int k = 0; k < 5; k++) {
         const uint64_t x = col[5 + k] + c;
         l[k] = k < 4 ? (x & M52) : x;
         c = x >> 52;
     }
+}
+}  // namespace f64
+
+template <class C>
+H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
+{
+    using namespace f64;
+    double A[5], B[5];
+    A[0] = u52d(bits52<-4>(a.v)); A[1] = u52d(bits52<48>(a.v)); A[2] = u52d(bits52<100>(a.v));
+    A[3] = u52d(bits52<152>(a.v)); A[4] = u52d(bits52<204>(a.v));
+    B[0] = u52d(bits52<0>(b.v)); B[1] = u52d(bits52<52>(b.v)); B[2] = u52d(bits52<104>(b.v));
+    B[3] = u52d(bits52<156>(b.v)); B[4] = u52d(bits52<208>(b.v));
+    uint64_t l[5];
+    mont52<C>(A, B, l);
+    // 52-bit limbs -> 8 x 32 words
     uint32_t w[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) {

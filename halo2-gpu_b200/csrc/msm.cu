@@ -52,7 +52,7 @@ static constexpr uint64_t MSM_PIPE_MIN = 1ull << 18;  // host scalars from here 
 static constexpr int MSM_PIPE_PIECES = 8;
 
 static int g_msm_window_override = 0;
-static int g_msm_acc_variant = 0;  // call structure of the accumulation kernel (0, 1, 2)
+static int g_msm_acc_variant = 6;  // form and call structure of the accumulation kernel (0..6)
 static int g_msm_pair_rounds = 0;  // batch-affine pairing rounds before the XYZZ accumulation (0..3)
 constexpr int PR_T = 128;          // pairing rounds: threads per CTA
 constexpr int PR_E = 8;            // pairing rounds: input entries per thread (at most 4 additions)
@@ -414,6 +414,53 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_z(const uint32_t* __r
             xyzzz_madd(acc, qx, qy, one);
         }
         st_xyzzz(head ? &heads[t] : &buckets[b], acc, r256);
+    }
+}
+
+// The same accumulation in the FP64 lazy form (R' = 2^260, lazy64.cuh):
+// bases are read in the same x 2^261 storage form and halved modulo p on
+// load; buckets leave in the same canonical memory image.
+__global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __restrict__ sorted,
+                                                             const uint32_t* __restrict__ offsets, uint64_t NB,
+                                                             uint32_t K, const G1Affine* __restrict__ bases,
+                                                             uint64_t phi_off, G1Xyzz* __restrict__ buckets,
+                                                             G1Xyzz* __restrict__ heads)
+{
+    const FqD one = fd_from_r261(to_r261(Fq::one()));            // 1 in the form (2^260 mod p)
+    const FqD r256 = fd_from_words(Fq::one());                    // 2^256 mod p, for the stores
+    const uint32_t M = offsets[NB];
+    const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = (uint32_t)(t * K);
+        const uint32_t end = ((uint64_t)start + K < (uint64_t)M) ? start + K : M;
+        uint64_t lo = 0, hi = NB;  // offsets[lo] <= start < offsets[hi]
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= start) lo = mid; else hi = mid;
+        }
+        uint64_t b = lo;
+        uint32_t next = offsets[b + 1];
+        bool head = offsets[b] < start;
+        G1XyzzD acc = xyzzd_inf();
+        for (uint32_t e = start; e < end; e++) {
+            if (e == next) {
+                st_xyzzd(head ? &heads[t] : &buckets[b], acc, r256);
+                acc = xyzzd_inf();
+                head = false;
+                do { b++; next = offsets[b + 1]; } while (next == e);
+            }
+            const uint32_t ent = sorted[e];
+            const uint32_t v = ent & ~SIGN_BIT;
+            const bool phi = (v & 1u) != 0;
+            const G1Affine P = ld_affine(&bases[(v >> 1) + (phi ? phi_off : 0)]);    // phi(P) precomputed
+            if (is_inf(P)) continue;
+            const FqD qx = fd_from_r261(P.x);                              // < p
+            FqD qy = fd_from_r261(P.y);                                    // < p
+            if (ent & SIGN_BIT) qy = fd_sub<FqCfg, 2>(fd_zero<FqCfg>(), qy);  // 2p - y < 2p
+            xyzzd_madd(acc, qx, qy, one);
+        }
+        st_xyzzd(head ? &heads[t] : &buckets[b], acc, r256);
     }
 }
 
@@ -792,7 +839,10 @@ __global__ void k_write_inf(G1Jac* out)
 // The lazy accumulation (window tables are stored in its form; plain bases
 // are converted by the split kernel) unless pairing rounds or an older
 // variant run.
-static bool msm_lazy(const MsmPlan& p) { return p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0); }
+static bool msm_lazy(const MsmPlan& p)
+{
+    return p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0 || g_msm_acc_variant == 6);
+}
 
 // Phases of one MSM on `st`: msm_begin clears the histogram, msm_split takes
 // points [lo, hi) through the GLV split (and base conversion) and the
@@ -864,6 +914,9 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
     if (p.R > 0)
         k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
+    else if (lazy && g_msm_acc_variant == 6)
+        k_msm_accumulate_d<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
+                                                     p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
     else if (lazy)
         k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
@@ -1162,15 +1215,18 @@ extern "C" RustError h2b_msm_device_table(const void* d_scalars, const void* d_t
 
 extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(window_bits, chunk); }
 
-// Form and call structure of the bucket-accumulation kernel: 0 = the lazy
-// R = 2^261 form with one-step carries (default; window tables always use
-// it); the normalised R = 2^256 limb form with 5 = two products per
-// out-of-line call, 1 = all products inline, 2 = one product per call, 3 and
-// 4 = one product per call with at most 128 / 96 registers (4 / 5 CTAs of 128
-// threads per SM).  Results are identical; only speed differs.
+// Form and call structure of the bucket-accumulation kernel: 6 = the lazy
+// R' = 2^260 form on the FP64 pipe (default; window tables use it too);
+// 0 = the lazy R = 2^261 form of 29-bit limbs with one-step carries (window
+// tables use it for every choice but 6); the normalised R = 2^256 limb form
+// with 5 = two products per out-of-line call, 1 = all products inline, 2 =
+// one product per call, 3 and 4 = one product per call with at most 128 / 96
+// registers (4 / 5 CTAs of 128 threads per SM).  Measured at 2^22 with the
+// witness-like scalar mix: 6 takes 12.26 ms, 0 13.56 ms.  Results are
+// identical; only speed differs.
 extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
-    if (v >= 0 && v <= 5) g_msm_acc_variant = v;
+    if (v >= 0 && v <= 6) g_msm_acc_variant = v;
 }
 
 // Batch-affine pairing rounds run before the XYZZ bucket accumulation

@@ -353,10 +353,11 @@ RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out,
                          uint64_t scratch_bytes, h2b_stream_t stream);
 /* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
-/* Form of the MSM bucket-accumulation kernel: 0 = lazy R = 2^261 limbs with one-step carries (default;
- * window-table MSMs always use it); normalised R = 2^256 limbs with 5 = two field products per
- * out-of-line call, 1 = all products inline, 2 = one product per call, 3 / 4 = one per call with 4 / 5
- * CTAs per SM.  Same results; tuning only. */
+/* Form of the MSM bucket-accumulation kernel: 6 = lazy R' = 2^260 limbs of 52 bits on the FP64 pipe
+ * (default; window-table MSMs use it too); 0 = lazy R = 2^261 limbs of 29 bits with one-step carries
+ * (window-table MSMs use it for every choice but 6); normalised R = 2^256 limbs with 5 = two field
+ * products per out-of-line call, 1 = all products inline, 2 = one product per call, 3 / 4 = one per call
+ * with 4 / 5 CTAs per SM.  Same results; tuning only. */
 void h2b_msm_set_accumulate_variant(int variant);
 /* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
  * MSM workspace-size queries depend on it (set it before sizing scratch). */

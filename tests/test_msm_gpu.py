@@ -177,3 +177,48 @@ def test_msm_pairing_rounds(h2b, orc, cuda, srs_small, rounds):
                 assert_limbs_equal(got, want, f"pairing rounds {rounds}")
     finally:
         L.h2b_msm_set_pair_rounds(0)
+
+
+@pytest.mark.parametrize("variant", [0, 5, 6])
+def test_msm_accumulate_forms(h2b, orc, cuda, srs_small, variant):
+    """Every bucket-accumulation form (h2b_msm_set_accumulate_variant: 0 =
+    29-bit lazy R = 2^261, 5 = normalised R = 2^256, 6 = FP64 lazy R' =
+    2^260) gives the oracle's bytes on the edge families: zero scalars and
+    infinity bases, equal points in a bucket (the doubling branch), P + (-P)
+    (infinity inside a bucket), a dense constant and the witness-like mix;
+    and over a window table."""
+    f = h2b.fields
+    _, srs = srs_small
+    n = 4096
+    L = h2b.lib()
+    L.h2b_msm_set_accumulate_variant(variant)
+    try:
+        cases = []
+        sc = orc.chacha_fr(190 + variant, n)
+        b = srs[:n].copy()
+        sc[::5] = 0
+        b[::7] = 0
+        cases.append((sc, b))
+        b2 = srs[:n].copy()
+        b2[1::2] = b2[0::2]
+        cases.append((np.tile(f.fr_mont_limbs([5, 5]), (n // 2, 1)), b2))
+        cases.append((np.tile(f.fr_mont_limbs([5, f.R_MOD - 5]), (n // 2, 1)), b2))
+        sc4 = orc.chacha_fr(195, n)
+        sc4[: n // 2] = f.fr_mont_limbs([0x022B5F6A3C1D0E8F94D049BB133111EBBF58476D1CE4E5B99E3779B97F4A7C15])
+        cases.append((sc4, srs[:n]))
+        mix = f.fr_mont_limbs([v % f.R_MOD for v in ([0x1F2E3D4C5B6A7988 * (i + 1) for i in range(n // 4)] +
+                                                     [i % 2 for i in range(n // 4)] +
+                                                     [f.limbs_to_ints(orc.chacha_fr(196, n // 2))[i] for i in
+                                                      range(n // 2)])])
+        cases.append((mix, srs[:n]))
+        for sc_, b_ in cases:
+            want = orc.msm(sc_, b_)
+            for got in all_variants(h2b, sc_, b_):
+                assert_limbs_equal(got, want, f"accumulate variant {variant}")
+        # over a window table (tables use the lazy forms 0 or 6)
+        table = h2b.msm_table_precompute(h2b.to_dev(srs[:n]), n)
+        out = h2b.dev_empty(96)
+        h2b.msm_device_table(h2b.to_dev(mix), table, n, out, n)
+        assert_limbs_equal(h2b.to_host(out, (12,)), orc.msm(mix, srs[:n]), f"table, variant {variant}")
+    finally:
+        L.h2b_msm_set_accumulate_variant(0)
