@@ -413,10 +413,10 @@ H2B_DEV G1XyzzD xyzzd_dbl_affine(const FqD& qx, const FqD& qy)
 
 // madd-2008-s: acc += (qx, qy), q affine and not infinity.  PP == 0 mod p
 // exactly when P is, so the equal-x test reads the square.
-H2B_DEV void xyzzd_madd(G1XyzzD& acc, const FqD& qx, const FqD& qy, const FqD& one)
+H2B_DEV void xyzzd_madd(G1XyzzD& acc, const FqD& qx, const FqD& qy)
 {
     if (is_inf(acc)) {
-        acc.X = qx; acc.Y = qy; acc.ZZ = one; acc.ZZZ = one;
+        acc.X = qx; acc.Y = qy; acc.ZZ = fd_one<FqCfg>(); acc.ZZZ = fd_one<FqCfg>();
         return;
     }
     const Fd2<FqCfg> us = fd_mul2(qx, acc.ZZ, qy, acc.ZZZ);   // U2 < 1.015p, S2 < 1.03p
@@ -440,8 +440,9 @@ H2B_DEV void xyzzd_madd(G1XyzzD& acc, const FqD& qx, const FqD& qy, const FqD& o
 
 // Canonical memory image of the accumulator (infinity stays ZZ = 0): four
 // products by 2^256 mod p (each below 1.07p), then conditional subtractions.
-static __device__ __noinline__ void st_xyzzd(G1Xyzz* dst, const G1XyzzD p, const FqD r256)
+static __device__ __noinline__ void st_xyzzd(G1Xyzz* dst, const G1XyzzD p)
 {
+    const FqD r256 = fd_r256<FqCfg>();
     const Fd2<FqCfg> a = fd_mul2(p.X, r256, p.Y, r256);
     const Fd2<FqCfg> b = fd_mul2(p.ZZ, r256, p.ZZZ, r256);
     G1Xyzz r;

@@ -625,9 +625,16 @@ namespace f64 {
 template <class C>
 H2B_DEV void mont52(const double (&A)[5], const double (&B)[5], uint64_t (&l)[5])
 {
-    uint64_t col[10];
-#pragma unroll
-    for (int k = 0; k < 10; k++) col[k] = 0 - bias(k);
+    // every constant below is a constexpr variable, so it is folded at
+    // compile time (a constexpr call in a plain expression may be evaluated
+    // on the device)
+    constexpr uint64_t B0 = bias(0), B1 = bias(1), B2 = bias(2), B3 = bias(3), B4 = bias(4);
+    constexpr uint64_t B5 = bias(5), B6 = bias(6), B7 = bias(7), B8 = bias(8), B9 = bias(9);
+    constexpr double P0 = (double)p52<C>(0), P1 = (double)p52<C>(1), P2 = (double)p52<C>(2);
+    constexpr double P3 = (double)p52<C>(3), P4 = (double)p52<C>(4);
+    constexpr uint64_t NP = C::NP52;
+    const double PD[5] = {P0, P1, P2, P3, P4};
+    uint64_t col[10] = {0 - B0, 0 - B1, 0 - B2, 0 - B3, 0 - B4, 0 - B5, 0 - B6, 0 - B7, 0 - B8, 0 - B9};
 #pragma unroll
     for (int i = 0; i < 5; i++) {
         uint64_t hp = 0;
@@ -644,11 +651,11 @@ H2B_DEV void mont52(const double (&A)[5], const double (&B)[5], uint64_t (&l)[5]
     for (int i = 0; i < 5; i++) {
         const uint64_t t = col[i];
         const uint64_t tl = t & M52;
-        const double qd = u52d((tl * C::NP52) & M52);
-        uint64_t hp = dbits(__fma_rz(qd, (double)p52<C>(0), C104)) + (t >> 52) + (tl != 0 ? 1u : 0u);
+        const double qd = u52d((tl * NP) & M52);
+        uint64_t hp = dbits(__fma_rz(qd, PD[0], C104)) + (t >> 52) + (tl != 0 ? 1u : 0u);
 #pragma unroll
         for (int j = 1; j < 5; j++) {
-            const double pj = (double)p52<C>(j);
+            const double pj = PD[j];
             const double h = __fma_rz(qd, pj, C104);
             const double lo = __fma_rn(qd, pj, __dsub_rn(C104_52, h));
             col[i + j] = col[i + j] + (dbits(lo) + hp);

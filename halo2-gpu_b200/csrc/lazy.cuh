@@ -81,12 +81,23 @@ H2B_DEV Fz<C> fz_add(const Fz<C>& a, const Fz<C>& b)
 // almost-normalised b; the top one is when b <= K p - 3 * 2^232 in value
 // (kp29(K, 8) >= K p / 2^232 - 1 and b's top limb <= b / 2^232), which holds
 // for every b below (K - 0.001) p.
+// the borrow-adjusted limbs as compile-time constants (constexpr variables,
+// so the loop in kp29 is never evaluated on the device)
+template <class C, int K>
+struct KP29 {
+    static constexpr uint32_t l0 = kp29_adj<C>(K, 0), l1 = kp29_adj<C>(K, 1), l2 = kp29_adj<C>(K, 2),
+                              l3 = kp29_adj<C>(K, 3), l4 = kp29_adj<C>(K, 4), l5 = kp29_adj<C>(K, 5),
+                              l6 = kp29_adj<C>(K, 6), l7 = kp29_adj<C>(K, 7), l8 = kp29_adj<C>(K, 8);
+};
+
 template <class C, int K>
 H2B_DEV Fz<C> fz_sub(const Fz<C>& a, const Fz<C>& b)
 {
+    using L = KP29<C, K>;
+    const uint32_t kp[9] = {L::l0, L::l1, L::l2, L::l3, L::l4, L::l5, L::l6, L::l7, L::l8};
     uint32_t d[9];
 #pragma unroll
-    for (int i = 0; i < 9; i++) d[i] = a.l[i] + kp29_adj<C>(K, i) - b.l[i];
+    for (int i = 0; i < 9; i++) d[i] = a.l[i] + kp[i] - b.l[i];
     return fz_carry<C>(d);
 }
 

@@ -42,6 +42,79 @@ __host__ __device__ constexpr uint64_t kp52(int K, int i)
     return i < 4 ? (t & f64::M52) : t;
 }
 
+// word w of R mod p = 2^256 mod p (the Montgomery one)
+template <class C>
+__host__ __device__ constexpr uint32_t oword(int w)
+{
+    return w == 0 ? C::O0 : w == 1 ? C::O1 : w == 2 ? C::O2 : w == 3 ? C::O3 : w == 4 ? C::O4
+         : w == 5 ? C::O5 : w == 6 ? C::O6 : C::O7;
+}
+
+// limb i of 2^(256 + s) mod p in the 52-bit grid, s in 0..4 (compile-time:
+// 2^s (2^256 mod p) reduced by repeated subtraction of p)
+template <class C>
+__host__ __device__ constexpr uint64_t r2x52(int s, int i)
+{
+    uint64_t x[5] = {0, 0, 0, 0, 0};
+    for (int k = 0; k < 5; k++) {
+        uint64_t r = 0;
+        for (int w = 0; w < 8; w++) {
+            const int off = 32 * w + s - 52 * k;
+            if (off >= 0 && off < 52) r |= (uint64_t)oword<C>(w) << off;
+            else if (off < 0 && off > -32) r |= (uint64_t)(oword<C>(w) >> (-off));
+        }
+        x[k] = k < 4 ? (r & f64::M52) : r;
+    }
+    for (int it = 0; it < 32; it++) {
+        bool ge = true;
+        for (int k = 4; k >= 0; k--) {
+            if (x[k] != f64::p52<C>(k)) {
+                ge = x[k] > f64::p52<C>(k);
+                break;
+            }
+        }
+        if (!ge) break;
+        int64_t borrow = 0;
+        for (int k = 0; k < 5; k++) {
+            int64_t d = (int64_t)x[k] - (int64_t)f64::p52<C>(k) - borrow;
+            borrow = d < 0 ? 1 : 0;
+            x[k] = (uint64_t)(d + (borrow && k < 4 ? (int64_t)1 << 52 : 0));
+        }
+    }
+    return x[i];
+}
+
+// constants of the form as immediates: 1 (= 2^260 mod p) and the store
+// factor 2^256 mod p
+template <class C>
+H2B_DEV Fd<C> fd_one()
+{
+    constexpr uint64_t a0 = r2x52<C>(4, 0), a1 = r2x52<C>(4, 1), a2 = r2x52<C>(4, 2), a3 = r2x52<C>(4, 3),
+                       a4 = r2x52<C>(4, 4);
+    return Fd<C>{{a0, a1, a2, a3, a4}};
+}
+
+template <class C>
+H2B_DEV Fd<C> fd_r256()
+{
+    constexpr uint64_t a0 = r2x52<C>(0, 0), a1 = r2x52<C>(0, 1), a2 = r2x52<C>(0, 2), a3 = r2x52<C>(0, 3),
+                       a4 = r2x52<C>(0, 4);
+    return Fd<C>{{a0, a1, a2, a3, a4}};
+}
+
+// the limbs of p and of K p as compile-time constants
+template <class C>
+struct P52 {
+    static constexpr uint64_t l0 = f64::p52<C>(0), l1 = f64::p52<C>(1), l2 = f64::p52<C>(2),
+                              l3 = f64::p52<C>(3), l4 = f64::p52<C>(4);
+};
+template <class C, int K>
+struct KP52 {
+    static constexpr int64_t l0 = (int64_t)kp52<C>(K, 0), l1 = (int64_t)kp52<C>(K, 1),
+                             l2 = (int64_t)kp52<C>(K, 2), l3 = (int64_t)kp52<C>(K, 3),
+                             l4 = (int64_t)kp52<C>(K, 4);
+};
+
 // signed limb sums -> normalised limbs (serial carry; the value is >= 0)
 template <class C>
 H2B_DEV Fd<C> fd_norm(const int64_t (&d)[5])
@@ -71,9 +144,11 @@ H2B_DEV Fd<C> fd_add(const Fd<C>& a, const Fd<C>& b)
 template <class C, int K>
 H2B_DEV Fd<C> fd_sub(const Fd<C>& a, const Fd<C>& b)
 {
+    using L = KP52<C, K>;
+    const int64_t kp[5] = {L::l0, L::l1, L::l2, L::l3, L::l4};
     int64_t d[5];
 #pragma unroll
-    for (int i = 0; i < 5; i++) d[i] = (int64_t)a.l[i] - (int64_t)b.l[i] + (int64_t)kp52<C>(K, i);
+    for (int i = 0; i < 5; i++) d[i] = (int64_t)a.l[i] - (int64_t)b.l[i] + kp[i];
     return fd_norm<C>(d);
 }
 
@@ -134,11 +209,13 @@ H2B_DEV bool fd_is_zero(const Fd<C>& a)
 template <class C>
 H2B_DEV bool fd_is_zero_mod(const Fd<C>& a)
 {
+    using L = P52<C>;
+    const uint64_t pl[5] = {L::l0, L::l1, L::l2, L::l3, L::l4};
     uint64_t z = 0, e = 0;
 #pragma unroll
     for (int i = 0; i < 5; i++) {
         z |= a.l[i];
-        e |= a.l[i] ^ f64::p52<C>(i);
+        e |= a.l[i] ^ pl[i];
     }
     return z == 0 || e == 0;
 }
@@ -161,11 +238,13 @@ H2B_DEV Fd<C> fd_from_words(const Fp<C>& a)
 template <class C>
 H2B_DEV Fd<C> fd_from_r261(const Fp<C>& v)
 {
+    using L = P52<C>;
+    const uint64_t pl[5] = {L::l0, L::l1, L::l2, L::l3, L::l4};
     Fd<C> t = fd_from_words<C>(v);
     const uint64_t m = 0 - (t.l[0] & 1u);
     int64_t d[5];
 #pragma unroll
-    for (int i = 0; i < 5; i++) d[i] = (int64_t)(t.l[i] + (f64::p52<C>(i) & m));
+    for (int i = 0; i < 5; i++) d[i] = (int64_t)(t.l[i] + (pl[i] & m));
     t = fd_norm<C>(d);
     Fd<C> r;
 #pragma unroll

@@ -426,8 +426,6 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
                                                              uint64_t phi_off, G1Xyzz* __restrict__ buckets,
                                                              G1Xyzz* __restrict__ heads)
 {
-    const FqD one = fd_from_r261(to_r261(Fq::one()));            // 1 in the form (2^260 mod p)
-    const FqD r256 = fd_from_words(Fq::one());                    // 2^256 mod p, for the stores
     const uint32_t M = offsets[NB];
     const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
@@ -445,7 +443,7 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
         G1XyzzD acc = xyzzd_inf();
         for (uint32_t e = start; e < end; e++) {
             if (e == next) {
-                st_xyzzd(head ? &heads[t] : &buckets[b], acc, r256);
+                st_xyzzd(head ? &heads[t] : &buckets[b], acc);
                 acc = xyzzd_inf();
                 head = false;
                 do { b++; next = offsets[b + 1]; } while (next == e);
@@ -458,9 +456,9 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
             const FqD qx = fd_from_r261(P.x);                              // < p
             FqD qy = fd_from_r261(P.y);                                    // < p
             if (ent & SIGN_BIT) qy = fd_sub<FqCfg, 2>(fd_zero<FqCfg>(), qy);  // 2p - y < 2p
-            xyzzd_madd(acc, qx, qy, one);
+            xyzzd_madd(acc, qx, qy);
         }
-        st_xyzzd(head ? &heads[t] : &buckets[b], acc, r256);
+        st_xyzzd(head ? &heads[t] : &buckets[b], acc);
     }
 }
 

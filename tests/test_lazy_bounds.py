@@ -1,10 +1,12 @@
-"""The value bounds behind the lazy accumulation form (csrc/lazy.cuh,
-csrc/curve.cuh xyzzz_madd / xyzzz_dbl_affine), re-derived with exact
-rational arithmetic: every subtraction a - b + K p must see b below
-(K - 0.001) p, every product input must keep the 64-bit column sums exact,
-and the accumulator bounds (X < 5.39p, Y < 3.34p, ZZ, ZZZ < 2p) must be
-stable from one addition to the next.  Also checks the borrow-adjusted K p
-limbs the kernels add."""
+"""The value bounds behind the lazy accumulation forms (csrc/lazy.cuh with
+csrc/curve.cuh xyzzz_madd / xyzzz_dbl_affine, R = 2^261; csrc/lazy64.cuh with
+xyzzd_madd / xyzzd_dbl_affine, R' = 2^260), re-derived with exact rational
+arithmetic: every subtraction a - b + K p must see b below (K - 0.001) p,
+every product input must keep the column sums exact, and the accumulator
+bounds (R = 2^261: X < 5.39p, Y < 3.34p, ZZ, ZZZ < 2p; R' = 2^260: X < 5.4p,
+Y < 3.45p, ZZ, ZZZ < 1.2p) must be stable from one addition to the next.
+Also checks the borrow-adjusted K p limbs of the 29-bit form and the K p
+limbs of the 52-bit form."""
 from fractions import Fraction as Q
 
 P = 0x30644E72E131A029B85045B68181585D97816A916871CA8D3C208C16D87CFD47
@@ -12,8 +14,12 @@ R = 1 << 261
 EPS = Q(P, R)                   # product of a p and b p is below (1 + EPS a b) p
 
 
+EPS_260 = Q(P, 1 << 260)        # the FP64 form's R'
+_eps = [EPS]
+
+
 def mul(a, b):
-    return 1 + EPS * a * b
+    return 1 + _eps[0] * a * b
 
 
 def sub(a, b, K):
@@ -94,3 +100,36 @@ def test_column_sums_fit_64_bits():
     # squares use doubled limbs (2 a_j < 2^30.1)
     assert 5 * lim * (2 * lim) + lim * lim + 9 * ((1 << 29) - 1) ** 2 + (1 << 35) < 1 << 64
     assert _p29(8) < (1 << 29)
+
+
+def test_fp64_form_bounds_are_stable():
+    _eps[0] = EPS_260
+    try:
+        qx, qy = Q(1), Q(2)              # canonical (halved from the stored form); negated 2p - y
+        B = (Q(54, 10), Q(345, 100), Q(12, 10), Q(12, 10))
+        X3, Y3, ZZ3, ZZZ3, inner = madd(*B, qx, qy)
+        assert all(a <= b for a, b in zip((X3, Y3, ZZ3, ZZZ3), B))
+        assert qx <= B[0] and qy <= B[1]  # the infinity start (acc = q, ZZ = ZZZ = 1)
+        assert max(inner) < Q(72, 10)     # largest product input, below 2^257 / p
+        assert max(inner) * P < 1 << 257
+        dX, dY, dZZ, dZZZ = dbl_affine(qx, qy)
+        assert dX <= B[0] and dY <= B[1] and dZZ <= B[2] and dZZZ <= B[3]
+        assert mul(B[0], 1) < 2          # the store product by 2^256 mod p
+    finally:
+        _eps[0] = EPS
+
+
+def _p52(i):
+    return (P >> (52 * i)) & ((1 << 52) - 1)
+
+
+def test_fp64_form_limbs():
+    # K p in the 52-bit grid (kp52): normalised, the top limb holding the rest
+    for K in (2, 3, 4, 5, 6):
+        limbs = [((K * P) >> (52 * i)) & ((1 << 52) - 1) if i < 4 else (K * P) >> 208 for i in range(5)]
+        assert sum(l << (52 * i) for i, l in enumerate(limbs)) == K * P
+        assert limbs[4] < 1 << 52
+    # every lazy value stays below 2^257, so its top limb is below 2^49 and
+    # the signed limb sums of a - b + K p stay far inside 64 bits
+    assert 8 * P < 1 << 257
+    assert sum(_p52(i) << (52 * i) for i in range(5)) == P
