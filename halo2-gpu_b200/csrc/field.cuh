@@ -698,6 +698,60 @@ H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
     return r;
 }
 
+// The 29-bit limb form (Fl: value below 2p, R = 2^256) through the FP64
+// core: the limbs are re-sliced into 52-bit limbs (one operand as 16 a, still
+// below 2^260), and the result, below (1 + 64 p / 2^260) p < 1.76 p, is
+// sliced back, so it keeps the Fl invariant.  Its dependent chain is five
+// reduction digits instead of nine, which is what the single-warp tails
+// (window doubling chain, bucket-reduction Horner steps) wait on.
+namespace f64 {
+// bits [S, S + 52) of sum l[k] 2^(29 k) (S < 0: zeros below bit 0)
+template <int S>
+H2B_DEV uint64_t bits52_of29(const uint32_t (&l)[9])
+{
+    uint64_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const int off = 29 * k - S;
+        if (off >= 0 && off < 52) r |= (uint64_t)l[k] << off;
+        else if (off < 0 && off > -29) r |= (uint64_t)(l[k] >> (-off));
+    }
+    return r & M52;
+}
+
+// bits [S, S + 29) of sum l[i] 2^(52 i)
+template <int S>
+H2B_DEV uint32_t bits29_of52(const uint64_t (&l)[5])
+{
+    uint64_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        const int off = 52 * i - S;
+        if (off >= 0 && off < 29) r |= l[i] << off;
+        else if (off < 0 && off > -52) r |= l[i] >> (-off);
+    }
+    return (uint32_t)r & M29;
+}
+}  // namespace f64
+
+template <class C>
+H2B_DEV Fl<C> mul_f64_l(const Fl<C>& a, const Fl<C>& b)
+{
+    using namespace f64;
+    double A[5], B[5];
+    A[0] = u52d(bits52_of29<-4>(a.l)); A[1] = u52d(bits52_of29<48>(a.l)); A[2] = u52d(bits52_of29<100>(a.l));
+    A[3] = u52d(bits52_of29<152>(a.l)); A[4] = u52d(bits52_of29<204>(a.l));
+    B[0] = u52d(bits52_of29<0>(b.l)); B[1] = u52d(bits52_of29<52>(b.l)); B[2] = u52d(bits52_of29<104>(b.l));
+    B[3] = u52d(bits52_of29<156>(b.l)); B[4] = u52d(bits52_of29<208>(b.l));
+    uint64_t l[5];
+    mont52<C>(A, B, l);
+    Fl<C> r;
+    r.l[0] = bits29_of52<0>(l); r.l[1] = bits29_of52<29>(l); r.l[2] = bits29_of52<58>(l);
+    r.l[3] = bits29_of52<87>(l); r.l[4] = bits29_of52<116>(l); r.l[5] = bits29_of52<145>(l);
+    r.l[6] = bits29_of52<174>(l); r.l[7] = bits29_of52<203>(l); r.l[8] = bits29_of52<232>(l);
+    return r;
+}
+
 // ---- Fl arithmetic kept in limb form (values < 2p, limbs < 2^29) ---------
 
 // word w of 2m (8 x 32 grid) and its limb i in the 29-bit grid
@@ -795,6 +849,11 @@ H2B_DEV Fl<C> fl_zero()
 // about a fifth of a product (measured: 42 G/s out of line against 54.7 G/s
 // inline), so the paired forms compute two independent products per call,
 // which also gives the scheduler two dependency chains to interleave.
+// H2B_FL_F64 selects the FP64 core for the latency-oriented forms used by
+// the single-warp tails (fl_mul_ilp / fl_sqr_ilp).
+#ifndef H2B_FL_F64
+#define H2B_FL_F64 1
+#endif
 template <class C>
 __device__ __noinline__ Fl<C> fl_mul(const Fl<C> a, const Fl<C> b)
 {
@@ -811,13 +870,21 @@ __device__ __noinline__ Fl<C> fl_sqr(const Fl<C> a)
 template <class C>
 __device__ __noinline__ Fl<C> fl_mul_ilp(const Fl<C> a, const Fl<C> b)
 {
+#if H2B_FL_F64
+    return mul_f64_l<C>(a, b);
+#else
     return mul29_ilp<C>(a, b);
+#endif
 }
 
 template <class C>
 __device__ __noinline__ Fl<C> fl_sqr_ilp(const Fl<C> a)
 {
+#if H2B_FL_F64
+    return mul_f64_l<C>(a, a);
+#else
     return sqr29_ilp<C>(a);
+#endif
 }
 
 template <class C>
@@ -843,10 +910,10 @@ __device__ __noinline__ Fl2<C> fl_sqr2(const Fl<C> a0, const Fl<C> a1)
     return r;
 }
 
-// The product behind operator* is the 29-bit column form (measured on B200:
-// 54.7 G products/s with the 8 x 32 conversions, against 41.5 G for the
-// mad.lo/mad.hi CIOS above and 46.9 G for its mad.wide variant).  One
-// out-of-line body per field: kernels that chain many products (curve
+// The product behind operator* is the FP64 form (mont_mul_f64; the 29-bit
+// column form measured 54.7 G products/s with the 8 x 32 conversions in a
+// four-chain probe, against 41.5 G for the mad.lo/mad.hi CIOS above and
+// 46.9 G for its mad.wide variant).  One out-of-line body per field: kernels that chain many products (curve
 // formulas, the quotient interpreter) otherwise inline hundreds of
 // instructions per product and starve on instruction fetch.  H2B_INLINE_MUL=1
 // restores full inlining for kernels that want it.
