@@ -568,6 +568,8 @@ def main():
     ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the built-in MSM window / chunk and NTT pass settings (no autotuner)")
     args = ap.parse_args()
     if args.case == "serve":
         import torch
@@ -602,6 +604,16 @@ def main():
     dom = f.EvaluationDomain(5, K_NTT)
     assert dom.extended_k == K_EXT
     d_srs = h2b.srs_device(0x5EED + 0x1000 * rank, n_msm)
+    # per-(op, k) settings from the autotuner's cache for this GPU and build
+    # (tuned here when absent), before any scratch is sized
+    tuning = None
+    if not args.no_tune:
+        at = importlib.import_module("halo2_gpu_b200.autotune")
+        r = at.autotune(h2b, msm_ks=(14, 16, 18, 20, 22), ntt_ks=tuple(range(14, 25)), d_bases=d_srs)
+        tuning = {"cache": "tuned" if r["tuned"] else "cached", "key": r["key"],
+                  "msm": {k: {x: e[x] for x in ("window", "chunk", "auto_window", "ms", "auto_ms")}
+                          for k, e in r["msm"].items()},
+                  "ntt": {k: {x: e[x] for x in ("stages", "auto_stages", "ms", "auto_ms")} for k, e in r["ntt"].items()}}
     d_sc = h2b.random_fr_device(n_msm, 1000 + rank, 1)
     d_ntt_in = h2b.random_fr_device(n_ntt, 2000 + rank, 0)
     d_ext = h2b.dev_empty(32 * n_ext)
@@ -719,6 +731,7 @@ def main():
                 "product_frac_passes": ntt_modmul / (ntt_kernel_ms * 1e-3) / probe["h2b_probe_modmul"]},
         "batch_invert": {"ms": bi_ms, "elements_per_s": n_bi / (bi_ms * 1e-3), "apply_kernel_ms": bi_kernel_ms},
         "roofline": roofline, "product_roofline": products, "clocks": clk, "gpu_launches": launches,
+        "tuning": tuning,
     }
 
     # ---- end to end through the reference-facing C ABI with host buffers ----

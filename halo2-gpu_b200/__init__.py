@@ -176,6 +176,9 @@ _SIGS = {
     "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_msm_window_bits": (ctypes.c_int, [_u64]),
     "h2b_batch_invert_noalloc": (RustError, [_vp, _u32, _u64, _vp]),
+    "h2b_tune_set": (_i32, [_u32, _u32, _i32]),
+    "h2b_tune_get": (_i32, [_u32, _u32]),
+    "h2b_tune_clear": (None, []),
 }
 
 PROF_MSM_ACCUMULATE, PROF_MSM_TOTAL, PROF_NTT_PASSES, PROF_BATCH_INVERT, PROF_QUOTIENT, PROF_PERMUTE_SORT = range(6)

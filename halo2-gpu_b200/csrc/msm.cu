@@ -59,6 +59,7 @@ constexpr int PR_E = 8;            // pairing rounds: input entries per thread (
 static uint64_t pr_ctas(uint64_t entries) { return (entries + (uint64_t)PR_T * PR_E - 1) / ((uint64_t)PR_T * PR_E); }
 
 uint64_t fq_batch_invert_scratch(uint64_t n);
+int tune_value(int param, int log_n);  // tune.cu
 RustError fq_batch_invert(Fq* d, uint64_t n, void* scratch, uint64_t scratch_bytes, cudaStream_t st);
 
 void msm_set_pair_rounds(int rounds)
@@ -73,11 +74,23 @@ void msm_set_tuning(int window_bits, int chunk)
     g_msm_chunk_override = chunk;
 }
 
-static int choose_c(uint64_t n)
+static int floor_log2(uint64_t n)
 {
     int lg = 0;
     while ((1ull << (lg + 1)) <= n) lg++;
+    return lg;
+}
+
+// `plain`: an MSM over plain bases, whose window width may come from the
+// per-size tuning table; a window table's width is fixed when it is built.
+static int choose_c(uint64_t n, bool plain = false)
+{
+    const int lg = floor_log2(n);
     if (g_msm_window_override >= 4 && g_msm_window_override <= 20) return g_msm_window_override;
+    if (plain) {
+        const int tuned = tune_value(0, lg);
+        if (tuned) return tuned;
+    }
     if (lg >= 21) return 16;
     if (lg >= 19) return 15;
     if (lg >= 17) return 13;
@@ -112,7 +125,11 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1
     // not drop where buckets are long: on the 64-job batch (16 streams) a
     // fixed K = 32 took 133 ms over a window table against 85 ms at 128.
     const uint64_t k_fit = p.max_entries / std::max<uint64_t>(1, ACC_TARGET_CHUNKS / std::max(concurrent, 1u));
+    // A tuned chunk size applies to an MSM that runs alone (batched MSMs keep
+    // the formula, which accounts for the MSMs running beside them).
+    const int tuned_k = concurrent <= 1 ? tune_value(1, floor_log2(n)) : 0;
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override
+          : tuned_k > 0            ? (uint32_t)tuned_k
                                    : (uint32_t)std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
     // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
     p.R = tn ? 0 : g_msm_pair_rounds;
@@ -132,13 +149,13 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1
     return p;
 }
 
-MsmPlan msm_plan(uint64_t n) { return plan_core(n, choose_c(n), 0); }
+MsmPlan msm_plan(uint64_t n) { return plan_core(n, choose_c(n, true), 0); }
 
 MsmPlan msm_plan_table(uint64_t n, uint64_t tn) { return plan_core(n, choose_c(tn), tn); }
 
 MsmPlan msm_plan_shared(uint64_t n, uint64_t tn, uint32_t concurrent)
 {
-    return tn ? plan_core(n, choose_c(tn), tn, concurrent) : plan_core(n, choose_c(n), 0, concurrent);
+    return tn ? plan_core(n, choose_c(tn), tn, concurrent) : plan_core(n, choose_c(n, true), 0, concurrent);
 }
 
 void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host)
@@ -1128,10 +1145,14 @@ __global__ void k_table_affine(const G1Xyzz* __restrict__ tmp, const Fq* __restr
     }
 }
 
+// Layout of a window table for tn bases: the untuned window width, which
+// msm_plan_table also uses, so tuning never changes a table's meaning.
+static MsmPlan table_layout_plan(uint64_t tn) { return plan_core(tn, choose_c(tn), 0); }
+
 // Entries encode the table point as 2 (w tn + i) + half in 31 bits.
 static bool table_fits(uint64_t tn)
 {
-    const MsmPlan p = msm_plan(tn);
+    const MsmPlan p = table_layout_plan(tn);
     return tn > 0 && tn <= MSM_MAX_LENGTH && 2 * (uint64_t)p.W * tn < (1ull << 31);
 }
 
@@ -1141,7 +1162,7 @@ static bool table_fits(uint64_t tn)
 extern "C" uint64_t h2b_msm_table_points(uint64_t n)
 {
     if (!table_fits(n)) return 0;
-    return 2 * (uint64_t)msm_plan(n).W * n;
+    return 2 * (uint64_t)table_layout_plan(n).W * n;
 }
 
 extern "C" uint64_t h2b_msm_table_precompute_workspace_size(uint64_t n)
@@ -1159,7 +1180,7 @@ extern "C" RustError h2b_msm_table_precompute(const void* d_bases, uint64_t n, v
                                               uint64_t scratch_bytes, cudaStream_t stream)
 {
     if (!table_fits(n)) return err(cudaErrorInvalidValue, "h2b_msm_table_precompute: n out of range");
-    const MsmPlan p = msm_plan(n);
+    const MsmPlan p = table_layout_plan(n);
     ScratchArena ar(scratch, scratch_bytes);
     G1Xyzz* tmp = ar.take_n<G1Xyzz>(n);
     Fq* den = ar.take_n<Fq>(n);

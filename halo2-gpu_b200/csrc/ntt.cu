@@ -296,6 +296,15 @@ __global__ void __launch_bounds__(NTT_THREADS, NTT_MIN_BLOCKS) k_ntt_pass(NttBat
 static int g_max_pass_stages = 9;  // tuned per k by ntt_set_pass_stages()
 
 int ntt_pass_stages() { return g_max_pass_stages; }
+int tune_value(int param, int log_n);  // tune.cu
+
+// Stages per pass for a transform of 2^logn points: the per-size tuning
+// table's entry when the autotuner set one, else the global setting.
+static int pass_stages_for(int logn)
+{
+    const int tuned = tune_value(2, logn);
+    return tuned ? tuned : g_max_pass_stages;
+}
 void ntt_set_pass_stages(int b)
 {
     if (b >= 1 && b <= 10) g_max_pass_stages = b;
@@ -308,7 +317,8 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
 {
     if (logn - first <= 0) return ok();
     int todo = logn - first;
-    int passes = (todo + g_max_pass_stages - 1) / g_max_pass_stages;
+    const int max_stages = pass_stages_for(logn);
+    int passes = (todo + max_stages - 1) / max_stages;
     int base = todo / passes, extra = todo % passes;
     int s0 = first;
     prof_begin(PROF_NTT_PASSES, st);
