@@ -90,7 +90,16 @@ static int choose_c(uint64_t n, bool plain = false)
     if (plain) {
         const int tuned = tune_value(0, lg);
         if (tuned) return tuned;
+        // plain-base widths from autotuner runs on B200 (witness-like scalar
+        // mix): 16 bits from 2^20 (5.40 -> 4.36 ms with the chunk rule below),
+        // 13 bits from 2^14 (2^16: 1.79 -> 1.45 ms)
+        if (lg >= 20) return 16;
+        if (lg >= 19) return 15;
+        if (lg >= 14) return 13;
+        if (lg >= 10) return 10;
+        return 7;
     }
+    // window tables keep the widths their layout was measured with
     if (lg >= 21) return 16;
     if (lg >= 19) return 15;
     if (lg >= 17) return 13;
@@ -127,10 +136,16 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1
     const uint64_t k_fit = p.max_entries / std::max<uint64_t>(1, ACC_TARGET_CHUNKS / std::max(concurrent, 1u));
     // A tuned chunk size applies to an MSM that runs alone (batched MSMs keep
     // the formula, which accounts for the MSMs running beside them).
+    // An MSM that runs alone takes half the fitted chunk, at most 64 (B200
+    // autotuner runs: 2^22 128 -> 64 entries 11.89 -> 11.45 ms; 2^20 at 16
+    // bits chose 32 entries): twice the chunks hide more of the
+    // accumulation's latency than the extra chunk heads cost the fixup.
     const int tuned_k = concurrent <= 1 ? tune_value(1, floor_log2(n)) : 0;
+    const uint64_t k_rule = concurrent <= 1 ? std::min<uint64_t>(64, std::max<uint64_t>(ACC_MIN_K, k_fit / 2))
+                                            : std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override
           : tuned_k > 0            ? (uint32_t)tuned_k
-                                   : (uint32_t)std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
+                                   : (uint32_t)k_rule;
     // pairing rounds: round r leaves at most cap[r-1]/2 + NB/2 entries
     p.R = tn ? 0 : g_msm_pair_rounds;
     p.cap[0] = p.max_entries;
