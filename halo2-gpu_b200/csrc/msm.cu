@@ -136,13 +136,17 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1
     const uint64_t k_fit = p.max_entries / std::max<uint64_t>(1, ACC_TARGET_CHUNKS / std::max(concurrent, 1u));
     // A tuned chunk size applies to an MSM that runs alone (batched MSMs keep
     // the formula, which accounts for the MSMs running beside them).
-    // An MSM that runs alone takes half the fitted chunk, at most 64 (B200
-    // autotuner runs: 2^22 128 -> 64 entries 11.89 -> 11.45 ms; 2^20 at 16
-    // bits chose 32 entries): twice the chunks hide more of the
-    // accumulation's latency than the extra chunk heads cost the fixup.
-    const int tuned_k = concurrent <= 1 ? tune_value(1, floor_log2(n)) : 0;
-    const uint64_t k_rule = concurrent <= 1 ? std::min<uint64_t>(64, std::max<uint64_t>(ACC_MIN_K, k_fit / 2))
-                                            : std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
+    // A plain-base MSM that runs alone takes half the fitted chunk, at most
+    // 64 (B200 autotuner runs: 2^22 128 -> 64 entries 11.89 -> 11.45 ms;
+    // 2^20 at 16 bits chose 32 entries): twice the chunks hide more of the
+    // accumulation's latency than the extra chunk heads cost the fixup.  Not
+    // over a window table: its single bucket set holds W times longer
+    // buckets, which at 64 entries span more than DENSE_LIMIT chunks and take
+    // the dense path (k = 22 prover-shaped proof 398 -> 438 ms).
+    const bool alone_plain = concurrent <= 1 && tn == 0;
+    const int tuned_k = alone_plain ? tune_value(1, floor_log2(n)) : 0;
+    const uint64_t k_rule = alone_plain ? std::min<uint64_t>(64, std::max<uint64_t>(ACC_MIN_K, k_fit / 2))
+                                        : std::min<uint64_t>(128, std::max<uint64_t>(ACC_MIN_K, k_fit));
     p.K = g_msm_chunk_override > 0 ? (uint32_t)g_msm_chunk_override
           : tuned_k > 0            ? (uint32_t)tuned_k
                                    : (uint32_t)k_rule;

@@ -5,8 +5,9 @@
 //
 // The autotuner (halo2-gpu_b200/autotune.py) times candidate settings for
 // each (parameter, log2 size) on the GPU it runs on and writes the winners
-// here; the MSM planner (msm.cu, plain MSMs only: a window table's layout is
-// fixed by the window width it was built with) and the NTT pass planner
+// here; the MSM planner (msm.cu, plain-base MSMs only: a window table's
+// layout is fixed by the window width it was built with, and its long
+// buckets want the chunk rule) and the NTT pass planner
 // (ntt.cu) read them.  0 means "automatic" (the built-in formula).  Every
 // setting gives the same results; only the time changes.  Workspace-size
 // queries depend on the MSM entries, so set them before sizing scratch.

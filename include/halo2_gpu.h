@@ -415,7 +415,7 @@ int h2b_ntt_get_pass_stages(void);
 /* Per-size tuning table written by the autotuner (no counterpart in the reference, whose MSM window width
  * and NTT stage split are fixed formulas: halo2_proofs/cuda/src/multiexp.cu:260-300,
  * halo2_proofs/cuda/include/kernel/ntt_combine.h:90-94).  param 0 = MSM window bits (10..16; plain-base
- * MSMs only), 1 = MSM sorted entries per accumulation chunk (8..512; MSMs that run alone), 2 = NTT radix-2
+ * MSMs only), 1 = MSM sorted entries per accumulation chunk (8..512; plain-base MSMs that run alone), 2 = NTT radix-2
  * stages per shared-memory pass (1..10), each for inputs of 2^log_n (floor of log2 for an MSM).  value 0 =
  * automatic.  Results never change, only times; MSM workspace sizes depend on entries 0 and 1, so set them
  * before sizing scratch.  h2b_tune_set returns 0, or -1 for an unknown param, log_n > 32 or a value out of
