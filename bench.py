@@ -376,10 +376,18 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
         torch.cuda.reset_peak_memory_stats()
         r = plain.serve([(0.0, k, 8 + k)])
         service[k] = (float(r["latency_s"][0]), torch.cuda.max_memory_allocated() / 1e9)
+    # the same proofs with the Fiat-Shamir transcript (commitments read back
+    # and absorbed before each challenge), alone
+    with P.Server(res, 1, budget, transcript=True) as plain_t:
+        service_t = {}
+        for k in ks:
+            plain_t.serve([(0.0, k, 7 + k)])
+            service_t[k] = float(plain_t.serve([(0.0, k, 8 + k)])["latency_s"][0])
     served.serve([(0.0, k, 9 + k) for k in ks for _ in range(slots)])   # untimed: every worker's pools warm
     mean_s = sum(w * service[k][0] for k, w in zip(ks, weights))
     out = {"requests": count, "slots": slots, "hbm_budget_GB": budget >> 30,
            "service_ms_alone": {str(k): round(v[0] * 1e3, 2) for k, v in service.items()},
+           "service_ms_alone_transcript": {str(k): round(v * 1e3, 2) for k, v in service_t.items()},
            "prove_k20": {"proofs_per_s": round(1.0 / service[20][0], 3), "ms": round(service[20][0] * 1e3, 2),
                          "hbm_peak_GB": round(service[20][1], 2)},
            "capacity_plain_per_s": round(1.0 / mean_s, 3), "loads": {}}

@@ -20,16 +20,23 @@ order:
   8. opening: SHPLONK over the committed polynomials at x and their
      rotations (shplonk.py), 2 commits.
 
-Challenges come from a seeded generator, not a transcript, and the witness
-does not satisfy the circuit, so the outputs are deterministic GPU work, not
-a proof: whole-proof parity needs the Rust transcript and serde.  What this
-measures is the served prover's device side: proofs/s and latency when
+The vanishing argument's random polynomial is committed with the grand
+products and opened at x.  Challenges come from a seeded generator, or, with
+`transcript=True`, from the Fiat-Shamir transcript (transcript.py: BLAKE2b,
+Challenge255) in the reference's order: the verifying key and the public
+instance rows, the advice commitments, theta, A' and S', beta and gamma, the
+grand products and the random polynomial, y, the h pieces, x, the
+evaluations, then SHPLONK's y, v, W, u, W'.  The witness is seeded random
+data that does not satisfy the circuit, so the outputs are deterministic GPU
+work, not a valid proof, and whole-proof parity needs the Rust crates.  What
+this measures is the served prover's device side: proofs/s and latency when
 requests of uneven k share one GPU.
 
 `Server` runs such requests with `slots` worker threads, each on its own
 stream (the GPU overlaps them), admitting a request when a slot is free and
 the HBM budget allows; `plain` runs them one at a time.
 """
+import hashlib
 import queue
 import threading
 import time
@@ -39,6 +46,9 @@ import numpy as np
 from . import fields as F
 from . import rules as R
 from . import shplonk
+from . import transcript as T
+
+NUM_PUBLIC = 8   # rows of the instance column that are public inputs (absorbed into the transcript)
 
 _torch = None
 
@@ -111,6 +121,24 @@ class Resident:
         return outs
 
 
+    def vk_repr(self, k, stream=None):
+        """One Fr scalar standing for the 2^k verifying key in the transcript:
+        BLAKE2b of its compressed fixed and permutation commitments, mod r
+        (halo2's `vk.hash_into` absorbs `vk.transcript_repr`, a BLAKE2b digest
+        of the pinned verifying key; this key has no pinned form, so its
+        commitments stand in).  Computed once per k."""
+        if not hasattr(self, "_vk_repr"):
+            self._vk_repr = {}
+        if k not in self._vk_repr:
+            outs = self.keygen(k, stream)
+            (stream if stream is not None else _t().cuda.current_stream()).synchronize()
+            h = hashlib.blake2b(digest_size=64, person=b"Halo2-Verify-Key")
+            for o in outs:
+                h.update(T.compress(T.commitment_to_affine(o.cpu().numpy().view(np.uint64))))
+            self._vk_repr[k] = int.from_bytes(h.digest(), "little") % F.R_MOD
+        return self._vk_repr[k]
+
+
 def _slice(t, i, n):
     """Elements [i n, (i + 1) n) of a device field vector."""
     return t[32 * n * i: 32 * n * (i + 1)]
@@ -119,8 +147,14 @@ def _slice(t, i, n):
 class ProofWorkload:
     """The device work of one proof of size 2^k (see the module docstring)."""
 
-    def __init__(self, res, k, seed):
-        self.res, self.k, self.seed = res, k, seed
+    def __init__(self, res, k, seed, transcript=False):
+        """transcript=False draws the challenges from a generator seeded with
+        `seed`; transcript=True runs the Fiat-Shamir transcript
+        (transcript.Blake2bWrite): every commitment is read back and absorbed
+        before the next challenge is squeezed, and `self.proof` holds the
+        proof bytes (commitments and evaluations in the order written)."""
+        self.res, self.k, self.seed, self.transcript = res, k, seed, transcript
+        self.proof = None
 
     def run(self, stream):
         """Issues everything on `stream` (the calling thread blocks only where
@@ -132,9 +166,27 @@ class ProofWorkload:
         pk = res.key(k)
         dom = pk["dom"]
         tn = 1 << res.kmax
-        rng = np.random.default_rng(seed)
-        chal = lambda: int(rng.integers(1, 1 << 62))  # noqa: E731
+        tr = T.Blake2bWrite() if self.transcript else None
+        if tr is None:
+            rng = np.random.default_rng(seed)
+            chal = lambda: int(rng.integers(1, 1 << 62))  # noqa: E731
+        else:
+            chal = tr.squeeze_challenge
+        drawn = []
+        self.challenges = drawn
+        _draw = chal
+
+        def chal():
+            drawn.append(_draw())
+            return drawn[-1]
         sc = lambda v: F.fr_mont_limbs([v % F.R_MOD])  # noqa: E731
+
+        def absorb(outs):
+            """Reads the phase's commitments back (waits for `stream`) and
+            writes them to the transcript."""
+            if tr is not None:
+                for o in outs:
+                    tr.write_point(T.commitment_to_affine(o.cpu().numpy().view(np.uint64)))
         with torch.cuda.stream(stream):
             commits, evals, pending = [], [], []
             probe = h2b.dev_empty(32)
@@ -152,14 +204,22 @@ class ProofWorkload:
                 jobs = h2b.msm_batch_jobs([p[0] for p in pending], [res.table] * len(pending),
                                           [p[1] for p in pending], [p[2] for p in pending], table_n=tn)
                 h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
+                outs = [p[1] for p in pending]
                 pending.clear()
+                absorb(outs)
 
             # 1-2. witness and advice commitments
             adv = [h2b.random_fr_device(n, seed * 64 + i, 1, stream) for i in range(4)]
             inst = h2b.random_fr_device(n, seed * 64 + 4, 0, stream)
+            if tr is not None:
+                # the verifying key (its commitments, as one scalar) and the public inputs
+                tr.common_scalar(res.vk_repr(k, stream))
+                for v in F.fr_from_mont_limbs(h2b.to_host(inst[: 32 * NUM_PUBLIC])):
+                    tr.common_scalar(int(v))
             for a in adv:
                 commit(a)
             flush()
+            theta = chal()
             # 3. lookup: the input takes values of the table; permute-sort, commit A', S'
             gen = torch.Generator(device="cuda")
             gen.manual_seed(seed)
@@ -170,7 +230,8 @@ class ProofWorkload:
             commit(pa)
             commit(ps)
             flush()
-            # 4. permutation grand products (2 sets of 2 columns), lookup grand product
+            # 4. permutation grand products (2 sets of 2 columns), lookup grand product,
+            #    and the vanishing argument's random polynomial
             beta, gamma = sc(chal()), sc(chal())
             d_beta, d_gamma = h2b.to_dev(beta, stream), h2b.to_dev(gamma, stream)
             d_delta = h2b.to_dev(F.fr_mont_limbs([F.DELTA]), stream)
@@ -190,7 +251,10 @@ class ProofWorkload:
             h2b.lookup_product_device(zl, pa, ps, lin, pk["table_col"], d_beta, d_gamma, n, stream=stream)
             h2b.grand_product_device(zl, d_one, n, stream=stream)
             commit(zl)
+            h_rand = h2b.random_fr_device(n, seed * 64 + 5, 0, stream)
+            commit(h_rand)
             flush()
+            y = chal()
             # 5. lagrange_to_coeff of the per-proof polynomials
             lag = adv + [inst] + zs + [zl, pa, ps, lin]
             coef = [h2b.dev_empty(32 * n) for _ in lag]
@@ -199,7 +263,6 @@ class ProofWorkload:
             # 6. per extended part: coset-part NTTs, gate / permutation / lookup quotients.
             #    Columns: advice 0-3, instance 4, z 5-6, lookup z 7, A' 8, S' 9,
             #    compressed input 10, fixed 11-13, sigma 14-17, l0 18, l_last 19, l_active 20.
-            y, theta = chal(), chal()
             d_y = h2b.to_dev(sc(y), stream)
             keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
             allc = coef + keyp
@@ -251,19 +314,27 @@ class ProofWorkload:
                 queries += [(coef[idx], at(r)) for r in rots.get(idx, (0,))]
             queries += [(c, at(0)) for c in pk["fixed"] + pk["sigma"]]
             queries += [(_slice(hc, i, n), at(0)) for i in range(dom.quotient_poly_degree)]
+            queries += [(h_rand, at(0))]
             cws = h2b.dev_empty(h2b.lib().h2b_msm_table_workspace_size(n, tn))
 
             def commit_now(d):
                 out = h2b.dev_empty(96)
                 h2b.msm_device_table(d, res.table, tn, out, n, ws=cws, stream=stream)
                 commits.append(out)
+                absorb([out])
                 return out
 
-            opened, _, l_at_u = shplonk.open_queries(h2b, queries, iter([chal(), chal(), chal()]), commit_now,
-                                                     stream=stream)
+            def write_evals(values):
+                if tr is not None:
+                    for e in values:
+                        tr.write_scalar(e % F.R_MOD)
+
+            opened, _, l_at_u = shplonk.open_queries(h2b, queries, iter(chal, None), commit_now, stream=stream,
+                                                     on_evals=write_evals)
             if l_at_u != 0:
                 raise RuntimeError("SHPLONK linearisation does not vanish at u")
             evals.append(torch.from_numpy(np.ascontiguousarray(F.fr_mont_limbs(opened)).view(np.uint8).reshape(-1)))
+        self.proof = tr.finalize() if tr is not None else None
         return commits, evals
 
 
@@ -288,8 +359,10 @@ class Server:
     Latency is arrival to completion of the request's stream, measured on the
     host clock."""
 
-    def __init__(self, res, slots, hbm_budget):
-        self.res, self.slots, self.budget = res, slots, hbm_budget
+    def __init__(self, res, slots, hbm_budget, transcript=False):
+        """transcript=True proves with the Fiat-Shamir transcript; each
+        request's outputs then carry its proof bytes third."""
+        self.res, self.slots, self.budget, self.transcript = res, slots, hbm_budget, transcript
         self.in_use = 0
         self.cv = threading.Condition()
         self.streams = [_t().cuda.Stream() for _ in range(slots)]
@@ -330,8 +403,11 @@ class Server:
                     self.cv.wait()
                 self.in_use += need
             try:
-                out = ProofWorkload(self.res, k, seed).run(st)
+                w = ProofWorkload(self.res, k, seed, self.transcript)
+                out = w.run(st)
                 st.synchronize()
+                if self.transcript:
+                    out = (out[0], out[1], w.proof)
                 finish(time.perf_counter(), out, None)
             except Exception as e:  # handed to serve(), which raises it
                 finish(time.perf_counter(), None, e)
@@ -365,7 +441,7 @@ class Server:
                 if err is not None:
                     errors.append(err)
                 elif keep_outputs:
-                    outs[i] = ([c.cpu() for c in out[0]], [e.cpu() for e in out[1]])
+                    outs[i] = ([c.cpu() for c in out[0]], [e.cpu() for e in out[1]]) + tuple(out[2:])
                 with lock:
                     left[0] -= 1
                     if left[0] == 0:

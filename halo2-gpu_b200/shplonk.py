@@ -119,16 +119,21 @@ class Shplonk:
         return t
 
 
-def open_queries(h2b, queries, challenges, commit, stream=None):
+def open_queries(h2b, queries, challenges, commit, stream=None, on_evals=None):
     """SHPLONK opening of `queries` = [(device poly, point)] (all of length n).
-    `challenges` yields three ints (y, v, u); `commit(d_poly)` returns the
-    96-byte device commitment of a length-n polynomial.  Returns
-    (evaluations in query order, [W, W'], L(u)) with L(u) == 0 for a sound
-    opening."""
+    `challenges` yields three ints, drawn in the transcript order of the
+    reference's SHPLONK prover: y and v after the evaluations, u after the
+    first commitment W (so a lazy generator over a Fiat-Shamir transcript
+    sees W before it squeezes u); `commit(d_poly)` returns the 96-byte device
+    commitment of a length-n polynomial; `on_evals(evals)` (optional) gets
+    the evaluations before y is drawn.  Returns (evaluations in query order,
+    [W, W'], L(u)) with L(u) == 0 for a sound opening."""
     n = queries[0][0].numel() // 32
     sp = Shplonk(h2b, n, stream)
     # evaluations, and the point set of every polynomial (by identity)
     evals, point_sets, polys = sp.eval_many(queries), {}, {}
+    if on_evals is not None:
+        on_evals(evals)
     for (d, x), e in zip(queries, evals):
         key = d.data_ptr()
         polys[key] = d
@@ -137,7 +142,7 @@ def open_queries(h2b, queries, challenges, commit, stream=None):
     sets = {}
     for key, pe in point_sets.items():
         sets.setdefault(tuple(sorted(pe)), []).append(key)
-    y, v, u = (next(challenges) % P for _ in range(3))
+    y, v = (next(challenges) % P for _ in range(2))
     super_points = sorted({x for s in sets for x in s})
     # h = sum_i v^i (sum_j y^j (p_ij - r_ij)) / Z_{S_i}
     h = sp.zeros()
@@ -147,13 +152,11 @@ def open_queries(h2b, queries, challenges, commit, stream=None):
         num = bufs[0]
         num.zero_()
         short = [0] * len(pts)
-        r_at_u = 0
         for j, key in enumerate(keys):
             yj = pow(y, j, P)
             sp.madd(num, polys[key], yj)
             r = _interpolate(list(pts), [point_sets[key][x] for x in pts])
             short = [(a + yj * b) % P for a, b in zip(short, r)]
-            r_at_u = (r_at_u + yj * _eval_host(r, u)) % P
         sp.sub_short(num, short)
         cur, other = bufs
         for pt in pts:                   # divide by (X - s) for every point of the set
@@ -162,8 +165,11 @@ def open_queries(h2b, queries, challenges, commit, stream=None):
         vi = pow(v, i, P)
         sp.madd(h, cur, vi)
         diff = [x for x in super_points if x not in pts]
-        lin_terms.append((keys, vi * _vanishing_at(diff, u) % P, r_at_u))
+        lin_terms.append((keys, vi, diff, short))
     w = commit(h)
+    u = next(challenges) % P
+    # per rotation set: v^i Z_{T\S_i}(u) and the combined interpolant at u
+    lin_terms = [(keys, vi * _vanishing_at(diff, u) % P, _eval_host(short, u)) for keys, vi, diff, short in lin_terms]
     # L = sum_i v^i Z_{T\S_i}(u) sum_j y^j (p_ij - r_ij(u)) - Z_T(u) h
     lx = sp.zeros()
     const = 0

@@ -62,10 +62,10 @@ def test_served_outputs_match_alone(h2b):
         tight = tight_srv.serve(reqs, keep_outputs=True)["outputs"]
     for a, m in zip(alone, tight):
         assert a == _bytes(m)
-    # each request's outputs: 4 advice + A' + S' + 2 z + lookup z + 3 h pieces + the 2 SHPLONK
-    # commitments, and the 28 opened evaluations
+    # each request's outputs: 4 advice + A' + S' + 2 z + lookup z + the vanishing argument's
+    # random polynomial + 3 h pieces + the 2 SHPLONK commitments, and the 29 opened evaluations
     c, e = alone[0]
-    assert len(c) == 96 * 14 and len(e) == 32 * 28
+    assert len(c) == 96 * 15 and len(e) == 32 * 29
     # the first commitment is the advice column's MSM over the plain SRS
     n = 1 << 12
     adv0 = h2b.random_fr_device(n, 11 * 64, 1)
@@ -100,3 +100,63 @@ def test_keygen_commitments(h2b):
         h2b.msm_device(poly, res.srs, out, n, h2b.msm_workspace(n))
         torch.cuda.synchronize()
         assert out.cpu().numpy().tobytes() == got.cpu().numpy().tobytes()
+
+
+@pytest.mark.gpu
+def test_transcript_proof_replays(h2b):
+    """With the Fiat-Shamir transcript, the proof bytes are the same alone and
+    in a concurrent mix, and a reader that replays them (verifying-key scalar,
+    public rows, then the proof in the prover's order) recovers every
+    commitment the device computed, every evaluation, and every challenge."""
+    import torch
+    P = _prover(h2b)
+    T = importlib.import_module(h2b.__name__ + ".transcript")
+    F = h2b.fields
+    res = P.Resident(h2b, 11)
+    reqs = [(0.0, 10, 21), (0.0, 11, 22), (0.0, 10, 23)]
+    with P.Server(res, 1, 1 << 36, transcript=True) as one:
+        alone = [one.serve([r], keep_outputs=True)["outputs"][0] for r in reqs]
+    with P.Server(res, 3, 1 << 36, transcript=True) as srv:
+        mixed = srv.serve(reqs, keep_outputs=True)["outputs"]
+    for a, m in zip(alone, mixed):
+        assert a[2] == m[2] and _bytes(a[:2]) == _bytes(m[:2])
+    assert alone[0][2] != alone[2][2]
+
+    st = torch.cuda.Stream()
+    w = P.ProofWorkload(res, 10, 21, transcript=True)
+    commits, evals = w.run(st)
+    st.synchronize()
+    proof = w.proof
+    assert proof == alone[0][2] and len(proof) == 32 * (15 + 29)
+    r = T.Blake2bRead(proof)
+    r.common_scalar(res.vk_repr(10))
+    inst = h2b.random_fr_device(1 << 10, 21 * 64 + 4, 0)
+    for v in F.fr_from_mont_limbs(h2b.to_host(inst[: 32 * P.NUM_PUBLIC])):
+        r.common_scalar(int(v))
+    pts, ch = [], []
+
+    def points(m):
+        pts.extend(r.read_point() for _ in range(m))
+
+    points(4)                                                # advice
+    ch.append(r.squeeze_challenge())                         # theta
+    points(2)                                                # A', S'
+    ch += [r.squeeze_challenge(), r.squeeze_challenge()]     # beta, gamma
+    points(4)                                                # 2 z, lookup z, random polynomial
+    ch.append(r.squeeze_challenge())                         # y
+    points(3)                                                # h pieces
+    ch.append(r.squeeze_challenge())                         # x
+    ev = [r.read_scalar() for _ in range(29)]
+    ch += [r.squeeze_challenge(), r.squeeze_challenge()]     # SHPLONK y, v
+    points(1)                                                # W
+    ch.append(r.squeeze_challenge())                         # u
+    points(1)                                                # W'
+    assert r.remaining() == 0
+    assert ch == w.challenges
+    assert pts == [T.commitment_to_affine(c.cpu().numpy().view(np.uint64)) for c in commits]
+    assert ev == F.fr_from_mont_limbs(evals[0].numpy().view(np.uint64).reshape(-1, 4))
+    # advice commitments do not depend on challenges; the grand products do
+    c0, _ = P.ProofWorkload(res, 10, 21).run(st)
+    st.synchronize()
+    assert all(torch.equal(a.cpu(), b.cpu()) for a, b in zip(c0[:4], commits[:4]))
+    assert not torch.equal(c0[6].cpu(), commits[6].cpu())
