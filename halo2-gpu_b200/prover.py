@@ -73,7 +73,8 @@ def _bytes_per_proof(k):
 class Resident:
     """State kept on the device across requests: the SRS window table and,
     per k, the proving-key polynomials (fixed, sigma, Lagrange selectors) in
-    coefficient form, the lookup table column and the domain constants."""
+    coefficient form and their extended coset parts (key_cosets), the lookup
+    table column and the domain constants."""
 
     def __init__(self, h2b, kmax, seed=0x5EED):
         self.h2b = h2b
@@ -81,6 +82,7 @@ class Resident:
         self.srs = h2b.srs_device(seed, 1 << kmax)
         self.table = h2b.msm_table_precompute(self.srs, 1 << kmax)
         self.pk = {}
+        self._lock = threading.Lock()
         g = R.Graph()
         self.parts = np.array(R.plonk_and_fibonacci(g), dtype=np.uint64)
         self.rules = np.array(g.rules, dtype=np.uint64)
@@ -102,6 +104,29 @@ class Resident:
             pk["table_col"] = tab_col
             self.pk[k] = pk
         return self.pk[k]
+
+    def key_cosets(self, k, stream=None):
+        """The 4 extended coset parts of the 2^k key polynomials (3 fixed, 4
+        permutation, 3 Lagrange selectors), computed once and kept resident,
+        as halo2's ProvingKey keeps `fixed_cosets` and the permutation cosets
+        from keygen on: a proof then transforms only its own 11 polynomials
+        per part.  [part][polynomial] device vectors."""
+        pk = self.key(k)
+        with self._lock:
+            if "cosets" not in pk:
+                torch, h2b, n, dom = _t(), self.h2b, 1 << k, pk["dom"]
+                keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
+                st = stream if stream is not None else torch.cuda.current_stream()
+                cos = []
+                with torch.cuda.stream(st):
+                    for j in range(1 << (dom.extended_k - k)):
+                        outs = [h2b.dev_empty(32 * n) for _ in keyp]
+                        shift = pow(dom.extended_omega, j, F.R_MOD)
+                        h2b.fft_many_to_device(6, k, k, keyp, outs, dom.omega, F.ZETA * shift % F.R_MOD, stream=st)
+                        cos.append(outs)
+                st.synchronize()
+                pk["cosets"] = cos
+        return pk["cosets"]
 
     def keygen(self, k, stream=None):
         """Verifying-key commitments of the 2^k key (keygen_vk's GPU part,
@@ -264,17 +289,17 @@ class ProofWorkload:
             #    Columns: advice 0-3, instance 4, z 5-6, lookup z 7, A' 8, S' 9,
             #    compressed input 10, fixed 11-13, sigma 14-17, l0 18, l_last 19, l_active 20.
             d_y = h2b.to_dev(sc(y), stream)
-            keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
-            allc = coef + keyp
-            parts = [h2b.dev_empty(32 * n) for _ in allc]
+            kcos = res.key_cosets(k, stream)
+            own = [h2b.dev_empty(32 * n) for _ in coef]
             hs = [h2b.dev_empty(32 * n) for _ in range(1 << (dom.extended_k - k))]
             ext_w = dom.extended_omega
             nws = h2b.dev_empty(h2b.lib()._halo2_fft_many_to_device_workspace_size(6, k, k))
             beta_v = F.fr_from_mont_limbs(beta)[0]
             for j, hj in enumerate(hs):
                 shift = pow(ext_w, j, F.R_MOD)
-                h2b.fft_many_to_device(6, k, k, allc, parts, dom.omega, F.ZETA * shift % F.R_MOD, ws=nws,
+                h2b.fft_many_to_device(6, k, k, coef, own, dom.omega, F.ZETA * shift % F.R_MOD, ws=nws,
                                        stream=stream)
+                parts = own + kcos[j]
                 h2b.quotient_device(parts[11:14], [parts[4]], parts[0:4], sc(theta), res.consts, y, res.rules,
                                     res.parts, n, 1, 0, n, hj, None, stream=stream)
                 h2b.quotient_permutation_device(hj, parts[18], parts[19], parts[20], parts[5:7], parts[14:18],
@@ -283,7 +308,7 @@ class ProofWorkload:
                                                 stream=stream)
                 h2b.quotient_lookups_device(hj, parts[10], parts[7], parts[8], parts[9], parts[18], parts[19],
                                             parts[20], d_beta, d_gamma, d_y, n, stream=stream)
-            del parts
+            del parts, own
             # 7. h on the extended coset: gather the parts, divide by the vanishing
             #    polynomial, back to coefficients (extended_to_coeff), commit its pieces
             en = len(hs) * n
@@ -423,7 +448,7 @@ class Server:
         for _, k, _ in reqs:
             if self.bytes_for(k) > self.budget:
                 raise ValueError(f"a 2^{k} proof needs more than the {self.budget}-byte budget")
-            self.res.key(k)
+            self.res.key_cosets(k)
         torch.cuda.synchronize()
         done = [None] * len(reqs)
         outs = [None] * len(reqs)
