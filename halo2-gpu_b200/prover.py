@@ -49,6 +49,8 @@ from . import shplonk
 from . import transcript as T
 
 NUM_PUBLIC = 8   # rows of the instance column that are public inputs (absorbed into the transcript)
+# the proof's commitments in the order they are written
+COMMIT_LABELS = ("adv0", "adv1", "adv2", "adv3", "pa", "ps", "z0", "z1", "zl", "hr", "h0", "h1", "h2", "W", "W2")
 
 _torch = None
 
@@ -79,10 +81,12 @@ class Resident:
     def __init__(self, h2b, kmax, seed=0x5EED):
         self.h2b = h2b
         self.kmax = kmax
+        self.tau = seed % F.R_MOD   # the synthetic SRS's trapdoor: [tau^i] G, never a ceremony
         self.srs = h2b.srs_device(seed, 1 << kmax)
         self.table = h2b.msm_table_precompute(self.srs, 1 << kmax)
         self.pk = {}
         self._lock = threading.Lock()
+        self._lag_tables = {}
         g = R.Graph()
         self.parts = np.array(R.plonk_and_fibonacci(g), dtype=np.uint64)
         self.rules = np.array(g.rules, dtype=np.uint64)
@@ -104,6 +108,31 @@ class Resident:
             pk["table_col"] = tab_col
             self.pk[k] = pk
         return self.pk[k]
+
+    def lagrange_table(self, k):
+        """Window table of the 2^k Lagrange bases [L_i(tau)] G of the same
+        SRS (ParamsKZG's g_lagrange, halo2_proofs/src/poly/kzg/commitment.rs:
+        158-186), so commit_lagrange commits a column's values directly.  The
+        scalars L_i(tau) = (1/n) sum_j tau^j w^(-ij) are the inverse NTT of the
+        powers of tau; the points come from the SRS kernel.  Built once per k,
+        with the monomial table's geometry (2^kmax points, the Lagrange bases
+        first, SRS points after them that an MSM of 2^k scalars never reads),
+        so its window width is the one measured for the monomial table: a table
+        of only 2^k points takes narrower windows, whose single bucket set
+        holds longer buckets (k = 16 proof 17.3 -> 21.0 ms)."""
+        with self._lock:
+            if k not in self._lag_tables:
+                torch, h2b, n, tn = _t(), self.h2b, 1 << k, 1 << self.kmax
+                dom = F.EvaluationDomain(4, k)
+                lam = h2b.dev_empty(32 * n)
+                h2b.fft_normal_to_device(2, k, h2b.powers_device(self.tau, n), lam, dom.omega_inv,
+                                         dom.ifft_divisor)
+                bases = self.srs.clone()
+                h2b.call("h2b_srs_from_powers", h2b.ptr(bases), h2b.ptr(lam), n,
+                         h2b.ptr(h2b.to_dev(F.g1_pow2_table(256))), h2b.stream_handle())
+                self._lag_tables[k] = h2b.msm_table_precompute(bases, tn)
+                torch.cuda.synchronize()
+        return self._lag_tables[k]
 
     def key_cosets(self, k, stream=None):
         """The 4 extended coset parts of the 2^k key polynomials (3 fixed, 4
@@ -215,19 +244,27 @@ class ProofWorkload:
         with torch.cuda.stream(stream):
             commits, evals, pending = [], [], []
             probe = h2b.dev_empty(32)
+            lag_tab = res.lagrange_table(k)
             slots = h2b.msm_batch_jobs([probe] * 4, [res.table] * 4, [probe] * 4, [n] * 4, table_n=tn)
-            msm_ws = h2b.msm_batch_workspace(slots, 4, 4)
+            msm_ws = h2b.msm_batch_workspace(slots, 4, 4)   # both tables have 2^kmax points
 
-            def commit(d, m=n):
+            def commit(d, lagrange=False):
+                """Queues the commitment of a length-n vector: Lagrange values
+                over the Lagrange bases (commit_lagrange), coefficients over
+                the monomial SRS (commit)."""
                 out = h2b.dev_empty(96)
-                pending.append((d, out, m))
+                pending.append((d, out, lagrange))
                 commits.append(out)
 
             def flush():
                 """The commitments of one phase as one batch: each MSM on its own
                 forked stream, so their serial tails overlap."""
-                jobs = h2b.msm_batch_jobs([p[0] for p in pending], [res.table] * len(pending),
-                                          [p[1] for p in pending], [p[2] for p in pending], table_n=tn)
+                jobs = h2b.MsmJob * len(pending)
+                jobs = jobs()
+                for i, (d, out, lagr) in enumerate(pending):
+                    jobs[i].d_scalars, jobs[i].d_out, jobs[i].n = d.data_ptr(), out.data_ptr(), n
+                    jobs[i].d_bases = (lag_tab if lagr else res.table).data_ptr()
+                    jobs[i].table_n = tn
                 h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
                 outs = [p[1] for p in pending]
                 pending.clear()
@@ -242,7 +279,7 @@ class ProofWorkload:
                 for v in F.fr_from_mont_limbs(h2b.to_host(inst[: 32 * NUM_PUBLIC])):
                     tr.common_scalar(int(v))
             for a in adv:
-                commit(a)
+                commit(a, lagrange=True)
             flush()
             theta = chal()
             # 3. lookup: the input takes values of the table; permute-sort, commit A', S'
@@ -252,8 +289,8 @@ class ProofWorkload:
             lin = pk["table"].view(256, 32)[idx].reshape(-1)
             pa, ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
             h2b.permute_expression_pair_device(lin, pk["table_col"], pa, ps, n, n - 10, stream=stream)
-            commit(pa)
-            commit(ps)
+            commit(pa, lagrange=True)
+            commit(ps, lagrange=True)
             flush()
             # 4. permutation grand products (2 sets of 2 columns), lookup grand product,
             #    and the vanishing argument's random polynomial
@@ -271,11 +308,11 @@ class ProofWorkload:
                                                d_gamma, d_delta, d_om, d_dw, n, stream=stream)
                 h2b.grand_product_device(z, d_one, n, stream=stream)
                 zs.append(z)
-                commit(z)
             zl = h2b.dev_empty(32 * n)
             h2b.lookup_product_device(zl, pa, ps, lin, pk["table_col"], d_beta, d_gamma, n, stream=stream)
             h2b.grand_product_device(zl, d_one, n, stream=stream)
-            commit(zl)
+            for z in zs + [zl]:
+                commit(z, lagrange=True)
             h_rand = h2b.random_fr_device(n, seed * 64 + 5, 0, stream)
             commit(h_rand)
             flush()
@@ -334,12 +371,22 @@ class ProofWorkload:
             w = dom.omega
             at = lambda r: x * pow(w, r % n, F.R_MOD) % F.R_MOD  # noqa: E731
             rots = {0: (0, -1), 3: (0, 1, 2), 5: (0, 1, -3), 6: (0, 1, -3), 7: (0, 1), 8: (0, -1)}
-            queries = []
+            queries, labels = [], []
+            names = {0: "adv0", 1: "adv1", 2: "adv2", 3: "adv3", 5: "z0", 6: "z1", 7: "zl", 8: "pa", 9: "ps"}
             for idx in (0, 1, 2, 3, 5, 6, 7, 8, 9):
                 queries += [(coef[idx], at(r)) for r in rots.get(idx, (0,))]
+                labels += [(names[idx], at(r)) for r in rots.get(idx, (0,))]
             queries += [(c, at(0)) for c in pk["fixed"] + pk["sigma"]]
+            labels += [(f"vk{i}", at(0)) for i in range(len(pk["fixed"]) + len(pk["sigma"]))]
             queries += [(_slice(hc, i, n), at(0)) for i in range(dom.quotient_poly_degree)]
+            labels += [(f"h{i}", at(0)) for i in range(dom.quotient_poly_degree)]
             queries += [(h_rand, at(0))]
+            labels += [("hr", at(0))]
+            # what a verifier needs besides the proof: each query's polynomial
+            # (a label) and point, in the order the evaluations were written;
+            # labels name the proof's commitments in order (COMMIT_LABELS) or
+            # the verifying key's commitments ("vk0".., fixed then sigma)
+            self.query_labels = labels
             cws = h2b.dev_empty(h2b.lib().h2b_msm_table_workspace_size(n, tn))
 
             def commit_now(d):
@@ -449,6 +496,7 @@ class Server:
             if self.bytes_for(k) > self.budget:
                 raise ValueError(f"a 2^{k} proof needs more than the {self.budget}-byte budget")
             self.res.key_cosets(k)
+            self.res.lagrange_table(k)
         torch.cuda.synchronize()
         done = [None] * len(reqs)
         outs = [None] * len(reqs)

@@ -66,11 +66,14 @@ def test_served_outputs_match_alone(h2b):
     # random polynomial + 3 h pieces + the 2 SHPLONK commitments, and the 29 opened evaluations
     c, e = alone[0]
     assert len(c) == 96 * 15 and len(e) == 32 * 29
-    # the first commitment is the advice column's MSM over the plain SRS
+    # the first commitment is the MSM of the advice column's coefficient form over the plain SRS
     n = 1 << 12
     adv0 = h2b.random_fr_device(n, 11 * 64, 1)
+    dom = h2b.fields.EvaluationDomain(4, 12)
+    adv0_c = h2b.dev_empty(32 * n)
+    h2b.fft_normal_to_device(2, 12, adv0, adv0_c, dom.omega_inv, dom.ifft_divisor)
     out = h2b.dev_empty(96)
-    h2b.msm_device(adv0, res.srs, out, n, h2b.msm_workspace(n))
+    h2b.msm_device(adv0_c, res.srs, out, n, h2b.msm_workspace(n))
     torch.cuda.synchronize()
     assert out.cpu().numpy().tobytes() == c[:96]
     # distinct seeds give distinct outputs
@@ -155,6 +158,22 @@ def test_transcript_proof_replays(h2b):
     assert ch == w.challenges
     assert pts == [T.commitment_to_affine(c.cpu().numpy().view(np.uint64)) for c in commits]
     assert ev == F.fr_from_mont_limbs(evals[0].numpy().view(np.uint64).reshape(-1, 4))
+    # the opening verifies: F == (tau - u) W' with the SRS trapdoor (the G1
+    # form of SHPLONK's pairing check); a changed evaluation breaks it
+    V = importlib.import_module(h2b.__name__ + ".verify")
+    vk = res.keygen(10)
+    torch.cuda.synchronize()
+    cm = dict(zip(P.COMMIT_LABELS, pts))
+    cm.update({f"vk{i}": T.commitment_to_affine(c.cpu().numpy().view(np.uint64)) for i, c in enumerate(vk)})
+    x = ch[4]
+    assert w.query_labels[0] == ("adv0", x) and len(w.query_labels) == 29
+    sy, sv, su = ch[5], ch[6], ch[7]
+    assert V.shplonk_check_trapdoor(cm, w.query_labels, ev, sy, sv, su, cm["W"], cm["W2"], res.tau)
+    bad = list(ev)
+    bad[3] = (bad[3] + 1) % F.R_MOD
+    assert not V.shplonk_check_trapdoor(cm, w.query_labels, bad, sy, sv, su, cm["W"], cm["W2"], res.tau)
+    assert not V.shplonk_check_trapdoor(cm, w.query_labels, ev, sy, sv, (su + 1) % F.R_MOD, cm["W"], cm["W2"],
+                                        res.tau)
     # advice commitments do not depend on challenges; the grand products do
     c0, _ = P.ProofWorkload(res, 10, 21).run(st)
     st.synchronize()

@@ -1,0 +1,37 @@
+"""The G1 (trapdoor) form of SHPLONK's final pairing check
+(halo2-gpu_b200/verify.py) against an opening made by a pure-Python
+restatement of the SHPLONK prover, all on the host: a correct opening
+passes; a changed evaluation, challenge, commitment or W' fails."""
+import importlib
+import random
+
+from test_shplonk_gpu import _restate
+
+
+def test_trapdoor_check_accepts_opening_and_rejects_changes(h2b):
+    F = h2b.fields
+    S = importlib.import_module(h2b.__name__ + ".shplonk")
+    V = importlib.import_module(h2b.__name__ + ".verify")
+    p, rng = F.R_MOD, random.Random(5)
+    n, tau = 8, rng.randrange(2, p)
+    polys = [[rng.randrange(p) for _ in range(n)] for _ in range(4)]
+    x, w = rng.randrange(p), pow(F.ROOT_OF_UNITY, 1 << (F.S - 3), p)
+    queries = [(0, x), (0, x * w % p), (1, x), (2, x), (2, x * w % p), (2, x * w * w % p), (3, x)]
+    y, v, u = (rng.randrange(p) for _ in range(3))
+    h, q = _restate(polys, queries, y, v, u, p, S)
+
+    def commit(c):
+        return F.g1_mul(F.G1_GENERATOR, S._eval_host(c, tau))
+
+    cm = {i: commit(c) for i, c in enumerate(polys)}
+    W, W2 = commit(h), commit(q)
+    evals = [S._eval_host(polys[k], pt) for k, pt in queries]
+    assert V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, W, W2, tau)
+    bad = list(evals)
+    bad[4] = (bad[4] + 1) % p
+    assert not V.shplonk_check_trapdoor(cm, queries, bad, y, v, u, W, W2, tau)
+    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, (v + 1) % p, u, W, W2, tau)
+    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, W, F.g1_add(W2, F.G1_GENERATOR), tau)
+    cm2 = dict(cm)
+    cm2[3] = F.g1_add(cm[3], F.G1_GENERATOR)
+    assert not V.shplonk_check_trapdoor(cm2, queries, evals, y, v, u, W, W2, tau)
