@@ -432,10 +432,10 @@ __global__ void __launch_bounds__(BI_T) k_permutation_product(Fr* __restrict__ a
                                                               const Fr* __restrict__ pdeltaomega, uint64_t n)
 {
     const Fr beta = ld(pbeta), gamma = ld(pgamma), delta = ld(pdelta), omega = ld(pomega);
-    const Fr dw0 = ld(pdeltaomega);
+    const Fr dw0b = ld(pdeltaomega) * beta;   // the numerator's first column term is dw0 w^i beta
     const uint64_t base = (uint64_t)blockIdx.x * BI_TILE;
     Fr wstep = pow_u64(omega, BI_T);   // emit steps i by BI_T
-    Fr wi = Fr::one();
+    Fr wib = Fr::one();
     block_mont_trick<FrCfg>(
         base, n, nullptr,
         [&](uint64_t i) {
@@ -446,13 +446,17 @@ __global__ void __launch_bounds__(BI_T) k_permutation_product(Fr* __restrict__ a
         },
         [&](uint64_t i) { return ld(&acc[i]); },
         [&](uint64_t i, const Fr& inv, int j) {
-            wi = (j == 0) ? dw0 * pow_u64(omega, i) : wi * wstep;
+            // column c's term is dw0 w^i delta^c beta + gamma + v_c: the
+            // beta-scaled power is stepped (one product per row) and then
+            // by delta per column, so a row takes 2 ncols - 1 products here
+            wib = (j == 0) ? dw0b * pow_u64(omega, i) : wib * wstep;
             if (inv.is_zero()) { st(&acc[i], inv); return; }
-            Fr cur = wi;
-            Fr num = Fr::one();
-            for (int c = 0; c < ncols; c++) {
-                num = num * (cur * beta + gamma + ld(&cols.value[c][i]));
+            if (ncols == 0) { st(&acc[i], inv); return; }   // no columns: the numerator is 1
+            Fr cur = wib;
+            Fr num = cur + gamma + ld(&cols.value[0][i]);
+            for (int c = 1; c < ncols; c++) {
                 cur = cur * delta;
+                num = num * (cur + gamma + ld(&cols.value[c][i]));
             }
             st(&acc[i], inv * num);
         });
