@@ -164,6 +164,7 @@ _SIGS = {
     "h2b_ntt_get_pass_stages": (ctypes.c_int, []),
     "h2b_random_fr": (RustError, [_vp, _u64, _u64, ctypes.c_int, _vp]),
     "h2b_powers": (RustError, [_vp, _u64, _vp, _vp]),
+    "h2b_fibonacci_fr": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_srs_from_powers": (RustError, [_vp, _vp, _u64, _vp, _vp]),
     "h2b_prof_enable": (None, [ctypes.c_int]),
     "h2b_prof_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
@@ -692,6 +693,14 @@ def random_fr_device(n, seed, mix=0, stream=None):
 def powers_device(x, n, stream=None):
     d = dev_empty(32 * n)
     call("h2b_powers", ptr(d), n, ptr(to_dev(_scalar_bytes(x), stream)), stream_handle(stream))
+    return d
+
+
+def fibonacci_device(s0, s1, n, stream=None):
+    """out[0] = s0, out[1] = s1, out[i + 2] = out[i + 1] + out[i] (Fr, device)."""
+    d = dev_empty(32 * n)
+    seeds = np.concatenate([_scalar_bytes(s0), _scalar_bytes(s1)])
+    call("h2b_fibonacci_fr", ptr(d), n, ptr(to_dev(seeds, stream)), stream_handle(stream))
     return d
 
 

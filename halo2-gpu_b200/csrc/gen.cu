@@ -6,6 +6,11 @@
 //    uses.  `mix` = 1 gives the witness-like mix of the k=22 MSM workload:
 //    50% uniform, 30% uniform below 2^64, 20% uniform in {0, 1}.
 //  * h2b_powers: out[i] = x^i.
+//  * h2b_fibonacci_fr: out[0] = s0, out[1] = s1, out[i + 2] = out[i + 1] + out[i]
+//    (the witness of a Fibonacci rotation gate).  out[i] = s0 F(i-1) + s1 F(i)
+//    with F the Fibonacci numbers mod r, so each thread reaches its chunk
+//    start by fast doubling (F(2m) = F(m)(2F(m+1) - F(m)),
+//    F(2m+1) = F(m)^2 + F(m+1)^2) and then steps the recurrence.
 //  * h2b_srs_from_powers: out[i] = [s_i] G as affine points for Montgomery
 //    scalars s_i, by fixed-base double-and-add over a caller-supplied table
 //    of affine 2^j G (j < 256), then one inversion per point.  With
@@ -75,6 +80,32 @@ __global__ void k_powers(Fr* __restrict__ out, uint64_t n, const Fr* __restrict_
     }
 }
 
+constexpr int FIB_CHUNK = 64;
+__global__ void k_fibonacci(Fr* __restrict__ out, uint64_t n, const Fr* __restrict__ seeds)
+{
+    const Fr s0 = ld(&seeds[0]), s1 = ld(&seeds[1]);
+    uint64_t nthreads = (n + FIB_CHUNK - 1) / FIB_CHUNK;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nthreads;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i0 = t * FIB_CHUNK;
+        Fr a = Fr::zero(), b = Fr::one();          // (F(m), F(m + 1)) for m = the bits of i0 seen so far
+        for (int bit = 63; bit >= 0; bit--) {
+            if ((i0 >> bit) == 0) continue;
+            Fr c = a * (b + b - a);
+            Fr d = a * a + b * b;
+            if ((i0 >> bit) & 1) { a = d; b = c + d; } else { a = c; b = d; }
+        }
+        Fr cur = s0 * (b - a) + s1 * a;            // out[i0] = s0 F(i0 - 1) + s1 F(i0)
+        Fr nxt = s0 * a + s1 * b;                  // out[i0 + 1]
+        for (int j = 0; j < FIB_CHUNK && i0 + j < n; j++) {
+            st(&out[i0 + j], cur);
+            Fr sum = cur + nxt;
+            cur = nxt;
+            nxt = sum;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) k_srs(G1Affine* __restrict__ out, const Fr* __restrict__ scalars, uint64_t n,
                                              const G1Affine* __restrict__ table)
 {
@@ -114,6 +145,15 @@ extern "C" RustError h2b_powers(void* d_out, uint64_t n, const void* d_x, cudaSt
     uint64_t nthreads = (n + POW_CHUNK - 1) / POW_CHUNK;
     k_powers<<<grid_for(nthreads, 256, 148u * 16u), 256, 0, stream>>>((Fr*)d_out, n, (const Fr*)d_x);
     H2B_LAUNCHED("k_powers");
+    return ok();
+}
+
+extern "C" RustError h2b_fibonacci_fr(void* d_out, uint64_t n, const void* d_seeds, cudaStream_t stream)
+{
+    if (n == 0) return ok();
+    uint64_t nthreads = (n + FIB_CHUNK - 1) / FIB_CHUNK;
+    k_fibonacci<<<grid_for(nthreads, 128, 148u * 16u), 128, 0, stream>>>((Fr*)d_out, n, (const Fr*)d_seeds);
+    H2B_LAUNCHED("k_fibonacci");
     return ok();
 }
 

@@ -1,36 +1,42 @@
-"""Prover-shaped GPU workload and a serving loop around it.
+"""Prover for the config-3 circuit family and a serving loop around it.
 
-`ProofWorkload.run` issues, on one stream, the device work that `create_proof`
-(halo2_proofs/src/plonk/prover.rs:56-482) sends to the GPU for the config-3
-circuit family (4 advice, 3 fixed, 1 instance column; a standard-PLONK gate
-and a Fibonacci rotation gate; a 4-column copy permutation; one lookup into a
-2^8-entry table), through this library's entry points in the reference's
-order:
+`ProofWorkload.run` proves one instance of the circuit in `circuit.py` (4
+advice, 3 fixed, 1 instance column; a standard-PLONK gate and a Fibonacci
+rotation gate; a 4-column copy permutation; one lookup into a 2^8-entry
+table) with a satisfying witness synthesised on the device, issuing on one
+stream the device work of `create_proof`
+(halo2_proofs/src/plonk/prover.rs:140-622) through this library's entry
+points, in the reference's phase order:
 
-  1. witness columns (seeded, generated on the device: synthesis stands in);
-  2. advice commitments (MSMs over the resident SRS window table);
-  3. lookup: permute-sort of the input against the table, A' and S' commits;
-  4. permutation grand products (2 sets of 2 columns) and lookup grand
-     product, and their commits;
-  5. lagrange_to_coeff of the per-proof polynomials (iNTT);
-  6. per extended part (4): coset-part NTTs of every polynomial, the gate
-     quotient (evaluate_h), the permutation and the lookup quotients;
-  7. h: the parts gathered and brought to coefficients on the extended
-     coset, and its 3 pieces committed;
-  8. opening: SHPLONK over the committed polynomials at x and their
-     rotations (shplonk.py), 2 commits.
+  phase 1  the verifying key and the public inputs into the transcript;
+           advice commitments (commit_lagrange over the Lagrange bases);
+           theta
+  phase 2  lookup: permute-sort of the compressed input against the
+           compressed table over the usable rows, blinding rows, A' and S'
+           commitments; beta, gamma
+  phase 3  permutation grand products (2 sets of 2 columns, the carry of one
+           set seeding the next) and the lookup grand product, blinding rows,
+           their commitments; the vanishing argument's random polynomial
+           (the constant 1 with zero knowledge off, committed as g[0]:
+           halo2_proofs/src/plonk/vanishing/prover.rs:64-99); y
+  phase 4  lagrange_to_coeff of the per-proof polynomials; per extended part
+           the coset parts, the gate quotient, the permutation quotient, the
+           lookup product coset (the lookup's graph through the same
+           evaluator) and the lookup quotient; h gathered, divided by the
+           vanishing polynomial, brought to coefficients, its 3 pieces
+           committed; x
+  phase 5  evaluations in the transcript's order (advice, fixed, the random
+           polynomial's 1, sigma, permutation products, lookup), then the
+           SHPLONK opening (shplonk.py) of the queries in the reference's
+           order, with h folded to sum_i x^(n i) h_i (vanishing/prover.rs:
+           190-240).
 
-The vanishing argument's random polynomial is committed with the grand
-products and opened at x.  Challenges come from a seeded generator, or, with
-`transcript=True`, from the Fiat-Shamir transcript (transcript.py: BLAKE2b,
-Challenge255) in the reference's order: the verifying key and the public
-instance rows, the advice commitments, theta, A' and S', beta and gamma, the
-grand products and the random polynomial, y, the h pieces, x, the
-evaluations, then SHPLONK's y, v, W, u, W'.  The witness is seeded random
-data that does not satisfy the circuit, so the outputs are deterministic GPU
-work, not a valid proof, and whole-proof parity needs the Rust crates.  What
-this measures is the served prover's device side: proofs/s and latency when
-requests of uneven k share one GPU.
+Challenges come from the Fiat-Shamir transcript (transcript.py) when
+`transcript=True`, and from a seeded generator otherwise (same device work,
+no proof bytes).  `verify.verify_proof` checks a proof from its bytes, the
+public inputs and the verifying key.  Blinding values come from this
+library's seeded device generator, not the reference's ChaCha RNG, so proof
+bytes are this build's own; parity of the bytes is unpinned.
 
 `Server` runs such requests with `slots` worker threads, each on its own
 stream (the GPU overlaps them), admitting a request when a slot is free and
@@ -43,14 +49,15 @@ import time
 
 import numpy as np
 
+from . import circuit as C
 from . import fields as F
-from . import rules as R
 from . import shplonk
 from . import transcript as T
 
-NUM_PUBLIC = 8   # rows of the instance column that are public inputs (absorbed into the transcript)
+NUM_PUBLIC = C.NUM_PUBLIC
 # the proof's commitments in the order they are written
-COMMIT_LABELS = ("adv0", "adv1", "adv2", "adv3", "pa", "ps", "z0", "z1", "zl", "hr", "h0", "h1", "h2", "W", "W2")
+COMMIT_LABELS = ("adv0", "adv1", "adv2", "adv3", "pa", "ps", "z0", "z1", "zl", "random", "h0", "h1", "h2", "W", "W2")
+NUM_EVALS = len(C.ADVICE_QUERIES) + len(C.FIXED_QUERIES) + 1 + 4 + 5 + 5
 
 _torch = None
 
@@ -65,18 +72,18 @@ def _t():
 
 def _bytes_per_proof(k):
     """Device memory one in-flight proof of size 2^k holds besides its MSM
-    scratch (upper bound): 11 Lagrange and 11 coefficient polynomials, 21
-    coset parts, 4 quotient parts, 8 extended-domain vectors, 2 Kate
-    quotients, evaluation scratch and small tensors."""
+    scratch (upper bound): 10 Lagrange and 10 coefficient polynomials, 10
+    coset parts, 4 quotient parts, the lookup product coset, 8
+    extended-domain vectors, the opening's buffers and small tensors."""
     n = 1 << k
     return 64 * 32 * n + (64 << 20)
 
 
 class Resident:
-    """State kept on the device across requests: the SRS window table and,
-    per k, the proving-key polynomials (fixed, sigma, Lagrange selectors) in
-    coefficient form and their extended coset parts (key_cosets), the lookup
-    table column and the domain constants."""
+    """State kept on the device across requests: the SRS and its window
+    table, the Lagrange-basis window table per k, and per k the circuit's
+    proving key (circuit.ProvingKey) with the extended coset parts of its
+    key polynomials."""
 
     def __init__(self, h2b, kmax, seed=0x5EED):
         self.h2b = h2b
@@ -87,26 +94,13 @@ class Resident:
         self.pk = {}
         self._lock = threading.Lock()
         self._lag_tables = {}
-        g = R.Graph()
-        self.parts = np.array(R.plonk_and_fibonacci(g), dtype=np.uint64)
-        self.rules = np.array(g.rules, dtype=np.uint64)
-        self.consts = F.fr_mont_limbs(g.constants)
+        self._cosets = {}
+        self._vk = {}
 
     def key(self, k):
-        if k not in self.pk:
-            h2b, n = self.h2b, 1 << k
-            dom = F.EvaluationDomain(4, k)
-            rnd = lambda s: h2b.random_fr_device(n, s, 0)  # noqa: E731
-            pk = {"dom": dom,
-                  "fixed": [rnd(1000 * k + i) for i in range(3)],
-                  "sigma": [rnd(1000 * k + 10 + i) for i in range(4)],
-                  "lag": [rnd(1000 * k + 20 + i) for i in range(3)],  # l0, l_last, l_active
-                  "table": h2b.random_fr_device(256, 1000 * k + 30, 0),
-                  "t_evals": h2b.to_dev(F.fr_mont_limbs(dom.t_evaluations))}
-            tab_col = _t().zeros(32 * n, dtype=_t().uint8, device="cuda")
-            tab_col[: 32 * 256] = pk["table"]
-            pk["table_col"] = tab_col
-            self.pk[k] = pk
+        with self._lock:
+            if k not in self.pk:
+                self.pk[k] = C.ProvingKey(self.h2b, k)
         return self.pk[k]
 
     def lagrange_table(self, k):
@@ -123,7 +117,7 @@ class Resident:
         with self._lock:
             if k not in self._lag_tables:
                 torch, h2b, n, tn = _t(), self.h2b, 1 << k, 1 << self.kmax
-                dom = F.EvaluationDomain(4, k)
+                dom = F.EvaluationDomain(C.DEGREE, k)
                 lam = h2b.dev_empty(32 * n)
                 h2b.fft_normal_to_device(2, k, h2b.powers_device(self.tau, n), lam, dom.omega_inv,
                                          dom.ifft_divisor)
@@ -136,15 +130,15 @@ class Resident:
 
     def key_cosets(self, k, stream=None):
         """The 4 extended coset parts of the 2^k key polynomials (3 fixed, 4
-        permutation, 3 Lagrange selectors), computed once and kept resident,
-        as halo2's ProvingKey keeps `fixed_cosets` and the permutation cosets
-        from keygen on: a proof then transforms only its own 11 polynomials
-        per part.  [part][polynomial] device vectors."""
+        permutation, l_0, l_last, l_active), computed once and kept
+        resident, as halo2's ProvingKey keeps `fixed_cosets` and the
+        permutation cosets from keygen on: a proof then transforms only its
+        own 10 polynomials per part.  [part][polynomial] device vectors."""
         pk = self.key(k)
         with self._lock:
-            if "cosets" not in pk:
-                torch, h2b, n, dom = _t(), self.h2b, 1 << k, pk["dom"]
-                keyp = pk["fixed"] + pk["sigma"] + pk["lag"]
+            if k not in self._cosets:
+                torch, h2b, n, dom = _t(), self.h2b, 1 << k, pk.dom
+                keyp = pk.fixed + pk.sigma + pk.lag
                 st = stream if stream is not None else torch.cuda.current_stream()
                 cos = []
                 with torch.cuda.stream(st):
@@ -154,8 +148,8 @@ class Resident:
                         h2b.fft_many_to_device(6, k, k, keyp, outs, dom.omega, F.ZETA * shift % F.R_MOD, stream=st)
                         cos.append(outs)
                 st.synchronize()
-                pk["cosets"] = cos
-        return pk["cosets"]
+                self._cosets[k] = cos
+        return self._cosets[k]
 
     def keygen(self, k, stream=None):
         """Verifying-key commitments of the 2^k key (keygen_vk's GPU part,
@@ -165,7 +159,7 @@ class Resident:
         the Lagrange form with Lagrange bases).  Returns 96-byte device images."""
         torch, h2b = _t(), self.h2b
         pk, n, tn = self.key(k), 1 << k, 1 << self.kmax
-        polys = pk["fixed"] + pk["sigma"]
+        polys = pk.fixed + pk.sigma
         st = stream if stream is not None else torch.cuda.current_stream()
         with torch.cuda.stream(st):
             outs = [h2b.dev_empty(96) for _ in polys]
@@ -174,6 +168,21 @@ class Resident:
             h2b.msm_batch(jobs, len(polys), len(polys), ws, stream=st)
         return outs
 
+    def verifying_key(self, k, stream=None):
+        """The host verifying key of the 2^k circuit (verify.VerifyingKey):
+        its fixed and permutation commitments as affine points, and the
+        transcript scalar standing for it."""
+        if k not in self._vk:
+            from . import verify as V
+            outs = self.keygen(k, stream)
+            (stream if stream is not None else _t().cuda.current_stream()).synchronize()
+            pts = [T.commitment_to_affine(o.cpu().numpy().view(np.uint64)) for o in outs]
+            h = hashlib.blake2b(digest_size=64, person=b"Halo2-Verify-Key")
+            for pt in pts:
+                h.update(T.compress(pt))
+            rep = int.from_bytes(h.digest(), "little") % F.R_MOD
+            self._vk[k] = V.VerifyingKey(k, pts[:3], pts[3:], rep)
+        return self._vk[k]
 
     def vk_repr(self, k, stream=None):
         """One Fr scalar standing for the 2^k verifying key in the transcript:
@@ -181,16 +190,17 @@ class Resident:
         (halo2's `vk.hash_into` absorbs `vk.transcript_repr`, a BLAKE2b digest
         of the pinned verifying key; this key has no pinned form, so its
         commitments stand in).  Computed once per k."""
-        if not hasattr(self, "_vk_repr"):
-            self._vk_repr = {}
-        if k not in self._vk_repr:
-            outs = self.keygen(k, stream)
-            (stream if stream is not None else _t().cuda.current_stream()).synchronize()
-            h = hashlib.blake2b(digest_size=64, person=b"Halo2-Verify-Key")
-            for o in outs:
-                h.update(T.compress(T.commitment_to_affine(o.cpu().numpy().view(np.uint64))))
-            self._vk_repr[k] = int.from_bytes(h.digest(), "little") % F.R_MOD
-        return self._vk_repr[k]
+        return self.verifying_key(k, stream).transcript_repr
+
+    def device_bytes(self):
+        """Device memory held resident: SRS and its window table, Lagrange
+        window tables, proving keys and their coset parts."""
+        total = self.srs.numel() + self.table.numel() + sum(t.numel() for t in self._lag_tables.values())
+        for k, pk in self.pk.items():
+            total += pk.device_bytes()
+        for cos in self._cosets.values():
+            total += sum(t.numel() for part in cos for t in part)
+        return total
 
 
 def _slice(t, i, n):
@@ -198,42 +208,63 @@ def _slice(t, i, n):
     return t[32 * n * i: 32 * n * (i + 1)]
 
 
-class ProofWorkload:
-    """The device work of one proof of size 2^k (see the module docstring)."""
+_G_JAC = None
 
-    def __init__(self, res, k, seed, transcript=False):
+
+def _generator_image():
+    """The 96-byte Jacobian image of G = g[0] (Montgomery Fq {1, 2, 1})."""
+    global _G_JAC
+    if _G_JAC is None:
+        _G_JAC = F.fq_mont_limbs([1, 2, 1]).reshape(-1)
+    return _G_JAC
+
+
+class ProofWorkload:
+    """One proof of the 2^k circuit (see the module docstring)."""
+
+    def __init__(self, res, k, seed, transcript=False, tamper=None, check_degree=False):
         """transcript=False draws the challenges from a generator seeded with
         `seed`; transcript=True runs the Fiat-Shamir transcript
         (transcript.Blake2bWrite): every commitment is read back and absorbed
         before the next challenge is squeezed, and `self.proof` holds the
-        proof bytes (commitments and evaluations in the order written)."""
-        self.res, self.k, self.seed, self.transcript = res, k, seed, transcript
+        proof bytes.  `tamper(advice, instance)`, if given, may change the
+        synthesised witness before anything is committed (tests use it to
+        break one cell).  check_degree=True reads back whether the top n of
+        h's 4n coefficients are zero (`self.h_degree_ok`): they are exactly
+        when every constraint holds on the whole domain, the quotient
+        identity h = sum_i y^i C_i / (X^n - 1) with deg h < 3n."""
+        self.res, self.k, self.seed, self.transcript, self.tamper = res, k, seed, transcript, tamper
+        self.check_degree = check_degree
+        self.h_degree_ok = None
         self.proof = None
+        self.public = None
 
     def run(self, stream):
         """Issues everything on `stream` (the calling thread blocks only where
-        an entry point synchronises: the permute-sort and the permutation
-        quotient); returns the commitments (96 B each) and evaluations (32 B
-        each) as device tensors, complete once `stream` is."""
+        an entry point synchronises: the permute-sort's error check and the
+        opening's evaluations); returns the commitments (96 B each, in
+        COMMIT_LABELS order) and the evaluations (32 B each, transcript order)
+        as device tensors, complete once `stream` is."""
         torch, h2b, res = _t(), self.res.h2b, self.res
         k, n, seed = self.k, 1 << self.k, self.seed
+        p = F.R_MOD
         pk = res.key(k)
-        dom = pk["dom"]
+        dom, u = pk.dom, pk.u
         tn = 1 << res.kmax
         tr = T.Blake2bWrite() if self.transcript else None
         if tr is None:
             rng = np.random.default_rng(seed)
-            chal = lambda: int(rng.integers(1, 1 << 62))  # noqa: E731
+            _draw = lambda: int(rng.integers(1, 1 << 62))  # noqa: E731
         else:
-            chal = tr.squeeze_challenge
+            _draw = tr.squeeze_challenge
         drawn = []
         self.challenges = drawn
-        _draw = chal
 
         def chal():
             drawn.append(_draw())
             return drawn[-1]
-        sc = lambda v: F.fr_mont_limbs([v % F.R_MOD])  # noqa: E731
+        sc = lambda v: F.fr_mont_limbs([v % p])  # noqa: E731
+        sh = h2b.stream_handle(stream)
 
         def absorb(outs):
             """Reads the phase's commitments back (waits for `stream`) and
@@ -241,8 +272,9 @@ class ProofWorkload:
             if tr is not None:
                 for o in outs:
                     tr.write_point(T.commitment_to_affine(o.cpu().numpy().view(np.uint64)))
+
         with torch.cuda.stream(stream):
-            commits, evals, pending = [], [], []
+            commits, pending = [], []
             probe = h2b.dev_empty(32)
             lag_tab = res.lagrange_table(k)
             slots = h2b.msm_batch_jobs([probe] * 4, [res.table] * 4, [probe] * 4, [n] * 4, table_n=tn)
@@ -259,135 +291,143 @@ class ProofWorkload:
             def flush():
                 """The commitments of one phase as one batch: each MSM on its own
                 forked stream, so their serial tails overlap."""
-                jobs = h2b.MsmJob * len(pending)
-                jobs = jobs()
+                jobs = (h2b.MsmJob * len(pending))()
                 for i, (d, out, lagr) in enumerate(pending):
                     jobs[i].d_scalars, jobs[i].d_out, jobs[i].n = d.data_ptr(), out.data_ptr(), n
                     jobs[i].d_bases = (lag_tab if lagr else res.table).data_ptr()
                     jobs[i].table_n = tn
                 h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
-                outs = [p[1] for p in pending]
+                outs = [q[1] for q in pending]
                 pending.clear()
                 absorb(outs)
 
-            # 1-2. witness and advice commitments
-            adv = [h2b.random_fr_device(n, seed * 64 + i, 1, stream) for i in range(4)]
-            inst = h2b.random_fr_device(n, seed * 64 + 4, 0, stream)
+            def blind(t, start, tag):
+                """Rows [start, n) of a column from the seeded device generator."""
+                t[32 * start:] = h2b.random_fr_device(n - start, ((seed << 4) + tag) & (2 ** 64 - 1), 0, stream)
+
+            # phase 1: witness, verifying key and public inputs, advice commitments
+            adv, inst, public = C.synthesize(h2b, pk, seed, stream)
+            if self.tamper is not None:
+                self.tamper(adv, inst)
+            self.public = public
             if tr is not None:
-                # the verifying key (its commitments, as one scalar) and the public inputs
                 tr.common_scalar(res.vk_repr(k, stream))
-                for v in F.fr_from_mont_limbs(h2b.to_host(inst[: 32 * NUM_PUBLIC])):
-                    tr.common_scalar(int(v))
+                for v in public:
+                    tr.common_scalar(v)
             for a in adv:
                 commit(a, lagrange=True)
             flush()
-            theta = chal()
-            # 3. lookup: the input takes values of the table; permute-sort, commit A', S'
-            gen = torch.Generator(device="cuda")
-            gen.manual_seed(seed)
-            idx = torch.randint(0, 256, (n,), device="cuda", generator=gen)
-            lin = pk["table"].view(256, 32)[idx].reshape(-1)
+            chal()                                   # theta (one input and one table expression: no compression)
+            # phase 2: lookup permute over the usable rows, blinding rows, A' and S'
+            b_col, t_col = adv[C.ADV_B], pk.fixed_values[C.FIX_TABLE]
             pa, ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
-            h2b.permute_expression_pair_device(lin, pk["table_col"], pa, ps, n, n - 10, stream=stream)
+            h2b.permute_expression_pair_device(b_col, t_col, pa, ps, n, u, stream=stream)
+            blind(pa, u, 8)
+            blind(ps, u, 9)
             commit(pa, lagrange=True)
             commit(ps, lagrange=True)
             flush()
-            # 4. permutation grand products (2 sets of 2 columns), lookup grand product,
-            #    and the vanishing argument's random polynomial
-            beta, gamma = sc(chal()), sc(chal())
-            d_beta, d_gamma = h2b.to_dev(beta, stream), h2b.to_dev(gamma, stream)
-            d_delta = h2b.to_dev(F.fr_mont_limbs([F.DELTA]), stream)
-            d_om = h2b.to_dev(F.fr_mont_limbs([dom.omega]), stream)
+            beta, gamma = chal(), chal()
+            # phase 3: permutation products (2 sets of 2 columns), lookup product, random polynomial
+            d_beta, d_gamma = h2b.to_dev(sc(beta), stream), h2b.to_dev(sc(gamma), stream)
+            d_delta = h2b.to_dev(sc(F.DELTA), stream)
+            d_om = h2b.to_dev(sc(dom.omega), stream)
             d_one = h2b.to_dev(sc(1), stream)
-            zs = []
-            for s in range(2):
+            cols = [adv[C.ADV_A], adv[C.ADV_B], adv[C.ADV_C], inst]
+            zs, prefix = [], d_one
+            for s in range(len(cols) // C.CHUNK_LEN):
+                mod = h2b.dev_empty(32 * n)
+                h2b.call("_halo2_poly_fill_one", h2b.ptr(mod), n, sh)
+                d_dw = h2b.to_dev(sc(pow(F.DELTA, C.CHUNK_LEN * s, p)), stream)
+                sl = slice(C.CHUNK_LEN * s, C.CHUNK_LEN * (s + 1))
+                h2b.permutation_product_device(mod, pk.sigma_values[sl], cols[sl], d_beta, d_gamma, d_delta, d_om,
+                                               d_dw, u, stream=stream)
                 z = h2b.dev_empty(32 * n)
-                h2b.call("_halo2_poly_fill_one", h2b.ptr(z), n, h2b.stream_handle(stream))
-                d_dw = h2b.to_dev(sc(pow(F.DELTA, 2 * s, F.R_MOD)), stream)
-                h2b.permutation_product_device(z, pk["sigma"][2 * s: 2 * s + 2], adv[2 * s: 2 * s + 2], d_beta,
-                                               d_gamma, d_delta, d_om, d_dw, n, stream=stream)
-                h2b.grand_product_device(z, d_one, n, stream=stream)
+                z[:32] = prefix
+                z[32: 32 * (u + 1)] = mod[: 32 * u]
+                h2b.grand_product_device(z, prefix, u, offset=1, stream=stream)
+                prefix = z[32 * u: 32 * (u + 1)]     # the carry: this set's last value seeds the next set
+                blind(z, u + 1, 10 + s)
                 zs.append(z)
-            zl = h2b.dev_empty(32 * n)
-            h2b.lookup_product_device(zl, pa, ps, lin, pk["table_col"], d_beta, d_gamma, n, stream=stream)
-            h2b.grand_product_device(zl, d_one, n, stream=stream)
+            zl, ratio = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+            h2b.lookup_product_device(ratio, pa, ps, b_col, t_col, d_beta, d_gamma, u, stream=stream)
+            zl[:32] = d_one
+            zl[32: 32 * (u + 1)] = ratio[: 32 * u]
+            h2b.grand_product_device(zl, d_one, u, offset=1, stream=stream)
+            blind(zl, u + 1, 12)
+            del ratio
             for z in zs + [zl]:
                 commit(z, lagrange=True)
-            h_rand = h2b.random_fr_device(n, seed * 64 + 5, 0, stream)
-            commit(h_rand)
             flush()
+            g_img = h2b.to_dev(_generator_image(), stream)       # the random polynomial's commitment, g[0]
+            commits.append(g_img)
+            if tr is not None:
+                tr.write_point(F.G1_GENERATOR)
             y = chal()
-            # 5. lagrange_to_coeff of the per-proof polynomials
-            lag = adv + [inst] + zs + [zl, pa, ps, lin]
+            # phase 4: coefficients, the quotient per extended part, h
+            lag = adv + [inst] + zs + [zl, pa, ps]
             coef = [h2b.dev_empty(32 * n) for _ in lag]
             h2b.fft_many_to_device(2, k, k, lag, coef, dom.omega_inv, dom.ifft_divisor, stream=stream)
             del lag
-            # 6. per extended part: coset-part NTTs, gate / permutation / lookup quotients.
-            #    Columns: advice 0-3, instance 4, z 5-6, lookup z 7, A' 8, S' 9,
-            #    compressed input 10, fixed 11-13, sigma 14-17, l0 18, l_last 19, l_active 20.
+            ca, ci, cz, czl, cpa, cps = coef[0:4], coef[4], coef[5:7], coef[7], coef[8], coef[9]
             d_y = h2b.to_dev(sc(y), stream)
             kcos = res.key_cosets(k, stream)
             own = [h2b.dev_empty(32 * n) for _ in coef]
+            tv = h2b.dev_empty(32 * n)
             hs = [h2b.dev_empty(32 * n) for _ in range(1 << (dom.extended_k - k))]
-            ext_w = dom.extended_omega
             nws = h2b.dev_empty(h2b.lib()._halo2_fft_many_to_device_workspace_size(6, k, k))
-            beta_v = F.fr_from_mont_limbs(beta)[0]
+            g_rules, g_parts, g_consts = pk.gates
+            l_rules, l_parts, l_consts = pk.lookup_graph
+            bg = np.concatenate([sc(beta), sc(gamma)])
             for j, hj in enumerate(hs):
-                shift = pow(ext_w, j, F.R_MOD)
-                h2b.fft_many_to_device(6, k, k, coef, own, dom.omega, F.ZETA * shift % F.R_MOD, ws=nws,
-                                       stream=stream)
-                parts = own + kcos[j]
-                h2b.quotient_device(parts[11:14], [parts[4]], parts[0:4], sc(theta), res.consts, y, res.rules,
-                                    res.parts, n, 1, 0, n, hj, None, stream=stream)
-                h2b.quotient_permutation_device(hj, parts[18], parts[19], parts[20], parts[5:7], parts[14:18],
-                                                parts[0:4], beta, gamma, sc(y), F.fr_mont_limbs([F.DELTA]),
-                                                sc(beta_v * F.ZETA), sc(shift), sc(dom.omega), 2, -3, 1, n, n,
+                shift = pow(dom.extended_omega, j, p)
+                h2b.fft_many_to_device(6, k, k, coef, own, dom.omega, F.ZETA * shift % p, ws=nws, stream=stream)
+                fx, sg, (l0, llast, lact) = kcos[j][0:3], kcos[j][3:7], kcos[j][7:10]
+                a_p, i_p, z_p, zl_p, pa_p, ps_p = own[0:4], own[4], own[5:7], own[7], own[8], own[9]
+                h2b.quotient_device(fx, [i_p], a_p, [], g_consts, y, g_rules, g_parts, n, 1, 0, n, hj,
+                                    stream=stream)
+                h2b.quotient_permutation_device(hj, l0, llast, lact, z_p, sg, [a_p[0], a_p[1], a_p[2], i_p], beta,
+                                                gamma, sc(y), sc(F.DELTA), sc(beta * F.ZETA), sc(shift),
+                                                sc(dom.omega), C.CHUNK_LEN, -(C.BLINDING_FACTORS + 1), 1, n, n,
                                                 stream=stream)
-                h2b.quotient_lookups_device(hj, parts[10], parts[7], parts[8], parts[9], parts[18], parts[19],
-                                            parts[20], d_beta, d_gamma, d_y, n, stream=stream)
-            del parts, own
-            # 7. h on the extended coset: gather the parts, divide by the vanishing
-            #    polynomial, back to coefficients (extended_to_coeff), commit its pieces
+                h2b.quotient_device(fx, [i_p], a_p, bg, l_consts, y, l_rules, l_parts, n, 1, 0, n, tv,
+                                    stream=stream)
+                h2b.quotient_lookups_device(hj, tv, zl_p, pa_p, ps_p, l0, llast, lact, d_beta, d_gamma, d_y, n,
+                                            stream=stream)
+            del own, tv
             en = len(hs) * n
             ext, hc = h2b.dev_empty(32 * en), h2b.dev_empty(32 * en)
             tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64), stream)
-            h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), len(hs), n,
-                     h2b.stream_handle(stream))
-            h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk["t_evals"]),
-                     len(dom.t_evaluations), en, h2b.stream_handle(stream))
+            h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), len(hs), n, sh)
+            h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk.t_evals),
+                     len(dom.t_evaluations), en, sh)
             h2b.fft_many_to_device(2, dom.extended_k, dom.extended_k, [ext], [hc], dom.extended_omega_inv,
                                    dom.extended_ifft_divisor, stream=stream)
             del ext, hs
             zp = h2b.to_dev(F.fr_mont_limbs([dom.g_coset_inv, dom.g_coset]), stream)
-            h2b.call("_halo2_distribute_powers_zeta", h2b.ptr(hc), h2b.ptr(zp), 2, en, h2b.stream_handle(stream))
-            for i in range(dom.quotient_poly_degree):
-                commit(_slice(hc, i, n))
+            h2b.call("_halo2_distribute_powers_zeta", h2b.ptr(hc), h2b.ptr(zp), 2, en, sh)
+            if self.check_degree:
+                self.h_degree_ok = not bool(hc[32 * n * dom.quotient_poly_degree:].any().item())
+            pieces = [_slice(hc, i, n) for i in range(dom.quotient_poly_degree)]
+            for piece in pieces:
+                commit(piece)
             flush()
-            # 8. opening (SHPLONK): the committed polynomials at x and their
-            #    rotations -- advice 0 at x, x w^-1; advice 3 (Fibonacci) at x, x w,
-            #    x w^2; the permutation products at x, x w, x w^last; the lookup
-            #    product at x, x w; A' at x, x w^-1; the rest at x
             x = chal()
-            w = dom.omega
-            at = lambda r: x * pow(w, r % n, F.R_MOD) % F.R_MOD  # noqa: E731
-            rots = {0: (0, -1), 3: (0, 1, 2), 5: (0, 1, -3), 6: (0, 1, -3), 7: (0, 1), 8: (0, -1)}
-            queries, labels = [], []
-            names = {0: "adv0", 1: "adv1", 2: "adv2", 3: "adv3", 5: "z0", 6: "z1", 7: "zl", 8: "pa", 9: "ps"}
-            for idx in (0, 1, 2, 3, 5, 6, 7, 8, 9):
-                queries += [(coef[idx], at(r)) for r in rots.get(idx, (0,))]
-                labels += [(names[idx], at(r)) for r in rots.get(idx, (0,))]
-            queries += [(c, at(0)) for c in pk["fixed"] + pk["sigma"]]
-            labels += [(f"vk{i}", at(0)) for i in range(len(pk["fixed"]) + len(pk["sigma"]))]
-            queries += [(_slice(hc, i, n), at(0)) for i in range(dom.quotient_poly_degree)]
-            labels += [(f"h{i}", at(0)) for i in range(dom.quotient_poly_degree)]
-            queries += [(h_rand, at(0))]
-            labels += [("hr", at(0))]
-            # what a verifier needs besides the proof: each query's polynomial
-            # (a label) and point, in the order the evaluations were written;
-            # labels name the proof's commitments in order (COMMIT_LABELS) or
-            # the verifying key's commitments ("vk0".., fixed then sigma)
+            # phase 5: h folded at x, the queries in the reference's order, the evaluations
+            xn = pow(x, n, p)
+            h_x = h2b.dev_empty(32 * n)
+            h_x.zero_()
+            for i, piece in enumerate(pieces):
+                h2b.call("_halo2_poly_multiply_add", h2b.ptr(h_x), h2b.ptr(piece),
+                         h2b.ptr(h2b.to_dev(sc(pow(xn, i, p)), stream)), n, sh)
+            queries, labels = open_queries_for(dom, x, {
+                **{f"adv{i}": c for i, c in enumerate(ca)}, "z0": cz[0], "z1": cz[1], "zl": czl, "pa": cpa,
+                "ps": cps, **{f"fixed{i}": c for i, c in enumerate(pk.fixed)},
+                **{f"sigma{i}": c for i, c in enumerate(pk.sigma)}, "h": h_x, "random": pk.random_poly})
             self.query_labels = labels
+            order = transcript_eval_order(dom, x)
             cws = h2b.dev_empty(h2b.lib().h2b_msm_table_workspace_size(n, tn))
+            written = []
 
             def commit_now(d):
                 out = h2b.dev_empty(96)
@@ -397,17 +437,65 @@ class ProofWorkload:
                 return out
 
             def write_evals(values):
-                if tr is not None:
-                    for e in values:
-                        tr.write_scalar(e % F.R_MOD)
+                at = dict(zip(labels, values))
+                for lab in order:
+                    written.append(at[lab])
+                    if tr is not None:
+                        tr.write_scalar(at[lab] % p)
 
-            opened, _, l_at_u = shplonk.open_queries(h2b, queries, iter(chal, None), commit_now, stream=stream,
-                                                     on_evals=write_evals)
+            _, _, l_at_u = shplonk.open_queries(h2b, queries, iter(chal, None), commit_now, stream=stream,
+                                                on_evals=write_evals)
             if l_at_u != 0:
                 raise RuntimeError("SHPLONK linearisation does not vanish at u")
-            evals.append(torch.from_numpy(np.ascontiguousarray(F.fr_mont_limbs(opened)).view(np.uint8).reshape(-1)))
+            evals = [torch.from_numpy(np.ascontiguousarray(F.fr_mont_limbs(written)).view(np.uint8).reshape(-1))]
         self.proof = tr.finalize() if tr is not None else None
         return commits, evals
+
+
+def _rot(dom, x, r):
+    return x * pow(dom.omega, r % dom.n, F.R_MOD) % F.R_MOD
+
+
+def open_queries_for(dom, x, polys):
+    """The opening's queries in the order create_proof builds them
+    (halo2_proofs/src/plonk/prover.rs:569-614): advice queries, then each
+    permutation set at x and w x and every set but the last at w^last x
+    (permutation/prover.rs:339-379), the lookup's five (lookup/verifier.rs:
+    175-210 order), fixed queries, the permutation polynomials at x, then
+    h folded and the random polynomial at x.  `polys` maps labels to
+    whatever stands for each polynomial (device vectors for the prover,
+    commitments for the verifier).  Returns ([(poly, point)], [(label, point)])."""
+    q = [(f"adv{c}", r) for c, r in C.ADVICE_QUERIES]
+    sets = len(C.PERM_COLUMNS) // C.CHUNK_LEN
+    for s in range(sets):
+        q += [(f"z{s}", 0), (f"z{s}", 1)]
+    for s in reversed(range(sets - 1)):
+        q.append((f"z{s}", -(C.BLINDING_FACTORS + 1)))
+    q += [("zl", 0), ("pa", 0), ("ps", 0), ("pa", -1), ("zl", 1)]
+    q += [(f"fixed{c}", r) for c, r in C.FIXED_QUERIES]
+    q += [(f"sigma{i}", 0) for i in range(len(C.PERM_COLUMNS))]
+    q += [("h", 0), ("random", 0)]
+    labels = [(lab, _rot(dom, x, r)) for lab, r in q]
+    return [(polys[lab], pt) for lab, pt in labels], labels
+
+
+def transcript_eval_order(dom, x):
+    """The (label, point) of each evaluation in the order the prover writes
+    them (prover.rs:386-560 and the verifier's reads, verifier.rs:200-225):
+    advice, fixed, the random polynomial, the permutation polynomials, each
+    permutation set's z(x), z(w x) and (all but the last set) z(w^last x),
+    then the lookup's z(x), z(w x), A'(x), A'(w^-1 x), S'(x)."""
+    o = [(f"adv{c}", r) for c, r in C.ADVICE_QUERIES]
+    o += [(f"fixed{c}", r) for c, r in C.FIXED_QUERIES]
+    o += [("random", 0)]
+    o += [(f"sigma{i}", 0) for i in range(len(C.PERM_COLUMNS))]
+    sets = len(C.PERM_COLUMNS) // C.CHUNK_LEN
+    for s in range(sets):
+        o += [(f"z{s}", 0), (f"z{s}", 1)]
+        if s + 1 < sets:
+            o.append((f"z{s}", -(C.BLINDING_FACTORS + 1)))
+    o += [("zl", 0), ("zl", 1), ("pa", 0), ("pa", -1), ("ps", 0)]
+    return [(lab, _rot(dom, x, r)) for lab, r in o]
 
 
 def requests(count, rate, seed, ks=(16, 18, 20, 22), weights=(0.4, 0.3, 0.2, 0.1)):
@@ -432,10 +520,15 @@ class Server:
     host clock."""
 
     def __init__(self, res, slots, hbm_budget, transcript=False):
-        """transcript=True proves with the Fiat-Shamir transcript; each
-        request's outputs then carry its proof bytes third."""
+        """hbm_budget counts every device byte the prover holds: the resident
+        state (the SRS and its window tables, proving keys and their coset
+        parts, Resident.device_bytes) and the requests in flight.
+        transcript=True proves with the Fiat-Shamir transcript; each
+        request's outputs then carry its proof bytes third and its public
+        inputs fourth."""
         self.res, self.slots, self.budget, self.transcript = res, slots, hbm_budget, transcript
         self.in_use = 0
+        self.avail = hbm_budget
         self.cv = threading.Condition()
         self.streams = [_t().cuda.Stream() for _ in range(slots)]
         self.q = queue.Queue()
@@ -471,7 +564,7 @@ class Server:
             k, seed, finish = job
             need = self.bytes_for(k)
             with self.cv:
-                while self.in_use + need > self.budget and self.in_use > 0:
+                while self.in_use + need > self.avail and self.in_use > 0:
                     self.cv.wait()
                 self.in_use += need
             try:
@@ -479,7 +572,7 @@ class Server:
                 out = w.run(st)
                 st.synchronize()
                 if self.transcript:
-                    out = (out[0], out[1], w.proof)
+                    out = (out[0], out[1], w.proof, w.public)
                 finish(time.perf_counter(), out, None)
             except Exception as e:  # handed to serve(), which raises it
                 finish(time.perf_counter(), None, e)
@@ -493,11 +586,16 @@ class Server:
         latencies (s), the makespan and, if asked, each request's outputs."""
         torch = _t()
         for _, k, _ in reqs:
-            if self.bytes_for(k) > self.budget:
-                raise ValueError(f"a 2^{k} proof needs more than the {self.budget}-byte budget")
             self.res.key_cosets(k)
             self.res.lagrange_table(k)
+            if self.transcript:
+                self.res.verifying_key(k)
         torch.cuda.synchronize()
+        self.avail = self.budget - self.res.device_bytes()
+        for _, k, _ in reqs:
+            if self.bytes_for(k) > self.avail:
+                raise ValueError(f"a 2^{k} proof needs {self.bytes_for(k)} bytes beside the resident "
+                                 f"{self.res.device_bytes()}, more than the {self.budget}-byte budget")
         done = [None] * len(reqs)
         outs = [None] * len(reqs)
         errors = []

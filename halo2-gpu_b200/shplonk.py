@@ -9,10 +9,16 @@ challenges y, v, u (from a seeded generator here, not a transcript):
   q_i(X) = sum_j y^j (p_ij(X) - r_ij(X)) / Z_{S_i}(X)   r_ij interpolates p_ij on S_i
   h(X)   = sum_i v^i q_i(X)                             -> commitment W
   L(X)   = sum_i v^i Z_{T \\ S_i}(u) sum_j y^j (p_ij(X) - r_ij(u)) - Z_T(u) h(X)
-  h'(X)  = L(X) / (X - u)                               -> commitment W'
+  h'(X)  = L(X) / ((X - u) Z_{T \\ S_0}(u))              -> commitment W'
 
 with T the union of all points.  L(u) = 0 whenever every evaluation is
 right, so the division is exact; `open_queries` returns it for checking.
+W' is normalised by the first set's coefficient 1 / Z_{T \\ S_0}(u), as the
+reference's prover scales its final quotient (prover.rs:423-430) and its
+verifier divides every set's coefficient by Z_{T \\ S_0}(u)
+(verifier.rs:82-96).  The factor is folded into L's coefficients here:
+set i enters with v^i Z_{T \\ S_i}(u) / Z_{T \\ S_0}(u) and h with
+-Z_T(u) / Z_{T \\ S_0}(u) = -Z_{S_0}(u), so no extra pass scales the quotient.
 Device
 work: Horner evaluations (_halo2_eval_polynomial), linear combinations
 (_halo2_poly_multiply_add), the interpolant subtraction
@@ -168,9 +174,11 @@ def open_queries(h2b, queries, challenges, commit, stream=None, on_evals=None):
         lin_terms.append((keys, vi, diff, short))
     w = commit(h)
     u = next(challenges) % P
-    # per rotation set: v^i Z_{T\S_i}(u) and the combined interpolant at u
-    lin_terms = [(keys, vi * _vanishing_at(diff, u) % P, _eval_host(short, u)) for keys, vi, diff, short in lin_terms]
-    # L = sum_i v^i Z_{T\S_i}(u) sum_j y^j (p_ij - r_ij(u)) - Z_T(u) h
+    # per rotation set: v^i Z_{T\S_i}(u) / Z_{T\S_0}(u) and the combined interpolant at u
+    z0_diff_inv = pow(_vanishing_at(lin_terms[0][2], u), -1, P)
+    lin_terms = [(keys, vi * _vanishing_at(diff, u) * z0_diff_inv % P, _eval_host(short, u))
+                 for keys, vi, diff, short in lin_terms]
+    # L / Z_{T\S_0}(u) = sum_i v^i Z_{T\S_i}(u) / Z_{T\S_0}(u) sum_j y^j (p_ij - r_ij(u)) - Z_{S_0}(u) h
     lx = sp.zeros()
     const = 0
     for keys, c_i, r_at_u in lin_terms:
@@ -178,7 +186,7 @@ def open_queries(h2b, queries, challenges, commit, stream=None, on_evals=None):
             sp.madd(lx, polys[key], c_i * pow(y, j, P))
         const = (const + c_i * r_at_u) % P
     h2b.call("_halo2_poly_sub_scalar_at_zero", h2b.ptr(lx), h2b.ptr(sp._scalar(const)), sp.sh)
-    sp.madd(lx, h, -_vanishing_at(super_points, u))
+    sp.madd(lx, h, -_vanishing_at(list(sets)[0], u))
     l_at_u = sp.eval(lx, u)
     q = sp.zeros()
     sp.div_linear(lx, q, u)

@@ -16,6 +16,8 @@
  *   o_batch_invert          zero-preserving Montgomery trick,
  *                           halo2_proofs/cuda/include/kernel/inverse.h:10-63
  *   o_grand_product         halo2_proofs/src/cuda/culib.rs:202-230 semantics
+ *   o_fr_eval, o_fr_eval_many  Horner evaluation, eval_polynomial,
+ *                           halo2_proofs/src/arithmetic.rs (coefficients low first)
  *   o_lookup_product        lookup_product_cpu, halo2_proofs/src/cpu/arithmetic.rs:158-197
  *   o_permutation_product   permutation_product_cpu, halo2_proofs/src/cpu/arithmetic.rs:287-327
  *   o_permute_pair          permute_expression_pair_seq,
@@ -267,32 +269,38 @@ static inline uint64_t bitrev64(uint64_t x, int k)
     return r;
 }
 
-/* In-place radix-2 DIT with natural-order input/output: A_j = sum a_i w^(ij). */
+/* In-place radix-2 DIT with natural-order input/output: A_j = sum a_i w^(ij).
+ * Each stage is one parallel loop over its n/2 butterflies (so the last
+ * stages, with few blocks, still use every thread), as best_fft splits its
+ * work over the host threads. */
 static void fft_inplace(fe* a, int k, fe w)
 {
     uint64_t n = 1ull << k;
-    for (uint64_t i = 0; i < n; i++) {
-        uint64_t j = bitrev64(i, k);
-        if (i < j) { fe t = a[i]; a[i] = a[j]; a[j] = t; }
+#pragma omp parallel for schedule(static) if (n >= (1u << 14))
+    for (long i = 0; i < (long)n; i++) {
+        uint64_t j = bitrev64((uint64_t)i, k);
+        if ((uint64_t)i < j) { fe t = a[i]; a[i] = a[j]; a[j] = t; }
     }
-    /* twiddle table w^e, e < n/2 */
+    /* twiddle table w^e, e < n/2, in chunks that start from w^(chunk start) */
     uint64_t half = n / 2;
     fe* tw = (fe*)malloc(sizeof(fe) * (half ? half : 1));
-    if (half) {
-        tw[0] = f_one(&FR);
-        for (uint64_t e = 1; e < half; e++) tw[e] = f_mul(&FR, tw[e - 1], w);
+    const uint64_t TC = 4096;
+#pragma omp parallel for schedule(static) if (half >= (1u << 14))
+    for (long c = 0; c < (long)((half + TC - 1) / TC); c++) {
+        uint64_t e0 = (uint64_t)c * TC, e1 = e0 + TC < half ? e0 + TC : half;
+        fe p = f_pow_u64(&FR, w, e0);
+        for (uint64_t e = e0; e < e1; e++) { tw[e] = p; p = f_mul(&FR, p, w); }
     }
     for (int s = 0; s < k; s++) {
         uint64_t m = 1ull << s, step = n >> (s + 1);
 #pragma omp parallel for schedule(static) if (n >= (1u << 14))
-        for (long blk = 0; blk < (long)(n >> (s + 1)); blk++) {
-            uint64_t base = (uint64_t)blk << (s + 1);
-            for (uint64_t j = 0; j < m; j++) {
-                fe x = a[base + j];
-                fe y = f_mul(&FR, a[base + j + m], tw[j * step]);
-                a[base + j] = f_add(&FR, x, y);
-                a[base + j + m] = f_sub(&FR, x, y);
-            }
+        for (long t = 0; t < (long)half; t++) {
+            uint64_t j = (uint64_t)t & (m - 1);
+            uint64_t base = ((uint64_t)t >> s) << (s + 1);
+            fe x = a[base + j];
+            fe y = f_mul(&FR, a[base + j + m], tw[j * step]);
+            a[base + j] = f_add(&FR, x, y);
+            a[base + j + m] = f_sub(&FR, x, y);
         }
     }
     free(tw);
@@ -320,12 +328,14 @@ int o_ntt(uint32_t type, uint32_t log_n, uint32_t log_ext, const fe* in, fe* out
         memcpy(out, in, n * sizeof(fe));
         fe z[3] = {f_one(&FR), ZETA, ZETA2};
         if (type == 3) {
-            for (uint64_t i = 0; i < N; i++) out[i] = f_mul(&FR, out[i], z[i % 3]);
+#pragma omp parallel for schedule(static) if (n >= (1u << 14))
+            for (long i = 0; i < (long)n; i++) out[i] = f_mul(&FR, out[i], z[i % 3]);
             fft_inplace(out, (int)log_ext, *omega);
         } else {
             fft_inplace(out, (int)log_ext, *omega);
             fe zi[3] = {f_one(&FR), ZETA2, ZETA};
-            for (uint64_t i = 0; i < N; i++) out[i] = f_mul(&FR, f_mul(&FR, out[i], *divisor), zi[i % 3]);
+#pragma omp parallel for schedule(static) if (N >= (1u << 14))
+            for (long i = 0; i < (long)N; i++) out[i] = f_mul(&FR, f_mul(&FR, out[i], *divisor), zi[i % 3]);
         }
         return 0;
     }
@@ -386,7 +396,29 @@ static jac j_from_aff(aff a)
     return r;
 }
 
-static jac j_madd(jac p, aff a) { return j_add(p, j_from_aff(a)); }
+/* Mixed addition p + a with a affine (Z2 = 1): the formulas of j_add with
+ * U1 = X1 and S1 = Y1, 8M + 3S -- the bucket addition of halo2curves'
+ * multiexp (affine bases added into projective buckets). */
+static jac j_madd(jac p, aff a)
+{
+    if (a_is_inf(&a)) return p;
+    if (j_is_inf(&p)) return j_from_aff(a);
+    const field_t* F = &FQ;
+    fe Z1Z1 = f_mul(F, p.Z, p.Z);
+    fe U2 = f_mul(F, a.x, Z1Z1);
+    fe S2 = f_mul(F, f_mul(F, a.y, p.Z), Z1Z1);
+    fe H = f_sub(F, U2, p.X), R = f_sub(F, S2, p.Y);
+    if (f_is_zero(H)) {
+        if (f_is_zero(R)) return j_dbl(p);
+        return j_inf();
+    }
+    fe HH = f_mul(F, H, H), HHH = f_mul(F, H, HH), V = f_mul(F, p.X, HH);
+    jac r;
+    r.X = f_sub(F, f_sub(F, f_mul(F, R, R), HHH), f_dbl(F, V));
+    r.Y = f_sub(F, f_mul(F, R, f_sub(F, V, r.X)), f_mul(F, p.Y, HHH));
+    r.Z = f_mul(F, p.Z, H);
+    return r;
+}
 
 /* The reference's 96-byte result image: affine with Z = 1, or (0, 1, 0). */
 static jac j_normalize(jac p)
@@ -437,7 +469,9 @@ int o_g1_on_curve(const aff* p)
     return f_eq(lhs, rhs);
 }
 
-/* [tau^i] G for i < n (small n: one scalar multiplication per point). */
+/* [tau^i] G for i < n: fixed-base multiplication over byte windows, with a
+ * table T[w][d] = [d 256^w] G (32 x 255 affine points, built once per call),
+ * so each point costs 32 mixed additions and one inversion. */
 void o_srs(const fe* tau, size_t n, aff* out)
 {
     aff g;
@@ -445,12 +479,31 @@ void o_srs(const fe* tau, size_t n, aff* out)
     fe* pw = (fe*)malloc(sizeof(fe) * (n ? n : 1));
     fe p = f_one(&FR);
     for (size_t i = 0; i < n; i++) { pw[i] = p; p = f_mul(&FR, p, *tau); }
-#pragma omp parallel for schedule(dynamic, 16)
+    aff* T = (aff*)malloc(sizeof(aff) * 32 * 255);
+    jac base = j_from_aff(g);
+    for (int w = 0; w < 32; w++) {
+        jac acc = base;
+        for (int d = 1; d <= 255; d++) {
+            jac q = j_normalize(acc);
+            T[w * 255 + d - 1].x = q.X;
+            T[w * 255 + d - 1].y = q.Y;
+            acc = j_add(acc, base);
+        }
+        for (int b = 0; b < 8; b++) base = j_dbl(base);
+    }
+#pragma omp parallel for schedule(dynamic, 64)
     for (long i = 0; i < (long)n; i++) {
-        jac r = j_normalize(j_mul(j_from_aff(g), f_from_mont(&FR, pw[i])));
+        fe s = f_from_mont(&FR, pw[i]);
+        jac r = j_inf();
+        for (int w = 0; w < 32; w++) {
+            unsigned d = (unsigned)((s.v[w >> 3] >> (8 * (w & 7))) & 0xFF);
+            if (d) r = j_madd(r, T[w * 255 + d - 1]);
+        }
+        r = j_normalize(r);
         if (j_is_inf(&r)) { out[i].x = f_zero(); out[i].y = f_zero(); }
         else { out[i].x = r.X; out[i].y = r.Y; }
     }
+    free(T);
     free(pw);
 }
 
@@ -803,6 +856,22 @@ int o_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+/* f(x_j) for m points at once: each thread runs Horner for its share of the
+ * points in one pass over the coefficients (Montgomery in, Montgomery out). */
+void o_fr_eval_many(const fe* coeffs, size_t n, const fe* xs, size_t m, fe* out)
+{
+    const long B = 8;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long j0 = 0; j0 < (long)m; j0 += B) {
+        long cnt = (long)m - j0 < B ? (long)m - j0 : B;
+        fe acc[8];
+        for (long t = 0; t < cnt; t++) acc[t] = f_zero();
+        for (long i = (long)n - 1; i >= 0; i--)
+            for (long t = 0; t < cnt; t++) acc[t] = f_add(&FR, f_mul(&FR, acc[t], xs[j0 + t]), coeffs[i]);
+        for (long t = 0; t < cnt; t++) out[j0 + t] = acc[t];
+    }
 }
 
 /* f(x) = sum_i c_i x^i by Horner (Montgomery in, Montgomery out). */

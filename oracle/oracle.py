@@ -56,6 +56,8 @@ def lib():
         _lib.o_from_mont.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
         _lib.o_fr_pow.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p]
         _lib.o_fr_eval.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+        _lib.o_fr_eval_many.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_void_p]
         for n in ("o_field_mul", "o_field_add", "o_field_sub"):
             getattr(_lib, n).argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib.o_field_inv.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
@@ -231,6 +233,15 @@ def fr_eval(coeffs, x):
     xx = _fe(x)
     out = np.zeros((1, 4), dtype=np.uint64)
     lib().o_fr_eval(_p(c), c.shape[0], _p(xx), _p(out))
+    return out
+
+
+def fr_eval_many(coeffs, xs):
+    """[sum_i c_i x^i for x in xs] (Montgomery limbs in and out), threads over the points."""
+    c = _fe(coeffs)
+    pts = _fe(xs)
+    out = np.zeros((pts.shape[0], 4), dtype=np.uint64)
+    lib().o_fr_eval_many(_p(c), c.shape[0], _p(pts), pts.shape[0], _p(out))
     return out
 
 

@@ -112,3 +112,25 @@ def test_full_size_roundtrip_k22_ext24(h2b, orc, cuda):
     got = [f.from_mont(v) * zi[i % 3] % f.R_MOD for v, i in zip(f.limbs_to_ints(back[sel]), sel)]
     want = [f.from_mont(v) for v in f.limbs_to_ints(a[sel])]
     assert got == want
+
+
+def test_full_size_coset_extension_k22_ext24_against_cpu(h2b, orc, cuda):
+    """coeff_to_extended 2^22 -> 2^24 (the k=22 benchmark's coset NTT) checked
+    against the CPU, not against a device inverse: output i is the input
+    polynomial at zeta * w_ext^i, evaluated by the oracle's Horner at 259
+    indices -- 0, 1, 2, N/2 and N-1, and one seeded index in every 2^16 block
+    of the output.  Bit-exact."""
+    import random
+    f = h2b.fields
+    k, ek = 22, 24
+    d = f.EvaluationDomain(5, k)
+    n, N = 1 << k, 1 << ek
+    d_a = h2b.random_fr_device(n, 4321)
+    d_ext = h2b.dev_empty(32 * N)
+    h2b.fft_many_to_device(3, k, ek, [d_a], [d_ext], d.extended_omega, 1, input_on_device=True)
+    rng = random.Random(22)
+    idx = sorted({0, 1, 2, N // 2, N - 1} | {b + rng.randrange(1 << 16) for b in range(0, N, 1 << 16)})
+    pts = [f.ZETA * pow(d.extended_omega, i, f.R_MOD) % f.R_MOD for i in idx]
+    want = orc.fr_eval_many(h2b.to_host(d_a), f.fr_mont_limbs(pts))
+    ext = h2b.to_host(d_ext)
+    assert_limbs_equal(ext[np.array(idx)], want, "coset extension 2^22 -> 2^24 vs CPU evaluation")

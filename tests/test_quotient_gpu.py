@@ -42,7 +42,7 @@ def run_both(h2b, orc, g, parts, nf, ni, na, nch, nq, rot_scale, row_start, row_
     assert_limbs_equal(got, want, "host quotient")
 
 
-@pytest.mark.parametrize("nq,rot_scale", [(1 << 10, 1), (1 << 12, 4), (1 << 16, 4)])
+@pytest.mark.parametrize("nq,rot_scale", [(1 << 10, 1), (1 << 12, 4), (1 << 16, 4), (1 << 18, 1)])
 def test_plonk_fibonacci_gates(h2b, orc, cuda, nq, rot_scale):
     g = R.Graph()
     parts = R.plonk_and_fibonacci(g)
@@ -76,8 +76,8 @@ def test_degenerate_zero_columns(h2b, orc, cuda):
     run_both(h2b, orc, g, parts, 1, 0, 1, 0, 1 << 9, 1, 0, 1 << 9)
 
 
-def test_lookup_quotient(h2b, orc, cuda):
-    n = 1 << 14
+@pytest.mark.parametrize("n", [1 << 14, 1 << 20])
+def test_lookup_quotient(h2b, orc, cuda, n):
     arrs = [orc.chacha_fr(10 + i, n) for i in range(8)]
     beta, gamma, y = (orc.chacha_fr(30 + i, 1) for i in range(3))
     want = orc.quotient_lookups(*arrs, beta, gamma, y)
@@ -86,10 +86,10 @@ def test_lookup_quotient(h2b, orc, cuda):
     assert_limbs_equal(h2b.to_host(d[0]), want, "lookup quotient")
 
 
-@pytest.mark.parametrize("ncols,chunk_len", [(4, 2), (5, 2), (3, 3)])
-def test_permutation_quotient(h2b, orc, cuda, ncols, chunk_len):
+@pytest.mark.parametrize("ncols,chunk_len,n", [(4, 2, 1 << 12), (5, 2, 1 << 12), (3, 3, 1 << 12), (4, 2, 1 << 20)])
+def test_permutation_quotient(h2b, orc, cuda, ncols, chunk_len, n):
+    """Up to one full extended part of the k = 20 proof (2^20 rows, 4 columns in 2 sets)."""
     f = h2b.fields
-    n = 1 << 12
     nsets = (ncols + chunk_len - 1) // chunk_len
     values = orc.chacha_fr(1, n)
     cols = [orc.chacha_fr(10 + i, n) for i in range(ncols)]

@@ -27,7 +27,8 @@ def _synth_div(coeffs, s, p):
 
 
 def _restate(polys, queries, y, v, u, p, S):
-    """Host SHPLONK: returns h and h' coefficient lists."""
+    """Host SHPLONK: returns h and h' coefficient lists, h' normalised by
+    1 / Z_{T\\S_0}(u) as the reference's prover does (prover.rs:423-430)."""
     pe = {}
     for k, x in queries:
         pe.setdefault(k, {})[x] = S._eval_host(polys[k], x)
@@ -36,6 +37,8 @@ def _restate(polys, queries, y, v, u, p, S):
         sets.setdefault(tuple(sorted(d)), []).append(k)
     n = len(polys[0])
     sup = sorted({x for s in sets for x in s})
+    first = list(sets)[0]
+    z0_diff_inv = pow(S._vanishing_at([x for x in sup if x not in first], u), -1, p)
     h = [0] * n
     lx = [0] * n
     const = 0
@@ -54,13 +57,13 @@ def _restate(polys, queries, y, v, u, p, S):
             num = _synth_div(num, s, p)
         vi = pow(v, i, p)
         h = [(a + vi * b) % p for a, b in zip(h, num)]
-        c = vi * S._vanishing_at([x for x in sup if x not in pts], u) % p
+        c = vi * S._vanishing_at([x for x in sup if x not in pts], u) * z0_diff_inv % p
         for j, k in enumerate(ks):
             cj = c * pow(y, j, p) % p
             lx = [(a + cj * b) % p for a, b in zip(lx, polys[k])]
         const = (const + c * r_u) % p
     lx[0] = (lx[0] - const) % p
-    zt = S._vanishing_at(sup, u)
+    zt = S._vanishing_at(sup, u) * z0_diff_inv % p       # = Z_{S_0}(u)
     lx = [(a - zt * b) % p for a, b in zip(lx, h)]
     assert S._eval_host(lx, u) == 0
     return h, _synth_div(lx, u, p)

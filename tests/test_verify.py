@@ -35,3 +35,27 @@ def test_trapdoor_check_accepts_opening_and_rejects_changes(h2b):
     cm2 = dict(cm)
     cm2[3] = F.g1_add(cm[3], F.G1_GENERATOR)
     assert not V.shplonk_check_trapdoor(cm2, queries, evals, y, v, u, W, W2, tau)
+
+
+def test_trapdoor_check_rejects_an_unnormalised_w2(h2b):
+    """W' must be the commitment to L(X) / ((X - u) Z_{T\\S_0}(u)), as the
+    reference's prover scales it (shplonk/prover.rs:423-430): the quotient
+    without the factor fails the check whenever Z_{T\\S_0}(u) != 1."""
+    F = h2b.fields
+    S = importlib.import_module(h2b.__name__ + ".shplonk")
+    V = importlib.import_module(h2b.__name__ + ".verify")
+    p, rng = F.R_MOD, random.Random(9)
+    n, tau = 8, rng.randrange(2, p)
+    polys = [[rng.randrange(p) for _ in range(n)] for _ in range(3)]
+    x, w = rng.randrange(p), pow(F.ROOT_OF_UNITY, 1 << (F.S - 3), p)
+    queries = [(0, x), (1, x), (1, x * w % p), (2, x * w % p)]
+    y, v, u = (rng.randrange(p) for _ in range(3))
+    h, q = _restate(polys, queries, y, v, u, p, S)
+    commit = lambda c: F.g1_mul(F.G1_GENERATOR, S._eval_host(c, tau))  # noqa: E731
+    cm = {i: commit(c) for i, c in enumerate(polys)}
+    evals = [S._eval_host(polys[k], pt) for k, pt in queries]
+    assert V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, commit(h), commit(q), tau)
+    z0_diff = S._vanishing_at([x * w % p], u)          # T \ S_0 for S_0 = {x}
+    assert z0_diff != 1
+    raw = [c * z0_diff % p for c in q]
+    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, commit(h), commit(raw), tau)
