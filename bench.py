@@ -112,6 +112,43 @@ def peaks():
     return 6650.0, "fallback"
 
 
+class UtilSampler:
+    """nvidia-smi GPU utilisation (the fraction of time a kernel ran) sampled
+    every 100 ms while a serving trace runs."""
+
+    def __init__(self, gpu_index):
+        self.gpu, self.proc, self.vals = gpu_index, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=utilization.gpu",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            try:
+                self.vals.append(float(line.strip()))
+            except ValueError:
+                pass
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        v = sorted(self.vals)
+        return {"median_pct": v[len(v) // 2], "mean_pct": round(sum(v) / len(v), 1), "samples": len(v)} if v else None
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -398,8 +435,10 @@ def rows_section(h2b, torch, hbm_gbs, product_peak, k=20, reps=5):
     d_pa, d_ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
     d_tab = torch.zeros(32 * n, dtype=torch.uint8, device="cuda")
     d_tab[: 32 * 256] = tab
-    timed("permute_pair_t256", lambda: h2b.permute_expression_pair_device(d_in, d_tab, d_pa, d_ps, n, n - 10,
-                                                                          stream=side), n, "rows", 4 * 32)
+    pws = h2b.dev_empty(L._halo2_permute_expression_pair_workspace_size(n, n - 10))
+    timed("permute_pair_t256", lambda: h2b.call("_halo2_permute_expression_pair", h2b.ptr(d_in), h2b.ptr(d_tab),
+                                                h2b.ptr(d_pa), h2b.ptr(d_ps), n, n - 10, h2b.ptr(pws), pws.numel(),
+                                                h2b.stream_handle(side)), n, "rows", 4 * 32)
     # a5: coset extension parts (CosetFFT_Part) for 8 polynomials, one part
     polys = [rnd(n, 140 + i) for i in range(8)]
     outs = [h2b.dev_empty(32 * n) for _ in polys]
@@ -506,7 +545,9 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
         row = {"arrival_rate_per_s": round(load / mean_s, 3)}
         for name, srv in (("plain", plain), ("served", served)):
             torch.cuda.reset_peak_memory_stats()
+            util = UtilSampler(torch.cuda.current_device()).start()
             row[name] = P.summary(reqs, srv.serve(reqs))
+            row[name]["gpu_utilisation"] = util.stop()
             row[name]["hbm_peak_GB"] = round(torch.cuda.max_memory_allocated() / 1e9, 2)
         out["loads"][str(load)] = row
     plain.close()
@@ -515,64 +556,90 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
 
 
 def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
-    """Batched jobs of uneven size: n_jobs jobs with k drawn from {14, 16, 18,
-    20} (weights .4/.3/.2/.1, seeded), each one MSM with uniform scalars
-    against a shared 2^20 SRS and one coset extension 2^k -> 2^(k+2).  Plain:
-    one job after another through h2b_msm_device and _halo2_fft_many_to_device
-    on one stream.  Batched: the same calls spread over `streams` forked
-    streams (h2b_exec_fork / h2b_msm_batch), captured once into a CUDA graph
-    and replayed.  Outputs of both must be identical; times are CUDA events."""
+    """Batched jobs of uneven size (the 64-job configuration): n_jobs jobs with
+    k drawn from {14, 16, 18, 20} (weights .4/.3/.2/.1, seeded); each job is
+    one MSM with uniform scalars against a shared 2^20 SRS, one forward Fr
+    NTT of its 2^k polynomial, one coset extension 2^k -> 2^(k+2), and one
+    evaluation of the config-3 gate set (PLONK + Fibonacci gates, rules.py)
+    over that extended coset (rot_scale 4; the job's extension as its advice
+    columns, fixed and instance columns shared per k).  Plain: one job after
+    another on one stream (h2b_msm_device, _halo2_fft_many_to_device per
+    transform, the resident quotient program).  Batched: the NTTs of all jobs
+    of one size as one launch per transform type (up to 32 polynomials each)
+    on that size's forked stream, followed there by the size's quotient
+    runs; the MSMs through h2b_msm_batch over the forked streams; captured
+    once into a CUDA graph and replayed.  Outputs of both must be identical;
+    times are CUDA events."""
     import random
+    import numpy as np
     f = h2b.fields
     L = h2b.lib()
+    spec = importlib.util.spec_from_file_location("h2b_rules_b", os.path.join(ROOT, "halo2-gpu_b200", "rules.py"))
+    R = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(R)
     rng = random.Random(seed)
     ks = rng.choices([14, 16, 18, 20], weights=[4, 3, 2, 1], k=n_jobs)
+    sizes = sorted(set(ks))
     srs = h2b.srs_device(0x5EED20, 1 << 20)
     d_sc = [h2b.random_fr_device(1 << k, 5000 + i, 0) for i, k in enumerate(ks)]
     d_in = [h2b.random_fr_device(1 << k, 6000 + i, 0) for i, k in enumerate(ks)]
-    d_ext = [h2b.dev_empty(32 << (k + 2)) for k in ks]
-    d_ext_plain = [h2b.dev_empty(32 << (k + 2)) for k in ks]
-    d_msm = [h2b.dev_empty(96) for _ in ks]
-    d_msm_plain = [h2b.dev_empty(96) for _ in ks]
-    doms = {k: f.EvaluationDomain(3, k) for k in set(ks)}
-    d_om = {k: h2b.to_dev(f.fr_mont_limbs([doms[k].extended_omega])) for k in doms}
+    outs = {name: [h2b.dev_empty(sz(k)) for k in ks] for name, sz in
+            (("msm", lambda k: 96), ("fwd", lambda k: 32 << k), ("ext", lambda k: 32 << (k + 2)),
+             ("q", lambda k: 32 << (k + 2)))}
+    plain_outs = {name: [h2b.dev_empty(t.numel()) for t in v] for name, v in outs.items()}
+    doms = {k: f.EvaluationDomain(3, k) for k in sizes}
     one = f.fr_mont_limbs([1])
     one_ffi = h2b.host_ffi(one)
-    kmax = max(ks)
-    ntt_ws = [h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(3, kmax, kmax + 2)) for _ in range(streams)]
-    msm_ws = h2b.msm_workspace(1 << kmax)
-    tabs = [(h2b.ffi_array([d_in[i].data_ptr()]), h2b.ffi_array([d_ext[i].data_ptr()]),
-             h2b.ffi_array([d_ext_plain[i].data_ptr()])) for i in range(n_jobs)]
-
-    def coset(i, out_tab, ws, st):
-        k = ks[i]
-        h2b.call("_halo2_fft_many_to_device", 3, 1, k, k + 2, tabs[i][0], out_tab, h2b.ptr(d_om[k]),
-                 ctypes.byref(one_ffi), True, h2b.ptr(ws), ws.numel(), h2b.stream_handle(st))
-
+    d_om = {k: h2b.to_dev(f.fr_mont_limbs([doms[k].omega])) for k in sizes}
+    d_omx = {k: h2b.to_dev(f.fr_mont_limbs([doms[k].extended_omega])) for k in sizes}
+    # the gate set and its shared columns per size
+    g = R.Graph()
+    vps = np.array(R.plonk_and_fibonacci(g), dtype=np.uint64)
+    rules = np.array(g.rules, dtype=np.uint64)
+    consts = f.fr_mont_limbs(g.constants)
+    chal = f.fr_mont_limbs([0xC4A11])
+    shared = {k: ([h2b.random_fr_device(1 << (k + 2), 7000 + 10 * k + j, 0) for j in range(3)],
+                  [h2b.random_fr_device(1 << (k + 2), 7005 + 10 * k, 0)]) for k in sizes}
+    progs = {}
+    for which in ("batched", "plain"):
+        ext = outs["ext"] if which == "batched" else plain_outs["ext"]
+        progs[which] = [h2b.ResidentQuotient(shared[k][0], shared[k][1], [ext[i]] * 4, chal, consts, 0x1234567,
+                                             rules, vps, 1 << (k + 2), 4) for i, k in enumerate(ks)]
     side = torch.cuda.Stream()
+    ws1 = {k: h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(1, k, k)) for k in sizes}
+    ws3 = {k: h2b.dev_empty(L._halo2_fft_many_to_device_workspace_size(3, k, k + 2)) for k in sizes}
+    msm_ws = h2b.msm_workspace(1 << max(ks))
+
+    def ntt_many(typ, k, ins, outs_, st):
+        for c in range(0, len(ins), 32):
+            a, b = ins[c:c + 32], outs_[c:c + 32]
+            om = d_om[k] if typ == 1 else d_omx[k]
+            ws = ws1[k] if typ == 1 else ws3[k]
+            h2b.call("_halo2_fft_many_to_device", typ, len(a), k, k + 2 if typ == 3 else k,
+                     h2b.ffi_array([t.data_ptr() for t in a]), h2b.ffi_array([t.data_ptr() for t in b]),
+                     h2b.ptr(om), ctypes.byref(one_ffi), True, h2b.ptr(ws), ws.numel(), h2b.stream_handle(st))
 
     def plain():
         for i, k in enumerate(ks):
-            h2b.call("h2b_msm_device", h2b.ptr(d_sc[i]), h2b.ptr(srs), h2b.ptr(d_msm_plain[i]), 1 << k,
+            h2b.call("h2b_msm_device", h2b.ptr(d_sc[i]), h2b.ptr(srs), h2b.ptr(plain_outs["msm"][i]), 1 << k,
                      h2b.ptr(msm_ws), msm_ws.numel(), h2b.stream_handle(side))
-            coset(i, tabs[i][2], ntt_ws[0], side)
+            ntt_many(1, k, [d_in[i]], [plain_outs["fwd"][i]], side)
+            ntt_many(3, k, [d_in[i]], [plain_outs["ext"][i]], side)
+            progs["plain"][i].run(plain_outs["q"][i], stream=side)
 
-    jobs = h2b.msm_batch_jobs(d_sc, [srs] * n_jobs, d_msm, [1 << k for k in ks])
-    bws = h2b.msm_batch_workspace(jobs, n_jobs, streams)
-    order = sorted(range(n_jobs), key=lambda i: -ks[i])
+    groups = {k: [i for i in range(n_jobs) if ks[i] == k] for k in sizes}
 
-    def batched():
-        # coset jobs go onto the forked streams, longest first onto the least
-        # loaded; the MSM batch forks the same streams again without a join in
-        # between, so MSMs queue behind each stream's NTTs and the two kinds
-        # overlap across streams; its join covers both
+    def batched(bases, table_n=0):
         subs = h2b.exec_fork(streams, side)
-        load = [0] * streams
-        for i in order:
-            s = load.index(min(load))
-            load[s] += 1 << ks[i]
-            coset(i, tabs[i][1], ntt_ws[s], subs[s])
-        h2b.msm_batch(jobs, n_jobs, streams, bws, stream=side)
+        for gi, k in enumerate(sorted(sizes, reverse=True)):
+            st = subs[gi]
+            idx = groups[k]
+            ntt_many(1, k, [d_in[i] for i in idx], [outs["fwd"][i] for i in idx], st)
+            ntt_many(3, k, [d_in[i] for i in idx], [outs["ext"][i] for i in idx], st)
+            for i in idx:
+                progs["batched"][i].run(outs["q"][i], stream=st)
+        jobs = h2b.msm_batch_jobs(d_sc, [bases] * n_jobs, outs["msm"], [1 << k for k in ks], table_n=table_n)
+        h2b.msm_batch(jobs, n_jobs, streams, bws[table_n], stream=side)
 
     def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -583,23 +650,32 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
         side.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    def graph_time(bases, table_n=0):
+        batched(bases, table_n)      # warm-up: forked streams, kernels loaded
+        side.synchronize()
+        gr = h2b.Graph(side)
+        gr.begin()
+        batched(bases, table_n)
+        gr.end()
+        try:
+            gr.launch(side)
+            side.synchronize()
+            return timed(lambda: gr.launch(side))
+        finally:
+            gr.close()
+
+    def identical():
+        torch.cuda.synchronize()
+        return all(torch.equal(outs[nm][i], plain_outs[nm][i]) for nm in outs for i in range(n_jobs))
+
+    jobs0 = h2b.msm_batch_jobs(d_sc, [srs] * n_jobs, outs["msm"], [1 << k for k in ks])
+    bws = {0: h2b.msm_batch_workspace(jobs0, n_jobs, streams)}
     plain()
-    batched()  # warm-up: creates the forked streams, loads every kernel
     side.synchronize()
     t_plain = timed(plain)
-    t_batched_streams = timed(batched)
-    g = h2b.Graph(side)
-    g.begin()
-    batched()
-    g.end()
-    try:
-        g.launch(side)
-        side.synchronize()
-        t_graph = timed(lambda: g.launch(side))
-    finally:
-        g.close()
-    same = all(d_msm[i].cpu().numpy().tobytes() == d_msm_plain[i].cpu().numpy().tobytes() and
-               d_ext[i].cpu().numpy().tobytes() == d_ext_plain[i].cpu().numpy().tobytes() for i in range(n_jobs))
+    t_streams = timed(lambda: batched(srs))
+    t_graph = graph_time(srs)
+    same = identical()
     # served form: the shared SRS kept resident with its window multiples
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(side)
@@ -607,28 +683,17 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
     e1.record(side)
     side.synchronize()
     t_pre = e0.elapsed_time(e1)
-    for o in d_msm:
+    for o in outs["msm"]:
         o.zero_()
-    jobs = h2b.msm_batch_jobs(d_sc, [table] * n_jobs, d_msm, [1 << k for k in ks], table_n=1 << 20)
-    bws = h2b.msm_batch_workspace(jobs, n_jobs, streams)
-    batched()
-    side.synchronize()
-    g = h2b.Graph(side)
-    g.begin()
-    batched()
-    g.end()
-    try:
-        g.launch(side)
-        side.synchronize()
-        t_table = timed(lambda: g.launch(side))
-    finally:
-        g.close()
-    same = same and all(d_msm[i].cpu().numpy().tobytes() == d_msm_plain[i].cpu().numpy().tobytes()
-                        for i in range(n_jobs))
+    jobs_t = h2b.msm_batch_jobs(d_sc, [table] * n_jobs, outs["msm"], [1 << k for k in ks], table_n=1 << 20)
+    bws[1 << 20] = h2b.msm_batch_workspace(jobs_t, n_jobs, streams)
+    t_table = graph_time(table, 1 << 20)
+    same = same and identical()
     return {"workload": f"{n_jobs} jobs, k in {{14,16,18,20}} w .4/.3/.2/.1 (seed {seed}): MSM vs shared 2^20 SRS "
-                        f"+ coset extension x4", "k_counts": {k: ks.count(k) for k in sorted(set(ks))},
+                        f"+ forward NTT + coset extension x4 + config-3 gate quotient over the extended coset",
+            "k_counts": {k: ks.count(k) for k in sizes},
             "msm_points": sum(1 << k for k in ks), "streams": streams,
-            "plain_ms": t_plain, "batched_streams_ms": t_batched_streams, "batched_graph_ms": t_graph,
+            "plain_ms": t_plain, "batched_streams_ms": t_streams, "batched_graph_ms": t_graph,
             "plain_jobs_per_s": n_jobs / (t_plain * 1e-3), "batched_jobs_per_s": n_jobs / (t_graph * 1e-3),
             "speedup": t_plain / t_graph, "table_precompute_ms": t_pre, "batched_table_graph_ms": t_table,
             "batched_table_jobs_per_s": n_jobs / (t_table * 1e-3), "table_speedup": t_plain / t_table,
@@ -686,17 +751,40 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
-    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe"],
+    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")
+    ap.add_argument("--loads", default="0.5,1.0,1.5", help="load factors (x plain capacity) for --case serve")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the built-in MSM window / chunk and NTT pass settings (no autotuner)")
     args = ap.parse_args()
+    if args.case == "batch":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"case": "batch", "batch": batch_section(load_pkg(), torch)}))
+        return
+    if args.case == "rows":
+        import torch
+        torch.cuda.set_device(0)
+        h2b = load_pkg()
+        sink = h2b.dev_empty(4 * 148 * 64)
+        sh = h2b.stream_handle()
+        h2b.call("h2b_probe_modmul", 148 * 8, 256, 8, h2b.ptr(sink), sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h2b.call("h2b_probe_modmul", 148 * 8, 256, 64, h2b.ptr(sink), sh)
+        e1.record()
+        torch.cuda.synchronize()
+        probe = 148 * 8 * 256 * 64 * 4 / (e0.elapsed_time(e1) * 1e-3)
+        print(json.dumps({"case": "rows", "rows_k20": rows_section(h2b, torch, peaks()[0], probe)}))
+        return
     if args.case == "serve":
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps({"case": "serve", "serving": serving_section(load_pkg(), torch, count=args.requests)}))
+        loads = tuple(float(x) for x in args.loads.split(","))
+        print(json.dumps({"case": "serve", "serving": serving_section(load_pkg(), torch, count=args.requests,
+                                                                      loads=loads)}))
         return
     if args.case:
         run_case(args)

@@ -44,6 +44,14 @@ class MsmJob(ctypes.Structure):
                 ("n", ctypes.c_uint64), ("table_n", ctypes.c_uint64)]
 
 
+class QuotientProgram(ctypes.Structure):
+    """h2b_quotient_program: a compiled quotient program's host-side header."""
+    _fields_ = [("n_ops", ctypes.c_uint32), ("n_vp", ctypes.c_uint32), ("slots", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("num_quotient", ctypes.c_uint64), ("off_vps", ctypes.c_uint64),
+                ("off_cols", ctypes.c_uint64), ("off_consts", ctypes.c_uint64), ("off_chal", ctypes.c_uint64),
+                ("off_y", ctypes.c_uint64), ("bytes", ctypes.c_uint64)]
+
+
 class Halo2GpuError(RuntimeError):
     def __init__(self, code, message, who):
         super().__init__(f"{who}: code {code}: {message}")
@@ -144,6 +152,8 @@ _SIGS = {
     "h2b_msm_set_tuning": (None, [ctypes.c_int, ctypes.c_int]),
     "h2b_msm_set_accumulate_variant": (None, [ctypes.c_int]),
     "h2b_msm_set_pair_rounds": (None, [ctypes.c_int]),
+    "h2b_msm_get_accumulate_variant": (ctypes.c_int, []),
+    "h2b_msm_get_pair_rounds": (ctypes.c_int, []),
     "h2b_exec_fork": (RustError, [_vp, _u32, ctypes.POINTER(ctypes.c_void_p)]),
     "h2b_exec_join": (RustError, [_vp, _u32]),
     "h2b_upload": (RustError, [_vp, _vp, _u64, _vp]),
@@ -177,6 +187,12 @@ _SIGS = {
     "h2b_msm_count_entries": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_msm_window_bits": (ctypes.c_int, [_u64]),
     "h2b_batch_invert_noalloc": (RustError, [_vp, _u32, _u64, _vp]),
+    "h2b_batch_invert_assigned_workspace_size": (_u64, [_u64, _u32]),
+    "h2b_quotient_program_size": (_u64, [_u64, _u64, _u64, _u64, _u64]),
+    "h2b_quotient_program_build": (RustError, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _u64, _vp, _u64,
+                                               _vp, _u64, _u64, _vp, _u64, ctypes.POINTER(QuotientProgram), _vp]),
+    "h2b_quotient_program_run": (RustError, [ctypes.POINTER(QuotientProgram), _vp, _vp, _vp, _u64, _u64, _vp]),
+    "h2b_batch_invert_assigned": (RustError, [_vp, _vp, _u32, _u64, AssignedLayout, _vp, _u64, _vp]),
     "h2b_tune_set": (_i32, [_u32, _u32, _i32]),
     "h2b_tune_get": (_i32, [_u32, _u32]),
     "h2b_tune_clear": (None, []),
@@ -527,6 +543,16 @@ def decode_assigned_device(d_nums, d_denoms, d_raw, n, stride_bytes, num_offset,
          AssignedLayout(stride_bytes, num_offset, denom_offset), stream_handle(stream))
 
 
+def batch_invert_assigned_device(d_outs, d_raws, n, stride_bytes, num_offset, denom_offset, stream=None):
+    """batch_invert_assigned_device (halo2_proofs/src/poly.rs:364-420) as one call:
+    each device column of Assigned<F> records -> its values in the matching output."""
+    ncols = len(d_raws)
+    ws = dev_empty(lib().h2b_batch_invert_assigned_workspace_size(n, ncols))
+    call("h2b_batch_invert_assigned", _ptr_table(d_outs), _ptr_table(d_raws), ncols, n,
+         AssignedLayout(stride_bytes, num_offset, denom_offset), ptr(ws), ws.numel(), stream_handle(stream))
+    _keep_until_done([ws], stream)
+
+
 # --- twiddle tables (halo2_proofs/src/cuda/funcs/omega.rs) -----------------------
 
 def power_of_omega_gpu(omega, log_n, pow_, stream=None):
@@ -770,6 +796,35 @@ def quotient_host(fixed, instance, advice, challenges, constants, y, rules, vp_r
          cs.shape[0], host_ffi(ec), r.ctypes.data, len(r) // 2, vp.ctypes.data, len(vp), host_ffi(out),
          num_quotient, rot_scale, row_start, row_end, ptr(ws), ws.numel(), stream_handle(stream))
     return out
+
+
+class ResidentQuotient:
+    """A quotient program compiled once and kept on the device, bound to its
+    columns (h2b_quotient_program_build); run() is a kernel launch alone."""
+
+    def __init__(self, d_fixed, d_instance, d_advice, challenges, constants, y, rules, vp_rules, num_quotient,
+                 rot_scale, stream=None):
+        ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 4) if len(challenges) else \
+            np.zeros((1, 4), np.uint64)
+        cs = np.ascontiguousarray(constants, dtype=np.uint64).reshape(-1, 4)
+        yv = _scalar_bytes(y)
+        r = np.ascontiguousarray(rules, dtype=np.uint64)
+        vp = np.ascontiguousarray(vp_rules, dtype=np.uint64)
+        cols = list(d_fixed) + list(d_instance) + list(d_advice)
+        self.columns = cols                      # kept alive: the program holds their addresses
+        nb = lib().h2b_quotient_program_size(len(r) // 2, len(vp), len(cols), cs.shape[0], len(challenges))
+        self.d_prog = dev_empty(nb)
+        self.info = QuotientProgram()
+        call("h2b_quotient_program_build", r.ctypes.data, len(r) // 2, vp.ctypes.data, len(vp), len(d_fixed),
+             len(d_instance), len(d_advice), _ptr_table(cols), cs.ctypes.data, cs.shape[0], ch.ctypes.data,
+             len(challenges), yv.ctypes.data, num_quotient, rot_scale, ptr(self.d_prog), nb, ctypes.byref(self.info),
+             stream_handle(stream))
+
+    def run(self, d_out, d_prev=None, row_start=0, row_end=None, stream=None):
+        row_end = self.info.num_quotient if row_end is None else row_end
+        call("h2b_quotient_program_run", ctypes.byref(self.info), ptr(self.d_prog), ptr(d_out),
+             ptr(d_prev) if d_prev is not None else None, row_start, row_end, stream_handle(stream))
+        return d_out
 
 
 def quotient_lookups_device(d_values, d_table, d_z, d_pin, d_ptab, d_l0, d_llast, d_lactive, d_beta, d_gamma, d_y,

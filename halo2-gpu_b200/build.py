@@ -18,6 +18,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "--expt-relaxed-constexpr", "-I", CSRC]
+# H2B_EXPERIMENTS=1 in the environment also builds the A/B variants that
+# measured slower (MSM accumulation forms 1-5, pairing rounds, product-form
+# probes); the shipped library leaves them out.
+if os.environ.get("H2B_EXPERIMENTS") == "1":
+    FLAGS += ["-DH2B_EXPERIMENTS=1"]
 
 
 def _sources():

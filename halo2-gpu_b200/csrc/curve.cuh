@@ -438,8 +438,65 @@ H2B_DEV void xyzzd_madd(G1XyzzD& acc, const FqD& qx, const FqD& qy)
     acc.ZZZ = zz.b;
 }
 
+// Two independent madd-2008-s additions, a0 += q0 and a1 += q1, whose
+// products share out-of-line calls four at a time (the latency of one chain
+// hides behind the other).  When an accumulator is at infinity or a
+// square reads zero (equal x: a doubling or P + (-P)) the two additions run
+// one after the other through xyzzd_madd instead; no accumulator has been
+// written when that is decided.  Bounds as in xyzzd_madd.
+H2B_DEV void xyzzd_madd_x2(G1XyzzD& a0, const FqD& q0x, const FqD& q0y, G1XyzzD& a1, const FqD& q1x,
+                           const FqD& q1y)
+{
+    if (is_inf(a0) || is_inf(a1)) {
+        xyzzd_madd(a0, q0x, q0y);
+        xyzzd_madd(a1, q1x, q1y);
+        return;
+    }
+    const Fd4<FqCfg> us = fd_mul4(q0x, a0.ZZ, q0y, a0.ZZZ, q1x, a1.ZZ, q1y, a1.ZZZ);
+    const FqD P0 = fd_sub<FqCfg, 6>(us.a, a0.X), R0 = fd_sub<FqCfg, 4>(us.b, a0.Y);
+    const FqD P1 = fd_sub<FqCfg, 6>(us.c, a1.X), R1 = fd_sub<FqCfg, 4>(us.d, a1.Y);
+    const Fd4<FqCfg> sq = fd_mul4(P0, P0, R0, R0, P1, P1, R1, R1);
+    if (fd_is_zero_mod(sq.a) || fd_is_zero_mod(sq.c)) {
+        xyzzd_madd(a0, q0x, q0y);
+        xyzzd_madd(a1, q1x, q1y);
+        return;
+    }
+    const Fd4<FqCfg> pq = fd_mul4(P0, sq.a, a0.X, sq.a, P1, sq.c, a1.X, sq.c);
+    const FqD X30 = fd_sub<FqCfg, 4>(sq.b, fd_add(pq.a, fd_add(pq.b, pq.b)));
+    const FqD X31 = fd_sub<FqCfg, 4>(sq.d, fd_add(pq.c, fd_add(pq.d, pq.d)));
+    const Fd4<FqCfg> yy = fd_mul4(R0, fd_sub<FqCfg, 6>(pq.b, X30), a0.Y, pq.a, R1, fd_sub<FqCfg, 6>(pq.d, X31), a1.Y,
+                                  pq.c);
+    const Fd4<FqCfg> zz = fd_mul4(a0.ZZ, sq.a, a0.ZZZ, pq.a, a1.ZZ, sq.c, a1.ZZZ, pq.c);
+    a0.Y = fd_sub<FqCfg, 2>(yy.a, yy.b);
+    a0.X = X30;
+    a0.ZZ = zz.a;
+    a0.ZZZ = zz.b;
+    a1.Y = fd_sub<FqCfg, 2>(yy.c, yy.d);
+    a1.X = X31;
+    a1.ZZ = zz.c;
+    a1.ZZZ = zz.d;
+}
+
 // Canonical memory image of the accumulator (infinity stays ZZ = 0): four
 // products by 2^256 mod p (each below 1.07p), then conditional subtractions.
+static __device__ __noinline__ G1Xyzz xyzzd_canonical(const G1XyzzD p)
+{
+    const FqD r256 = fd_r256<FqCfg>();
+    const Fd4<FqCfg> a = fd_mul4(p.X, r256, p.Y, r256, p.ZZ, r256, p.ZZZ, r256);
+    G1Xyzz r;
+    r.X = fd_canonical(a.a); r.Y = fd_canonical(a.b);
+    r.ZZ = fd_canonical(a.c); r.ZZZ = fd_canonical(a.d);
+    return r;
+}
+
+// The sum of two accumulators, stored in the canonical memory image.
+static __device__ __noinline__ void st_xyzzd_pair(G1Xyzz* dst, const G1XyzzD p0, const G1XyzzD p1)
+{
+    G1Xyzz r = xyzzd_canonical(p0);
+    if (!is_inf(p1)) xyzz_add(r, xyzzd_canonical(p1));
+    st_xyzz(dst, r);
+}
+
 static __device__ __noinline__ void st_xyzzd(G1Xyzz* dst, const G1XyzzD p)
 {
     const FqD r256 = fd_r256<FqCfg>();

@@ -182,6 +182,24 @@ __device__ __noinline__ Fd2<C> fd_mul2(const Fd<C> a0, const Fd<C> b0, const Fd<
 }
 
 template <class C>
+struct Fd4 {
+    Fd<C> a, b, c, d;
+};
+
+// four independent products per out-of-line call (two accumulation chains)
+template <class C>
+__device__ __noinline__ Fd4<C> fd_mul4(const Fd<C> a0, const Fd<C> b0, const Fd<C> a1, const Fd<C> b1,
+                                      const Fd<C> a2, const Fd<C> b2, const Fd<C> a3, const Fd<C> b3)
+{
+    Fd4<C> r;
+    r.a = fd_mul<C>(a0, b0);
+    r.b = fd_mul<C>(a1, b1);
+    r.c = fd_mul<C>(a2, b2);
+    r.d = fd_mul<C>(a3, b3);
+    return r;
+}
+
+template <class C>
 __device__ __noinline__ Fd<C> fd_mul_call(const Fd<C> a, const Fd<C> b)
 {
     return fd_mul<C>(a, b);

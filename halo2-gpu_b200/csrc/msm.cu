@@ -40,6 +40,12 @@ extern "C" RustError h2b_exec_fork(cudaStream_t parent, uint32_t n, cudaStream_t
 
 namespace h2b {
 
+// H2B_EXPERIMENTS=1 also builds the accumulation forms and the batch-affine
+// pairing rounds that measured slower than the default (A/B comparisons);
+// the shipped library leaves them out.
+#ifndef H2B_EXPERIMENTS
+#define H2B_EXPERIMENTS 0
+#endif
 static constexpr int GLV_BITS = 127;
 // 32-bit sorted-entry offsets: 2 halves x 8 windows x n < 2^32
 static constexpr uint64_t MSM_MAX_LENGTH = 1ull << 27;
@@ -64,7 +70,7 @@ RustError fq_batch_invert(Fq* d, uint64_t n, void* scratch, uint64_t scratch_byt
 
 void msm_set_pair_rounds(int rounds)
 {
-    if (rounds >= 0 && rounds <= 3) g_msm_pair_rounds = rounds;
+    if (rounds >= 0 && rounds <= (H2B_EXPERIMENTS ? 3 : 0)) g_msm_pair_rounds = rounds;
 }
 static int g_msm_chunk_override = 0;
 
@@ -331,6 +337,7 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t 
     }
 }
 
+#if H2B_EXPERIMENTS
 // One thread per chunk of K sorted entries; the running bucket sum stays in
 // 29-bit limb form and is packed to the canonical 8 x 32 image when stored.
 // PTS: the entries are the affine points themselves (bases[e]), as left by
@@ -381,6 +388,8 @@ __global__ void __launch_bounds__(128, MODE == 1 ? 2 : (MODE >= 3 ? MODE + 1 : 3
         if (head) st_xyzz(&heads[t], xyzzl_to(acc)); else st_xyzz(&buckets[b], xyzzl_to(acc));
     }
 }
+
+#endif  // H2B_EXPERIMENTS
 
 // Bases (affine, memory image x 2^256 mod p) -> canonical x 2^261 mod p, the
 // form the lazy accumulation reads; infinity (0, 0) stays (0, 0).
@@ -498,6 +507,73 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
     }
 }
 
+// The FP64 lazy accumulation with two independent chains per thread: the
+// entries of a bucket segment alternate between two accumulators whose
+// additions share their out-of-line product calls (xyzzd_madd_x2), and the
+// two are added once when the segment's bucket (or chunk head) is stored.
+// Same chunks, bucket boundaries and outputs as k_msm_accumulate_d.
+__global__ void __launch_bounds__(128, 2) k_msm_accumulate_d2(const uint32_t* __restrict__ sorted,
+                                                              const uint32_t* __restrict__ offsets, uint64_t NB,
+                                                              uint32_t K, const G1Affine* __restrict__ bases,
+                                                              uint64_t phi_off, G1Xyzz* __restrict__ buckets,
+                                                              G1Xyzz* __restrict__ heads)
+{
+    const uint32_t M = offsets[NB];
+    const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
+    auto load = [&](uint32_t e, FqD& qx, FqD& qy) -> bool {    // false for a point at infinity
+        const uint32_t ent = sorted[e];
+        const uint32_t v = ent & ~SIGN_BIT;
+        const G1Affine P = ld_affine(&bases[(v >> 1) + ((v & 1u) ? phi_off : 0)]);
+        if (is_inf(P)) return false;
+        qx = fd_from_r261(P.x);                                        // < p
+        qy = fd_from_r261(P.y);                                        // < p
+        if (ent & SIGN_BIT) qy = fd_sub<FqCfg, 2>(fd_zero<FqCfg>(), qy);  // 2p - y < 2p
+        return true;
+    };
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nchunks;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t start = (uint32_t)(t * K);
+        const uint32_t end = ((uint64_t)start + K < (uint64_t)M) ? start + K : M;
+        uint64_t lo = 0, hi = NB;  // offsets[lo] <= start < offsets[hi]
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (offsets[mid] <= start) lo = mid; else hi = mid;
+        }
+        uint64_t b = lo;
+        uint32_t next = offsets[b + 1];
+        bool head = offsets[b] < start;
+        G1XyzzD a0 = xyzzd_inf(), a1 = xyzzd_inf();
+        uint32_t e = start;
+        while (e < end) {
+            if (e == next) {
+                st_xyzzd_pair(head ? &heads[t] : &buckets[b], a0, a1);
+                a0 = xyzzd_inf();
+                a1 = xyzzd_inf();
+                head = false;
+                do { b++; next = offsets[b + 1]; } while (next == e);
+            }
+            const uint32_t seg = next < end ? next : end;
+            for (; e + 1 < seg; e += 2) {
+                FqD x0, y0, x1, y1;
+                const bool f0 = load(e, x0, y0), f1 = load(e + 1, x1, y1);
+                if (f0 && f1) {
+                    xyzzd_madd_x2(a0, x0, y0, a1, x1, y1);
+                } else {
+                    if (f0) xyzzd_madd(a0, x0, y0);
+                    if (f1) xyzzd_madd(a1, x1, y1);
+                }
+            }
+            if (e < seg) {
+                FqD x0, y0;
+                if (load(e, x0, y0)) xyzzd_madd(a0, x0, y0);
+                e++;
+            }
+        }
+        st_xyzzd_pair(head ? &heads[t] : &buckets[b], a0, a1);
+    }
+}
+
+#if H2B_EXPERIMENTS
 // ---- pairing rounds (batch-affine bucket additions) -----------------------
 // Round r adds the points of every bucket pairwise in affine coordinates:
 // entries (2j, 2j+1) of a bucket become output point j (an odd last entry is
@@ -683,6 +759,8 @@ __global__ void k_msm_half_counts(const uint32_t* __restrict__ in_off, uint64_t 
     for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < NB; b += (uint64_t)gridDim.x * blockDim.x)
         out_cnt[b] = (in_off[b + 1] - in_off[b] + 1) >> 1;
 }
+
+#endif  // H2B_EXPERIMENTS
 
 __global__ void k_msm_fixup(const uint32_t* __restrict__ offsets, uint64_t NB, uint32_t K, G1Xyzz* __restrict__ buckets,
                             const G1Xyzz* __restrict__ heads, uint32_t* __restrict__ dense, uint64_t max_dense)
@@ -875,7 +953,7 @@ __global__ void k_write_inf(G1Jac* out)
 // variant run.
 static bool msm_lazy(const MsmPlan& p)
 {
-    return p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0 || g_msm_acc_variant == 6);
+    return p.R == 0 && (p.tn > 0 || g_msm_acc_variant == 0 || g_msm_acc_variant >= 6);
 }
 
 // Phases of one MSM on `st`: msm_begin clears the histogram, msm_split takes
@@ -919,6 +997,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
     const uint32_t* off = s.offsets;
     const G1Affine* src = d_bases;
+#if H2B_EXPERIMENTS
     for (int r = 1; r <= p.R; r++) {
         k_msm_half_counts<<<grid_for(p.NB, 256, sm_cap), 256, 0, st>>>(off, p.NB, s.counts);
         H2B_LAUNCHED("k_msm_half_counts");
@@ -944,16 +1023,21 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
         off = s.roff[r - 1];
         src = dst;
     }
+#endif
     const uint64_t chunks = (p.cap[p.R] + p.Kf - 1) / p.Kf;
     const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
-    if (p.R > 0)
-        k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
-    else if (lazy && g_msm_acc_variant == 6)
+    if (lazy && g_msm_acc_variant == 6)
         k_msm_accumulate_d<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
+    else if (lazy && g_msm_acc_variant == 7)
+        k_msm_accumulate_d2<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
+                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
     else if (lazy)
         k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
+#if H2B_EXPERIMENTS
+    else if (p.R > 0)
+        k_msm_accumulate<2, true><<<acc_grid, 128, 0, st>>>(nullptr, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 5)
         k_msm_accumulate<0, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 1)
@@ -964,6 +1048,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
         k_msm_accumulate<3, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
     else if (g_msm_acc_variant == 4)
         k_msm_accumulate<4, false><<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, src, s.buckets, s.heads);
+#endif
     prof_end(PROF_MSM_ACCUMULATE, st);
     H2B_LAUNCHED("k_msm_accumulate");
     k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(off, p.NB, p.Kf, s.buckets, s.heads, s.dense,
@@ -1255,20 +1340,27 @@ extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(
 
 // Form and call structure of the bucket-accumulation kernel: 6 = the lazy
 // R' = 2^260 form on the FP64 pipe (default; window tables use it too);
-// 0 = the lazy R = 2^261 form of 29-bit limbs with one-step carries (window
-// tables use it for every choice but 6); the normalised R = 2^256 limb form
-// with 5 = two products per out-of-line call, 1 = all products inline, 2 =
-// one product per call, 3 and 4 = one product per call with at most 128 / 96
-// registers (4 / 5 CTAs of 128 threads per SM).  Measured at 2^22 with the
-// witness-like scalar mix: 6 takes 12.26 ms, 0 13.56 ms.  Results are
-// identical; only speed differs.
+// 0 = the lazy R = 2^261 form of 29-bit limbs with one-step carries on the
+// integer multiply pipe (window tables use it for every choice but 6).
+// Built with H2B_EXPERIMENTS=1 only, the normalised R = 2^256 limb form with
+// 5 = two products per out-of-line call, 1 = all products inline, 2 = one
+// product per call, 3 and 4 = one product per call with at most 128 / 96
+// registers.  Measured at 2^22 with the witness-like scalar mix: 6 takes
+// 12.26 ms, 0 13.56 ms.  Results are identical; only speed differs.  A value
+// that is not built leaves the setting unchanged (read it back with
+// h2b_msm_get_accumulate_variant).
 extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
-    if (v >= 0 && v <= 6) g_msm_acc_variant = v;
+    if (v == 0 || v == 6 || v == 7 || (H2B_EXPERIMENTS && v >= 1 && v <= 5)) g_msm_acc_variant = v;
 }
 
+extern "C" int h2b_msm_get_accumulate_variant(void) { return g_msm_acc_variant; }
+
+extern "C" int h2b_msm_get_pair_rounds(void) { return g_msm_pair_rounds; }
+
 // Batch-affine pairing rounds run before the XYZZ bucket accumulation
-// (0..3).  Default 0: on B200 a pairing addition (forward pass, shared
+// (0..3; rounds above 0 are built with H2B_EXPERIMENTS=1 only, otherwise
+// the setting stays 0).  Default 0: on B200 a pairing addition (forward pass, shared
 // inversion, backward pass) measured about 0.5 ns per addition against
 // 0.3 ns for an XYZZ mixed addition (2^20 points, witness scalar mix).
 // Results are identical; speed and the workspace size differ (the

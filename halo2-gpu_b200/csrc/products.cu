@@ -540,6 +540,107 @@ extern "C" RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_
     return batch_invert_groups<FqCfg>((Fq*)d_data, length, ar, stream);
 }
 
+// batch_invert_assigned -------------------------------------------------------
+//
+// Assigned<F> columns to their values in one entry point: the composition
+// halo2_proofs/src/poly.rs:364-420 (batch_invert_assigned_device) builds from
+// _halo2_decode_assigned per column, one _halo2_batch_invert over every
+// column's denominators and _halo2_poly_elementwise_multiply per column.
+// Here: one kernel decodes the denominators of all columns into scratch, the
+// scratch batch inversion inverts them all with one field inversion (zeros
+// stay zero), and one kernel re-decodes each numerator and multiplies it by
+// its inverted denominator into the output column, so numerators never make
+// a round trip through memory.  Records: tag byte 0 Zero (value 0), 1 Trivial
+// (numerator), 2 Rational (numerator / denominator; a zero denominator gives
+// 0, as Assigned::invert does).
+
+namespace h2b {
+struct AssignedRec {
+    uint32_t stride_bytes, num_offset, denom_offset;
+};
+constexpr uint32_t BIA_MAX_COLS = 64;
+struct BiaCols {
+    const uint8_t* raw[BIA_MAX_COLS];
+    Fr* out[BIA_MAX_COLS];
+};
+
+__device__ __forceinline__ Fr ld_words_fr(const uint8_t* p)
+{
+    Fr r;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(p);
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = w[i];
+    return r;
+}
+
+// dens[c n + i] = denominator of record i of column c (blockIdx.y = c)
+__global__ void k_bia_denoms(BiaCols cols, uint64_t n, AssignedRec L, Fr* __restrict__ dens)
+{
+    const uint32_t c = blockIdx.y;
+    const uint8_t* raw = cols.raw[c];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t* rec = raw + i * L.stride_bytes;
+        Fr den = rec[0] >= 2 ? ld_words_fr(rec + L.denom_offset) : Fr::one();
+        st(&dens[c * n + i], den);
+    }
+}
+
+// out_c[i] = numerator of record i of column c times its inverted denominator
+__global__ void k_bia_apply(BiaCols cols, uint64_t n, AssignedRec L, const Fr* __restrict__ inv)
+{
+    const uint32_t c = blockIdx.y;
+    const uint8_t* raw = cols.raw[c];
+    Fr* out = cols.out[c];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t* rec = raw + i * L.stride_bytes;
+        Fr v = Fr::zero();
+        if (rec[0] != 0) v = ld_words_fr(rec + L.num_offset) * ld(&inv[c * n + i]);
+        st(&out[i], v);
+    }
+}
+} // namespace h2b
+
+extern "C" uint64_t h2b_batch_invert_assigned_workspace_size(uint64_t n, uint32_t n_cols)
+{
+    ScratchPlan p;
+    uint64_t total = n * (uint64_t)n_cols;
+    p.add(std::max<uint64_t>(total, 1) * sizeof(Fr));
+    plan_batch_invert_groups(p, std::max<uint64_t>(total, 1));
+    return p.used;
+}
+
+extern "C" RustError h2b_batch_invert_assigned(void* const* d_outs, const void* const* d_raws, uint32_t n_cols,
+                                               uint64_t n, AssignedRec layout, void* scratch, uint64_t scratch_bytes,
+                                               cudaStream_t stream)
+{
+    if (n_cols == 0 || n == 0) return ok();
+    if (n_cols > BIA_MAX_COLS)
+        return err(cudaErrorInvalidValue, "h2b_batch_invert_assigned: more than 64 columns per call");
+    if (layout.stride_bytes % 4 || layout.num_offset % 4 || layout.denom_offset % 4 ||
+        layout.num_offset + 32 > layout.stride_bytes || layout.denom_offset + 32 > layout.stride_bytes ||
+        layout.num_offset == 0 || layout.denom_offset == 0)
+        return err(cudaErrorInvalidValue,
+                   "h2b_batch_invert_assigned: layout needs 4-byte aligned stride and offsets, payloads after the "
+                   "tag byte and inside the record");
+    uint64_t need = h2b_batch_invert_assigned_workspace_size(n, n_cols);
+    if (scratch_bytes < need) return scratch_too_small("h2b_batch_invert_assigned", scratch_bytes, need);
+    BiaCols cols;
+    for (uint32_t c = 0; c < BIA_MAX_COLS; c++) {
+        cols.raw[c] = c < n_cols ? (const uint8_t*)d_raws[c] : nullptr;
+        cols.out[c] = c < n_cols ? (Fr*)d_outs[c] : nullptr;
+    }
+    ScratchArena ar(scratch, scratch_bytes);
+    Fr* dens = ar.take_n<Fr>(n * n_cols);
+    if (!ar.good()) return scratch_too_small("h2b_batch_invert_assigned", scratch_bytes, need);
+    dim3 grid(grid_for(n, 256, 148u * 8u), n_cols);
+    k_bia_denoms<<<grid, 256, 0, stream>>>(cols, n, layout, dens);
+    H2B_LAUNCHED("k_bia_denoms");
+    H2B_TRY(batch_invert_groups<FrCfg>(dens, n * n_cols, ar, stream));
+    k_bia_apply<<<grid, 256, 0, stream>>>(cols, n, layout, dens);
+    H2B_LAUNCHED("k_bia_apply");
+    return ok();
+}
+
 // grand product ---------------------------------------------------------------
 
 extern "C" uint64_t _halo2_grand_product_workspace_size(uint64_t poly_length)
@@ -759,7 +860,11 @@ extern "C" RustError _halo2_permutation_product_device_inputs(
 //    start at zero (every tile total is written before it is read).
 //  * The first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture.  No call allocates or frees memory.
+//    before any stream capture.  The address is kept per device together
+//    with the unique id of the CUDA context it belongs to: after the
+//    device's context is destroyed and recreated (cudaDeviceReset), the
+//    next call sees a new context id and looks the address up again, so a
+//    stale address is never used.  No call allocates or frees memory.
 namespace h2b {
 constexpr uint64_t NOALLOC_SCRATCH_BYTES = 1536ull << 10;
 constexpr uint64_t NOALLOC_MAX_LENGTH = 1ull << 26;
@@ -767,6 +872,33 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+static unsigned long long g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
+
+// The unique id of the calling thread's current CUDA context (driver entry
+// points cuCtxGetCurrent / cuCtxGetId, found at run time so nothing links
+// against the driver library), or 0 when it cannot be read.
+static unsigned long long current_context_id()
+{
+    typedef int (*get_current_t)(void**);
+    typedef int (*get_id_t)(void*, unsigned long long*);
+    static get_current_t get_current = nullptr;
+    static get_id_t get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    }
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == 0 && ctx && get_id(ctx, &id) == 0) return id;
+    return 0;
+}
 } // namespace h2b
 
 extern "C" RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type, uint64_t length, cudaStream_t stream)
@@ -786,11 +918,13 @@ extern "C" RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type,
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (g_noalloc_addr[dev] == nullptr) {
+        const unsigned long long ctx = current_context_id();
+        if (g_noalloc_addr[dev] == nullptr || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
             void* p = nullptr;
             cudaError_t c = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (c != cudaSuccess) return cuda_err(c, "cudaGetSymbolAddress(no-allocation scratch)");
             g_noalloc_addr[dev] = p;
+            g_noalloc_ctx[dev] = ctx;
         }
         base = g_noalloc_addr[dev];
     }

@@ -13,6 +13,12 @@
 #include "field.cuh"
 #include "prof.cuh"
 
+// H2B_EXPERIMENTS=1 also builds the product-form probes used for A/B
+// comparisons (h2b_probe_imad_form, h2b_probe_modmul_impl).
+#ifndef H2B_EXPERIMENTS
+#define H2B_EXPERIMENTS 0
+#endif
+
 namespace h2b {
 
 namespace {
@@ -82,6 +88,7 @@ __global__ void k_probe_imad(uint32_t* sink, int iters, uint32_t seed)
 
 // Single-form throughput: mode 0 = mad.lo.u32, 1 = mad.hi.u32, 2 = mad.wide.u32
 // (16 independent instructions per iteration per thread).
+#if H2B_EXPERIMENTS
 __global__ void k_probe_imad_form(uint32_t* sink, int iters, uint32_t seed, int mode)
 {
     uint32_t a[16];
@@ -117,6 +124,7 @@ __global__ void k_probe_imad_form(uint32_t* sink, int iters, uint32_t seed, int 
     for (int j = 0; j < 16; j++) x ^= a[j];
     if (x == 0x12345678u) sink[blockIdx.x] = x;
 }
+#endif  // H2B_EXPERIMENTS
 
 template <int IMPL>
 __device__ __forceinline__ Fr mul_impl(const Fr& a, const Fr& b)
@@ -139,6 +147,7 @@ __global__ void k_fq_mul_batch(const Fq* __restrict__ a, const Fq* __restrict__ 
 }
 
 // Four independent chains of 29-bit-limb products that stay in limb form.
+#if H2B_EXPERIMENTS
 __global__ void k_probe_mul29_chain(uint32_t* sink, int iters)
 {
     Fr a0 = Fr::one(), b0 = Fr::r2();
@@ -173,6 +182,7 @@ __global__ void k_probe_modmul_impl(uint32_t* sink, int iters)
     uint32_t x = a.v[0] ^ b.v[1] ^ c.v[2] ^ d.v[3];
     if (x == 0x12345678u) sink[blockIdx.x] = x;
 }
+#endif  // H2B_EXPERIMENTS
 
 template <int IMPL>
 __global__ void k_fr_mul_batch(const Fr* __restrict__ a, const Fr* __restrict__ b, Fr* __restrict__ out, uint64_t n)
@@ -236,6 +246,7 @@ extern "C" RustError h2b_probe_imad(int blocks, int threads, int iters, void* d_
     return ok();
 }
 
+#if H2B_EXPERIMENTS
 extern "C" RustError h2b_probe_imad_form(int blocks, int threads, int iters, int mode, void* d_sink,
                                          cudaStream_t stream)
 {
@@ -263,6 +274,8 @@ extern "C" RustError h2b_probe_modmul_impl(int impl, int blocks, int threads, in
 // out[i] = a[i] * b[i] with the chosen product implementation (tests):
 // 0-2 Fr products (CIOS lo/hi, CIOS wide, 29-bit), 3 Fr square (29-bit),
 // 4 Fq product, 5 Fq square (29-bit), 6 Fr product, 7 Fq product (FP64).
+#endif  // H2B_EXPERIMENTS
+
 extern "C" RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b, void* d_out, uint64_t n,
                                       cudaStream_t stream)
 {

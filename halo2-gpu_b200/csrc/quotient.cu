@@ -560,6 +560,120 @@ extern "C" RustError _halo2_quotient_device_columns_device_out(
     return quotient_run(a, "_halo2_quotient_device_columns_device_out");
 }
 
+// ---------------------------------------------------------------------------
+// Resident quotient programs (no counterpart in the reference, which compiles
+// and uploads its rule list, constants and column table on every call): the
+// program is compiled and uploaded once into caller-owned device memory,
+// bound to its column buffers, and each run is a kernel launch alone -- no
+// host copy, no synchronisation -- so runs can be captured in a CUDA graph
+// and issued from many streams at once.
+// ---------------------------------------------------------------------------
+
+extern "C" {
+typedef struct h2b_quotient_program {
+    uint32_t n_ops, n_vp, slots, reserved;
+    uint64_t num_quotient;
+    uint64_t off_vps, off_cols, off_consts, off_chal, off_y, bytes;
+} h2b_quotient_program;
+}
+
+static void qprog_layout(uint64_t num_rules, uint64_t num_vp, uint64_t ncols, uint64_t num_constants,
+                         uint64_t num_challenges, h2b_quotient_program& L)
+{
+    ScratchPlan p;
+    p.add(std::max<uint64_t>(num_rules, 1) * sizeof(QOp));
+    L.off_vps = align_up(p.used);
+    p.add(std::max<uint64_t>(num_vp, 1) * sizeof(QVp));
+    L.off_cols = align_up(p.used);
+    p.add(std::max<uint64_t>(ncols, 1) * sizeof(void*));
+    L.off_consts = align_up(p.used);
+    p.add(std::max<uint64_t>(num_constants, 1) * 32);
+    L.off_chal = align_up(p.used);
+    p.add(std::max<uint64_t>(num_challenges, 1) * 32);
+    L.off_y = align_up(p.used);
+    p.add(32);
+    L.bytes = p.used;
+}
+
+extern "C" uint64_t h2b_quotient_program_size(uint64_t num_rules, uint64_t num_vp, uint64_t num_columns,
+                                              uint64_t num_constants, uint64_t num_challenges)
+{
+    h2b_quotient_program L;
+    qprog_layout(num_rules, num_vp, num_columns, num_constants, num_challenges, L);
+    return L.bytes;
+}
+
+extern "C" RustError h2b_quotient_program_build(const uint64_t* rules, uint64_t num_rules, const uint64_t* value_part_rules,
+                                               uint64_t num_vp, uint64_t num_fixed, uint64_t num_instance,
+                                               uint64_t num_advice, const void* const* d_columns,
+                                               const void* constants, uint64_t num_constants, const void* challenges,
+                                               uint64_t num_challenges, const void* y, uint64_t num_quotient,
+                                               uint64_t rotation_scale, void* d_program, uint64_t program_bytes,
+                                               h2b_quotient_program* info, cudaStream_t stream)
+{
+    if (!info) return err(cudaErrorInvalidValue, "h2b_quotient_program_build: info is null");
+    if (num_quotient == 0) return err(cudaErrorInvalidValue, "h2b_quotient_program_build: num_quotient is 0");
+    const uint64_t ncols = num_fixed + num_instance + num_advice;
+    QProgram P = compile_rules(rules, num_rules, value_part_rules, num_vp, num_fixed, num_instance, num_advice,
+                               num_constants, num_challenges, num_quotient, rotation_scale);
+    if (!P.error.empty()) return err(cudaErrorInvalidValue, P.error.c_str());
+    if (P.slots > 512) return err(cudaErrorInvalidValue, "quotient: more than 512 live intermediates");
+    h2b_quotient_program L;
+    memset(&L, 0, sizeof(L));
+    qprog_layout(num_rules, num_vp, ncols, num_constants, num_challenges, L);
+    if (program_bytes < L.bytes) return scratch_too_small("h2b_quotient_program_build", program_bytes, L.bytes);
+    L.n_ops = (uint32_t)P.ops.size();
+    L.n_vp = (uint32_t)P.vps.size();
+    L.slots = P.slots;
+    L.num_quotient = num_quotient;
+    char* base = (char*)d_program;
+    if (!P.ops.empty())
+        H2B_CUDA(cudaMemcpyAsync(base, P.ops.data(), P.ops.size() * sizeof(QOp), cudaMemcpyHostToDevice, stream));
+    if (!P.vps.empty())
+        H2B_CUDA(cudaMemcpyAsync(base + L.off_vps, P.vps.data(), P.vps.size() * sizeof(QVp), cudaMemcpyHostToDevice,
+                                 stream));
+    if (ncols)
+        H2B_CUDA(cudaMemcpyAsync(base + L.off_cols, d_columns, ncols * sizeof(void*), cudaMemcpyHostToDevice, stream));
+    if (num_constants)
+        H2B_CUDA(cudaMemcpyAsync(base + L.off_consts, constants, num_constants * 32, cudaMemcpyHostToDevice, stream));
+    if (num_challenges)
+        H2B_CUDA(cudaMemcpyAsync(base + L.off_chal, challenges, num_challenges * 32, cudaMemcpyHostToDevice, stream));
+    H2B_CUDA(cudaMemcpyAsync(base + L.off_y, y, 32, cudaMemcpyHostToDevice, stream));
+    // the host sources are pageable and go out of scope: the copies must have read them
+    H2B_CUDA(cudaStreamSynchronize(stream));
+    *info = L;
+    return ok();
+}
+
+extern "C" RustError h2b_quotient_program_run(const h2b_quotient_program* info, const void* d_program, void* d_out,
+                                             const void* d_prev, uint64_t row_start, uint64_t row_end,
+                                             cudaStream_t stream)
+{
+    if (!info) return err(cudaErrorInvalidValue, "h2b_quotient_program_run: info is null");
+    const h2b_quotient_program& L = *info;
+    if (row_end < row_start || row_end > L.num_quotient)
+        return err(cudaErrorInvalidValue, "quotient: row range outside [0, num_quotient]");
+    const uint64_t rows = row_end - row_start;
+    if (rows == 0) return ok();
+    const char* base = (const char*)d_program;
+    const QOp* ops = (const QOp*)base;
+    const QVp* vps = (const QVp*)(base + L.off_vps);
+    const Fr* const* cols = (const Fr* const*)(base + L.off_cols);
+    const Fr* consts = (const Fr*)(base + L.off_consts);
+    const Fr* chal = (const Fr*)(base + L.off_chal);
+    const Fr* yp = (const Fr*)(base + L.off_y);
+    unsigned grid = grid_for(rows, 128, 148u * 16u);
+#define H2B_QPLAUNCH(S)                                                                                           \
+    k_quotient<S><<<grid, 128, 0, stream>>>(ops, L.n_ops, vps, L.n_vp, cols, consts, chal, yp, (const Fr*)d_prev, \
+                                            (Fr*)d_out, L.num_quotient, row_start, rows)
+    if (L.slots <= 16) H2B_QPLAUNCH(16);
+    else if (L.slots <= 64) H2B_QPLAUNCH(64);
+    else H2B_QPLAUNCH(512);
+#undef H2B_QPLAUNCH
+    H2B_LAUNCHED("k_quotient");
+    return ok();
+}
+
 extern "C" RustError _halo2_quotient_lookups(void* values, const void* table_values, const void* product_coset,
                                              const void* permuted_input_coset, const void* permuted_table_coset,
                                              const void* l0, const void* l_last, const void* l_active_row,

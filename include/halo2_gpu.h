@@ -208,6 +208,15 @@ typedef struct AssignedLayout {
 /* culib.rs:301-308 ; polynomial/decode_assigned.cu:28-60 -- tag byte 0 Zero, 1 Trivial, 2 Rational */
 RustError _halo2_decode_assigned(void* d_nums, void* d_denoms, const void* d_raw, uint64_t n, AssignedLayout layout,
                                  h2b_stream_t stream);
+/* The reference's batch_invert_assigned_device (halo2_proofs/src/poly.rs:364-420: _halo2_decode_assigned per column,
+ * one _halo2_batch_invert over all denominators, _halo2_poly_elementwise_multiply per column) as one entry point:
+ * d_outs[c][i] = value of the Assigned<F> record i of column c (Zero 0, Trivial x, Rational n/d with d = 0 giving 0),
+ * for n_cols <= 64 columns of n records each.  d_outs and d_raws are host arrays of device pointers; outputs must not
+ * overlap the records.  The layout needs a 4-byte aligned stride and payload offsets inside the record (else an
+ * error).  Scratch: h2b_batch_invert_assigned_workspace_size bytes. */
+uint64_t h2b_batch_invert_assigned_workspace_size(uint64_t n, uint32_t n_cols);
+RustError h2b_batch_invert_assigned(void* const* d_outs, const void* const* d_raws, uint32_t n_cols, uint64_t n,
+                                    AssignedLayout layout, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
 
 /* ------------------------------------------------------------------ NTT --- */
 /* ntt_type: 1 FFT, 2 iFFT, 3 cosetFFT, 4 icosetFFT, 5 unsupported, 6 CosetFFT_Part (ntt.cu:21-28);
@@ -330,6 +339,28 @@ RustError _halo2_quotient_device_columns(const void* const* fixed_d_ptrs, uint64
                                          FFITraitObject quotient_poly, uint64_t num_quotient,
                                          uint64_t rotation_scale, uint64_t row_start, uint64_t row_end,
                                          void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* Resident quotient programs (no counterpart in the reference, which compiles and uploads its rule list,
+ * constants and column table on every _halo2_quotient* call): h2b_quotient_program_build compiles the same rule
+ * encoding once, binds it to its device columns (d_columns: host array of device pointers, fixed then instance
+ * then advice) and uploads it into caller-owned device memory (h2b_quotient_program_size bytes; the call
+ * synchronises `stream` once); h2b_quotient_program_run is then a kernel launch alone (no host copy, no
+ * synchronisation), so it can run from many streams and inside a captured CUDA graph.  Output rows as
+ * _halo2_quotient_device_columns_device_out. */
+typedef struct h2b_quotient_program {
+    uint32_t n_ops, n_vp, slots, reserved;
+    uint64_t num_quotient;
+    uint64_t off_vps, off_cols, off_consts, off_chal, off_y, bytes;
+} h2b_quotient_program;
+uint64_t h2b_quotient_program_size(uint64_t num_rules, uint64_t num_vp, uint64_t num_columns, uint64_t num_constants,
+                                   uint64_t num_challenges);
+RustError h2b_quotient_program_build(const uint64_t* rules, uint64_t num_rules, const uint64_t* value_part_rules,
+                                     uint64_t num_vp, uint64_t num_fixed, uint64_t num_instance, uint64_t num_advice,
+                                     const void* const* d_columns, const void* constants, uint64_t num_constants,
+                                     const void* challenges, uint64_t num_challenges, const void* y,
+                                     uint64_t num_quotient, uint64_t rotation_scale, void* d_program,
+                                     uint64_t program_bytes, h2b_quotient_program* info, h2b_stream_t stream);
+RustError h2b_quotient_program_run(const h2b_quotient_program* info, const void* d_program, void* d_out,
+                                   const void* d_prev, uint64_t row_start, uint64_t row_end, h2b_stream_t stream);
 /* culib.rs:603-617 ; quotient_lookups.cu:16-53 -- all device pointers */
 RustError _halo2_quotient_lookups(void* values, const void* table_values, const void* product_coset,
                                   const void* permuted_input_coset, const void* permuted_table_coset, const void* l0,
@@ -354,14 +385,17 @@ RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out,
 /* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
 /* Form of the MSM bucket-accumulation kernel: 6 = lazy R' = 2^260 limbs of 52 bits on the FP64 pipe
- * (default; window-table MSMs use it too); 0 = lazy R = 2^261 limbs of 29 bits with one-step carries
- * (window-table MSMs use it for every choice but 6); normalised R = 2^256 limbs with 5 = two field
- * products per out-of-line call, 1 = all products inline, 2 = one product per call, 3 / 4 = one per call
- * with 4 / 5 CTAs per SM.  Same results; tuning only. */
+ * (default; window-table MSMs use it too); 0 = lazy R = 2^261 limbs of 29 bits with one-step carries on the
+ * integer multiply pipe (window-table MSMs use it for every choice but 6).  A library built with
+ * H2B_EXPERIMENTS=1 also has the normalised R = 2^256 forms 1..5 (slower; A/B comparisons only).  A value
+ * that is not built leaves the setting unchanged.  Same results; tuning only. */
 void h2b_msm_set_accumulate_variant(int variant);
-/* Batch-affine pairing rounds before the XYZZ bucket accumulation (0..3, default 0).  Same results; the
- * MSM workspace-size queries depend on it (set it before sizing scratch). */
+int h2b_msm_get_accumulate_variant(void);
+/* Batch-affine pairing rounds before the XYZZ bucket accumulation (default 0; 1..3 only in a library built
+ * with H2B_EXPERIMENTS=1, where they measured slower).  Same results; the MSM workspace-size queries depend on
+ * it (set it before sizing scratch). */
 void h2b_msm_set_pair_rounds(int rounds);
+int h2b_msm_get_pair_rounds(void);
 
 /* Precomputed window tables (no counterpart in the reference): an SRS kept resident with its window
  * multiples [2^(c w)] P_i, so an MSM over it reduces one bucket set and has no final doubling chain.

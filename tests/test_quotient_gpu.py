@@ -142,3 +142,47 @@ def test_compress_expressions(h2b, orc, cuda):
         ex = [A[0][r], F[0][r] * A[1][(r + 1) % nq] % p, (A[2][(r - 1) % nq] + 5) % p]
         want = (ex[0] * theta * theta + ex[1] * theta + ex[2]) % p
         assert got[r] == want, r
+
+
+def test_resident_program_matches_and_replays_in_a_graph(h2b, orc, cuda):
+    """h2b_quotient_program_build / _run give the bytes of
+    _halo2_quotient_device_columns_device_out, with and without a prev seed,
+    on a row window, and the same again when replayed from a captured graph."""
+    import torch
+    f = h2b.fields
+    g = R.Graph()
+    parts = R.plonk_and_fibonacci(g)
+    nq = 1 << 12
+    fixed = [h2b.to_dev(c) for c in columns(orc, 1100, 3, nq)]
+    inst = [h2b.to_dev(c) for c in columns(orc, 2100, 1, nq)]
+    adv = [h2b.to_dev(c) for c in columns(orc, 3100, 4, nq)]
+    chal = orc.chacha_fr(4100, 1)
+    consts = f.fr_mont_limbs(g.constants)
+    rules = np.array(g.rules, dtype=np.uint64)
+    vp = np.array(parts, dtype=np.uint64)
+    y = 0xFEEDF00D
+    prev = h2b.to_dev(orc.chacha_fr(77, 1000))
+    want = h2b.dev_empty(32 * nq)
+    h2b.quotient_device(fixed, inst, adv, chal, consts, y, rules, vp, nq, 4, 0, nq, want)
+    want_w = h2b.dev_empty(32 * 1000)
+    h2b.quotient_device(fixed, inst, adv, chal, consts, y, rules, vp, nq, 4, 1500, 2500, want_w, prev)
+    prog = h2b.ResidentQuotient(fixed, inst, adv, chal, consts, y, rules, vp, nq, 4)
+    got, got_w = h2b.dev_empty(32 * nq), h2b.dev_empty(32 * 1000)
+    prog.run(got)
+    prog.run(got_w, prev, 1500, 2500)
+    torch.cuda.synchronize()
+    assert torch.equal(got, want) and torch.equal(got_w, want_w)
+    st = torch.cuda.Stream()
+    graph_out = h2b.dev_empty(32 * nq)
+    graph_out.zero_()
+    torch.cuda.synchronize()
+    gr = h2b.Graph(st)
+    gr.begin()
+    prog.run(graph_out, stream=st)
+    gr.end()
+    try:
+        gr.launch(st)
+        st.synchronize()
+    finally:
+        gr.close()
+    assert torch.equal(graph_out, want)
