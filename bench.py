@@ -709,7 +709,17 @@ def run_case(args):
     f = h2b.fields
     sh = h2b.stream_handle()
     n = 1 << args.log_n
-    if args.case == "probe":
+    if args.case == "permute":
+        tab = h2b.random_fr_device(256, 130, 0)
+        d_tab = torch.zeros(32 * n, dtype=torch.uint8, device="cuda")
+        d_tab[: 32 * 256] = tab
+        idx = torch.randint(0, 256, (n,), device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+        d_in = tab.view(256, 32)[idx].reshape(-1).contiguous()
+        d_pa, d_ps = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+        pws = h2b.dev_empty(L._halo2_permute_expression_pair_workspace_size(n, n - 10))
+        fn = lambda: h2b.call("_halo2_permute_expression_pair", h2b.ptr(d_in), h2b.ptr(d_tab),  # noqa: E731
+                              h2b.ptr(d_pa), h2b.ptr(d_ps), n, n - 10, h2b.ptr(pws), pws.numel(), sh)
+    elif args.case == "probe":
         sink = h2b.dev_empty(4 * 148 * 64)
         fn = lambda: h2b.call("h2b_probe_modmul", 148 * 8, 256, 64, h2b.ptr(sink), sh)  # noqa: E731
     elif args.case == "msm":
@@ -751,7 +761,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
-    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch"],
+    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")

@@ -172,6 +172,8 @@ _SIGS = {
     "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
     "h2b_ntt_set_pass_stages": (None, [ctypes.c_int]),
     "h2b_ntt_get_pass_stages": (ctypes.c_int, []),
+    "h2b_ntt_set_radix4": (None, [ctypes.c_int]),
+    "h2b_ntt_get_radix4": (ctypes.c_int, []),
     "h2b_random_fr": (RustError, [_vp, _u64, _u64, ctypes.c_int, _vp]),
     "h2b_powers": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_fibonacci_fr": (RustError, [_vp, _u64, _vp, _vp]),

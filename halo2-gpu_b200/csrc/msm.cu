@@ -507,11 +507,14 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
     }
 }
 
+#if H2B_EXPERIMENTS
 // The FP64 lazy accumulation with two independent chains per thread: the
 // entries of a bucket segment alternate between two accumulators whose
 // additions share their out-of-line product calls (xyzzd_madd_x2), and the
 // two are added once when the segment's bucket (or chunk head) is stored.
-// Same chunks, bucket boundaries and outputs as k_msm_accumulate_d.
+// Same chunks, bucket boundaries and outputs as k_msm_accumulate_d.  Measured
+// at 2^22 with the witness mix: 25.7 ms against 11.4 ms (255 registers and
+// spills halve the warps per SM; the second chain does not make up for it).
 __global__ void __launch_bounds__(128, 2) k_msm_accumulate_d2(const uint32_t* __restrict__ sorted,
                                                               const uint32_t* __restrict__ offsets, uint64_t NB,
                                                               uint32_t K, const G1Affine* __restrict__ bases,
@@ -573,7 +576,6 @@ __global__ void __launch_bounds__(128, 2) k_msm_accumulate_d2(const uint32_t* __
     }
 }
 
-#if H2B_EXPERIMENTS
 // ---- pairing rounds (batch-affine bucket additions) -----------------------
 // Round r adds the points of every bucket pairwise in affine coordinates:
 // entries (2j, 2j+1) of a bucket become output point j (an odd last entry is
@@ -1029,9 +1031,11 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     if (lazy && g_msm_acc_variant == 6)
         k_msm_accumulate_d<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
+#if H2B_EXPERIMENTS
     else if (lazy && g_msm_acc_variant == 7)
         k_msm_accumulate_d2<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                       p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
+#endif
     else if (lazy)
         k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
                                                      p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
@@ -1345,13 +1349,14 @@ extern "C" void h2b_msm_set_tuning(int window_bits, int chunk) { msm_set_tuning(
 // Built with H2B_EXPERIMENTS=1 only, the normalised R = 2^256 limb form with
 // 5 = two products per out-of-line call, 1 = all products inline, 2 = one
 // product per call, 3 and 4 = one product per call with at most 128 / 96
-// registers.  Measured at 2^22 with the witness-like scalar mix: 6 takes
+// registers, and 7 = the FP64 lazy form with two accumulation chains per
+// thread (25.7 ms at 2^22).  Measured at 2^22 with the witness-like scalar mix: 6 takes
 // 12.26 ms, 0 13.56 ms.  Results are identical; only speed differs.  A value
 // that is not built leaves the setting unchanged (read it back with
 // h2b_msm_get_accumulate_variant).
 extern "C" void h2b_msm_set_accumulate_variant(int v)
 {
-    if (v == 0 || v == 6 || v == 7 || (H2B_EXPERIMENTS && v >= 1 && v <= 5)) g_msm_acc_variant = v;
+    if (v == 0 || v == 6 || (H2B_EXPERIMENTS && v >= 1 && v <= 7)) g_msm_acc_variant = v;
 }
 
 extern "C" int h2b_msm_get_accumulate_variant(void) { return g_msm_acc_variant; }

@@ -289,6 +289,131 @@ __global__ void __launch_bounds__(NTT_THREADS, NTT_MIN_BLOCKS) k_ntt_pass(NttBat
     }
 }
 
+// The same pass with radix-4 steps: a thread takes four elements of a group
+// at positions q, q + 2^h, q + 2^(h+1), q + 2^(h+1) + 2^h and runs two
+// consecutive radix-2 stages on them in registers (four products in two
+// independent pairs, three twiddle loads), so shared memory is read and
+// written and the CTA synchronises once per two stages.  An odd stage count
+// runs one radix-2 stage first (DIT) or last (DIF).  Same tile layout,
+// twiddle indexing and outputs as k_ntt_pass.
+constexpr int NTT4_THREADS = 256;
+template <bool DIT>
+__global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const Fr* __restrict__ tw, int logn,
+                                                               int s0, int nst, int lS, int lG)
+{
+    const Fr* src = B.src[blockIdx.y];
+    Fr* a = B.dst[blockIdx.y];
+    extern __shared__ uint4 smem_raw[];
+    Fr* sm = reinterpret_cast<Fr*>(smem_raw);
+    const uint32_t Smask = (1u << lS) - 1;
+    const uint32_t g0 = blockIdx.x << lG;
+    const uint32_t elems = 1u << (lG + nst);
+    const bool wide = lS >= lG;
+    auto locate = [&](uint32_t idx, uint32_t& slot) -> uint32_t {
+        if (wide) {
+            const uint32_t gl = idx & ((1u << lG) - 1), j = idx >> lG;
+            const uint32_t g = g0 + gl;
+            slot = (gl << nst) + j;
+            return ((g >> lS) << (lS + nst)) + (j << lS) + (g & Smask);
+        }
+        const uint32_t bl = idx >> (lS + nst), rem = idx & ((1u << (lS + nst)) - 1);
+        const uint32_t j = rem >> lS, gl = (bl << lS) + (rem & Smask);
+        slot = (gl << nst) + j;
+        return ((g0 >> lS) << (lS + nst)) + idx;
+    };
+    for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint32_t slot;
+        const uint32_t addr = locate(idx, slot);
+        sm[slot] = ld(&src[addr]);
+    }
+    __syncthreads();
+    char* const smb = reinterpret_cast<char*>(sm);
+    const char* const twb = reinterpret_cast<const char*>(tw);
+    auto twid = [&](uint32_t lowm, uint32_t r, int sh) -> Fr {
+        return ldg(reinterpret_cast<const Fr*>(twb + (((((lowm << lS) + r) << sh)) << 5)));
+    };
+    // one radix-2 stage t
+    auto stage2 = [&](int t) {
+        const int s = s0 + t;
+        const int h = DIT ? t : nst - t - 1;
+        const uint32_t lo = (1u << h) - 1;
+        const int sh = DIT ? logn - s - 1 : s;
+        const uint32_t nbf = elems >> 1;
+        for (uint32_t b = threadIdx.x; b < nbf; b += blockDim.x) {
+            const uint32_t m = b & ((1u << (nst - 1)) - 1), gl = b >> (nst - 1);
+            const uint32_t r = (g0 + gl) & Smask;
+            const uint32_t lowm = m & lo, q = m + (m & ~lo);
+            Fr* px = reinterpret_cast<Fr*>(smb + (((gl << nst) + q) << 5));
+            Fr* py = reinterpret_cast<Fr*>(smb + (((gl << nst) + q + (1u << h)) << 5));
+            const Fr x = *px, y = *py, w = twid(lowm, r, sh);
+            if (DIT) {
+                const Fr yw = y * w;
+                *px = x + yw;
+                *py = x - yw;
+            } else {
+                *px = x + y;
+                *py = (x - y) * w;
+            }
+        }
+        __syncthreads();
+    };
+    // two stages t, t + 1 as radix-4 steps
+    auto stage4 = [&](int t) {
+        const int h = DIT ? t : nst - t - 2;           // the smaller of the two spans is 2^h
+        const uint32_t lo = (1u << h) - 1;
+        const uint32_t nq = elems >> 2;
+        for (uint32_t qi = threadIdx.x; qi < nq; qi += blockDim.x) {
+            const uint32_t m4 = qi & ((1u << (nst - 2)) - 1), gl = qi >> (nst - 2);
+            const uint32_t r = (g0 + gl) & Smask;
+            const uint32_t lowm = m4 & lo, q = lowm + ((m4 >> h) << (h + 2));
+            char* const gb = smb + ((gl << nst) << 5);
+            Fr* p0 = reinterpret_cast<Fr*>(gb + (q << 5));
+            Fr* p1 = reinterpret_cast<Fr*>(gb + ((q + (1u << h)) << 5));
+            Fr* p2 = reinterpret_cast<Fr*>(gb + ((q + (2u << h)) << 5));
+            Fr* p3 = reinterpret_cast<Fr*>(gb + ((q + (3u << h)) << 5));
+            const Fr a0 = *p0, a1 = *p1, a2 = *p2, a3 = *p3;
+            if (DIT) {
+                // stage t (span 2^h): (p0, p1), (p2, p3) share w_h; stage t + 1 (span 2^(h+1)):
+                // (p0, p2) takes lowm, (p1, p3) takes lowm + 2^h
+                const int sh0 = logn - (s0 + t) - 1, sh1 = sh0 - 1;
+                const Fr wh = twid(lowm, r, sh0), wa = twid(lowm, r, sh1), wb = twid(lowm + (1u << h), r, sh1);
+                const Fr t1 = a1 * wh, t3 = a3 * wh;
+                const Fr b0 = a0 + t1, b1 = a0 - t1, b2 = a2 + t3, b3 = a2 - t3;
+                const Fr u2 = b2 * wa, u3 = b3 * wb;
+                *p0 = b0 + u2;
+                *p2 = b0 - u2;
+                *p1 = b1 + u3;
+                *p3 = b1 - u3;
+            } else {
+                // stage t (span 2^(h+1)): (p0, p2) takes lowm, (p1, p3) lowm + 2^h;
+                // stage t + 1 (span 2^h): (p0, p1), (p2, p3) share w_h
+                const int sh0 = s0 + t, sh1 = sh0 + 1;
+                const Fr wa = twid(lowm, r, sh0), wb = twid(lowm + (1u << h), r, sh0), wh = twid(lowm, r, sh1);
+                const Fr b0 = a0 + a2, b1 = a1 + a3;
+                const Fr b2 = (a0 - a2) * wa, b3 = (a1 - a3) * wb;
+                *p0 = b0 + b1;
+                *p1 = (b0 - b1) * wh;
+                *p2 = b2 + b3;
+                *p3 = (b2 - b3) * wh;
+            }
+        }
+        __syncthreads();
+    };
+    int t = 0;
+    if (DIT && (nst & 1)) stage2(t++);
+    for (; t + 1 < nst; t += 2) stage4(t);
+    if (t < nst) stage2(t);
+    for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
+        uint32_t slot;
+        const uint32_t addr = locate(idx, slot);
+        st(&a[addr], sm[slot]);
+    }
+}
+
+static int g_ntt_radix4 = 0;   // 1: the passes run k_ntt_pass4
+void ntt_set_radix4(int on) { g_ntt_radix4 = on ? 1 : 0; }
+int ntt_get_radix4() { return g_ntt_radix4; }
+
 // ---------------------------------------------------------------------------
 // host-side pass planning
 // ---------------------------------------------------------------------------
@@ -329,7 +454,13 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
         const dim3 grid((unsigned)(1ull << (logn - nst - lG)), (unsigned)count);
         size_t smem = (size_t)(1ull << (lG + nst)) * sizeof(Fr);
         int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 1)));
-        if (dit)
+        if (g_ntt_radix4 && nst >= 2) {
+            threads = (int)std::min<uint64_t>(NTT4_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 2)));
+            if (dit)
+                k_ntt_pass4<true><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
+            else
+                k_ntt_pass4<false><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
+        } else if (dit)
             k_ntt_pass<true><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
         else
             k_ntt_pass<false><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);
@@ -715,6 +846,10 @@ extern "C" int32_t _halo2_get_fft_split_radix(uint32_t ntt_type, uint32_t log_n,
     }
     return -1;
 }
+
+// Radix-4 pass steps (1) or radix-2 stages (0, default); same results.
+extern "C" void h2b_ntt_set_radix4(int on) { ntt_set_radix4(on); }
+extern "C" int h2b_ntt_get_radix4(void) { return ntt_get_radix4(); }
 
 extern "C" void h2b_ntt_set_pass_stages(int stages) { ntt_set_pass_stages(stages); }
 extern "C" int h2b_ntt_get_pass_stages(void) { return ntt_pass_stages(); }

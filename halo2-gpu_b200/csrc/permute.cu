@@ -313,6 +313,13 @@ __global__ void k_pp_count(const Key* __restrict__ input, uint64_t u, const Key*
     }
 }
 
+// The single-CTA path's count: ranks go into a per-block histogram in shared
+// memory (d <= PP_SMALL bins), each block adds its nonzero bins once, so the
+// global counters see one atomic per block and rank instead of one per row.
+__global__ void __launch_bounds__(256) k_pp_count_small(const Key* __restrict__ input, uint64_t u,
+                                                        const Key* __restrict__ table, HashSet hs,
+                                                        uint32_t* __restrict__ acount, uint32_t* __restrict__ misc);
+
 // Per rank: used = the input holds the value; left = the table copies that
 // no first occurrence takes.
 __global__ void k_pp_flags(const uint32_t* __restrict__ acount, const uint32_t* __restrict__ tcount, uint32_t d,
@@ -477,6 +484,31 @@ __global__ void __launch_bounds__(1024) k_pp_small_scan(const uint32_t* __restri
     }
 }
 
+__global__ void __launch_bounds__(256) k_pp_count_small(const Key* __restrict__ input, uint64_t u,
+                                                        const Key* __restrict__ table, HashSet hs,
+                                                        uint32_t* __restrict__ acount, uint32_t* __restrict__ misc)
+{
+    if (misc[PP_LARGE]) return;
+    const uint32_t d = misc[PP_D];
+    __shared__ uint32_t hist[PP_SMALL];
+    for (uint32_t r = threadIdx.x; r < d; r += blockDim.x) hist[r] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < u; i += (uint64_t)gridDim.x * blockDim.x) {
+        const Key k = ld_key(&input[i]);
+        const uint64_t s = hs_find(hs, table, k, 0, false, misc + PP_ERR);
+        if (s == ~0ull) {
+            atomicOr(misc + PP_ERR, PP_ERR_MISSING);
+        } else {
+            const uint32_t r = hs.rank[s];
+            if (r < d) atomicAdd(&hist[r], 1u);
+            else atomicOr(misc + PP_ERR, PP_ERR_FULL);
+        }
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < d; r += blockDim.x)
+        if (hist[r]) atomicAdd(&acount[r], hist[r]);
+}
+
 static uint64_t pp_slots(uint64_t u)
 {
     uint64_t s = 1024;
@@ -565,9 +597,8 @@ extern "C" RustError _halo2_permute_expression_pair(const void* d_compressed_inp
     // single-CTA path for few distinct values (skipped on the device otherwise)
     k_pp_small_sort<<<1, 1024, 0, stream>>>(distinct, misc, table, hs, dm, tcount, acount);
     H2B_LAUNCHED("k_pp_small_sort");
-    k_pp_count<<<grid_for((u + 31) / 32, 8, 148u * 16u), 256, 0, stream>>>(input, u, table, hs, acount,
-                                                                          misc + PP_ERR, misc + PP_LARGE);
-    H2B_LAUNCHED("k_pp_count");
+    k_pp_count_small<<<grid_for(u, 256, 148u * 2u), 256, 0, stream>>>(input, u, table, hs, acount, misc);
+    H2B_LAUNCHED("k_pp_count_small");
     k_pp_small_scan<<<1, 1024, 0, stream>>>(acount, tcount, misc, astart, uexcl, lstart);
     H2B_LAUNCHED("k_pp_small_scan");
     k_pp_emit<<<grid_for(n, 256, 148u * 8u), 256, 0, stream>>>(dm, astart, uexcl, lstart, misc + PP_D, u, n, pin, ptab,

@@ -446,6 +446,10 @@ RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_t length, v
 /* Radix-2 stages per shared-memory NTT pass (1..10). */
 void h2b_ntt_set_pass_stages(int stages);
 int h2b_ntt_get_pass_stages(void);
+/* NTT passes as radix-4 steps (1: a thread runs two stages on four elements in registers) or radix-2
+ * stages (0).  Same results. */
+void h2b_ntt_set_radix4(int on);
+int h2b_ntt_get_radix4(void);
 /* Per-size tuning table written by the autotuner (no counterpart in the reference, whose MSM window width
  * and NTT stage split are fixed formulas: halo2_proofs/cuda/src/multiexp.cu:260-300,
  * halo2_proofs/cuda/include/kernel/ntt_combine.h:90-94).  param 0 = MSM window bits (10..16; plain-base

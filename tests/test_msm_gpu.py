@@ -181,7 +181,7 @@ def test_msm_pairing_rounds(h2b, orc, cuda, srs_small, rounds):
         L.h2b_msm_set_pair_rounds(0)
 
 
-@pytest.mark.parametrize("variant", [0, 5, 6])
+@pytest.mark.parametrize("variant", [0, 5, 6, 7])
 def test_msm_accumulate_forms(h2b, orc, cuda, srs_small, variant):
     """Every bucket-accumulation form (h2b_msm_set_accumulate_variant: 0 =
     29-bit lazy R = 2^261, 5 = normalised R = 2^256, 6 = FP64 lazy R' =

@@ -9,6 +9,16 @@ from conftest import assert_limbs_equal
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=[0, 1], ids=["radix2", "radix4"], autouse=True)
+def pass_kind(request, h2b):
+    """Every NTT test runs with the radix-2 and the radix-4 pass kernels."""
+    L = h2b.lib()
+    before = L.h2b_ntt_get_radix4()
+    L.h2b_ntt_set_radix4(request.param)
+    yield request.param
+    L.h2b_ntt_set_radix4(before)
+
+
 def mont(h2b, x):
     return h2b.fields.fr_mont_limbs([x])
 
