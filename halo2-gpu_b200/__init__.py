@@ -154,6 +154,8 @@ _SIGS = {
     "h2b_msm_set_pair_rounds": (None, [ctypes.c_int]),
     "h2b_msm_get_accumulate_variant": (ctypes.c_int, []),
     "h2b_msm_get_pair_rounds": (ctypes.c_int, []),
+    "h2b_msm_set_prefetch": (None, [ctypes.c_int]),
+    "h2b_msm_get_prefetch": (ctypes.c_int, []),
     "h2b_exec_fork": (RustError, [_vp, _u32, ctypes.POINTER(ctypes.c_void_p)]),
     "h2b_exec_join": (RustError, [_vp, _u32]),
     "h2b_upload": (RustError, [_vp, _vp, _u64, _vp]),

@@ -73,6 +73,7 @@ void msm_set_pair_rounds(int rounds)
     if (rounds >= 0 && rounds <= (H2B_EXPERIMENTS ? 3 : 0)) g_msm_pair_rounds = rounds;
 }
 static int g_msm_chunk_override = 0;
+static uint32_t g_msm_prefetch = 0;   // entries ahead whose point the accumulation prefetches into L2 (0: none)
 
 void msm_set_tuning(int window_bits, int chunk)
 {
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
                                                              const uint32_t* __restrict__ offsets, uint64_t NB,
                                                              uint32_t K, const G1Affine* __restrict__ bases,
                                                              uint64_t phi_off, G1Xyzz* __restrict__ buckets,
-                                                             G1Xyzz* __restrict__ heads)
+                                                             G1Xyzz* __restrict__ heads, uint32_t pf)
 {
     const uint32_t M = offsets[NB];
     const uint64_t nchunks = (M + (uint64_t)K - 1) / K;
@@ -492,6 +493,11 @@ __global__ void __launch_bounds__(128, 3) k_msm_accumulate_d(const uint32_t* __r
                 acc = xyzzd_inf();
                 head = false;
                 do { b++; next = offsets[b + 1]; } while (next == e);
+            }
+            if (pf && e + pf < end) {   // bring the point pf entries ahead into L2 (no registers held)
+                const uint32_t vn = sorted[e + pf] & ~SIGN_BIT;
+                const G1Affine* pn = &bases[(vn >> 1) + ((vn & 1u) ? phi_off : 0)];
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(pn));
             }
             const uint32_t ent = sorted[e];
             const uint32_t v = ent & ~SIGN_BIT;
@@ -1030,7 +1036,8 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
     if (lazy && g_msm_acc_variant == 6)
         k_msm_accumulate_d<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
-                                                     p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads);
+                                                     p.tn ? (uint64_t)p.W * p.tn : p.n, s.buckets, s.heads,
+                                                     g_msm_prefetch);
 #if H2B_EXPERIMENTS
     else if (lazy && g_msm_acc_variant == 7)
         k_msm_accumulate_d2<<<acc_grid, 128, 0, st>>>(s.sorted, off, p.NB, p.Kf, p.tn ? d_bases : s.rbases,
@@ -1360,6 +1367,14 @@ extern "C" void h2b_msm_set_accumulate_variant(int v)
 }
 
 extern "C" int h2b_msm_get_accumulate_variant(void) { return g_msm_acc_variant; }
+
+// Distance (sorted entries ahead, 0..64) at which the FP64 accumulation
+// prefetches the next points into L2; 0 turns it off.  Same results.
+extern "C" void h2b_msm_set_prefetch(int distance)
+{
+    if (distance >= 0 && distance <= 64) g_msm_prefetch = (uint32_t)distance;
+}
+extern "C" int h2b_msm_get_prefetch(void) { return (int)g_msm_prefetch; }
 
 extern "C" int h2b_msm_get_pair_rounds(void) { return g_msm_pair_rounds; }
 

@@ -76,6 +76,17 @@ __global__ void __launch_bounds__(TW_T) k_twiddles(const Fr* __restrict__ lut, F
     }
 }
 
+// tw[e] = lo[e mod 2^TW2_LOG] * hi[e >> TW2_LOG] with lo[j] = w^j and
+// hi[j] = w^(2^TW2_LOG j): one independent product per twiddle, both factors
+// from small tables that stay in cache.
+constexpr int TW2_LOG = 10;
+__global__ void k_twiddles_fill(const Fr* __restrict__ lo, const Fr* __restrict__ hi, Fr* __restrict__ tw,
+                                uint64_t half)
+{
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < half; e += (uint64_t)gridDim.x * blockDim.x)
+        st(&tw[e], ldg(&lo[e & ((1u << TW2_LOG) - 1)]) * ldg(&hi[e >> TW2_LOG]));
+}
+
 __device__ __forceinline__ uint64_t bitrev(uint64_t x, int k)
 {
     return k == 0 ? 0 : (__brevll(x) >> (64 - k));
@@ -410,7 +421,7 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
     }
 }
 
-static int g_ntt_radix4 = 0;   // 1: the passes run k_ntt_pass4
+static int g_ntt_radix4 = 1;   // 1 (default): the passes run k_ntt_pass4
 void ntt_set_radix4(int on) { g_ntt_radix4 = on ? 1 : 0; }
 int ntt_get_radix4() { return g_ntt_radix4; }
 
@@ -477,6 +488,7 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
 // parts) the coset powers c^i, i < n.
 struct NttScratch {
     Fr* tw = nullptr;
+    Fr* tw2 = nullptr;   // lo and hi factors of the two-level twiddle fill
     Fr* lut_w = nullptr;
     Fr* lut_c = nullptr;
     Fr* omega = nullptr;
@@ -488,6 +500,7 @@ static void plan_ntt(ScratchPlan& p, int log_size, bool data_slot, int log_data,
 {
     uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
     p.add_n<Fr>(half);
+    p.add_n<Fr>((1ull << TW2_LOG) + (half >> TW2_LOG) + 1);
     p.add_n<Fr>(64);
     p.add_n<Fr>(64);
     p.add_n<Fr>(1);
@@ -500,6 +513,7 @@ static NttScratch carve_ntt(ScratchArena& ar, int log_size, bool data_slot, int 
     NttScratch s;
     uint64_t half = log_size == 0 ? 1 : (1ull << (log_size - 1));
     s.tw = ar.take_n<Fr>(half);
+    s.tw2 = ar.take_n<Fr>((1ull << TW2_LOG) + (half >> TW2_LOG) + 1);
     s.lut_w = ar.take_n<Fr>(64);
     s.lut_c = ar.take_n<Fr>(64);
     s.omega = ar.take_n<Fr>(1);
@@ -516,8 +530,21 @@ static RustError make_twiddles(const Fr* d_omega, NttScratch& s, int logn, cudaS
     H2B_LAUNCHED("k_pow2_lut");
     uint64_t half = 1ull << (logn - 1);
     const uint64_t tile = (uint64_t)TW_T * TW_K;
-    k_twiddles<<<(unsigned)((half + tile - 1) / tile), TW_T, 0, st>>>(s.lut_w, s.tw, half);
+    if (half < (4ull << TW2_LOG)) {
+        k_twiddles<<<(unsigned)((half + tile - 1) / tile), TW_T, 0, st>>>(s.lut_w, s.tw, half);
+        H2B_LAUNCHED("k_twiddles");
+        return ok();
+    }
+    // lo[j] = w^j, j < 2^TW2_LOG; hi[j] = (w^(2^TW2_LOG))^j from the same power table shifted by TW2_LOG
+    const uint64_t nlo = 1ull << TW2_LOG, nhi = half >> TW2_LOG;
+    Fr* lo = s.tw2;
+    Fr* hi = s.tw2 + nlo;
+    k_twiddles<<<(unsigned)((nlo + tile - 1) / tile), TW_T, 0, st>>>(s.lut_w, lo, nlo);
     H2B_LAUNCHED("k_twiddles");
+    k_twiddles<<<(unsigned)((nhi + tile - 1) / tile), TW_T, 0, st>>>(s.lut_w + TW2_LOG, hi, nhi);
+    H2B_LAUNCHED("k_twiddles");
+    k_twiddles_fill<<<grid_for(half, 256, 148u * 16u), 256, 0, st>>>(lo, hi, s.tw, half);
+    H2B_LAUNCHED("k_twiddles_fill");
     return ok();
 }
 

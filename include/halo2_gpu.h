@@ -469,7 +469,8 @@ void h2b_tune_clear(void);
  * workspace, so it allocates and frees nothing.  length <= 2^26 (larger is
  * an error).  All calls share that array: calls that overlap on the GPU
  * race, so serialise them on one stream.  The first call on each device
- * looks up the array's address; make it before any stream capture. */
+ * (and the first after its CUDA context is recreated) looks up the array's
+ * address; make it before any stream capture. */
 RustError h2b_batch_invert_noalloc(void* d_data, uint32_t field_type, uint64_t length, h2b_stream_t stream);
 
 #ifdef __cplusplus
