@@ -408,6 +408,45 @@ def rows_section(h2b, torch, hbm_gbs, product_peak, k=20, reps=5):
     d_b, d_g, d_y = (h2b.to_dev(sc(s)) for s in (3, 5, 7))
     timed("lookup_quotient", lambda: h2b.quotient_lookups_device(*arrs, d_b, d_g, d_y, n, stream=side), n, "rows",
           9 * 32)
+    # a7-a9 together on one config-3 extended part: the reference's four per-part
+    # launches (gates, permutation, lookup expression, lookup constraints)
+    # against one h2b_quotient_fused launch; 22 arrays of 32 B per row are read
+    # once and one written by the fused pass
+    C = importlib.import_module(h2b.__name__ + ".circuit")
+    g_rules, g_parts, g_consts = C.gate_graph()
+    l_rules, l_parts, l_consts = C.lookup_product_graph()
+    qf, qi, qa = [rnd(n, 200 + i) for i in range(3)], [rnd(n, 210)], [rnd(n, 220 + i) for i in range(4)]
+    zs, sg = [rnd(n, 230 + i) for i in range(2)], [rnd(n, 240 + i) for i in range(4)]
+    zl, pa, ps = (rnd(n, 250 + i) for i in range(3))
+    lag3 = [rnd(n, 260 + i) for i in range(3)]
+    beta, gamma, yv = 0x1234567, 0x7654321, 0xABCDEF
+    pcols = [qa[0], qa[1], qa[2], qi[0]]
+    shift = pow(dom.extended_omega, 3, f.R_MOD)
+    dstart = beta * f.ZETA % f.R_MOD
+    bg = f.fr_mont_limbs([beta, gamma])
+    hj, tv, fo = h2b.dev_empty(32 * n), h2b.dev_empty(32 * n), h2b.dev_empty(32 * n)
+    d_bt, d_gm, d_yv = (h2b.to_dev(sc(s)) for s in (beta, gamma, yv))
+    last = -(C.BLINDING_FACTORS + 1)
+
+    def chain():
+        h2b.quotient_device(qf, qi, qa, [], g_consts, yv, g_rules, g_parts, n, 1, 0, n, hj, stream=side)
+        h2b.quotient_permutation_device(hj, *lag3, zs, sg, pcols, beta, gamma, yv, f.DELTA, dstart, shift, dom.omega,
+                                        C.CHUNK_LEN, last, 1, n, n, stream=side)
+        h2b.quotient_device(qf, qi, qa, bg, l_consts, yv, l_rules, l_parts, n, 1, 0, n, tv, stream=side)
+        h2b.quotient_lookups_device(hj, tv, zl, pa, ps, *lag3, d_bt, d_gm, d_yv, n, stream=side)
+
+    perm = dict(prods=zs, sigmas=sg, cols=pcols, beta=beta, gamma=gamma, delta=f.DELTA, delta_start=dstart,
+                ext_omega=shift, omega=dom.omega, chunk_len=C.CHUNK_LEN, last_rotation=last, rot_scale=1, isize=n)
+    look = [dict(rules=(bg, l_consts, l_rules, l_parts), z=zl, pin=pa, ptab=ps, beta=beta, gamma=gamma)]
+    no_ch = np.zeros((0, 4), np.uint64)
+    timed("quotient_part_chain", chain, n, "rows", 22 * 32)
+    timed("quotient_part_fused", lambda: h2b.quotient_fused_device(
+        qf, qi, qa, (no_ch, g_consts, g_rules, g_parts), yv, *lag3, perm, look, n, 1, 0, n, fo, stream=side),
+        n, "rows", 22 * 32)
+    torch.cuda.synchronize()
+    out["quotient_part_fused"]["identical_to_chain"] = bool(torch.equal(hj, fo))
+    out["quotient_part_fused"]["speedup_over_chain"] = round(out["quotient_part_chain"]["ms"] /
+                                                             out["quotient_part_fused"]["ms"], 3)
     # a10: permutation grand product (4 columns)
     mod = rnd(n, 90)
     pv, pp = [rnd(n, 91 + i) for i in range(4)], [rnd(n, 95 + i) for i in range(4)]
@@ -741,6 +780,26 @@ def run_case(args):
         ins, outs = h2b.ffi_array([d_in.data_ptr()]), h2b.ffi_array([d_ext.data_ptr()])
         fn = lambda: h2b.call("_halo2_fft_many_to_device", 3, 1, args.log_n, ek, ins, outs, h2b.ptr(d_om),
                               ctypes.byref(one_ffi), True, h2b.ptr(ws), ws.numel(), sh)
+    elif args.case == "quotient":
+        # one config-3 extended part through h2b_quotient_fused
+        C = importlib.import_module(h2b.__name__ + ".circuit")
+        import numpy as np
+        g_rules, g_parts, g_consts = C.gate_graph()
+        l_rules, l_parts, l_consts = C.lookup_product_graph()
+        rnd = lambda s: h2b.random_fr_device(n, s, 0)  # noqa: E731
+        qf, qi, qa = [rnd(200 + i) for i in range(3)], [rnd(210)], [rnd(220 + i) for i in range(4)]
+        lag3 = [rnd(260 + i) for i in range(3)]
+        dom = f.EvaluationDomain(4, args.log_n)
+        perm = dict(prods=[rnd(230), rnd(231)], sigmas=[rnd(240 + i) for i in range(4)],
+                    cols=[qa[0], qa[1], qa[2], qi[0]], beta=3, gamma=5, delta=f.DELTA, delta_start=11,
+                    ext_omega=dom.extended_omega, omega=dom.omega, chunk_len=C.CHUNK_LEN,
+                    last_rotation=-(C.BLINDING_FACTORS + 1), rot_scale=1, isize=n)
+        look = [dict(rules=(f.fr_mont_limbs([3, 5]), l_consts, l_rules, l_parts), z=rnd(250), pin=rnd(251),
+                     ptab=rnd(252), beta=3, gamma=5)]
+        gates = (np.zeros((0, 4), np.uint64), g_consts, g_rules, g_parts)
+        d_out = h2b.dev_empty(32 * n)
+        fn = lambda: h2b.quotient_fused_device(qf, qi, qa, gates, 7, *lag3, perm, look, n, 1, 0, n,  # noqa: E731
+                                               d_out)
     else:
         d = h2b.random_fr_device(n, 3000, 0)
         ws = h2b.dev_empty(L.h2b_batch_invert_workspace_size(n))
@@ -761,7 +820,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
-    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute"],
+    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute", "quotient"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")

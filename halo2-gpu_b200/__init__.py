@@ -52,6 +52,31 @@ class QuotientProgram(ctypes.Structure):
                 ("off_y", ctypes.c_uint64), ("bytes", ctypes.c_uint64)]
 
 
+class QuotientRules(ctypes.Structure):
+    """h2b_quotient_rules: one expression graph in the reference's rule encoding, host data."""
+    _fields_ = [("rules", ctypes.c_void_p), ("num_rules", ctypes.c_uint64), ("value_part_rules", ctypes.c_void_p),
+                ("num_vp", ctypes.c_uint64), ("constants", ctypes.c_void_p), ("num_constants", ctypes.c_uint64),
+                ("challenges", ctypes.c_void_p), ("num_challenges", ctypes.c_uint64)]
+
+
+class QuotientPermutationArgs(ctypes.Structure):
+    """h2b_quotient_permutation_args: the permutation argument of one extended part."""
+    _fields_ = [("n_sets", ctypes.c_uint64), ("chunk_len", ctypes.c_uint64), ("n_columns", ctypes.c_uint64),
+                ("product_cosets", ctypes.c_void_p), ("sigma_cosets", ctypes.c_void_p),
+                ("column_values", ctypes.c_void_p), ("beta", ctypes.c_void_p), ("gamma", ctypes.c_void_p),
+                ("delta", ctypes.c_void_p), ("delta_start", ctypes.c_void_p),
+                ("current_extended_omega", ctypes.c_void_p), ("omega", ctypes.c_void_p),
+                ("last_rotation", ctypes.c_int32), ("rot_scale", ctypes.c_int32), ("isize", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class QuotientLookupArgs(ctypes.Structure):
+    """h2b_quotient_lookup_args: one lookup of one extended part."""
+    _fields_ = [("product", QuotientRules), ("product_coset", ctypes.c_void_p),
+                ("permuted_input_coset", ctypes.c_void_p), ("permuted_table_coset", ctypes.c_void_p),
+                ("beta", ctypes.c_void_p), ("gamma", ctypes.c_void_p)]
+
+
 class Halo2GpuError(RuntimeError):
     def __init__(self, code, message, who):
         super().__init__(f"{who}: code {code}: {message}")
@@ -196,6 +221,12 @@ _SIGS = {
     "h2b_quotient_program_build": (RustError, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _u64, _vp, _u64,
                                                _vp, _u64, _u64, _vp, _u64, ctypes.POINTER(QuotientProgram), _vp]),
     "h2b_quotient_program_run": (RustError, [ctypes.POINTER(QuotientProgram), _vp, _vp, _vp, _u64, _u64, _vp]),
+    "h2b_quotient_fused": (RustError, [_vp, _u64, _vp, _u64, _vp, _u64, ctypes.POINTER(QuotientRules), _vp, _vp, _vp,
+                                       _vp, ctypes.POINTER(QuotientPermutationArgs),
+                                       ctypes.POINTER(QuotientLookupArgs), _u64, _u64, _u64, _u64, _u64, _vp, _u64,
+                                       _u64, _vp, _vp]),
+    "h2b_quotient_fused_set_blocks": (None, [ctypes.c_int]),
+    "h2b_quotient_fused_get_blocks": (ctypes.c_int, []),
     "h2b_batch_invert_assigned": (RustError, [_vp, _vp, _u32, _u64, AssignedLayout, _vp, _u64, _vp]),
     "h2b_tune_set": (_i32, [_u32, _u32, _i32]),
     "h2b_tune_get": (_i32, [_u32, _u32]),
@@ -829,6 +860,62 @@ class ResidentQuotient:
         call("h2b_quotient_program_run", ctypes.byref(self.info), ptr(self.d_prog), ptr(d_out),
              ptr(d_prev) if d_prev is not None else None, row_start, row_end, stream_handle(stream))
         return d_out
+
+
+def _rules_struct(graph, keep):
+    """QuotientRules for (challenges, constants, rules, value_part_rules); the
+    numpy arrays it points into are appended to `keep`."""
+    challenges, constants, rules, vp_rules = graph
+    ch = np.ascontiguousarray(challenges, dtype=np.uint64).reshape(-1, 4) if len(challenges) else \
+        np.zeros((1, 4), np.uint64)
+    cs = np.ascontiguousarray(constants, dtype=np.uint64).reshape(-1, 4) if len(constants) else \
+        np.zeros((1, 4), np.uint64)
+    r = np.ascontiguousarray(rules, dtype=np.uint64)
+    vp = np.ascontiguousarray(vp_rules, dtype=np.uint64)
+    keep += [ch, cs, r, vp]
+    return QuotientRules(r.ctypes.data, len(r) // 2, vp.ctypes.data, len(vp), cs.ctypes.data,
+                         len(constants) and cs.shape[0], ch.ctypes.data, len(challenges))
+
+
+def quotient_fused_device(d_fixed, d_instance, d_advice, gates, y, d_l0, d_llast, d_lactive, perm, lookups,
+                          num_quotient, rot_scale, row_start, row_end, d_out, out_stride=1, out_offset=0, scale=None,
+                          stream=None):
+    """h2b_quotient_fused: gates, permutation and lookups of one extended part in
+    one kernel.  `gates` and each lookup's `rules` are (challenges, constants,
+    rules, value_part_rules); `perm` is None or a dict with prods, sigmas, cols
+    (device tensors), beta, gamma, delta, delta_start, ext_omega, omega (ints),
+    chunk_len, last_rotation, rot_scale, isize; each lookup is a dict with rules,
+    z, pin, ptab (device tensors), beta, gamma (ints).  Scalars are integers."""
+    keep = []
+    g = _rules_struct(gates, keep)
+    yv = _scalar_bytes(y)
+    keep.append(yv)
+    pa = None
+    if perm is not None:
+        tabs = [_ptr_table(perm[k]) for k in ("prods", "sigmas", "cols")]
+        sc = [_scalar_bytes(perm[k]) for k in ("beta", "gamma", "delta", "delta_start", "ext_omega", "omega")]
+        keep += tabs + sc
+        pa = QuotientPermutationArgs(len(perm["prods"]), perm["chunk_len"], len(perm["cols"]),
+                                     ctypes.addressof(tabs[0]), ctypes.addressof(tabs[1]), ctypes.addressof(tabs[2]),
+                                     *[x.ctypes.data for x in sc], perm["last_rotation"], perm["rot_scale"],
+                                     perm["isize"], 0)
+    la = (QuotientLookupArgs * max(len(lookups), 1))()
+    for i, lk in enumerate(lookups):
+        bt, gm = _scalar_bytes(lk["beta"]), _scalar_bytes(lk["gamma"])
+        keep += [bt, gm]
+        la[i] = QuotientLookupArgs(_rules_struct(lk["rules"], keep), ptr(lk["z"]), ptr(lk["pin"]), ptr(lk["ptab"]),
+                                   bt.ctypes.data, gm.ctypes.data)
+    sv = None
+    if scale is not None:
+        sv = _scalar_bytes(scale)
+        keep.append(sv)
+    call("h2b_quotient_fused", _ptr_table(d_fixed), len(d_fixed), _ptr_table(d_instance), len(d_instance),
+         _ptr_table(d_advice), len(d_advice), ctypes.byref(g), yv.ctypes.data,
+         ptr(d_l0) if d_l0 is not None else None, ptr(d_llast) if d_llast is not None else None,
+         ptr(d_lactive) if d_lactive is not None else None, ctypes.byref(pa) if pa is not None else None, la,
+         len(lookups), num_quotient, rot_scale, row_start, row_end, ptr(d_out), out_stride, out_offset,
+         sv.ctypes.data if sv is not None else None, stream_handle(stream))
+    return d_out
 
 
 def quotient_lookups_device(d_values, d_table, d_z, d_pin, d_ptab, d_l0, d_llast, d_lactive, d_beta, d_gamma, d_y,

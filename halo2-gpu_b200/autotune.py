@@ -12,8 +12,9 @@ times candidate settings on the GPU it runs on and keeps the fastest:
   entries per accumulation chunk (automatic, 32, 64, 128, 256) at the chosen
   width.  Timed on the witness-like scalar mix (50 % uniform, 30 % < 2^64,
   20 % {0, 1}) over a prefix of a synthetic SRS.
-* op "ntt", k = log2 of the transform size: radix-2 stages per shared-memory
-  pass (6..10), timed on a forward FFT of uniform random coefficients; the
+* op "ntt", k = log2 of the transform size: stages per shared-memory pass
+  (6..11; 11 only with the radix-4 pass kernel, whose tiles hold 2^11
+  elements), timed on a forward FFT of uniform random coefficients; the
   setting then applies to every transform of that size (FFT, iFFT, coset
   extension passes).
 
@@ -36,7 +37,7 @@ import statistics
 PARAM_WINDOW, PARAM_CHUNK, PARAM_STAGES = 0, 1, 2
 WINDOW_RANGE = (10, 16)
 CHUNK_CANDIDATES = (0, 32, 64, 128, 256)
-STAGE_CANDIDATES = (6, 7, 8, 9, 10)
+STAGE_CANDIDATES = (6, 7, 8, 9, 10, 11)
 CACHE_VERSION = 1
 
 

@@ -73,7 +73,7 @@ void msm_set_pair_rounds(int rounds)
     if (rounds >= 0 && rounds <= (H2B_EXPERIMENTS ? 3 : 0)) g_msm_pair_rounds = rounds;
 }
 static int g_msm_chunk_override = 0;
-static uint32_t g_msm_prefetch = 0;   // entries ahead whose point the accumulation prefetches into L2 (0: none)
+static uint32_t g_msm_prefetch = 2;   // entries ahead whose point the accumulation prefetches into L2 (0: none)
 
 void msm_set_tuning(int window_bits, int chunk)
 {

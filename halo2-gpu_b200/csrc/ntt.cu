@@ -308,6 +308,42 @@ __global__ void __launch_bounds__(NTT_THREADS, NTT_MIN_BLOCKS) k_ntt_pass(NttBat
 // runs one radix-2 stage first (DIT) or last (DIF).  Same tile layout,
 // twiddle indexing and outputs as k_ntt_pass.
 constexpr int NTT4_THREADS = 256;
+constexpr int NTT4_LOG_TILE = 11;  // radix-4 passes: up to 2^11 elements (64 KB) per tile
+
+// The radix-4 pass keeps its tile as two planes of 16-byte halves (limbs 0-3
+// of every element, then limbs 4-7), element s at the swizzled index
+// s ^ (((s >> 2) ^ (s >> 3) ^ (s >> nst)) & 7).  The swizzle changes bits 0-2
+// from higher bits only, so it permutes every power-of-two tile.  With it the
+// eight lanes of each quarter-warp of a 16-byte access fall in eight
+// different bank groups for the slot patterns the pass makes: consecutive
+// slots, the stride-2/4/8 quadruples of the low-span stages and the
+// stride-2^nst slots of the wide load and store loops.  With whole 32-byte
+// elements at stride 32 bytes every access took 2 to 8 wavefronts instead of 1.
+struct NttTile4 {
+    uint4* lo;
+    uint4* hi;
+    int nst;
+    __device__ __forceinline__ uint32_t phys(uint32_t s) const
+    {
+        return s ^ (((s >> 2) ^ (s >> 3) ^ (s >> nst)) & 7u);
+    }
+    __device__ __forceinline__ Fr get(uint32_t s) const
+    {
+        const uint32_t p = phys(s);
+        const uint4 a = lo[p], b = hi[p];
+        Fr r;
+        r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+        r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+        return r;
+    }
+    __device__ __forceinline__ void put(uint32_t s, const Fr& x) const
+    {
+        const uint32_t p = phys(s);
+        lo[p] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+        hi[p] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+    }
+};
+
 template <bool DIT>
 __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const Fr* __restrict__ tw, int logn,
                                                                int s0, int nst, int lS, int lG)
@@ -315,10 +351,10 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
     const Fr* src = B.src[blockIdx.y];
     Fr* a = B.dst[blockIdx.y];
     extern __shared__ uint4 smem_raw[];
-    Fr* sm = reinterpret_cast<Fr*>(smem_raw);
     const uint32_t Smask = (1u << lS) - 1;
     const uint32_t g0 = blockIdx.x << lG;
     const uint32_t elems = 1u << (lG + nst);
+    const NttTile4 T{smem_raw, smem_raw + elems, nst};
     const bool wide = lS >= lG;
     auto locate = [&](uint32_t idx, uint32_t& slot) -> uint32_t {
         if (wide) {
@@ -335,10 +371,9 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
     for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
         uint32_t slot;
         const uint32_t addr = locate(idx, slot);
-        sm[slot] = ld(&src[addr]);
+        T.put(slot, ld(&src[addr]));
     }
     __syncthreads();
-    char* const smb = reinterpret_cast<char*>(sm);
     const char* const twb = reinterpret_cast<const char*>(tw);
     auto twid = [&](uint32_t lowm, uint32_t r, int sh) -> Fr {
         return ldg(reinterpret_cast<const Fr*>(twb + (((((lowm << lS) + r) << sh)) << 5)));
@@ -354,16 +389,15 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
             const uint32_t m = b & ((1u << (nst - 1)) - 1), gl = b >> (nst - 1);
             const uint32_t r = (g0 + gl) & Smask;
             const uint32_t lowm = m & lo, q = m + (m & ~lo);
-            Fr* px = reinterpret_cast<Fr*>(smb + (((gl << nst) + q) << 5));
-            Fr* py = reinterpret_cast<Fr*>(smb + (((gl << nst) + q + (1u << h)) << 5));
-            const Fr x = *px, y = *py, w = twid(lowm, r, sh);
+            const uint32_t ix = (gl << nst) + q, iy = ix + (1u << h);
+            const Fr x = T.get(ix), y = T.get(iy), w = twid(lowm, r, sh);
             if (DIT) {
                 const Fr yw = y * w;
-                *px = x + yw;
-                *py = x - yw;
+                T.put(ix, x + yw);
+                T.put(iy, x - yw);
             } else {
-                *px = x + y;
-                *py = (x - y) * w;
+                T.put(ix, x + y);
+                T.put(iy, (x - y) * w);
             }
         }
         __syncthreads();
@@ -377,35 +411,31 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
             const uint32_t m4 = qi & ((1u << (nst - 2)) - 1), gl = qi >> (nst - 2);
             const uint32_t r = (g0 + gl) & Smask;
             const uint32_t lowm = m4 & lo, q = lowm + ((m4 >> h) << (h + 2));
-            char* const gb = smb + ((gl << nst) << 5);
-            Fr* p0 = reinterpret_cast<Fr*>(gb + (q << 5));
-            Fr* p1 = reinterpret_cast<Fr*>(gb + ((q + (1u << h)) << 5));
-            Fr* p2 = reinterpret_cast<Fr*>(gb + ((q + (2u << h)) << 5));
-            Fr* p3 = reinterpret_cast<Fr*>(gb + ((q + (3u << h)) << 5));
-            const Fr a0 = *p0, a1 = *p1, a2 = *p2, a3 = *p3;
+            const uint32_t i0 = (gl << nst) + q, i1 = i0 + (1u << h), i2 = i0 + (2u << h), i3 = i0 + (3u << h);
+            const Fr a0 = T.get(i0), a1 = T.get(i1), a2 = T.get(i2), a3 = T.get(i3);
             if (DIT) {
-                // stage t (span 2^h): (p0, p1), (p2, p3) share w_h; stage t + 1 (span 2^(h+1)):
-                // (p0, p2) takes lowm, (p1, p3) takes lowm + 2^h
+                // stage t (span 2^h): (i0, i1), (i2, i3) share w_h; stage t + 1 (span 2^(h+1)):
+                // (i0, i2) takes lowm, (i1, i3) takes lowm + 2^h
                 const int sh0 = logn - (s0 + t) - 1, sh1 = sh0 - 1;
                 const Fr wh = twid(lowm, r, sh0), wa = twid(lowm, r, sh1), wb = twid(lowm + (1u << h), r, sh1);
                 const Fr t1 = a1 * wh, t3 = a3 * wh;
                 const Fr b0 = a0 + t1, b1 = a0 - t1, b2 = a2 + t3, b3 = a2 - t3;
                 const Fr u2 = b2 * wa, u3 = b3 * wb;
-                *p0 = b0 + u2;
-                *p2 = b0 - u2;
-                *p1 = b1 + u3;
-                *p3 = b1 - u3;
+                T.put(i0, b0 + u2);
+                T.put(i2, b0 - u2);
+                T.put(i1, b1 + u3);
+                T.put(i3, b1 - u3);
             } else {
-                // stage t (span 2^(h+1)): (p0, p2) takes lowm, (p1, p3) lowm + 2^h;
-                // stage t + 1 (span 2^h): (p0, p1), (p2, p3) share w_h
+                // stage t (span 2^(h+1)): (i0, i2) takes lowm, (i1, i3) lowm + 2^h;
+                // stage t + 1 (span 2^h): (i0, i1), (i2, i3) share w_h
                 const int sh0 = s0 + t, sh1 = sh0 + 1;
                 const Fr wa = twid(lowm, r, sh0), wb = twid(lowm + (1u << h), r, sh0), wh = twid(lowm, r, sh1);
                 const Fr b0 = a0 + a2, b1 = a1 + a3;
                 const Fr b2 = (a0 - a2) * wa, b3 = (a1 - a3) * wb;
-                *p0 = b0 + b1;
-                *p1 = (b0 - b1) * wh;
-                *p2 = b2 + b3;
-                *p3 = (b2 - b3) * wh;
+                T.put(i0, b0 + b1);
+                T.put(i1, (b0 - b1) * wh);
+                T.put(i2, b2 + b3);
+                T.put(i3, (b2 - b3) * wh);
             }
         }
         __syncthreads();
@@ -417,7 +447,7 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
     for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
         uint32_t slot;
         const uint32_t addr = locate(idx, slot);
-        st(&a[addr], sm[slot]);
+        st(&a[addr], T.get(slot));
     }
 }
 
@@ -434,16 +464,25 @@ static int g_max_pass_stages = 9;  // tuned per k by ntt_set_pass_stages()
 int ntt_pass_stages() { return g_max_pass_stages; }
 int tune_value(int param, int log_n);  // tune.cu
 
-// Stages per pass for a transform of 2^logn points: the per-size tuning
-// table's entry when the autotuner set one, else the global setting.
-static int pass_stages_for(int logn)
-{
-    const int tuned = tune_value(2, logn);
-    return tuned ? tuned : g_max_pass_stages;
-}
 void ntt_set_pass_stages(int b)
 {
-    if (b >= 1 && b <= 10) g_max_pass_stages = b;
+    if (b >= 1 && b <= 11) g_max_pass_stages = b;
+}
+
+// The radix-4 passes take tiles of up to 64 KB of shared memory (opt-in
+// above the 48 KB default), set once per process.
+static bool ntt4_smem_ready()
+{
+    static int state = 0;
+    if (state == 0) {
+        const int bytes = (1 << NTT4_LOG_TILE) * (int)sizeof(Fr);
+        bool ok_ = cudaFuncSetAttribute(k_ntt_pass4<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+                       cudaSuccess &&
+                   cudaFuncSetAttribute(k_ntt_pass4<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+                       cudaSuccess;
+        state = ok_ ? 1 : 2;
+    }
+    return state == 1;
 }
 
 // Runs radix-2 stages [first, logn) of `count` transforms in passes of at
@@ -453,7 +492,12 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
 {
     if (logn - first <= 0) return ok();
     int todo = logn - first;
-    const int max_stages = pass_stages_for(logn);
+    // radix-4 passes: tiles of up to 2^11 elements, 11 stages per pass unless
+    // the tuning table says otherwise; radix-2 passes: at most 10
+    const bool r4 = g_ntt_radix4 && ntt4_smem_ready();
+    const int tile_log = r4 ? NTT4_LOG_TILE : NTT_LOG_TILE;
+    const int tuned = tune_value(2, logn);
+    const int max_stages = std::min(tile_log, tuned ? tuned : (r4 ? NTT4_LOG_TILE : g_max_pass_stages));
     int passes = (todo + max_stages - 1) / max_stages;
     int base = todo / passes, extra = todo % passes;
     int s0 = first;
@@ -461,11 +505,13 @@ static RustError run_passes(NttBatch B, int count, const Fr* tw, int logn, bool 
     for (int p = 0; p < passes; p++) {
         int nst = base + (p < extra ? 1 : 0);
         const int lS = dit ? s0 : logn - s0 - nst;
-        const int lG = std::min(NTT_LOG_TILE - nst, logn - nst);
+        // a one-stage pass runs the radix-2 kernel, whose tile stays at 2^10
+        const bool pass4 = r4 && nst >= 2;
+        const int lG = std::min((pass4 ? tile_log : NTT_LOG_TILE) - nst, logn - nst);
         const dim3 grid((unsigned)(1ull << (logn - nst - lG)), (unsigned)count);
         size_t smem = (size_t)(1ull << (lG + nst)) * sizeof(Fr);
         int threads = (int)std::min<uint64_t>(NTT_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 1)));
-        if (g_ntt_radix4 && nst >= 2) {
+        if (pass4) {
             threads = (int)std::min<uint64_t>(NTT4_THREADS, std::max<uint64_t>(32, 1ull << (lG + nst - 2)));
             if (dit)
                 k_ntt_pass4<true><<<grid, threads, smem, st>>>(B, tw, logn, s0, nst, lS, lG);

@@ -718,3 +718,403 @@ extern "C" RustError _halo2_quotient_permutation(void* values, const void* l0, c
     H2B_LAUNCHED("k_perm_quotient");
     return ok();
 }
+
+// ---------------------------------------------------------------------------
+// Fused extended-part quotient (no counterpart in the reference, whose
+// evaluate_h runs one launcher per constraint family on each extended part:
+// halo2_proofs/src/plonk/evaluation.rs:1107-1417 calls
+// `_halo2_quotient_device_columns_device_out` for the gates,
+// `_halo2_quotient_permutation`, and per lookup the product expression
+// through `_halo2_quotient_device_columns_device_out` into `table_values`
+// followed by `_halo2_quotient_lookups`).  One kernel does all of it per row:
+//   value = Horner(0, y, gate value parts)
+//   value = permutation constraints folded in (as _halo2_quotient_permutation)
+//   per lookup: tv = Horner(0, y, its product expression's value parts),
+//               value = its five constraints folded in (as _halo2_quotient_lookups)
+//   out[(row - row_start) * out_stride + out_offset] = value (* scale)
+// so the accumulator is written once, table_values never exist, and with
+// out_stride = number of parts, out_offset = the part and scale = the part's
+// 1 / (X^n - 1) value the parts land interleaved in the extended array,
+// already divided by the vanishing polynomial
+// (`_halo2_extended_from_lagrange_vec_device` + `_halo2_divide_by_vanishing_poly`).
+// The whole program -- ops, constants, challenges, column pointers, scalars --
+// is one __grid_constant__ kernel parameter block: no device program memory,
+// no host synchronisation, capturable in a graph, and every op is a
+// warp-uniform constant-bank read.
+// ---------------------------------------------------------------------------
+
+namespace h2b {
+
+constexpr int FQ_MAX_OPS = 256, FQ_MAX_VPS = 64, FQ_MAX_CONSTS = 192, FQ_MAX_CHAL = 16, FQ_MAX_COLS = 64,
+              FQ_MAX_SETS = 8, FQ_MAX_PCOLS = 32, FQ_MAX_LOOKUPS = 8;
+constexpr unsigned FQ_THREADS = 128;
+
+struct FqLookup {
+    const Fr* z;
+    const Fr* pin;
+    const Fr* ptab;
+    Fr beta, gamma;
+    uint32_t op0, op1, vp0, vp1;
+};
+
+struct FusedParams {
+    QOp ops[FQ_MAX_OPS];
+    QVp vps[FQ_MAX_VPS];
+    Fr consts[FQ_MAX_CONSTS];
+    Fr chal[FQ_MAX_CHAL];
+    const Fr* cols[FQ_MAX_COLS];
+    const Fr* prods[FQ_MAX_SETS];
+    const Fr* sigmas[FQ_MAX_PCOLS];
+    const Fr* pcols[FQ_MAX_PCOLS];
+    FqLookup lk[FQ_MAX_LOOKUPS];
+    const Fr* l0;
+    const Fr* l_last;
+    const Fr* l_active;
+    Fr* out;
+    Fr y, beta, gamma, delta, delta_start, ext_omega, omega, scale;
+    uint64_t nq, isize, off_next, off_last, out_stride, out_offset;
+    uint32_t gate_ops, gate_vps, n_sets, chunk_len, n_pcols, n_lookups, has_scale, pad;
+};
+
+__device__ __forceinline__ Fr fq_fetch(const FusedParams& P, const Fr* slot, uint8_t src, uint32_t idx, uint64_t rot,
+                                       uint64_t row)
+{
+    switch (src) {
+    case SRC_FIXED:
+    case SRC_INSTANCE:
+    case SRC_ADVICE: {
+        uint64_t at = row + rot;
+        if (at >= P.nq) at -= P.nq;
+        return ldg(&P.cols[idx][at]);
+    }
+    case SRC_SLOT: return slot[idx];
+    case SRC_CONST: return P.consts[idx];
+    case SRC_CHALLENGE: return P.chal[idx];
+    default: return Fr::zero();
+    }
+}
+
+// ops [i0, i1) of the program on one row, then Horner(0, y, value parts [v0, v1))
+__device__ __forceinline__ Fr fq_run(const FusedParams& P, Fr* slot, uint32_t i0, uint32_t i1, uint32_t v0,
+                                     uint32_t v1, uint64_t row)
+{
+#pragma unroll 1
+    for (uint32_t i = i0; i < i1; i++) {
+        const QOp& op = P.ops[i];
+        const uint8_t kind = op.kind;
+        Fr res;
+        switch (kind) {
+        case OP_COPY: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row); break;
+        case OP_ADD: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) + fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
+        case OP_SUB: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) - fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
+        case OP_MUL: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) * fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
+        case OP_NEG: res = fneg(fq_fetch(P, slot, op.sa, op.ia, op.ra, row)); break;
+        case OP_DBL: res = fdbl(fq_fetch(P, slot, op.sa, op.ia, op.ra, row)); break;
+        default: res = Fr::zero();
+        }
+        slot[op.dst] = res;
+    }
+    Fr val = Fr::zero();
+#pragma unroll 1
+    for (uint32_t i = v0; i < v1; i++) {
+        const QVp v = P.vps[i];
+        val = val * P.y + (v.is_const ? P.consts[v.idx] : slot[v.idx]);
+    }
+    return val;
+}
+
+template <int MAXS, int MINB>
+__global__ void __launch_bounds__(FQ_THREADS, MINB) k_quotient_fused(const __grid_constant__ FusedParams P,
+                                                                     uint64_t row_start, uint64_t rows)
+{
+    Fr slot[MAXS];
+    const Fr one = Fr::one();
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    // omega^step, the factor between a thread's consecutive rows, once per block
+    __shared__ Fr s_wstep;
+    if (P.n_sets && threadIdx.x == 0) s_wstep = fpow_u64(P.omega, step);
+    __syncthreads();
+    const Fr wstep = P.n_sets ? s_wstep : one;
+    uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    // X-dependent factor of the identity permutation on this thread's first
+    // row, ext_omega * omega^row
+    Fr bt = P.n_sets ? P.ext_omega * fpow_u64(P.omega, row_start + r) : one;
+    for (; r < rows; r += step) {
+        const uint64_t row = row_start + r;
+        Fr v = fq_run(P, slot, 0, P.gate_ops, 0, P.gate_vps, row);
+        if (P.n_sets) {
+            uint64_t rn = row + P.off_next, rl = row + P.off_last;
+            if (rn >= P.isize) rn -= P.isize;
+            if (rl >= P.isize) rl -= P.isize;
+            const Fr l0v = ld(&P.l0[row]);
+            const Fr z0 = ld(&P.prods[0][row]);
+            v = v * P.y + (one - z0) * l0v;
+            const Fr zl = P.n_sets == 1 ? z0 : ld(&P.prods[P.n_sets - 1][row]);
+            v = v * P.y + (zl * zl - zl) * ld(&P.l_last[row]);
+            for (uint32_t s = 1; s < P.n_sets; s++)
+                v = v * P.y + (ld(&P.prods[s][row]) - ld(&P.prods[s - 1][rl])) * l0v;
+            const Fr la = ld(&P.l_active[row]);
+            Fr cur = P.delta_start * bt;
+            for (uint32_t s = 0; s < P.n_sets; s++) {
+                const uint32_t c0 = s * P.chunk_len;
+                const uint32_t c1 = c0 + P.chunk_len < P.n_pcols ? c0 + P.chunk_len : P.n_pcols;
+                Fr left = ld(&P.prods[s][rn]);
+                Fr right = ld(&P.prods[s][row]);
+                for (uint32_t c = c0; c < c1; c++) {
+                    const Fr cv = ld(&P.pcols[c][row]);
+                    left = left * (cv + P.beta * ld(&P.sigmas[c][row]) + P.gamma);
+                    right = right * (cv + cur + P.gamma);
+                    cur = cur * P.delta;
+                }
+                v = v * P.y + (left - right) * la;
+            }
+            bt = bt * wstep;
+        }
+        if (P.n_lookups) {
+            const uint64_t nx = row + 1 == P.nq ? 0 : row + 1;
+            const uint64_t pv = row == 0 ? P.nq - 1 : row - 1;
+            const Fr l0v = ld(&P.l0[row]), llast = ld(&P.l_last[row]), la = ld(&P.l_active[row]);
+            for (uint32_t l = 0; l < P.n_lookups; l++) {
+                const FqLookup& L = P.lk[l];
+                const Fr tv = fq_run(P, slot, L.op0, L.op1, L.vp0, L.vp1, row);
+                const Fr zi = ld(&L.z[row]), a = ld(&L.pin[row]), s = ld(&L.ptab[row]);
+                const Fr ams = a - s;
+                v = v * P.y + (one - zi) * l0v;
+                v = v * P.y + (zi * zi - zi) * llast;
+                v = v * P.y + (ld(&L.z[nx]) * (a + L.beta) * (s + L.gamma) - zi * tv) * la;
+                v = v * P.y + ams * l0v;
+                v = v * P.y + ams * (a - ld(&L.pin[pv])) * la;
+            }
+        }
+        if (P.has_scale) v = v * P.scale;
+        st(&P.out[r * P.out_stride + P.out_offset], v);
+    }
+}
+
+} // namespace h2b
+
+extern "C" {
+typedef struct h2b_quotient_rules {
+    const uint64_t* rules;
+    uint64_t num_rules;
+    const uint64_t* value_part_rules;
+    uint64_t num_vp;
+    const void* constants;
+    uint64_t num_constants;
+    const void* challenges;
+    uint64_t num_challenges;
+} h2b_quotient_rules;
+
+typedef struct h2b_quotient_permutation_args {
+    uint64_t n_sets, chunk_len, n_columns;
+    const void* const* product_cosets;
+    const void* const* sigma_cosets;
+    const void* const* column_values;
+    const void* beta;
+    const void* gamma;
+    const void* delta;
+    const void* delta_start;
+    const void* current_extended_omega;
+    const void* omega;
+    int32_t last_rotation, rot_scale, isize, reserved;
+} h2b_quotient_permutation_args;
+
+typedef struct h2b_quotient_lookup_args {
+    h2b_quotient_rules product;
+    const void* product_coset;
+    const void* permuted_input_coset;
+    const void* permuted_table_coset;
+    const void* beta;
+    const void* gamma;
+} h2b_quotient_lookup_args;
+}
+
+namespace {
+
+// Appends one compiled rule list to the parameter block: constants and
+// challenges get their own ranges, ops and value parts are relocated to them.
+RustError fq_append(FusedParams& P, uint32_t& n_ops, uint32_t& n_vps, uint32_t& n_consts, uint32_t& n_chal,
+                    const h2b_quotient_rules& R, uint64_t num_fixed, uint64_t num_instance, uint64_t num_advice,
+                    uint64_t nq, uint64_t rot_scale, uint32_t& slots, uint32_t& op0, uint32_t& op1, uint32_t& vp0,
+                    uint32_t& vp1)
+{
+    if (R.num_rules && !R.rules) return err(cudaErrorInvalidValue, "h2b_quotient_fused: rules pointer is null");
+    if (R.num_vp && !R.value_part_rules)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: value part rules pointer is null");
+    QProgram Q = compile_rules(R.rules, R.num_rules, R.value_part_rules, R.num_vp, num_fixed, num_instance,
+                               num_advice, R.num_constants, R.num_challenges, nq, rot_scale);
+    if (!Q.error.empty()) return err(cudaErrorInvalidValue, Q.error.c_str());
+    if (n_ops + Q.ops.size() > (size_t)FQ_MAX_OPS || n_vps + Q.vps.size() > (size_t)FQ_MAX_VPS ||
+        n_consts + R.num_constants > (uint64_t)FQ_MAX_CONSTS || n_chal + R.num_challenges > (uint64_t)FQ_MAX_CHAL)
+        return err(cudaErrorInvalidValue,
+                   "h2b_quotient_fused: program larger than the fused kernel's parameter block "
+                   "(256 ops, 64 value parts, 192 constants, 16 challenges)");
+    if (R.num_constants && !R.constants) return err(cudaErrorInvalidValue, "h2b_quotient_fused: constants pointer is null");
+    if (R.num_challenges && !R.challenges)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: challenges pointer is null");
+    memcpy(&P.consts[n_consts], R.constants, R.num_constants * 32);
+    memcpy(&P.chal[n_chal], R.challenges, R.num_challenges * 32);
+    op0 = n_ops;
+    for (QOp op : Q.ops) {
+        if (op.sa == SRC_CONST) op.ia += n_consts;
+        if (op.sb == SRC_CONST) op.ib += n_consts;
+        if (op.sa == SRC_CHALLENGE) op.ia += n_chal;
+        if (op.sb == SRC_CHALLENGE) op.ib += n_chal;
+        P.ops[n_ops++] = op;
+    }
+    op1 = n_ops;
+    vp0 = n_vps;
+    for (QVp v : Q.vps) {
+        if (v.is_const) v.idx += n_consts;
+        P.vps[n_vps++] = v;
+    }
+    vp1 = n_vps;
+    n_consts += (uint32_t)R.num_constants;
+    n_chal += (uint32_t)R.num_challenges;
+    slots = std::max(slots, Q.slots);
+    return ok();
+}
+
+Fr fr_from(const void* p)
+{
+    Fr r;
+    memcpy(&r, p, 32);
+    return r;
+}
+
+} // namespace
+
+// Register budget of the fused kernel, in blocks of 128 threads per SM: 3
+// (162 registers, no spills; the default), 4 (128 registers, a few spills)
+// or 5 (96 registers, more spills).  2^20 rows of a config-3 part: 1.416,
+// 1.500 and 1.489 ms (1.54 ms uncapped at 198 registers; the reference's
+// four per-part launches 1.50 ms).  Same results.
+static int g_fq_blocks = 3;
+extern "C" void h2b_quotient_fused_set_blocks(int blocks_per_sm)
+{
+    if (blocks_per_sm >= 3 && blocks_per_sm <= 5) g_fq_blocks = blocks_per_sm;
+}
+extern "C" int h2b_quotient_fused_get_blocks(void) { return g_fq_blocks; }
+
+extern "C" RustError h2b_quotient_fused(const void* const* fixed, uint64_t num_fixed, const void* const* instance,
+                                        uint64_t num_instance, const void* const* advice, uint64_t num_advice,
+                                        const h2b_quotient_rules* gates, const void* y, const void* l0,
+                                        const void* l_last, const void* l_active_row,
+                                        const h2b_quotient_permutation_args* perm,
+                                        const h2b_quotient_lookup_args* lookups, uint64_t num_lookups,
+                                        uint64_t num_quotient, uint64_t rotation_scale, uint64_t row_start,
+                                        uint64_t row_end, void* out, uint64_t out_stride, uint64_t out_offset,
+                                        const void* scale, cudaStream_t stream)
+{
+    if (num_quotient == 0) return err(cudaErrorInvalidValue, "h2b_quotient_fused: num_quotient is 0");
+    if (row_end < row_start || row_end > num_quotient)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: row range outside [0, num_quotient]");
+    const uint64_t rows = row_end - row_start;
+    if (rows == 0) return ok();
+    if (!gates || !y || !out || out_stride == 0)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: gates, y and out are required, out_stride >= 1");
+    const uint64_t ncols = num_fixed + num_instance + num_advice;
+    if (ncols > (uint64_t)FQ_MAX_COLS) return err(cudaErrorInvalidValue, "h2b_quotient_fused: more than 64 columns");
+    if (num_lookups > (uint64_t)FQ_MAX_LOOKUPS)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: more than 8 lookups");
+    if (num_lookups && !lookups) return err(cudaErrorInvalidValue, "h2b_quotient_fused: lookups pointer is null");
+    const bool has_perm = perm && perm->n_sets;
+    if ((has_perm || num_lookups) && (!l0 || !l_last || !l_active_row))
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: l0, l_last and l_active are required");
+
+    static thread_local FusedParams P;   // about 18 KB: kept off the stack
+    memset(&P, 0, sizeof(P));
+    uint64_t c = 0;
+    for (uint64_t i = 0; i < num_fixed; i++) P.cols[c++] = (const Fr*)fixed[i];
+    for (uint64_t i = 0; i < num_instance; i++) P.cols[c++] = (const Fr*)instance[i];
+    for (uint64_t i = 0; i < num_advice; i++) P.cols[c++] = (const Fr*)advice[i];
+    for (uint64_t i = 0; i < ncols; i++)
+        if (!P.cols[i]) return err(cudaErrorInvalidValue, "h2b_quotient_fused: null column pointer");
+
+    uint32_t n_ops = 0, n_vps = 0, n_consts = 0, n_chal = 0, slots = 1, op0, op1, vp0, vp1;
+    H2B_TRY(fq_append(P, n_ops, n_vps, n_consts, n_chal, *gates, num_fixed, num_instance, num_advice, num_quotient,
+                      rotation_scale, slots, op0, op1, vp0, vp1));
+    P.gate_ops = op1;
+    P.gate_vps = vp1;
+    for (uint64_t l = 0; l < num_lookups; l++) {
+        const h2b_quotient_lookup_args& A = lookups[l];
+        if (!A.product_coset || !A.permuted_input_coset || !A.permuted_table_coset || !A.beta || !A.gamma)
+            return err(cudaErrorInvalidValue, "h2b_quotient_fused: incomplete lookup arguments");
+        FqLookup& L = P.lk[l];
+        H2B_TRY(fq_append(P, n_ops, n_vps, n_consts, n_chal, A.product, num_fixed, num_instance, num_advice,
+                          num_quotient, rotation_scale, slots, L.op0, L.op1, L.vp0, L.vp1));
+        L.z = (const Fr*)A.product_coset;
+        L.pin = (const Fr*)A.permuted_input_coset;
+        L.ptab = (const Fr*)A.permuted_table_coset;
+        L.beta = fr_from(A.beta);
+        L.gamma = fr_from(A.gamma);
+    }
+    P.n_lookups = (uint32_t)num_lookups;
+    if (slots > 64)
+        return err(cudaErrorInvalidValue, "h2b_quotient_fused: more than 64 live intermediates");
+
+    if (has_perm) {
+        const h2b_quotient_permutation_args& A = *perm;
+        if (A.n_sets > (uint64_t)FQ_MAX_SETS || A.n_columns > (uint64_t)FQ_MAX_PCOLS || A.chunk_len == 0 ||
+            A.n_columns > A.n_sets * A.chunk_len)
+            return err(cudaErrorInvalidValue,
+                       "h2b_quotient_fused: permutation shape (at most 8 sets, 32 columns, columns <= sets * chunk_len)");
+        if (A.isize <= 0 || row_end > (uint64_t)A.isize)
+            return err(cudaErrorInvalidValue, "h2b_quotient_fused: permutation isize must cover the rows");
+        if (!A.product_cosets || (A.n_columns && (!A.sigma_cosets || !A.column_values)) || !A.beta || !A.gamma ||
+            !A.delta || !A.delta_start || !A.current_extended_omega || !A.omega)
+            return err(cudaErrorInvalidValue, "h2b_quotient_fused: incomplete permutation arguments");
+        for (uint64_t s = 0; s < A.n_sets; s++) {
+            P.prods[s] = (const Fr*)A.product_cosets[s];
+            if (!P.prods[s]) return err(cudaErrorInvalidValue, "h2b_quotient_fused: null product coset");
+        }
+        for (uint64_t i = 0; i < A.n_columns; i++) {
+            P.sigmas[i] = (const Fr*)A.sigma_cosets[i];
+            P.pcols[i] = (const Fr*)A.column_values[i];
+            if (!P.sigmas[i] || !P.pcols[i]) return err(cudaErrorInvalidValue, "h2b_quotient_fused: null permutation column");
+        }
+        P.n_sets = (uint32_t)A.n_sets;
+        P.chunk_len = (uint32_t)A.chunk_len;
+        P.n_pcols = (uint32_t)A.n_columns;
+        P.isize = (uint64_t)A.isize;
+        auto wrap = [&](int64_t rot) -> uint64_t {
+            int64_t o = (rot * (int64_t)A.rot_scale) % (int64_t)A.isize;
+            return (uint64_t)(o < 0 ? o + A.isize : o);
+        };
+        P.off_next = wrap(1);
+        P.off_last = wrap(A.last_rotation);
+        P.beta = fr_from(A.beta);
+        P.gamma = fr_from(A.gamma);
+        P.delta = fr_from(A.delta);
+        P.delta_start = fr_from(A.delta_start);
+        P.ext_omega = fr_from(A.current_extended_omega);
+        P.omega = fr_from(A.omega);
+    }
+    P.l0 = (const Fr*)l0;
+    P.l_last = (const Fr*)l_last;
+    P.l_active = (const Fr*)l_active_row;
+    P.out = (Fr*)out;
+    P.y = fr_from(y);
+    P.nq = num_quotient;
+    P.out_stride = out_stride;
+    P.out_offset = out_offset;
+    if (scale) {
+        P.has_scale = 1;
+        P.scale = fr_from(scale);
+    }
+    const unsigned grid = grid_for(rows, FQ_THREADS, 148u * 8u);
+    prof_begin(PROF_QUOTIENT, stream);
+#define H2B_FQ_LAUNCH(B)                                                                      \
+    do {                                                                                      \
+        if (slots <= 16) k_quotient_fused<16, B><<<grid, FQ_THREADS, 0, stream>>>(P, row_start, rows); \
+        else k_quotient_fused<64, B><<<grid, FQ_THREADS, 0, stream>>>(P, row_start, rows);   \
+    } while (0)
+    if (g_fq_blocks == 3) H2B_FQ_LAUNCH(3);
+    else if (g_fq_blocks == 5) H2B_FQ_LAUNCH(5);
+    else H2B_FQ_LAUNCH(4);
+#undef H2B_FQ_LAUNCH
+    prof_end(PROF_QUOTIENT, stream);
+    H2B_LAUNCHED("k_quotient_fused");
+    return ok();
+}

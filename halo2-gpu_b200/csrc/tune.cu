@@ -26,7 +26,7 @@ static bool tune_valid(uint32_t param, int32_t v)
     switch (param) {
     case 0: return v >= 10 && v <= 16;   // windows the default plans also use (sizes 2^10 .. 2^27)
     case 1: return v >= 8 && v <= 512;   // sorted entries per accumulation thread
-    case 2: return v >= 1 && v <= 10;    // radix-2 stages per shared-memory pass
+    case 2: return v >= 1 && v <= 11;    // radix-2 stages per shared-memory pass (11: radix-4 passes only)
     default: return false;
     }
 }

@@ -73,8 +73,8 @@ def _t():
 def _bytes_per_proof(k):
     """Device memory one in-flight proof of size 2^k holds besides its MSM
     scratch (upper bound): 10 Lagrange and 10 coefficient polynomials, 10
-    coset parts, 4 quotient parts, the lookup product coset, 8
-    extended-domain vectors, the opening's buffers and small tensors."""
+    coset parts, the extended-domain vectors, the unfused quotient's 4 parts
+    and lookup product coset, the opening's buffers and small tensors."""
     n = 1 << k
     return 64 * 32 * n + (64 << 20)
 
@@ -222,7 +222,7 @@ def _generator_image():
 class ProofWorkload:
     """One proof of the 2^k circuit (see the module docstring)."""
 
-    def __init__(self, res, k, seed, transcript=False, tamper=None, check_degree=False):
+    def __init__(self, res, k, seed, transcript=False, tamper=None, check_degree=False, fused_quotient=True):
         """transcript=False draws the challenges from a generator seeded with
         `seed`; transcript=True runs the Fiat-Shamir transcript
         (transcript.Blake2bWrite): every commitment is read back and absorbed
@@ -232,8 +232,15 @@ class ProofWorkload:
         break one cell).  check_degree=True reads back whether the top n of
         h's 4n coefficients are zero (`self.h_degree_ok`): they are exactly
         when every constraint holds on the whole domain, the quotient
-        identity h = sum_i y^i C_i / (X^n - 1) with deg h < 3n."""
+        identity h = sum_i y^i C_i / (X^n - 1) with deg h < 3n.
+        fused_quotient=True evaluates each extended part with one
+        h2b_quotient_fused launch that writes the part interleaved into the
+        extended array, already divided by X^n - 1; False runs the
+        reference's per-part launcher sequence (gates, permutation, lookup
+        expression, lookup constraints) and then gathers and divides.  The
+        proofs are the same bytes."""
         self.res, self.k, self.seed, self.transcript, self.tamper = res, k, seed, transcript, tamper
+        self.fused_quotient = fused_quotient
         self.check_degree = check_degree
         self.h_degree_ok = None
         self.proof = None
@@ -373,20 +380,37 @@ class ProofWorkload:
             d_y = h2b.to_dev(sc(y), stream)
             kcos = res.key_cosets(k, stream)
             own = [h2b.dev_empty(32 * n) for _ in coef]
-            tv = h2b.dev_empty(32 * n)
-            hs = [h2b.dev_empty(32 * n) for _ in range(1 << (dom.extended_k - k))]
+            n_parts = 1 << (dom.extended_k - k)
+            en = n_parts * n
+            ext = h2b.dev_empty(32 * en)
+            fused = self.fused_quotient
+            tv = None if fused else h2b.dev_empty(32 * n)
+            hs = [] if fused else [h2b.dev_empty(32 * n) for _ in range(n_parts)]
             nws = h2b.dev_empty(h2b.lib()._halo2_fft_many_to_device_workspace_size(6, k, k))
             g_rules, g_parts, g_consts = pk.gates
             l_rules, l_parts, l_consts = pk.lookup_graph
             bg = np.concatenate([sc(beta), sc(gamma)])
-            for j, hj in enumerate(hs):
+            no_chal = np.zeros((0, 4), np.uint64)
+            for j in range(n_parts):
                 shift = pow(dom.extended_omega, j, p)
                 h2b.fft_many_to_device(6, k, k, coef, own, dom.omega, F.ZETA * shift % p, ws=nws, stream=stream)
                 fx, sg, (l0, llast, lact) = kcos[j][0:3], kcos[j][3:7], kcos[j][7:10]
                 a_p, i_p, z_p, zl_p, pa_p, ps_p = own[0:4], own[4], own[5:7], own[7], own[8], own[9]
+                perm_cols = [a_p[0], a_p[1], a_p[2], i_p]
+                if fused:
+                    perm = dict(prods=z_p, sigmas=sg, cols=perm_cols, beta=beta, gamma=gamma, delta=F.DELTA,
+                                delta_start=beta * F.ZETA % p, ext_omega=shift, omega=dom.omega,
+                                chunk_len=C.CHUNK_LEN, last_rotation=-(C.BLINDING_FACTORS + 1), rot_scale=1, isize=n)
+                    look = dict(rules=(bg, l_consts, l_rules, l_parts), z=zl_p, pin=pa_p, ptab=ps_p, beta=beta,
+                                gamma=gamma)
+                    h2b.quotient_fused_device(fx, [i_p], a_p, (no_chal, g_consts, g_rules, g_parts), y, l0, llast,
+                                              lact, perm, [look], n, 1, 0, n, ext, n_parts, j,
+                                              dom.t_evaluations[j], stream=stream)
+                    continue
+                hj = hs[j]
                 h2b.quotient_device(fx, [i_p], a_p, [], g_consts, y, g_rules, g_parts, n, 1, 0, n, hj,
                                     stream=stream)
-                h2b.quotient_permutation_device(hj, l0, llast, lact, z_p, sg, [a_p[0], a_p[1], a_p[2], i_p], beta,
+                h2b.quotient_permutation_device(hj, l0, llast, lact, z_p, sg, perm_cols, beta,
                                                 gamma, sc(y), sc(F.DELTA), sc(beta * F.ZETA), sc(shift),
                                                 sc(dom.omega), C.CHUNK_LEN, -(C.BLINDING_FACTORS + 1), 1, n, n,
                                                 stream=stream)
@@ -395,12 +419,12 @@ class ProofWorkload:
                 h2b.quotient_lookups_device(hj, tv, zl_p, pa_p, ps_p, l0, llast, lact, d_beta, d_gamma, d_y, n,
                                             stream=stream)
             del own, tv
-            en = len(hs) * n
-            ext, hc = h2b.dev_empty(32 * en), h2b.dev_empty(32 * en)
-            tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64), stream)
-            h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), len(hs), n, sh)
-            h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk.t_evals),
-                     len(dom.t_evaluations), en, sh)
+            if not fused:
+                tab = h2b.to_dev(np.array([t.data_ptr() for t in hs], dtype=np.uint64), stream)
+                h2b.call("_halo2_extended_from_lagrange_vec_device", h2b.ptr(ext), h2b.ptr(tab), n_parts, n, sh)
+                h2b.call("_halo2_divide_by_vanishing_poly", h2b.ptr(ext), h2b.ptr(pk.t_evals),
+                         len(dom.t_evaluations), en, sh)
+            hc = h2b.dev_empty(32 * en)
             h2b.fft_many_to_device(2, dom.extended_k, dom.extended_k, [ext], [hc], dom.extended_omega_inv,
                                    dom.extended_ifft_divisor, stream=stream)
             del ext, hs

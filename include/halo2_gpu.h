@@ -361,6 +361,72 @@ RustError h2b_quotient_program_build(const uint64_t* rules, uint64_t num_rules, 
                                      uint64_t program_bytes, h2b_quotient_program* info, h2b_stream_t stream);
 RustError h2b_quotient_program_run(const h2b_quotient_program* info, const void* d_program, void* d_out,
                                    const void* d_prev, uint64_t row_start, uint64_t row_end, h2b_stream_t stream);
+
+/* Fused extended-part quotient (no counterpart in the reference: it replaces the
+ * per-part sequence of evaluation.rs:1107-1417 -- _halo2_quotient_device_columns_device_out
+ * for the gates, _halo2_quotient_permutation, and per lookup the product expression
+ * through _halo2_quotient_device_columns_device_out into table_values followed by
+ * _halo2_quotient_lookups -- with one kernel that evaluates all of it per row and
+ * writes the accumulator once):
+ *   out[(r - row_start) * out_stride + out_offset] = value(r) * scale   (scale optional)
+ * value(r) equals the composition of those launchers with prev = 0: the gate value
+ * parts in Horner order in y, then the permutation constraints (same arguments and
+ * rotation rules as _halo2_quotient_permutation over the rows of this call), then for
+ * each lookup its five constraints with table_values(r) = Horner(0, y, the product
+ * expression's value parts) and rows r +- 1 taken mod num_quotient. With out_stride =
+ * the number of extended parts, out_offset = the part and scale = 1 / t_evaluations[part]
+ * the result is the part's slice of _halo2_extended_from_lagrange_vec_device followed by
+ * _halo2_divide_by_vanishing_poly.
+ * Columns, sigma, product and lookup cosets and l0 / l_last / l_active are device
+ * pointers given in HOST arrays; y, beta, gamma, delta, delta_start, the coset shift,
+ * omega, scale, constants and challenges are HOST 32-byte Montgomery values (the whole
+ * program travels as the kernel's parameters: no device memory, no synchronisation,
+ * capturable in a CUDA graph). Limits: 64 columns, 256 compiled ops, 64 value parts,
+ * 192 constants, 16 challenges, 64 live intermediates, 8 permutation sets of at most
+ * 32 columns, 8 lookups; beyond them it returns cudaErrorInvalidValue and the separate
+ * entry points apply. */
+typedef struct h2b_quotient_rules {
+    const uint64_t* rules;            /* 2 words per rule, the reference encoding */
+    uint64_t num_rules;
+    const uint64_t* value_part_rules;
+    uint64_t num_vp;
+    const void* constants;            /* host, 32 bytes each */
+    uint64_t num_constants;
+    const void* challenges;           /* host, 32 bytes each */
+    uint64_t num_challenges;
+} h2b_quotient_rules;
+typedef struct h2b_quotient_permutation_args {
+    uint64_t n_sets, chunk_len, n_columns;
+    const void* const* product_cosets;   /* n_sets device pointers */
+    const void* const* sigma_cosets;     /* n_columns device pointers */
+    const void* const* column_values;    /* n_columns device pointers, permutation column order */
+    const void* beta;
+    const void* gamma;
+    const void* delta;
+    const void* delta_start;
+    const void* current_extended_omega;
+    const void* omega;
+    int32_t last_rotation, rot_scale, isize, reserved;
+} h2b_quotient_permutation_args;
+typedef struct h2b_quotient_lookup_args {
+    h2b_quotient_rules product;          /* the (input + beta)(table + gamma) expression */
+    const void* product_coset;
+    const void* permuted_input_coset;
+    const void* permuted_table_coset;
+    const void* beta;
+    const void* gamma;
+} h2b_quotient_lookup_args;
+RustError h2b_quotient_fused(const void* const* fixed, uint64_t num_fixed, const void* const* instance,
+                             uint64_t num_instance, const void* const* advice, uint64_t num_advice,
+                             const h2b_quotient_rules* gates, const void* y, const void* l0, const void* l_last,
+                             const void* l_active_row, const h2b_quotient_permutation_args* perm /* nullable */,
+                             const h2b_quotient_lookup_args* lookups, uint64_t num_lookups, uint64_t num_quotient,
+                             uint64_t rotation_scale, uint64_t row_start, uint64_t row_end, void* out,
+                             uint64_t out_stride, uint64_t out_offset, const void* scale /* nullable */,
+                             h2b_stream_t stream);
+/* register budget of the fused kernel: 3 (default), 4 or 5 blocks of 128 threads per SM; same results */
+void h2b_quotient_fused_set_blocks(int blocks_per_sm);
+int h2b_quotient_fused_get_blocks(void);
 /* culib.rs:603-617 ; quotient_lookups.cu:16-53 -- all device pointers */
 RustError _halo2_quotient_lookups(void* values, const void* table_values, const void* product_coset,
                                   const void* permuted_input_coset, const void* permuted_table_coset, const void* l0,
@@ -443,7 +509,7 @@ RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t stream
 uint64_t h2b_batch_invert_workspace_size(uint64_t length);
 RustError h2b_batch_invert(void* d_data, uint32_t field_type, uint64_t length, void* scratch, uint64_t scratch_bytes,
                            h2b_stream_t stream);
-/* Radix-2 stages per shared-memory NTT pass (1..10). */
+/* Radix-2 stages per shared-memory NTT pass (1..11; radix-2 pass kernels take at most 10, radix-4 ones 11). */
 void h2b_ntt_set_pass_stages(int stages);
 int h2b_ntt_get_pass_stages(void);
 /* NTT passes as radix-4 steps (1: a thread runs two stages on four elements in registers) or radix-2
@@ -454,7 +520,7 @@ int h2b_ntt_get_radix4(void);
  * and NTT stage split are fixed formulas: halo2_proofs/cuda/src/multiexp.cu:260-300,
  * halo2_proofs/cuda/include/kernel/ntt_combine.h:90-94).  param 0 = MSM window bits (10..16; plain-base
  * MSMs only), 1 = MSM sorted entries per accumulation chunk (8..512; plain-base MSMs that run alone), 2 = NTT radix-2
- * stages per shared-memory pass (1..10), each for inputs of 2^log_n (floor of log2 for an MSM).  value 0 =
+ * stages per shared-memory pass (1..11; at most 10 with the radix-2 pass kernel), each for inputs of 2^log_n (floor of log2 for an MSM).  value 0 =
  * automatic.  Results never change, only times; MSM workspace sizes depend on entries 0 and 1, so set them
  * before sizing scratch.  h2b_tune_set returns 0, or -1 for an unknown param, log_n > 32 or a value out of
  * range (the table is then unchanged). */

@@ -68,7 +68,7 @@ def test_apply_entries_sets_and_rejects(at):
 def test_table_validates_values(clean_table):
     L = clean_table
     assert L.h2b_tune_set(0, 22, 15) == 0 and L.h2b_tune_get(0, 22) == 15
-    for param, bad in ((0, 9), (0, 17), (1, 7), (1, 513), (2, 11), (3, 1)):
+    for param, bad in ((0, 9), (0, 17), (1, 7), (1, 513), (2, 12), (3, 1)):
         assert L.h2b_tune_set(param, 20, bad) == -1
     assert L.h2b_tune_set(0, 33, 12) == -1
     assert L.h2b_tune_get(0, 22) == 15 and L.h2b_tune_get(0, 20) == 0
@@ -122,7 +122,7 @@ def test_every_ntt_setting_is_bit_exact(h2b, orc, cuda, clean_table):
         c = d.g_coset * d.extended_omega % f.R_MOD
         cases = [(1, d.omega, 1), (2, d.omega_inv, d.ifft_divisor), (6, d.omega, c)]
         wants = [orc.ntt(t, k, k, a, f.fr_mont_limbs([om]), f.fr_mont_limbs([dv])) for t, om, dv in cases]
-        for st in range(1, 11):
+        for st in range(1, 12):
             assert L.h2b_tune_set(2, k, st) == 0
             for (t, om, dv), want in zip(cases, wants):
                 assert_limbs_equal(h2b.fft_normal(t, k, a, om, dv), want, f"k={k} type {t} stages {st}")
