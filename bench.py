@@ -554,7 +554,9 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
     slot) and served (`slots` worker streams under an HBM budget that counts
     the resident state).  Reports proofs/s over the makespan, p50/p99 latency
     (arrival to completion, host clock) and the device-memory high-water mark
-    of the run."""
+    of the run.  `concurrency_by_k` times a burst of same-k requests plain and
+    served; with each k's share of the plain prover's time it gives the
+    served/plain gain the mixed trace can reach at saturation."""
     P = importlib.import_module(h2b.__name__ + ".prover")
     V = importlib.import_module(h2b.__name__ + ".verify")
     res = P.Resident(h2b, kmax)
@@ -572,13 +574,27 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
         verified[str(k)] = bool(V.verify_proof(res.verifying_key(k), public, proof, res.tau))
     served.serve([(0.0, k, 9 + k) for k in ks for _ in range(slots)])   # untimed: every worker's pools warm
     mean_s = sum(w * service[k][0] for k, w in zip(ks, weights))
+    # what concurrency buys per k: a burst of same-k requests one at a time
+    # against the worker streams; with each k's share of the plain prover's
+    # time this bounds the served/plain gain of the mixed trace
+    conc = {}
+    for k in ks:
+        burst = [(0.0, k, 300 + 10 * k + i) for i in range(8 if k < 22 else 4)]
+        t_plain = plain.serve(burst)["makespan_s"]
+        t_served = served.serve(burst)["makespan_s"]
+        conc[str(k)] = {"requests": len(burst), "plain_s": round(t_plain, 4), "served_s": round(t_served, 4),
+                        "speedup": round(t_plain / t_served, 3)}
+    share = {k: w * service[k][0] / mean_s for k, w in zip(ks, weights)}
+    bound = 1.0 / sum(share[k] / conc[str(k)]["speedup"] for k in ks)
     out = {"requests": count, "slots": slots, "hbm_budget_GB": budget >> 30,
            "resident_GB": round(res.device_bytes() / 1e9, 2),
            "service_ms_alone": {str(k): round(v[0] * 1e3, 2) for k, v in service.items()},
            "proof_verifies": verified,
            "prove_k20": {"proofs_per_s": round(1.0 / service[20][0], 3), "ms": round(service[20][0] * 1e3, 2),
                          "hbm_peak_GB": round(service[20][1], 2)},
-           "capacity_plain_per_s": round(1.0 / mean_s, 3), "loads": {}}
+           "capacity_plain_per_s": round(1.0 / mean_s, 3),
+           "concurrency_by_k": conc, "plain_time_share_by_k": {str(k): round(v, 3) for k, v in share.items()},
+           "served_over_plain_bound_from_bursts": round(bound, 3), "loads": {}}
     for load in loads:
         reqs = P.requests(count, load / mean_s, seed, ks, weights)
         row = {"arrival_rate_per_s": round(load / mean_s, 3)}

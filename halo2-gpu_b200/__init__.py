@@ -195,6 +195,8 @@ _SIGS = {
     "h2b_msm_table_workspace_size": (_u64, [_u64, _u64]),
     "h2b_msm_device_table": (RustError, [_vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp]),
     "h2b_msm_batch": (RustError, [ctypes.POINTER(MsmJob), _u64, _u32, _vp, _u64, _vp]),
+    "h2b_msm_merged_workspace_size": (_u64, [ctypes.POINTER(MsmJob), _u64]),
+    "h2b_msm_merged": (RustError, [ctypes.POINTER(MsmJob), _u64, _vp, _u64, _vp]),
     "h2b_batch_invert_workspace_size": (_u64, [_u64]),
     "h2b_batch_invert": (RustError, [_vp, _u32, _u64, _vp, _u64, _vp]),
     "h2b_ntt_set_pass_stages": (None, [ctypes.c_int]),
@@ -446,6 +448,16 @@ def msm_device_table(d_scalars, d_table, table_n, d_out, n, ws=None, stream=None
 def msm_batch(jobs, count, streams, ws, stream=None):
     """h2b_msm_batch: count device MSMs overlapped on `streams` forked streams."""
     call("h2b_msm_batch", jobs, count, streams, ptr(ws), ws.numel(), stream_handle(stream))
+
+
+def msm_merged_workspace_bytes(jobs, count):
+    return lib().h2b_msm_merged_workspace_size(jobs, count)
+
+
+def msm_merged(jobs, count, ws, stream=None):
+    """h2b_msm_merged: up to 64 MSMs over one window table as one sorted,
+    accumulated and reduced run (job i's result in jobs[i].d_out)."""
+    call("h2b_msm_merged", jobs, count, ptr(ws), ws.numel(), stream_handle(stream))
 
 
 def exec_fork(n, stream=None):

@@ -221,3 +221,62 @@ extern "C" RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint
     }
     return h2b_exec_join(stream, streams);
 }
+
+// Merged MSMs over one window table (no counterpart in the reference, whose
+// prover commits one polynomial per `_halo2_multiexp*` call): every job must
+// name the same table (d_bases, table_n > 0); up to 64 jobs of any lengths
+// up to table_n run as one MSM whose bucket sets are the jobs'.  Results are
+// those of h2b_msm_device_table per job.
+static RustError merged_check(const h2b_msm_job* jobs, uint64_t count, uint64_t& n_total)
+{
+    if (count == 0 || count > MSM_MERGE_MAX)
+        return err((int)cudaErrorInvalidValue, "h2b_msm_merged: 1 to 64 jobs");
+    n_total = 0;
+    for (uint64_t i = 0; i < count; i++) {
+        if (jobs[i].table_n == 0 || jobs[i].d_bases != jobs[0].d_bases || jobs[i].table_n != jobs[0].table_n)
+            return err((int)cudaErrorInvalidValue, "h2b_msm_merged: jobs must share one window table");
+        if (jobs[i].n > jobs[i].table_n)
+            return err((int)cudaErrorInvalidValue, "h2b_msm_merged: job longer than its table");
+        if (!jobs[i].d_out || (jobs[i].n > 0 && !jobs[i].d_scalars))
+            return err((int)cudaErrorInvalidValue, "h2b_msm_merged: null pointer");
+        n_total += jobs[i].n;
+    }
+    return ok();
+}
+
+extern "C" uint64_t h2b_msm_merged_workspace_size(const h2b_msm_job* jobs, uint64_t count)
+{
+    uint64_t n_total = 0;
+    RustError e = merged_check(jobs, count, n_total);
+    if (e.code) {
+        free(e.message);
+        return 0;
+    }
+    const MsmPlan p = msm_plan_merged(std::max<uint64_t>(n_total, 1), jobs[0].table_n, (uint32_t)count);
+    ScratchPlan sp;
+    msm_plan_scratch(p, sp, false, false);
+    return sp.used;
+}
+
+extern "C" RustError h2b_msm_merged(const h2b_msm_job* jobs, uint64_t count, void* scratch, uint64_t scratch_bytes,
+                                    cudaStream_t stream)
+{
+    uint64_t n_total = 0;
+    H2B_TRY(merged_check(jobs, count, n_total));
+    const MsmPlan p = msm_plan_merged(std::max<uint64_t>(n_total, 1), jobs[0].table_n, (uint32_t)count);
+    ScratchPlan sp;
+    msm_plan_scratch(p, sp, false, false);
+    if (!scratch || scratch_bytes < sp.used) return scratch_too_small("h2b_msm_merged", scratch_bytes, sp.used);
+    ScratchArena ar(scratch, scratch_bytes);
+    const MsmScratch s = msm_carve(p, ar, false, false);
+    if (!ar.good()) return err((int)cudaErrorInvalidValue, "h2b_msm_merged: scratch carving failed");
+    const Fr* sc[MSM_MERGE_MAX];
+    uint64_t ns[MSM_MERGE_MAX];
+    G1Jac* outs[MSM_MERGE_MAX];
+    for (uint64_t i = 0; i < count; i++) {
+        sc[i] = (const Fr*)jobs[i].d_scalars;
+        ns[i] = jobs[i].n;
+        outs[i] = (G1Jac*)jobs[i].d_out;
+    }
+    return msm_run_merged(p, s, (uint32_t)count, sc, ns, (const G1Affine*)jobs[0].d_bases, outs, stream);
+}

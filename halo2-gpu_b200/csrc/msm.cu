@@ -184,6 +184,17 @@ MsmPlan msm_plan_shared(uint64_t n, uint64_t tn, uint32_t concurrent)
     return tn ? plan_core(n, choose_c(tn), tn, concurrent) : plan_core(n, choose_c(n, true), 0, concurrent);
 }
 
+// J MSMs over one window table of tn points, n_total scalars in all, as one
+// run: job j's entries go to bucket set j (J bucket sets of H buckets), so
+// the sort, the accumulation and the bucket reduction run once for all jobs.
+MsmPlan msm_plan_merged(uint64_t n_total, uint64_t tn, uint32_t J)
+{
+    MsmPlan p = plan_core(n_total, choose_c(tn), tn);
+    p.Wr = (int)J;
+    p.NB = (uint64_t)J * p.H;
+    return p;
+}
+
 void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool bases_host)
 {
     if (bases_host) sp.add(p.n * sizeof(G1Affine));
@@ -200,8 +211,8 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
     sp.add_n<G1Xyzz>(p.max_dense * DENSE_PIECES);     // dense pieces
     sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment weighted sums
     sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment plain sums
-    sp.add_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));  // per-bit sums
-    sp.add_n<G1Xyzz>(p.W);                            // window sums
+    sp.add_n<G1Xyzz>((uint64_t)std::max(p.W, p.Wr) * (p.NBITS + 1));  // per-bit sums
+    sp.add_n<G1Xyzz>(std::max(p.W, p.Wr));                            // window sums
     sp.add_n<G1Jac>(1);                               // result
     if (p.R >= 1) sp.add_n<G1Affine>(p.cap[1]);       // round outputs 1, 3
     if (p.R >= 2) sp.add_n<G1Affine>(p.cap[2]);       // round output 2
@@ -235,8 +246,8 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
     s.pieces = ar.take_n<G1Xyzz>(p.max_dense * DENSE_PIECES);
     s.segacc = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
     s.segrun = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
-    s.bits = ar.take_n<G1Xyzz>((uint64_t)p.W * (p.NBITS + 1));
-    s.wins = ar.take_n<G1Xyzz>(p.W);
+    s.bits = ar.take_n<G1Xyzz>((uint64_t)std::max(p.W, p.Wr) * (p.NBITS + 1));
+    s.wins = ar.take_n<G1Xyzz>(std::max(p.W, p.Wr));
     s.result = ar.take_n<G1Jac>(1);
     s.pts[0] = p.R >= 1 ? ar.take_n<G1Affine>(p.cap[1]) : nullptr;
     s.pts[1] = p.R >= 2 ? ar.take_n<G1Affine>(p.cap[2]) : nullptr;
@@ -300,9 +311,12 @@ __device__ __forceinline__ uint32_t window_bits(const uint4& s, int bit, int c)
 // For each digit: key = w*H + |d| - 1 (or ~0 for zero digits); the entry's
 // sign is the digit's sign flipped by the virtual scalar's sign.
 // Virtual points v0 <= i < n.
+// With a window table every window shares one bucket set, based at `kb`
+// (the job's bucket set in a merged run, 0 otherwise).
 template <bool SCATTER>
 __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t n, int c, int W, uint32_t H,
-                           uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted, uint64_t tn)
+                           uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted, uint64_t tn,
+                           uint32_t kb)
 {
     const unsigned lane = threadIdx.x & 31;
     const uint32_t full = 1u << c;
@@ -318,7 +332,7 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t 
             if (v > H) { d = (int32_t)v - (int32_t)full; carry = 1; }
             else { d = (int32_t)v; carry = 0; }
             uint32_t key = 0xffffffffu;
-            if (valid && d != 0) key = (tn ? 0u : (uint32_t)w * H) + (uint32_t)(d < 0 ? -d : d) - 1u;
+            if (valid && d != 0) key = (tn ? kb : (uint32_t)w * H) + (uint32_t)(d < 0 ? -d : d) - 1u;
             unsigned peers = __match_any_sync(0xffffffffu, key);
             int leader = __ffs(peers) - 1;
             if (!SCATTER) {
@@ -904,12 +918,13 @@ __global__ void __launch_bounds__(256) k_msm_bitsums(const G1Xyzz* __restrict__ 
     if (threadIdx.x == 0) st_xyzz(&bits[blockIdx.x], r);
 }
 
-// One warp per window (warps loop when there are more windows than warps),
-// the Horner steps on the lane-parallel formulas.
+// One warp per window (warps loop when there are more windows than warps in
+// the grid), the Horner steps on the lane-parallel formulas.
 __global__ void k_msm_wincombine(const G1Xyzz* __restrict__ bits, int W, int nbits, int log_l,
                                  G1Xyzz* __restrict__ wins)
 {
-    for (int w = (int)(threadIdx.x >> 5); w < W; w += (int)(blockDim.x >> 5)) {
+    const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+    for (int w = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); w < W; w += warps) {
         const G1Xyzz* T = bits + (uint64_t)w * (nbits + 1);
         G1XyzzL r = xyzzl_inf();
         for (int k = nbits - 1; k >= 0; k--) {
@@ -955,6 +970,22 @@ __global__ void k_write_inf(G1Jac* out)
     }
 }
 
+// A merged run over a window table: window j of the reduction is job j's
+// whole sum (the table already holds the window multiples), so each job's
+// result is its window sum in the reference's affine image, one lane per job.
+struct MsmOuts {
+    G1Jac* p[MSM_MERGE_MAX];
+};
+__global__ void k_msm_final_each(const G1Xyzz* __restrict__ wins, uint32_t J, const __grid_constant__ MsmOuts outs)
+{
+    const uint32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= J || (threadIdx.x & 31) != 0) return;
+    const G1Jac r = xyzz_to_jac_affine(ld_xyzz(&wins[j]));
+    st(&outs.p[j]->X, r.X);
+    st(&outs.p[j]->Y, r.Y);
+    st(&outs.p[j]->Z, r.Z);
+}
+
 // Runs steps 1-7 on device buffers; result (96 bytes) lands in s.result.
 // The lazy accumulation (window tables are stored in its form; plain bases
 // are converted by the split kernel) unless pairing rounds or an older
@@ -986,7 +1017,7 @@ static RustError msm_split(const MsmPlan& p, const MsmScratch& s, const Fr* d_sc
                                                               msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr, p.n);
     H2B_LAUNCHED("k_msm_glv");
     k_msm_sort<false><<<grid_for(2 * (hi - lo), 256, sm_cap), 256, 0, st>>>(vsc, 2 * lo, 2 * hi, p.c, p.W, p.H,
-                                                                              s.counts, nullptr, p.tn);
+                                                                              s.counts, nullptr, p.tn, 0u);
     H2B_LAUNCHED("k_msm_sort<hist>");
     return ok();
 }
@@ -999,7 +1030,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
     H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     k_msm_sort<true><<<grid_for(p.nv, 256, sm_cap), 256, 0, st>>>(vsc, 0, p.nv, p.c, p.W, p.H, s.cursor,
-                                                                    s.sorted, p.tn);
+                                                                    s.sorted, p.tn, 0u);
     H2B_LAUNCHED("k_msm_sort<scatter>");
     prof_begin(PROF_MSM_ACCUMULATE, st);
     // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
@@ -1074,7 +1105,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     H2B_LAUNCHED("k_msm_segments");
     k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
     H2B_LAUNCHED("k_msm_bitsums");
-    k_msm_wincombine<<<1, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
+    k_msm_wincombine<<<(p.Wr + 7) / 8, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
     H2B_LAUNCHED("k_msm_wincombine");
     k_msm_final<<<1, 32 * std::min(p.Wr, 8), 0, st>>>(s.wins, p.Wr, p.c, s.result);
     prof_end(PROF_MSM_TOTAL, st);
@@ -1092,6 +1123,71 @@ RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, co
     H2B_TRY(msm_begin(p, s, st));
     H2B_TRY(msm_split(p, s, d_scalars, d_bases, 0, p.n, st));
     return msm_finish(p, s, d_bases, st);
+}
+
+RustError msm_run_merged(const MsmPlan& p, const MsmScratch& s, uint32_t J, const Fr* const* scalars,
+                         const uint64_t* ns, const G1Affine* table, G1Jac* const* outs, cudaStream_t st)
+{
+    if (J == 0) return ok();
+    if (J > (uint32_t)MSM_MERGE_MAX || p.tn == 0 || (uint32_t)p.Wr != J)
+        return err(cudaErrorInvalidValue, "msm_run_merged: plan does not match the jobs");
+    const unsigned sm_cap = 148u * 16u;
+    uint4* vsc = reinterpret_cast<uint4*>(s.canon);
+    prof_begin(PROF_MSM_TOTAL, st);
+    H2B_CUDA(cudaMemsetAsync(s.counts, 0, p.NB * sizeof(uint32_t), st));
+    H2B_CUDA(cudaMemsetAsync(s.dense + p.max_dense, 0, sizeof(uint32_t), st));
+    uint64_t at = 0;   // job j's virtual scalars start at vsc + 2 * at
+    for (uint32_t j = 0; j < J; j++) {
+        if (ns[j] == 0) continue;
+        k_msm_glv<<<grid_for(ns[j], 256, sm_cap), 256, 0, st>>>(scalars[j], vsc + 2 * at, 0, ns[j], nullptr, nullptr,
+                                                                ns[j]);
+        H2B_LAUNCHED("k_msm_glv");
+        k_msm_sort<false><<<grid_for(2 * ns[j], 256, sm_cap), 256, 0, st>>>(vsc + 2 * at, 0, 2 * ns[j], p.c, p.W,
+                                                                              p.H, s.counts, nullptr, p.tn, j * p.H);
+        H2B_LAUNCHED("k_msm_sort<hist>");
+        at += ns[j];
+    }
+    H2B_CUDA(scan_u32(s.counts, p.NB, s.offsets, s.scan_tmp, st));
+    H2B_CUDA(cudaMemcpyAsync(s.cursor, s.offsets, p.NB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    at = 0;
+    for (uint32_t j = 0; j < J; j++) {
+        if (ns[j] == 0) continue;
+        k_msm_sort<true><<<grid_for(2 * ns[j], 256, sm_cap), 256, 0, st>>>(vsc + 2 * at, 0, 2 * ns[j], p.c, p.W, p.H,
+                                                                             s.cursor, s.sorted, p.tn, j * p.H);
+        H2B_LAUNCHED("k_msm_sort<scatter>");
+        at += ns[j];
+    }
+    prof_begin(PROF_MSM_ACCUMULATE, st);
+    const uint64_t chunks = (p.max_entries + p.Kf - 1) / p.Kf;
+    const unsigned acc_grid = grid_for(chunks, 128, 148u * 32u);
+    if (g_msm_acc_variant == 6)
+        k_msm_accumulate_d<<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.Kf, table, (uint64_t)p.W * p.tn,
+                                                     s.buckets, s.heads, g_msm_prefetch);
+    else
+        k_msm_accumulate_z<<<acc_grid, 128, 0, st>>>(s.sorted, s.offsets, p.NB, p.Kf, table, (uint64_t)p.W * p.tn,
+                                                     s.buckets, s.heads);
+    prof_end(PROF_MSM_ACCUMULATE, st);
+    H2B_LAUNCHED("k_msm_accumulate");
+    k_msm_fixup<<<grid_for(p.NB, 128, sm_cap), 128, 0, st>>>(s.offsets, p.NB, p.Kf, s.buckets, s.heads, s.dense,
+                                                            p.max_dense);
+    H2B_LAUNCHED("k_msm_fixup");
+    k_msm_dense_pieces<<<148 * 4, 256, 0, st>>>(s.offsets, p.max_dense, p.Kf, s.heads, s.dense, s.pieces);
+    H2B_LAUNCHED("k_msm_dense_pieces");
+    k_msm_dense_merge<<<148, DENSE_PIECES, 0, st>>>(p.max_dense, s.buckets, s.dense, s.pieces);
+    H2B_LAUNCHED("k_msm_dense_merge");
+    const uint64_t nseg = (uint64_t)p.Wr * p.S;
+    k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.Wr, p.H, p.L, p.S, s.segacc, s.segrun);
+    H2B_LAUNCHED("k_msm_segments");
+    k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
+    H2B_LAUNCHED("k_msm_bitsums");
+    k_msm_wincombine<<<(p.Wr + 7) / 8, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
+    H2B_LAUNCHED("k_msm_wincombine");
+    MsmOuts o;
+    for (uint32_t j = 0; j < J; j++) o.p[j] = outs[j];
+    k_msm_final_each<<<(J + 7) / 8, 256, 0, st>>>(s.wins, J, o);
+    prof_end(PROF_MSM_TOTAL, st);
+    H2B_LAUNCHED("k_msm_final_each");
+    return ok();
 }
 
 } // namespace h2b

@@ -70,6 +70,13 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
 MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool bases_host);
 RustError msm_run(const MsmPlan& p, const MsmScratch& s, const Fr* d_scalars, const G1Affine* d_bases,
                   cudaStream_t st);
+// Merged runs: up to MSM_MERGE_MAX MSMs over one window table of tn points
+// (n_total scalars in all) sorted, accumulated and reduced together, job j in
+// bucket set j; each job's 96-byte result goes to outs[j].
+constexpr uint32_t MSM_MERGE_MAX = 64;
+MsmPlan msm_plan_merged(uint64_t n_total, uint64_t tn, uint32_t J);
+RustError msm_run_merged(const MsmPlan& p, const MsmScratch& s, uint32_t J, const Fr* const* scalars,
+                         const uint64_t* ns, const G1Affine* table, G1Jac* const* outs, cudaStream_t st);
 void msm_set_tuning(int window_bits, int chunk);
 void msm_set_pair_rounds(int rounds);
 

@@ -222,7 +222,8 @@ def _generator_image():
 class ProofWorkload:
     """One proof of the 2^k circuit (see the module docstring)."""
 
-    def __init__(self, res, k, seed, transcript=False, tamper=None, check_degree=False, fused_quotient=True):
+    def __init__(self, res, k, seed, transcript=False, tamper=None, check_degree=False, fused_quotient=True,
+                 merged_msm=False):
         """transcript=False draws the challenges from a generator seeded with
         `seed`; transcript=True runs the Fiat-Shamir transcript
         (transcript.Blake2bWrite): every commitment is read back and absorbed
@@ -238,9 +239,15 @@ class ProofWorkload:
         extended array, already divided by X^n - 1; False runs the
         reference's per-part launcher sequence (gates, permutation, lookup
         expression, lookup constraints) and then gathers and divides.  The
-        proofs are the same bytes."""
+        proofs are the same bytes.  merged_msm=True commits each phase's
+        polynomials over one window table as one merged MSM (h2b_msm_merged);
+        False (the default) runs them as separate MSMs on forked streams
+        (h2b_msm_batch), which measured faster here (k = 16 / 20 / 22 proofs
+        17.8 / 79 / 280 ms against 18.6 / 81 / 286 ms merged): one MSM's sort
+        overlaps another's accumulation.  Same bytes."""
         self.res, self.k, self.seed, self.transcript, self.tamper = res, k, seed, transcript, tamper
         self.fused_quotient = fused_quotient
+        self.merged_msm = merged_msm
         self.check_degree = check_degree
         self.h_degree_ok = None
         self.proof = None
@@ -296,14 +303,25 @@ class ProofWorkload:
                 commits.append(out)
 
             def flush():
-                """The commitments of one phase as one batch: each MSM on its own
-                forked stream, so their serial tails overlap."""
-                jobs = (h2b.MsmJob * len(pending))()
-                for i, (d, out, lagr) in enumerate(pending):
-                    jobs[i].d_scalars, jobs[i].d_out, jobs[i].n = d.data_ptr(), out.data_ptr(), n
-                    jobs[i].d_bases = (lag_tab if lagr else res.table).data_ptr()
-                    jobs[i].table_n = tn
-                h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
+                """The commitments of one phase: those over the same window table
+                as one merged MSM (one sort, accumulation and reduction for
+                all), or each MSM on its own forked stream."""
+                if self.merged_msm:
+                    for lagr in (True, False):
+                        group = [q for q in pending if q[2] == lagr]
+                        if not group:
+                            continue
+                        jobs = h2b.msm_batch_jobs([q[0] for q in group], [lag_tab if lagr else res.table] * len(group),
+                                                  [q[1] for q in group], [n] * len(group), table_n=tn)
+                        ws = h2b.dev_empty(h2b.msm_merged_workspace_bytes(jobs, len(group)))
+                        h2b.msm_merged(jobs, len(group), ws, stream=stream)
+                else:
+                    jobs = (h2b.MsmJob * len(pending))()
+                    for i, (d, out, lagr) in enumerate(pending):
+                        jobs[i].d_scalars, jobs[i].d_out, jobs[i].n = d.data_ptr(), out.data_ptr(), n
+                        jobs[i].d_bases = (lag_tab if lagr else res.table).data_ptr()
+                        jobs[i].table_n = tn
+                    h2b.msm_batch(jobs, len(pending), len(pending), msm_ws, stream=stream)
                 outs = [q[1] for q in pending]
                 pending.clear()
                 absorb(outs)

@@ -504,6 +504,15 @@ typedef struct h2b_msm_job {
 uint64_t h2b_msm_batch_workspace_size(const h2b_msm_job* jobs, uint64_t count, uint32_t streams);
 RustError h2b_msm_batch(const h2b_msm_job* jobs, uint64_t count, uint32_t streams, void* scratch,
                         uint64_t scratch_bytes, h2b_stream_t stream);
+/* Up to 64 MSMs over ONE window table (every job names the same d_bases and table_n > 0; lengths may
+ * differ, each <= table_n) run as one MSM: one counting sort with job j's entries in bucket set j, one
+ * accumulation, one bucket reduction, one final kernel writing each job's 96-byte result to its d_out.
+ * Same results as h2b_msm_device_table per job (no counterpart in the reference, which commits one
+ * polynomial per _halo2_multiexp* call).  Scratch: h2b_msm_merged_workspace_size (0 if the jobs do not
+ * qualify).  No host synchronisation; device outputs. */
+uint64_t h2b_msm_merged_workspace_size(const h2b_msm_job* jobs, uint64_t count);
+RustError h2b_msm_merged(const h2b_msm_job* jobs, uint64_t count, void* scratch, uint64_t scratch_bytes,
+                         h2b_stream_t stream);
 /* Batch inversion whose CTAs share a single inversion through scratch
  * (h2b_batch_invert_workspace_size bytes); same semantics as _halo2_batch_invert. */
 uint64_t h2b_batch_invert_workspace_size(uint64_t length);

@@ -101,3 +101,87 @@ def test_table_argument_errors(h2b, cuda, table4k):
     with pytest.raises(h2b.Halo2GpuError):   # n above the table size
         h2b.msm_device_table(d_sc, table, 1 << 12, h2b.dev_empty(96), 8192, ws=h2b.dev_empty(1 << 20))
     assert h2b.lib().h2b_msm_table_points(1 << 28) == 0
+
+
+def _bytes(t):
+    return t.cpu().numpy().tobytes()
+
+
+def test_merged_jobs_over_one_table(h2b, orc, cuda, table4k):
+    """h2b_msm_merged: jobs of different lengths (full, partial, one point, an
+    empty job, a repeated scalar vector) over the shared 2^12 table give the
+    oracle's MSM per job and the bytes of h2b_msm_device_table."""
+    srs, _, table = table4k
+    tn = 1 << 12
+    lengths = [tn, 3000, 100, 1, 0, tn, 517]
+    scs = []
+    for i, m in enumerate(lengths):
+        sc = orc.chacha_fr(700 + i, max(m, 1))[:m] if m else np.zeros((0, 4), np.uint64)
+        if m > 10:
+            sc[::5] = 0
+        scs.append(sc)
+    scs[5] = scs[0].copy()                       # two jobs with the same scalars
+    d_scs = [h2b.to_dev(s) if len(s) else h2b.dev_empty(32) for s in scs]
+    outs = [h2b.dev_empty(96) for _ in lengths]
+    jobs = h2b.msm_batch_jobs(d_scs, [table] * len(lengths), outs, lengths, table_n=tn)
+    ws = h2b.dev_empty(h2b.msm_merged_workspace_bytes(jobs, len(lengths)))
+    h2b.msm_merged(jobs, len(lengths), ws)
+    for i, (m, sc) in enumerate(zip(lengths, scs)):
+        got = h2b.to_host(outs[i], (12,))
+        if m == 0:
+            assert_limbs_equal(got, h2b.to_host(_inf_image(h2b), (12,)), "empty job")
+            continue
+        assert_limbs_equal(got, orc.msm(sc, srs[:m]), f"merged job {i} (n={m})")
+        one = h2b.dev_empty(96)
+        h2b.msm_device_table(d_scs[i], table, tn, one, m)
+        assert _bytes(one) == _bytes(outs[i])
+
+
+def _inf_image(h2b):
+    """(0, 1, 0): the reference's image of the point at infinity."""
+    f = h2b.fields
+    img = np.zeros(12, np.uint64)
+    img[4:8] = f.fq_mont_limbs([1])[0]
+    return h2b.to_dev(img)
+
+
+def test_merged_64_jobs_k16_match_the_batch(h2b, cuda):
+    """The 64-job maximum at mixed lengths over a 2^16 table, witness-like and
+    uniform scalars: the same bytes as h2b_msm_batch over that table."""
+    n = 1 << 16
+    d_srs = h2b.srs_device(0x7AB1E, n)
+    table = h2b.msm_table_precompute(d_srs, n)
+    lengths = [n if i % 9 == 0 else (1 << (8 + i % 8)) + i for i in range(64)]
+    scs = [h2b.random_fr_device(m, 900 + i, i % 2) for i, m in enumerate(lengths)]
+    outs_m = [h2b.dev_empty(96) for _ in lengths]
+    outs_b = [h2b.dev_empty(96) for _ in lengths]
+    jm = h2b.msm_batch_jobs(scs, [table] * 64, outs_m, lengths, table_n=n)
+    jb = h2b.msm_batch_jobs(scs, [table] * 64, outs_b, lengths, table_n=n)
+    h2b.msm_merged(jm, 64, h2b.dev_empty(h2b.msm_merged_workspace_bytes(jm, 64)))
+    h2b.msm_batch(jb, 64, 8, h2b.msm_batch_workspace(jb, 64, 8))
+    torch.cuda.synchronize()
+    assert [_bytes(o) for o in outs_m] == [_bytes(o) for o in outs_b]
+
+
+def test_merged_argument_errors(h2b, cuda, table4k):
+    srs, d_srs, table = table4k
+    tn = 1 << 12
+    sc = h2b.dev_empty(32 * tn)
+    out = h2b.dev_empty(96)
+    L = h2b.lib()
+    other = h2b.msm_table_precompute(d_srs, tn)
+    bad = [h2b.msm_batch_jobs([sc, sc], [table, other], [out, out], [10, 10], table_n=tn),   # two tables
+           h2b.msm_batch_jobs([sc], [d_srs], [out], [10], table_n=0),                       # plain bases
+           h2b.msm_batch_jobs([sc], [table], [out], [tn + 1], table_n=tn)]                  # longer than table
+    for jobs in bad:
+        assert L.h2b_msm_merged_workspace_size(jobs, len(jobs)) == 0
+        with pytest.raises(h2b.Halo2GpuError, match="h2b_msm_merged"):
+            h2b.msm_merged(jobs, len(jobs), h2b.dev_empty(1 << 20))
+    many = h2b.msm_batch_jobs([sc] * 65, [table] * 65, [out] * 65, [1] * 65, table_n=tn)
+    assert L.h2b_msm_merged_workspace_size(many, 65) == 0
+    with pytest.raises(h2b.Halo2GpuError, match="1 to 64 jobs"):
+        h2b.msm_merged(many, 65, h2b.dev_empty(1 << 20))
+    ok = h2b.msm_batch_jobs([sc], [table], [out], [tn], table_n=tn)
+    need = L.h2b_msm_merged_workspace_size(ok, 1)
+    with pytest.raises(h2b.Halo2GpuError):
+        h2b.msm_merged(ok, 1, h2b.dev_empty(need - 256))

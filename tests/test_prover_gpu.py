@@ -181,12 +181,12 @@ def test_keygen_commitments(h2b):
         assert out.cpu().numpy().tobytes() == got.cpu().numpy().tobytes()
 
 
-def _prove(h2b, res, k, seed, tamper=None, check_degree=False, fused_quotient=True):
+def _prove(h2b, res, k, seed, tamper=None, check_degree=False, fused_quotient=True, merged_msm=False):
     import torch
     P = _prover(h2b)
     st = torch.cuda.Stream()
     w = P.ProofWorkload(res, k, seed, transcript=True, tamper=tamper, check_degree=check_degree,
-                        fused_quotient=fused_quotient)
+                        fused_quotient=fused_quotient, merged_msm=merged_msm)
     commits, evals = w.run(st)
     st.synchronize()
     return w, commits, evals
@@ -253,6 +253,9 @@ def test_proof_verifies_and_rejects_changes(h2b):
     # the reference's per-part launcher sequence gives the same proof bytes as the fused quotient pass
     w3, _, _ = _prove(h2b, res, k, 21, fused_quotient=False)
     assert w3.proof == proof
+    # and the merged phase commitments the same bytes as separate MSMs on forked streams
+    w4, _, _ = _prove(h2b, res, k, 21, merged_msm=True)
+    assert w4.proof == proof
 
 
 @pytest.mark.gpu
@@ -267,8 +270,8 @@ def test_proof_verifies_at_config_sizes(h2b, k):
     assert w.h_degree_ok, "h must have degree < 3n when every constraint holds"
     assert V.verify_proof(res.verifying_key(k), w.public, w.proof, res.tau)
     if k == 20:
-        w2, _, _ = _prove(h2b, res, k, 1000 + k, fused_quotient=False)
-        assert w2.proof == w.proof, "fused and per-launcher quotients must give the same proof"
+        w2, _, _ = _prove(h2b, res, k, 1000 + k, fused_quotient=False, merged_msm=True)
+        assert w2.proof == w.proof, "fused quotient and merged MSMs must not change the proof"
     bad = bytearray(w.proof)
     bad[-32 * 3] ^= 4                                 # inside the last evaluations
     assert not V.verify_proof(res.verifying_key(k), w.public, bytes(bad), res.tau)
