@@ -410,8 +410,10 @@ def rows_section(h2b, torch, hbm_gbs, product_peak, k=20, reps=5):
           9 * 32)
     # a7-a9 together on one config-3 extended part: the reference's four per-part
     # launches (gates, permutation, lookup expression, lookup constraints)
-    # against one h2b_quotient_fused launch; 22 arrays of 32 B per row are read
-    # once and one written by the fused pass
+    # against one h2b_quotient_fused launch; 20 arrays of 32 B per row are read
+    # once and one written by the fused pass (3 fixed, instance, 4 advice,
+    # 4 sigma, l0 / l_last / l_active, 2 permutation products, the lookup
+    # product and A' / S')
     C = importlib.import_module(h2b.__name__ + ".circuit")
     g_rules, g_parts, g_consts = C.gate_graph()
     l_rules, l_parts, l_consts = C.lookup_product_graph()
@@ -439,10 +441,10 @@ def rows_section(h2b, torch, hbm_gbs, product_peak, k=20, reps=5):
                 ext_omega=shift, omega=dom.omega, chunk_len=C.CHUNK_LEN, last_rotation=last, rot_scale=1, isize=n)
     look = [dict(rules=(bg, l_consts, l_rules, l_parts), z=zl, pin=pa, ptab=ps, beta=beta, gamma=gamma)]
     no_ch = np.zeros((0, 4), np.uint64)
-    timed("quotient_part_chain", chain, n, "rows", 22 * 32)
+    timed("quotient_part_chain", chain, n, "rows", 21 * 32)
     timed("quotient_part_fused", lambda: h2b.quotient_fused_device(
         qf, qi, qa, (no_ch, g_consts, g_rules, g_parts), yv, *lag3, perm, look, n, 1, 0, n, fo, stream=side),
-        n, "rows", 22 * 32)
+        n, "rows", 21 * 32)
     torch.cuda.synchronize()
     out["quotient_part_fused"]["identical_to_chain"] = bool(torch.equal(hj, fo))
     out["quotient_part_fused"]["speedup_over_chain"] = round(out["quotient_part_chain"]["ms"] /
