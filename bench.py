@@ -686,7 +686,7 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
 
     groups = {k: [i for i in range(n_jobs) if ks[i] == k] for k in sizes}
 
-    def batched(bases, table_n=0):
+    def batched(bases, table_n=0, merged=False):
         subs = h2b.exec_fork(streams, side)
         for gi, k in enumerate(sorted(sizes, reverse=True)):
             st = subs[gi]
@@ -696,7 +696,12 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
             for i in idx:
                 progs["batched"][i].run(outs["q"][i], stream=st)
         jobs = h2b.msm_batch_jobs(d_sc, [bases] * n_jobs, outs["msm"], [1 << k for k in ks], table_n=table_n)
-        h2b.msm_batch(jobs, n_jobs, streams, bws[table_n], stream=side)
+        if merged:
+            # all 64 MSMs as one run over the table, beside the transforms
+            h2b.msm_merged(jobs, n_jobs, bws["merged"], stream=subs[len(sizes)])
+            h2b.exec_join(streams, side)
+        else:
+            h2b.msm_batch(jobs, n_jobs, streams, bws[table_n], stream=side)
 
     def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -707,12 +712,12 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
         side.synchronize()
         return e0.elapsed_time(e1) / reps
 
-    def graph_time(bases, table_n=0):
-        batched(bases, table_n)      # warm-up: forked streams, kernels loaded
+    def graph_time(bases, table_n=0, merged=False):
+        batched(bases, table_n, merged)      # warm-up: forked streams, kernels loaded
         side.synchronize()
         gr = h2b.Graph(side)
         gr.begin()
-        batched(bases, table_n)
+        batched(bases, table_n, merged)
         gr.end()
         try:
             gr.launch(side)
@@ -746,6 +751,12 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
     bws[1 << 20] = h2b.msm_batch_workspace(jobs_t, n_jobs, streams)
     t_table = graph_time(table, 1 << 20)
     same = same and identical()
+    # the 64 MSMs over the table as one merged run (h2b_msm_merged)
+    for o in outs["msm"]:
+        o.zero_()
+    bws["merged"] = h2b.dev_empty(h2b.msm_merged_workspace_bytes(jobs_t, n_jobs))
+    t_merged = graph_time(table, 1 << 20, merged=True)
+    same = same and identical()
     return {"workload": f"{n_jobs} jobs, k in {{14,16,18,20}} w .4/.3/.2/.1 (seed {seed}): MSM vs shared 2^20 SRS "
                         f"+ forward NTT + coset extension x4 + config-3 gate quotient over the extended coset",
             "k_counts": {k: ks.count(k) for k in sizes},
@@ -754,7 +765,8 @@ def batch_section(h2b, torch, n_jobs=64, streams=16, reps=3, seed=4):
             "plain_jobs_per_s": n_jobs / (t_plain * 1e-3), "batched_jobs_per_s": n_jobs / (t_graph * 1e-3),
             "speedup": t_plain / t_graph, "table_precompute_ms": t_pre, "batched_table_graph_ms": t_table,
             "batched_table_jobs_per_s": n_jobs / (t_table * 1e-3), "table_speedup": t_plain / t_table,
-            "identical_outputs": same}
+            "batched_table_merged_graph_ms": t_merged, "batched_table_merged_jobs_per_s": n_jobs / (t_merged * 1e-3),
+            "table_merged_speedup": t_plain / t_merged, "identical_outputs": same}
 
 
 def run_case(args):
@@ -838,7 +850,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
-    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute", "quotient"],
+    ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute", "quotient",
+                                       "prove"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")
@@ -872,6 +885,27 @@ def main():
         loads = tuple(float(x) for x in args.loads.split(","))
         print(json.dumps({"case": "serve", "serving": serving_section(load_pkg(), torch, count=args.requests,
                                                                       loads=loads)}))
+        return
+    if args.case == "prove":
+        # config-3 proofs at 2^log_n one after another (transcript on), for
+        # launch lists of a whole proof: warmup untimed, then steps timed
+        import torch
+        torch.cuda.set_device(0)
+        h2b = load_pkg()
+        P = importlib.import_module(h2b.__name__ + ".prover")
+        res = P.Resident(h2b, args.log_n)
+        res.key_cosets(args.log_n)
+        res.lagrange_table(args.log_n)
+        st = torch.cuda.Stream()
+        ms = []
+        for i in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            P.ProofWorkload(res, args.log_n, 500 + i, transcript=True).run(st)
+            st.synchronize()
+            if i >= args.warmup:
+                ms.append(round((time.perf_counter() - t0) * 1e3, 2))
+        print(json.dumps({"case": "prove", "log_n": args.log_n, "proof_ms": ms}))
         return
     if args.case:
         run_case(args)
