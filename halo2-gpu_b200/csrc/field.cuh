@@ -698,6 +698,125 @@ H2B_DEV Fp<C> mont_mul_f64(const Fp<C>& a, const Fp<C>& b)
     return r;
 }
 
+// ---- residues in [0, 2p) ----------------------------------------------------
+// A chain of products and sums (an NTT pass) can keep its values in [0, 2p)
+// and make them canonical once at the end.  The FP64 product's bound with
+// a, b < 2p: 16 a b + Q p < 64 p^2 + 2^260 p, so the result is below
+// (64 p / 2^260 + 1) p < 1.76 p for both BN254 moduli (p < 2^253.6), and its closing
+// subtraction can be left out; a sum below 4p (< 2^256) or a difference in
+// (-2p, 2p) takes one correction by 2p.  Column bounds of the product do not
+// depend on the operands' size (every limb is below 2^52 and 16 a < 2^260).
+
+// word w of 2m (8 x 32 grid)
+template <class C>
+__host__ __device__ constexpr uint32_t m2word(int w)
+{
+    return (mword<C>(w) << 1) | (w > 0 ? mword<C>(w - 1) >> 31 : 0u);
+}
+
+// a b 2^-256 mod p in [0, 2p) for a, b < 2p
+template <class C>
+H2B_DEV Fp<C> mont_mul_f64_lazy(const Fp<C>& a, const Fp<C>& b)
+{
+    using namespace f64;
+    double A[5], B[5];
+    A[0] = u52d(bits52<-4>(a.v)); A[1] = u52d(bits52<48>(a.v)); A[2] = u52d(bits52<100>(a.v));
+    A[3] = u52d(bits52<152>(a.v)); A[4] = u52d(bits52<204>(a.v));
+    B[0] = u52d(bits52<0>(b.v)); B[1] = u52d(bits52<52>(b.v)); B[2] = u52d(bits52<104>(b.v));
+    B[3] = u52d(bits52<156>(b.v)); B[4] = u52d(bits52<208>(b.v));
+    uint64_t l[5];
+    mont52<C>(A, B, l);
+    Fp<C> r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int i0 = (32 * j) / 52, o = 32 * j - 52 * i0;
+        uint64_t x = l[i0] >> o;
+        if (i0 + 1 < 5) x |= l[i0 + 1] << (52 - o);
+        r.v[j] = (uint32_t)x;
+    }
+    return r;
+}
+
+// (a + b) mod 2p in [0, 2p) for a, b < 2p
+template <class C>
+H2B_DEV Fp<C> add2p(const Fp<C>& a, const Fp<C>& b)
+{
+    uint32_t t[8], s[8], bw;
+    asm("add.cc.u32  %0, %8, %16;\n\t"
+        "addc.cc.u32 %1, %9, %17;\n\t"
+        "addc.cc.u32 %2, %10, %18;\n\t"
+        "addc.cc.u32 %3, %11, %19;\n\t"
+        "addc.cc.u32 %4, %12, %20;\n\t"
+        "addc.cc.u32 %5, %13, %21;\n\t"
+        "addc.cc.u32 %6, %14, %22;\n\t"
+        "addc.u32    %7, %15, %23;"
+        : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7])
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(s[0]), "=r"(s[1]), "=r"(s[2]), "=r"(s[3]), "=r"(s[4]), "=r"(s[5]), "=r"(s[6]), "=r"(s[7]),
+          "=r"(bw)
+        : "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]),
+          "n"(m2word<C>(0)), "n"(m2word<C>(1)), "n"(m2word<C>(2)), "n"(m2word<C>(3)), "n"(m2word<C>(4)),
+          "n"(m2word<C>(5)), "n"(m2word<C>(6)), "n"(m2word<C>(7)));
+    Fp<C> r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = bw ? t[i] : s[i];
+    return r;
+}
+
+// (a - b) mod 2p in [0, 2p) for a, b < 2p
+template <class C>
+H2B_DEV Fp<C> sub2p(const Fp<C>& a, const Fp<C>& b)
+{
+    Fp<C> r;
+    uint32_t bw;
+    asm("sub.cc.u32  %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32    %8, 0, 0;"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(bw)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    const uint32_t q0 = bw & m2word<C>(0), q1 = bw & m2word<C>(1), q2 = bw & m2word<C>(2), q3 = bw & m2word<C>(3);
+    const uint32_t q4 = bw & m2word<C>(4), q5 = bw & m2word<C>(5), q6 = bw & m2word<C>(6), q7 = bw & m2word<C>(7);
+    asm("add.cc.u32  %0, %0, %8;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, %10;\n\t"
+        "addc.cc.u32 %3, %3, %11;\n\t"
+        "addc.cc.u32 %4, %4, %12;\n\t"
+        "addc.cc.u32 %5, %5, %13;\n\t"
+        "addc.cc.u32 %6, %6, %14;\n\t"
+        "addc.u32    %7, %7, %15;"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7])
+        : "r"(q0), "r"(q1), "r"(q2), "r"(q3), "r"(q4), "r"(q5), "r"(q6), "r"(q7));
+    return r;
+}
+
+// the canonical residue of a < 2p
+template <class C>
+H2B_DEV Fp<C> canon2p(const Fp<C>& a)
+{
+    Fp<C> r;
+    cond_sub<C>(r.v, a.v);
+    return r;
+}
+
 // The 29-bit limb form (Fl: value below 2p, R = 2^256) through the FP64
 // core: the limbs are re-sliced into 52-bit limbs (one operand as 16 a, still
 // below 2^260), and the result, below (1 + 64 p / 2^260) p < 1.76 p, is
@@ -754,12 +873,7 @@ H2B_DEV Fl<C> mul_f64_l(const Fl<C>& a, const Fl<C>& b)
 
 // ---- Fl arithmetic kept in limb form (values < 2p, limbs < 2^29) ---------
 
-// word w of 2m (8 x 32 grid) and its limb i in the 29-bit grid
-template <class C>
-__host__ __device__ constexpr uint32_t m2word(int w)
-{
-    return (mword<C>(w) << 1) | (w > 0 ? mword<C>(w - 1) >> 31 : 0u);
-}
+// limb i of 2m (m2word above) in the 29-bit grid
 template <class C>
 __host__ __device__ constexpr uint32_t p2_29(int i)
 {

@@ -344,6 +344,20 @@ struct NttTile4 {
     }
 };
 
+// Inside a radix-4 pass values stay in [0, 2p): products without their
+// closing subtraction, sums and differences corrected by 2p, one
+// canonicalisation per element at the store (field.cuh, residues in [0, 2p)).
+__device__ __forceinline__ Fr lz_mul(const Fr& a, const Fr& b)
+{
+#if H2B_MUL_F64
+    return mont_mul_f64_lazy<FrCfg>(a, b);
+#else
+    return a * b;
+#endif
+}
+__device__ __forceinline__ Fr lz_add(const Fr& a, const Fr& b) { return add2p<FrCfg>(a, b); }
+__device__ __forceinline__ Fr lz_sub(const Fr& a, const Fr& b) { return sub2p<FrCfg>(a, b); }
+
 template <bool DIT>
 __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const Fr* __restrict__ tw, int logn,
                                                                int s0, int nst, int lS, int lG)
@@ -392,12 +406,12 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
             const uint32_t ix = (gl << nst) + q, iy = ix + (1u << h);
             const Fr x = T.get(ix), y = T.get(iy), w = twid(lowm, r, sh);
             if (DIT) {
-                const Fr yw = y * w;
-                T.put(ix, x + yw);
-                T.put(iy, x - yw);
+                const Fr yw = lz_mul(y, w);
+                T.put(ix, lz_add(x, yw));
+                T.put(iy, lz_sub(x, yw));
             } else {
-                T.put(ix, x + y);
-                T.put(iy, (x - y) * w);
+                T.put(ix, lz_add(x, y));
+                T.put(iy, lz_mul(lz_sub(x, y), w));
             }
         }
         __syncthreads();
@@ -418,24 +432,24 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
                 // (i0, i2) takes lowm, (i1, i3) takes lowm + 2^h
                 const int sh0 = logn - (s0 + t) - 1, sh1 = sh0 - 1;
                 const Fr wh = twid(lowm, r, sh0), wa = twid(lowm, r, sh1), wb = twid(lowm + (1u << h), r, sh1);
-                const Fr t1 = a1 * wh, t3 = a3 * wh;
-                const Fr b0 = a0 + t1, b1 = a0 - t1, b2 = a2 + t3, b3 = a2 - t3;
-                const Fr u2 = b2 * wa, u3 = b3 * wb;
-                T.put(i0, b0 + u2);
-                T.put(i2, b0 - u2);
-                T.put(i1, b1 + u3);
-                T.put(i3, b1 - u3);
+                const Fr t1 = lz_mul(a1, wh), t3 = lz_mul(a3, wh);
+                const Fr b0 = lz_add(a0, t1), b1 = lz_sub(a0, t1), b2 = lz_add(a2, t3), b3 = lz_sub(a2, t3);
+                const Fr u2 = lz_mul(b2, wa), u3 = lz_mul(b3, wb);
+                T.put(i0, lz_add(b0, u2));
+                T.put(i2, lz_sub(b0, u2));
+                T.put(i1, lz_add(b1, u3));
+                T.put(i3, lz_sub(b1, u3));
             } else {
                 // stage t (span 2^(h+1)): (i0, i2) takes lowm, (i1, i3) lowm + 2^h;
                 // stage t + 1 (span 2^h): (i0, i1), (i2, i3) share w_h
                 const int sh0 = s0 + t, sh1 = sh0 + 1;
                 const Fr wa = twid(lowm, r, sh0), wb = twid(lowm + (1u << h), r, sh0), wh = twid(lowm, r, sh1);
-                const Fr b0 = a0 + a2, b1 = a1 + a3;
-                const Fr b2 = (a0 - a2) * wa, b3 = (a1 - a3) * wb;
-                T.put(i0, b0 + b1);
-                T.put(i1, (b0 - b1) * wh);
-                T.put(i2, b2 + b3);
-                T.put(i3, (b2 - b3) * wh);
+                const Fr b0 = lz_add(a0, a2), b1 = lz_add(a1, a3);
+                const Fr b2 = lz_mul(lz_sub(a0, a2), wa), b3 = lz_mul(lz_sub(a1, a3), wb);
+                T.put(i0, lz_add(b0, b1));
+                T.put(i1, lz_mul(lz_sub(b0, b1), wh));
+                T.put(i2, lz_add(b2, b3));
+                T.put(i3, lz_mul(lz_sub(b2, b3), wh));
             }
         }
         __syncthreads();
@@ -447,7 +461,7 @@ __global__ void __launch_bounds__(NTT4_THREADS, 2) k_ntt_pass4(NttBatch B, const
     for (uint32_t idx = threadIdx.x; idx < elems; idx += blockDim.x) {
         uint32_t slot;
         const uint32_t addr = locate(idx, slot);
-        st(&a[addr], T.get(slot));
+        st(&a[addr], canon2p<FrCfg>(T.get(slot)));
     }
 }
 

@@ -133,3 +133,34 @@ def test_fp64_form_limbs():
     # the signed limb sums of a - b + K p stay far inside 64 bits
     assert 8 * P < 1 << 257
     assert sum(_p52(i) << (52 * i) for i in range(5)) == P
+
+
+def test_ntt_residues_below_2p():
+    """The radix-4 NTT pass keeps values in [0, 2p) (field.cuh: mont_mul_f64_lazy,
+    add2p, sub2p, canon2p): for both BN254 moduli a product of operands below
+    2p leaves (16 a b + Q p) / 2^260 < (64 p / 2^260 + 1) p < 1.76 p < 2p
+    (Q < 2^260), a sum of two such values is below 4p < 2^256 (no carry out of
+    the 8 words), one subtraction of 2p brings a sum or a borrowed difference
+    back below 2p, and one subtraction of p makes a value below 2p canonical.
+    Exhaustive over the interval ends with exact integers."""
+    r = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+    for m in (P, r):
+        assert Q(64 * m, 1 << 260) + 1 < Q(176, 100)
+        assert 4 * m < 1 << 256
+        two = 2 * m
+        words = [(two >> (32 * w)) & 0xFFFFFFFF for w in range(8)]
+        # m2word<C>(w): (m_w << 1) | (m_{w-1} >> 31), as the device computes it
+        mw = [(m >> (32 * w)) & 0xFFFFFFFF for w in range(8)]
+        dev = [((mw[w] << 1) & 0xFFFFFFFF) | (mw[w - 1] >> 31 if w else 0) for w in range(8)]
+        assert dev == words
+        for a in (0, 1, m - 1, m, two - 1):
+            for b in (0, 1, m - 1, m, two - 1):
+                s = a + b
+                assert s < 1 << 256
+                s = s - two if s >= two else s
+                assert 0 <= s < two and s % m == (a + b) % m
+                d = a - b
+                d = d + two if d < 0 else d
+                assert 0 <= d < two and d % m == (a - b) % m
+            c = a - m if a >= m else a
+            assert 0 <= c < m and c == a % m
