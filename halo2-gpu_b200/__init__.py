@@ -206,6 +206,7 @@ _SIGS = {
     "h2b_random_fr": (RustError, [_vp, _u64, _u64, ctypes.c_int, _vp]),
     "h2b_powers": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_fibonacci_fr": (RustError, [_vp, _u64, _vp, _vp]),
+    "h2b_gather_fr": (RustError, [_vp, _vp, _u64, _vp, _u64, _vp]),
     "h2b_srs_from_powers": (RustError, [_vp, _vp, _u64, _vp, _vp]),
     "h2b_prof_enable": (None, [ctypes.c_int]),
     "h2b_prof_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
@@ -775,6 +776,19 @@ def fibonacci_device(s0, s1, n, stream=None):
     seeds = np.concatenate([_scalar_bytes(s0), _scalar_bytes(s1)])
     call("h2b_fibonacci_fr", ptr(d), n, ptr(to_dev(seeds, stream)), stream_handle(stream))
     return d
+
+
+def gather_fr_device(d_table, d_idx, stream=None):
+    """out[i] = table[idx[i]] for 32-byte elements (h2b_gather_fr); d_idx is a
+    device int64 tensor, indices outside the table give zero."""
+    torch = _torch()
+    idx = d_idx.contiguous()
+    if idx.dtype != torch.int64:
+        raise TypeError("gather_fr_device: indices must be int64")
+    n = idx.numel()
+    out = dev_empty(32 * n)
+    call("h2b_gather_fr", ptr(out), ptr(d_table), d_table.numel() // 32, ptr(idx), n, stream_handle(stream))
+    return out
 
 
 def srs_device(tau, n, stream=None):

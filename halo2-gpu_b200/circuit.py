@@ -239,12 +239,14 @@ def synthesize(h2b, pk, seed, stream=None):
         bi = torch.randint(0, TABLE_SIZE, (n,), device="cuda", generator=gen)
         ai[:NUM_PUBLIC] = torch.from_numpy(public).cuda()
         bi[pk.b_rows] = ai[pk.a_rows]
-        a = pk.small[ai]
-        b = pk.small[bi]
-        c = pk.c_table[ai * TABLE_SIZE + bi]
+        # the small values and c = QA a + QB b + QM a b + K come from tables of
+        # their Montgomery images by the library's row gather
+        a = h2b.gather_fr_device(pk.small, ai, st)
+        b = h2b.gather_fr_device(pk.small, bi, st)
+        c = h2b.gather_fr_device(pk.c_table, ai * TABLE_SIZE + bi, st)
         d = h2b.dev_empty(32 * n)
         h2b.call("h2b_fibonacci_fr", h2b.ptr(d), n, h2b.ptr(h2b.to_dev(fib_seeds, st)), h2b.stream_handle(st))
-        adv = [a.reshape(-1), b.reshape(-1), c.reshape(-1), d]
+        adv = [a, b, c, d]
         for i, col in enumerate(adv):
             col[32 * u:] = h2b.random_fr_device(n - u, (seed << 3) + i, 0, st)
         inst = torch.zeros(32 * n, dtype=torch.uint8, device="cuda")

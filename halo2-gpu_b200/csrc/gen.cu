@@ -11,6 +11,9 @@
 //    with F the Fibonacci numbers mod r, so each thread reaches its chunk
 //    start by fast doubling (F(2m) = F(m)(2F(m+1) - F(m)),
 //    F(2m+1) = F(m)^2 + F(m+1)^2) and then steps the recurrence.
+//  * h2b_gather_fr: out[i] = table[idx[i]] for 32-byte field elements (a
+//    witness column drawn from a table of values); an index outside the
+//    table gives zero.
 //  * h2b_srs_from_powers: out[i] = [s_i] G as affine points for Montgomery
 //    scalars s_i, by fixed-base double-and-add over a caller-supplied table
 //    of affine 2^j G (j < 256), then one inversion per point.  With
@@ -154,6 +157,34 @@ extern "C" RustError h2b_fibonacci_fr(void* d_out, uint64_t n, const void* d_see
     uint64_t nthreads = (n + FIB_CHUNK - 1) / FIB_CHUNK;
     k_fibonacci<<<grid_for(nthreads, 128, 148u * 16u), 128, 0, stream>>>((Fr*)d_out, n, (const Fr*)d_seeds);
     H2B_LAUNCHED("k_fibonacci");
+    return ok();
+}
+
+// One element per thread, two 16-byte loads and stores: HBM-bound.
+__global__ void k_gather_fr(uint4* __restrict__ out, const uint4* __restrict__ table, uint64_t table_len,
+                            const int64_t* __restrict__ idx, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const int64_t j = idx[i];
+        uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+        if (j >= 0 && (uint64_t)j < table_len) {
+            lo = __ldg(&table[2 * j]);
+            hi = __ldg(&table[2 * j + 1]);
+        }
+        out[2 * i] = lo;
+        out[2 * i + 1] = hi;
+    }
+}
+
+extern "C" RustError h2b_gather_fr(void* d_out, const void* d_table, uint64_t table_len, const int64_t* d_idx,
+                                   uint64_t n, cudaStream_t stream)
+{
+    if (n == 0) return ok();
+    if (!d_out || !d_idx || (table_len && !d_table))
+        return err(cudaErrorInvalidValue, "h2b_gather_fr: null pointer");
+    k_gather_fr<<<grid_for(n, 256, 148u * 16u), 256, 0, stream>>>((uint4*)d_out, (const uint4*)d_table, table_len,
+                                                                  d_idx, n);
+    H2B_LAUNCHED("k_gather_fr");
     return ok();
 }
 

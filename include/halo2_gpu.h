@@ -537,6 +537,52 @@ int32_t h2b_tune_set(uint32_t param, uint32_t log_n, int32_t value);
 int32_t h2b_tune_get(uint32_t param, uint32_t log_n);
 void h2b_tune_clear(void);
 
+/* ---------------------------------------- synthetic inputs (no reference counterpart) --- */
+
+/* n Montgomery Fr from a seed: mix 0 uniform, mix 1 the witness-like mix of the k = 22 MSM
+ * workload (50 % uniform, 30 % uniform below 2^64, 20 % in {0, 1}). */
+RustError h2b_random_fr(void* d_out, uint64_t n, uint64_t seed, int mix, h2b_stream_t stream);
+/* out[i] = x^i for i < n (d_x: one device Fr). */
+RustError h2b_powers(void* d_out, uint64_t n, const void* d_x, h2b_stream_t stream);
+/* out[i] = [s_i] G (affine, 64 B) for n device scalars, by fixed-base double-and-add over the
+ * caller's device table of 2^j G, j < 256; with s_i = tau^i the synthetic KZG SRS
+ * (unsafe_setup_with_s, halo2_proofs/src/poly/kzg/commitment.rs:132-200). */
+RustError h2b_srs_from_powers(void* d_out, const void* d_scalars, uint64_t n, const void* d_table256,
+                              h2b_stream_t stream);
+/* out[0] = s0, out[1] = s1, out[i + 2] = out[i + 1] + out[i] (d_seeds: two device Fr): the
+ * witness of a Fibonacci rotation gate. */
+RustError h2b_fibonacci_fr(void* d_out, uint64_t n, const void* d_seeds, h2b_stream_t stream);
+/* out[i] = table[idx[i]] for 32-byte elements (idx: n device int64); an index outside
+ * [0, table_len) gives zero.  A witness column drawn from a table of values. */
+RustError h2b_gather_fr(void* d_out, const void* d_table, uint64_t table_len, const int64_t* d_idx, uint64_t n,
+                        h2b_stream_t stream);
+
+/* ------------------------------------- measurement hooks (no reference counterpart) --- */
+
+/* MSM window width the built-in plan takes for n plain bases. */
+int h2b_msm_window_bits(uint64_t n);
+/* Nonzero signed digits (= sorted bucket entries) of the plain MSM of n device scalars, as one
+ * device uint64 at d_count. */
+RustError h2b_msm_count_entries(const void* d_scalars, uint64_t n, void* d_count, h2b_stream_t stream);
+/* Kernel launches this library has issued in the process. */
+uint64_t h2b_launch_count(void);
+/* CUDA-event timing of instrumented phases (id 0 MSM accumulation, 1 MSM total, 2 NTT passes,
+ * 3 batch inversion, 4 quotient, 5 permute-sort): enable, then read the summed ms and count. */
+void h2b_prof_enable(int on);
+int h2b_prof_read(int id, double* total_ms, int* count);
+/* Throughput probes: independent mad.lo / mad.hi chains, and four independent field products per
+ * thread in registers (the product-rate reference of the rooflines); d_sink receives results. */
+RustError h2b_probe_imad(int blocks, int threads, int iters, void* d_sink, h2b_stream_t stream);
+RustError h2b_probe_modmul(int blocks, int threads, int iters, void* d_sink, h2b_stream_t stream);
+/* out[i] = a[i] * b[i] with product implementation `impl` (tests: 0-2 Fr CIOS lo/hi, CIOS wide,
+ * 29-bit; 3 Fr square; 4 Fq product; 5 Fq square; 6 Fr, 7 Fq with the FP64 form). */
+RustError h2b_fr_mul_batch(int impl, const void* d_a, const void* d_b, void* d_out, uint64_t n,
+                           h2b_stream_t stream);
+/* MSM accumulation: prefetch into L2 the point this many sorted entries ahead (0..64, default 2;
+ * 0 turns it off).  Same results. */
+void h2b_msm_set_prefetch(int distance);
+int h2b_msm_get_prefetch(void);
+
 /* No counterpart in the reference.  Batch inversion with the semantics of
  * _halo2_batch_invert (in place, zeros stay zero, field_type 0 = Fr, 1 = Fq)
  * for callers that cannot allocate device memory: it keeps the scratch-free

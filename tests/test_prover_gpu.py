@@ -80,6 +80,24 @@ def test_fibonacci_generator(h2b):
 
 
 @pytest.mark.gpu
+def test_gather_rows(h2b):
+    """h2b_gather_fr: out[i] = table[idx[i]] for 32-byte rows; indices outside
+    the table (negative, equal to or past its length) give zero rows."""
+    import torch
+    rng = np.random.default_rng(5)
+    table = rng.integers(0, 256, (300, 32), dtype=np.uint8)
+    idx = rng.integers(0, 300, 100003).astype(np.int64)
+    idx[[0, 7, 99]] = [-1, 300, 1 << 40]
+    out = h2b.gather_fr_device(torch.from_numpy(table).cuda(), torch.from_numpy(idx).cuda())
+    want = np.zeros((idx.size, 32), np.uint8)
+    ok = (idx >= 0) & (idx < 300)
+    want[ok] = table[idx[ok]]
+    assert np.array_equal(out.cpu().numpy().reshape(-1, 32), want)
+    with pytest.raises(TypeError):
+        h2b.gather_fr_device(torch.from_numpy(table).cuda(), torch.zeros(4, dtype=torch.int32, device="cuda"))
+
+
+@pytest.mark.gpu
 def test_synthesised_witness_satisfies_the_circuit(h2b):
     """Gates on every row, copies on every wired cell, lookup inputs inside
     the table on the usable rows, the public inputs in the instance column:
