@@ -1075,6 +1075,18 @@ __device__ __noinline__ Fp<C> mont_sqr_outline(const Fp<C> a)
     return mont_sqr_sel<C>(a);
 }
 
+// a b 2^-256 mod p in [0, 2p) for a, b < 2p, out of line (residues in [0, 2p)
+// above; the 29-bit build returns the canonical product, which is below 2p too)
+template <class C>
+__device__ __noinline__ Fp<C> mont_mul_lazy_outline(const Fp<C> a, const Fp<C> b)
+{
+#if H2B_MUL_F64
+    return mont_mul_f64_lazy<C>(a, b);
+#else
+    return mont_mul_sel<C>(a, b);
+#endif
+}
+
 template <class C>
 H2B_DEV Fp<C> operator*(const Fp<C>& a, const Fp<C>& b)
 {

@@ -1035,8 +1035,8 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     prof_begin(PROF_MSM_ACCUMULATE, st);
     // pairing rounds: sorted entries -> pts[0] -> pts[1] -> pts[0]
     const uint32_t* off = s.offsets;
-    const G1Affine* src = d_bases;
 #if H2B_EXPERIMENTS
+    const G1Affine* src = d_bases;
     for (int r = 1; r <= p.R; r++) {
         k_msm_half_counts<<<grid_for(p.NB, 256, sm_cap), 256, 0, st>>>(off, p.NB, s.counts);
         H2B_LAUNCHED("k_msm_half_counts");

@@ -776,6 +776,14 @@ struct FusedParams {
     uint32_t gate_ops, gate_vps, n_sets, chunk_len, n_pcols, n_lookups, has_scale, pad;
 };
 
+// The fused pass keeps its intermediates in [0, 2p): products without their
+// closing subtraction, sums and differences corrected by 2p, the row's value
+// made canonical once before the store (field.cuh, residues in [0, 2p)).
+// Columns, constants and scalars enter canonical.
+__device__ __forceinline__ Fr zm(const Fr& a, const Fr& b) { return mont_mul_lazy_outline<FrCfg>(a, b); }
+__device__ __forceinline__ Fr za(const Fr& a, const Fr& b) { return add2p<FrCfg>(a, b); }
+__device__ __forceinline__ Fr zs(const Fr& a, const Fr& b) { return sub2p<FrCfg>(a, b); }
+
 __device__ __forceinline__ Fr fq_fetch(const FusedParams& P, const Fr* slot, uint8_t src, uint32_t idx, uint64_t rot,
                                        uint64_t row)
 {
@@ -805,11 +813,11 @@ __device__ __forceinline__ Fr fq_run(const FusedParams& P, Fr* slot, uint32_t i0
         Fr res;
         switch (kind) {
         case OP_COPY: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row); break;
-        case OP_ADD: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) + fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
-        case OP_SUB: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) - fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
-        case OP_MUL: res = fq_fetch(P, slot, op.sa, op.ia, op.ra, row) * fq_fetch(P, slot, op.sb, op.ib, op.rb, row); break;
-        case OP_NEG: res = fneg(fq_fetch(P, slot, op.sa, op.ia, op.ra, row)); break;
-        case OP_DBL: res = fdbl(fq_fetch(P, slot, op.sa, op.ia, op.ra, row)); break;
+        case OP_ADD: res = za(fq_fetch(P, slot, op.sa, op.ia, op.ra, row), fq_fetch(P, slot, op.sb, op.ib, op.rb, row)); break;
+        case OP_SUB: res = zs(fq_fetch(P, slot, op.sa, op.ia, op.ra, row), fq_fetch(P, slot, op.sb, op.ib, op.rb, row)); break;
+        case OP_MUL: res = zm(fq_fetch(P, slot, op.sa, op.ia, op.ra, row), fq_fetch(P, slot, op.sb, op.ib, op.rb, row)); break;
+        case OP_NEG: res = zs(Fr::zero(), fq_fetch(P, slot, op.sa, op.ia, op.ra, row)); break;
+        case OP_DBL: { const Fr x = fq_fetch(P, slot, op.sa, op.ia, op.ra, row); res = za(x, x); } break;
         default: res = Fr::zero();
         }
         slot[op.dst] = res;
@@ -818,7 +826,7 @@ __device__ __forceinline__ Fr fq_run(const FusedParams& P, Fr* slot, uint32_t i0
 #pragma unroll 1
     for (uint32_t i = v0; i < v1; i++) {
         const QVp v = P.vps[i];
-        val = val * P.y + (v.is_const ? P.consts[v.idx] : slot[v.idx]);
+        val = za(zm(val, P.y), v.is_const ? P.consts[v.idx] : slot[v.idx]);
     }
     return val;
 }
@@ -839,7 +847,7 @@ __global__ void __launch_bounds__(FQ_THREADS, MINB) k_quotient_fused(const __gri
     if (r >= rows) return;
     // X-dependent factor of the identity permutation on this thread's first
     // row, ext_omega * omega^row
-    Fr bt = P.n_sets ? P.ext_omega * fpow_u64(P.omega, row_start + r) : one;
+    Fr bt = P.n_sets ? P.ext_omega * fpow_u64(P.omega, row_start + r) : one;   // canonical
     for (; r < rows; r += step) {
         const uint64_t row = row_start + r;
         Fr v = fq_run(P, slot, 0, P.gate_ops, 0, P.gate_vps, row);
@@ -849,13 +857,13 @@ __global__ void __launch_bounds__(FQ_THREADS, MINB) k_quotient_fused(const __gri
             if (rl >= P.isize) rl -= P.isize;
             const Fr l0v = ld(&P.l0[row]);
             const Fr z0 = ld(&P.prods[0][row]);
-            v = v * P.y + (one - z0) * l0v;
+            v = za(zm(v, P.y), zm(zs(one, z0), l0v));
             const Fr zl = P.n_sets == 1 ? z0 : ld(&P.prods[P.n_sets - 1][row]);
-            v = v * P.y + (zl * zl - zl) * ld(&P.l_last[row]);
+            v = za(zm(v, P.y), zm(zs(zm(zl, zl), zl), ld(&P.l_last[row])));
             for (uint32_t s = 1; s < P.n_sets; s++)
-                v = v * P.y + (ld(&P.prods[s][row]) - ld(&P.prods[s - 1][rl])) * l0v;
+                v = za(zm(v, P.y), zm(zs(ld(&P.prods[s][row]), ld(&P.prods[s - 1][rl])), l0v));
             const Fr la = ld(&P.l_active[row]);
-            Fr cur = P.delta_start * bt;
+            Fr cur = zm(P.delta_start, bt);
             for (uint32_t s = 0; s < P.n_sets; s++) {
                 const uint32_t c0 = s * P.chunk_len;
                 const uint32_t c1 = c0 + P.chunk_len < P.n_pcols ? c0 + P.chunk_len : P.n_pcols;
@@ -863,11 +871,11 @@ __global__ void __launch_bounds__(FQ_THREADS, MINB) k_quotient_fused(const __gri
                 Fr right = ld(&P.prods[s][row]);
                 for (uint32_t c = c0; c < c1; c++) {
                     const Fr cv = ld(&P.pcols[c][row]);
-                    left = left * (cv + P.beta * ld(&P.sigmas[c][row]) + P.gamma);
-                    right = right * (cv + cur + P.gamma);
-                    cur = cur * P.delta;
+                    left = zm(left, za(za(cv, zm(P.beta, ld(&P.sigmas[c][row]))), P.gamma));
+                    right = zm(right, za(za(cv, cur), P.gamma));
+                    cur = zm(cur, P.delta);
                 }
-                v = v * P.y + (left - right) * la;
+                v = za(zm(v, P.y), zm(zs(left, right), la));
             }
             bt = bt * wstep;
         }
@@ -879,16 +887,16 @@ __global__ void __launch_bounds__(FQ_THREADS, MINB) k_quotient_fused(const __gri
                 const FqLookup& L = P.lk[l];
                 const Fr tv = fq_run(P, slot, L.op0, L.op1, L.vp0, L.vp1, row);
                 const Fr zi = ld(&L.z[row]), a = ld(&L.pin[row]), s = ld(&L.ptab[row]);
-                const Fr ams = a - s;
-                v = v * P.y + (one - zi) * l0v;
-                v = v * P.y + (zi * zi - zi) * llast;
-                v = v * P.y + (ld(&L.z[nx]) * (a + L.beta) * (s + L.gamma) - zi * tv) * la;
-                v = v * P.y + ams * l0v;
-                v = v * P.y + ams * (a - ld(&L.pin[pv])) * la;
+                const Fr ams = zs(a, s);
+                v = za(zm(v, P.y), zm(zs(one, zi), l0v));
+                v = za(zm(v, P.y), zm(zs(zm(zi, zi), zi), llast));
+                v = za(zm(v, P.y), zm(zs(zm(zm(ld(&L.z[nx]), za(a, L.beta)), za(s, L.gamma)), zm(zi, tv)), la));
+                v = za(zm(v, P.y), zm(ams, l0v));
+                v = za(zm(v, P.y), zm(zm(ams, zs(a, ld(&L.pin[pv]))), la));
             }
         }
-        if (P.has_scale) v = v * P.scale;
-        st(&P.out[r * P.out_stride + P.out_offset], v);
+        if (P.has_scale) v = zm(v, P.scale);
+        st(&P.out[r * P.out_stride + P.out_offset], canon2p<FrCfg>(v));
     }
 }
 
