@@ -851,7 +851,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-jobs section")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-prover section")
     ap.add_argument("--case", choices=["msm", "ntt", "bi", "serve", "probe", "rows", "batch", "permute", "quotient",
-                                       "prove"],
+                                       "prove", "table_widths"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")
@@ -885,6 +885,47 @@ def main():
         loads = tuple(float(x) for x in args.loads.split(","))
         print(json.dumps({"case": "serve", "serving": serving_section(load_pkg(), torch, count=args.requests,
                                                                       loads=loads)}))
+        return
+    if args.case == "table_widths":
+        # MSMs over window tables of 2^10..2^20 points built at each window
+        # width 10..18 (uniform and witness-mix scalars at the table's size,
+        # uniform at 1/16 of it); outputs must agree across widths
+        import hashlib
+        import torch
+        torch.cuda.set_device(0)
+        h2b = load_pkg()
+        L = h2b.lib()
+        out_rows = {}
+        for lg in range(10, 21):
+            tn = 1 << lg
+            srs = h2b.srs_device(0x7AB1E + lg, tn)
+            scs = {(tn, 1): h2b.random_fr_device(tn, 60 + lg, 1), (tn, 0): h2b.random_fr_device(tn, 70 + lg, 0),
+                   (max(tn >> 4, 1), 0): h2b.random_fr_device(max(tn >> 4, 1), 80 + lg, 0)}
+            ref = {}
+            for c in (10, 12, 13, 14, 15, 16, 17, 18):
+                L.h2b_msm_set_tuning(c, 0)
+                table = h2b.msm_table_precompute(srs, tn)
+                row = {}
+                for (n, mix), sc in scs.items():
+                    out = h2b.dev_empty(96)
+                    ws = h2b.dev_empty(L.h2b_msm_table_workspace_size(n, tn))
+                    for _ in range(2):
+                        h2b.msm_device_table(sc, table, tn, out, n, ws=ws)
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    for _ in range(5):
+                        h2b.msm_device_table(sc, table, tn, out, n, ws=ws)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    key = f"n=2^{n.bit_length() - 1} {'mix' if mix else 'uniform'}"
+                    digest = hashlib.sha256(out.cpu().numpy().tobytes()).hexdigest()
+                    ref.setdefault(key, digest)
+                    row[key] = {"ms": round(e0.elapsed_time(e1) / 5, 3), "same": digest == ref[key]}
+                out_rows[f"2^{lg} table, c={c}"] = row
+                del table
+            L.h2b_msm_set_tuning(0, 0)
+        print(json.dumps({"case": "table_widths", "rows": out_rows}))
         return
     if args.case == "prove":
         # config-3 proofs at 2^log_n one after another (transcript on), for

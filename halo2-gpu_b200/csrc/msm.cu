@@ -106,11 +106,16 @@ static int choose_c(uint64_t n, bool plain = false)
         if (lg >= 10) return 10;
         return 7;
     }
-    // window tables keep the widths their layout was measured with
-    if (lg >= 21) return 16;
-    if (lg >= 19) return 15;
-    if (lg >= 17) return 13;
-    if (lg >= 14) return 12;
+    // Window tables: every window's digits land in one bucket set of 2^(c-1)
+    // buckets, so a narrow window makes long buckets (2^18 points at 13 bits:
+    // about 1300 entries per bucket, nearly all taking the dense-bucket path).
+    // Widths from a sweep of c in 10..18 on B200 (bench.py --case
+    // table_widths; uniform / witness-mix scalars, n = table size): 2^18
+    // table 11.57 / 3.07 ms at 13 bits -> 1.80 / 1.48 ms at 16, 2^20 6.32 /
+    // 4.64 ms at 15 -> 4.91 / 3.46 ms at 16, 2^16 4.48 / 1.20 ms at 12 ->
+    // 1.02 / 0.85 ms at 13.
+    if (lg >= 17) return 16;
+    if (lg >= 13) return 13;
     if (lg >= 10) return 10;
     return 7;
 }
