@@ -107,8 +107,8 @@ static int choose_c(uint64_t n, bool plain = false)
         return 7;
     }
     // Window tables: every window's digits land in one bucket set of 2^(c-1)
-    // buckets, so a narrow window makes long buckets (2^18 points at 13 bits:
-    // about 1300 entries per bucket, nearly all taking the dense-bucket path).
+    // buckets, so a narrow window makes few, long buckets (2^18 points at 13
+    // bits: 4096 buckets of about 1300 entries).
     // Widths from a sweep of c in 10..18 on B200 (bench.py --case
     // table_widths; uniform / witness-mix scalars, n = table size): 2^18
     // table 11.57 / 3.07 ms at 13 bits -> 1.80 / 1.48 ms at 16, 2^20 6.32 /
