@@ -102,3 +102,25 @@ def test_twiddle_preflights_and_argument_errors(h2b, built_lib):
     # the decode hook has no outputs and accepts any rule list
     rules = np.zeros(4, np.uint64)
     L._halo2_quotient_decode(rules.ctypes.data, 2, 1 << 10, 1, 0, 1 << 10)
+
+
+def test_window_table_layouts(h2b, built_lib):
+    """A window table holds 2 W tn points (W slices of 2^(c w) P and their
+    endomorphism images); the width c follows the table size: 10 bits up to
+    2^12 points, 13 bits from 2^13, 16 bits from 2^17 (one shared bucket set
+    per table, so narrow windows make long buckets).  W covers the 127-bit
+    GLV halves with room for the top digit's carry.  Pure host: the layout
+    preflight and the MSM's window width for plain bases."""
+    L = built_lib
+    L.h2b_msm_table_points.restype = ctypes.c_uint64
+    L.h2b_msm_table_points.argtypes = [ctypes.c_uint64]
+
+    def windows(c):
+        w = (127 + c - 1) // c
+        return w + 1 if 127 - c * (w - 1) > c - 1 else w
+
+    for lg, c in ((10, 10), (12, 10), (13, 13), (16, 13), (17, 16), (20, 16), (22, 16)):
+        tn = 1 << lg
+        assert L.h2b_msm_table_points(tn) == 2 * windows(c) * tn, (lg, c)
+    assert windows(10) == 13 and windows(13) == 10 and windows(16) == 8
+    assert L.h2b_msm_table_points(1 << 28) == 0          # entries must stay 31-bit
