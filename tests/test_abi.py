@@ -124,3 +124,55 @@ def test_window_table_layouts(h2b, built_lib):
         assert L.h2b_msm_table_points(tn) == 2 * windows(c) * tn, (lg, c)
     assert windows(10) == 13 and windows(13) == 10 and windows(16) == 8
     assert L.h2b_msm_table_points(1 << 28) == 0          # entries must stay 31-bit
+
+
+def test_fused_quotient_and_merged_msm_reject_on_the_host(h2b, built_lib):
+    """h2b_quotient_fused and h2b_msm_merged check their arguments before any
+    device work: each bad call below returns cudaErrorInvalidValue with a
+    message (device pointers are stand-ins and never dereferenced)."""
+    import numpy as np
+    L = built_lib
+    fake = [ctypes.c_void_p(0x10000 + 0x1000 * i) for i in range(70)]
+    cols = (ctypes.c_void_p * 70)(*fake)
+    y = np.zeros(4, np.uint64)
+    rules = np.zeros(2, np.uint64)                        # one OP_ZERO rule
+    vp = np.array([3 | (0 << 4)], np.uint64)              # value part: intermediate 0
+    g = h2b.QuotientRules(rules.ctypes.data, 1, vp.ctypes.data, 1, None, 0, None, 0)
+
+    def fused(n_fixed=1, nq=1024, r0=0, r1=1024, gates=ctypes.byref(g), lookups=None, n_lookups=0, perm=None,
+              lag=True):
+        la = lookups if lookups is not None else (h2b.QuotientLookupArgs * 1)()
+        l = fake[60] if lag else None
+        return L.h2b_quotient_fused(cols, n_fixed, None, 0, None, 0, gates, y.ctypes.data, l, l, l, perm, la,
+                                    n_lookups, nq, 1, r0, r1, fake[61], 1, 0, None, None)
+
+    def bad(e, text):
+        assert e.code == 1, text
+        msg = ctypes.string_at(e.message).decode()
+        h2b._libc.free(e.message)
+        assert text in msg, msg
+
+    bad(fused(nq=0), "num_quotient is 0")
+    bad(fused(r0=10, r1=1025), "row range")
+    bad(fused(gates=None), "gates, y and out are required")
+    bad(fused(n_fixed=65), "more than 64 columns")
+    bad(fused(n_lookups=9, lookups=(h2b.QuotientLookupArgs * 9)()), "more than 8 lookups")
+    bad(fused(n_lookups=1, lag=False), "l0, l_last and l_active are required")
+    big_rules = np.zeros(2 * 300, np.uint64)
+    gbig = h2b.QuotientRules(big_rules.ctypes.data, 300, vp.ctypes.data, 1, None, 0, None, 0)
+    bad(fused(gates=ctypes.byref(gbig)), "parameter block")
+    pa = h2b.QuotientPermutationArgs(2, 1, 4, ctypes.addressof(cols), ctypes.addressof(cols), ctypes.addressof(cols),
+                                     *[y.ctypes.data] * 6, -6, 1, 1024, 0)
+    bad(fused(perm=ctypes.byref(pa)), "permutation shape")
+    # merged MSMs: one table, at most 64 jobs, each no longer than the table
+    jobs = (h2b.MsmJob * 2)()
+    for i in range(2):
+        jobs[i].d_scalars, jobs[i].d_bases, jobs[i].d_out, jobs[i].n, jobs[i].table_n = fake[i], fake[10], fake[20 + i], 8, 16
+    assert L.h2b_msm_merged_workspace_size(jobs, 2) > 0
+    jobs[1].d_bases = fake[11]
+    assert L.h2b_msm_merged_workspace_size(jobs, 2) == 0
+    bad(L.h2b_msm_merged(jobs, 2, fake[30], 1 << 30, None), "jobs must share one window table")
+    jobs[1].d_bases, jobs[1].n = fake[10], 17
+    bad(L.h2b_msm_merged(jobs, 2, fake[30], 1 << 30, None), "job longer than its table")
+    jobs[1].n = 8
+    bad(L.h2b_msm_merged(jobs, 2, fake[30], 16, None), "h2b_msm_merged")      # scratch too small
