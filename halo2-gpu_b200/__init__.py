@@ -207,6 +207,9 @@ _SIGS = {
     "h2b_powers": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_fibonacci_fr": (RustError, [_vp, _u64, _vp, _vp]),
     "h2b_gather_fr": (RustError, [_vp, _vp, _u64, _vp, _u64, _vp]),
+    "h2b_eval_many_workspace_size": (_u64, [_u64, _u64]),
+    "h2b_eval_many_device": (RustError, [_vp, _vp, _u64, _u64, _vp, _vp, _u64, _vp]),
+    "h2b_poly_linear_combination": (RustError, [_vp, _vp, _vp, _u64, _u64, ctypes.c_int, _vp]),
     "h2b_srs_from_powers": (RustError, [_vp, _vp, _u64, _vp, _vp]),
     "h2b_prof_enable": (None, [ctypes.c_int]),
     "h2b_prof_read": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
@@ -789,6 +792,33 @@ def gather_fr_device(d_table, d_idx, stream=None):
     out = dev_empty(32 * n)
     call("h2b_gather_fr", ptr(out), ptr(d_table), d_table.numel() // 32, ptr(idx), n, stream_handle(stream))
     return out
+
+
+def eval_many_device(d_polys, points, n, d_out=None, ws=None, stream=None):
+    """[p_i(z_i)] for up to 64 device polynomials of n coefficients
+    (h2b_eval_many_device); points are ints; returns the device results
+    (32 bytes each) without synchronising."""
+    count = len(d_polys)
+    pts = np.ascontiguousarray(fields.fr_mont_limbs([int(z) % fields.R_MOD for z in points]))
+    if d_out is None:
+        d_out = dev_empty(32 * count)
+    need = lib().h2b_eval_many_workspace_size(n, count)
+    if ws is None or ws.numel() < need:
+        ws = dev_empty(need)
+    call("h2b_eval_many_device", _ptr_table(d_polys), pts.ctypes.data, count, n, ptr(d_out), ptr(ws), ws.numel(),
+         stream_handle(stream))
+    return d_out
+
+
+def linear_combination_device(d_acc, d_polys, coeffs, n, accumulate=True, stream=None):
+    """acc = (acc if accumulate else 0) + sum_t coeffs[t] polys[t] over n
+    coefficients (h2b_poly_linear_combination; up to 64 terms; coefficients
+    are ints)."""
+    cs = np.ascontiguousarray(fields.fr_mont_limbs([int(c) % fields.R_MOD for c in coeffs])) if len(coeffs) else \
+        np.zeros((1, 4), np.uint64)
+    call("h2b_poly_linear_combination", ptr(d_acc), _ptr_table(d_polys), cs.ctypes.data, len(coeffs), n,
+         1 if accumulate else 0, stream_handle(stream))
+    return d_acc
 
 
 def srs_device(tau, n, stream=None):

@@ -71,8 +71,16 @@ static __device__ __forceinline__ Fr op_pow(const Fr* __restrict__ chain, uint64
 }
 
 // partial[b] = sum over the tile of a_i z^i (global exponents).
+static __device__ __forceinline__ void eval_partial_tile(const Fr* __restrict__ a, uint64_t n,
+                                                         const Fr* __restrict__ chain, Fr* __restrict__ partial);
 static __global__ void __launch_bounds__(EV_T) k_eval_partial(const Fr* __restrict__ a, uint64_t n,
                                                                const Fr* __restrict__ chain, Fr* __restrict__ partial)
+{
+    eval_partial_tile(a, n, chain, partial);
+}
+
+static __device__ __forceinline__ void eval_partial_tile(const Fr* __restrict__ a, uint64_t n,
+                                                         const Fr* __restrict__ chain, Fr* __restrict__ partial)
 {
     __shared__ Fr red[EV_T];
     const uint64_t base = blockIdx.x * EV_TILE;
@@ -95,8 +103,14 @@ static __global__ void __launch_bounds__(EV_T) k_eval_partial(const Fr* __restri
     if (c == 0) st(&partial[blockIdx.x], red[0]);
 }
 
+static __device__ __forceinline__ void eval_sum_block(const Fr* __restrict__ partial, uint64_t nb, Fr* __restrict__ out);
 static __global__ void __launch_bounds__(EV_T) k_eval_sum(const Fr* __restrict__ partial, uint64_t nb,
                                                            Fr* __restrict__ out)
+{
+    eval_sum_block(partial, nb, out);
+}
+
+static __device__ __forceinline__ void eval_sum_block(const Fr* __restrict__ partial, uint64_t nb, Fr* __restrict__ out)
 {
     __shared__ Fr red[EV_T];
     const int c = threadIdx.x;
@@ -117,6 +131,58 @@ static __global__ void k_op_madd(Fr* __restrict__ acc, const Fr* __restrict__ p,
     const Fr cc = ldg(c);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         st(&acc[i], ld(&acc[i]) + cc * ld(&p[i]));
+}
+
+// ---- many polynomials per launch (device polynomials of one length) --------
+
+constexpr int MANY_MAX = 64;
+struct EvMany {
+    const Fr* p[MANY_MAX];
+    Fr z[MANY_MAX];
+};
+struct LinTerms {
+    const Fr* p[MANY_MAX];
+    Fr c[MANY_MAX];
+};
+
+// chain[y CHAIN + i] = z_y^(2^i) (one thread per polynomial)
+static __global__ void k_op_chain_many(const __grid_constant__ EvMany E, Fr* __restrict__ chains)
+{
+    if (threadIdx.x != 0) return;
+    Fr c = E.z[blockIdx.x];
+    Fr* chain = chains + (uint64_t)blockIdx.x * CHAIN;
+    for (int i = 0; i < CHAIN; i++) {
+        st(&chain[i], c);
+        c = c * c;
+    }
+}
+
+// grid (tiles, polynomials): the tile partials of polynomial y
+static __global__ void __launch_bounds__(EV_T) k_eval_partial_many(const __grid_constant__ EvMany E, uint64_t n,
+                                                                    const Fr* __restrict__ chains,
+                                                                    Fr* __restrict__ partial, uint64_t nb)
+{
+    const uint32_t y = blockIdx.y;
+    eval_partial_tile(E.p[y], n, chains + (uint64_t)y * CHAIN, partial + (uint64_t)y * nb);
+}
+
+// block y: polynomial y's partials summed into out[y]
+static __global__ void __launch_bounds__(EV_T) k_eval_sum_many(const Fr* __restrict__ partial, uint64_t nb,
+                                                                Fr* __restrict__ out)
+{
+    eval_sum_block(partial + (uint64_t)blockIdx.x * nb, nb, out + blockIdx.x);
+}
+
+// acc[i] = (accumulate ? acc[i] : 0) + sum_t c_t p_t[i]: every polynomial
+// read once, the accumulator read and written once
+static __global__ void k_lin_comb(Fr* __restrict__ acc, const __grid_constant__ LinTerms L, uint32_t count,
+                                  uint64_t n, int accumulate)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        Fr s = accumulate ? ld(&acc[i]) : Fr::zero();
+        for (uint32_t t = 0; t < count; t++) s = s + L.c[t] * ld(&L.p[t][i]);
+        st(&acc[i], s);
+    }
 }
 
 // ---- Kate division ---------------------------------------------------------
@@ -542,5 +608,67 @@ extern "C" RustError _halo2_decode_assigned(void* d_nums, void* d_denoms, const 
     k_decode_assigned<<<grid_for(n, 256), 256, 0, stream>>>((Fr*)d_nums, (Fr*)d_denoms, (const uint8_t*)d_raw, n,
                                                             layout);
     H2B_LAUNCHED("k_decode_assigned");
+    return ok();
+}
+
+// ---------------------------------------------------------------------------
+// Many device polynomials per call (no counterpart in the reference, whose
+// batch evaluation and multiopen calculation stage HOST polynomial chunks;
+// a device-resident prover evaluates and combines its polynomials where they
+// are).  Up to 64 polynomials of n coefficients per call; points and
+// coefficients are host values carried in the kernel parameters.
+// ---------------------------------------------------------------------------
+
+extern "C" uint64_t h2b_eval_many_workspace_size(uint64_t n, uint64_t count)
+{
+    ScratchPlan sp;
+    sp.add_n<Fr>(std::max<uint64_t>(count, 1) * CHAIN);
+    sp.add_n<Fr>(std::max<uint64_t>(count, 1) * ev_blocks(n));
+    return sp.used;
+}
+
+extern "C" RustError h2b_eval_many_device(const void* const* d_polys, const void* points, uint64_t count, uint64_t n,
+                                          void* d_out, void* scratch, uint64_t scratch_bytes, cudaStream_t stream)
+{
+    if (count == 0) return ok();
+    if (count > (uint64_t)MANY_MAX) return err(cudaErrorInvalidValue, "h2b_eval_many_device: more than 64 polynomials");
+    if (n == 0 || !d_polys || !points || !d_out) return err(cudaErrorInvalidValue, "h2b_eval_many_device: bad arguments");
+    const uint64_t need = h2b_eval_many_workspace_size(n, count);
+    if (!scratch || scratch_bytes < need) return scratch_too_small("h2b_eval_many_device", scratch_bytes, need);
+    static thread_local EvMany E;
+    for (uint64_t i = 0; i < count; i++) {
+        if (!d_polys[i]) return err(cudaErrorInvalidValue, "h2b_eval_many_device: null polynomial");
+        E.p[i] = (const Fr*)d_polys[i];
+        memcpy(&E.z[i], (const char*)points + 32 * i, 32);
+    }
+    ScratchArena ar(scratch, scratch_bytes);
+    Fr* chains = ar.take_n<Fr>(count * CHAIN);
+    const uint64_t nb = ev_blocks(n);
+    Fr* partial = ar.take_n<Fr>(count * nb);
+    k_op_chain_many<<<(unsigned)count, 32, 0, stream>>>(E, chains);
+    H2B_LAUNCHED("k_op_chain_many");
+    k_eval_partial_many<<<dim3((unsigned)nb, (unsigned)count), EV_T, 0, stream>>>(E, n, chains, partial, nb);
+    H2B_LAUNCHED("k_eval_partial_many");
+    k_eval_sum_many<<<(unsigned)count, EV_T, 0, stream>>>(partial, nb, (Fr*)d_out);
+    H2B_LAUNCHED("k_eval_sum_many");
+    return ok();
+}
+
+extern "C" RustError h2b_poly_linear_combination(void* d_acc, const void* const* d_polys, const void* coeffs,
+                                                 uint64_t count, uint64_t n, int accumulate, cudaStream_t stream)
+{
+    if (n == 0) return ok();
+    if (count > (uint64_t)MANY_MAX)
+        return err(cudaErrorInvalidValue, "h2b_poly_linear_combination: more than 64 polynomials");
+    if (!d_acc || (count && (!d_polys || !coeffs)))
+        return err(cudaErrorInvalidValue, "h2b_poly_linear_combination: bad arguments");
+    static thread_local LinTerms T;
+    for (uint64_t t = 0; t < count; t++) {
+        if (!d_polys[t]) return err(cudaErrorInvalidValue, "h2b_poly_linear_combination: null polynomial");
+        T.p[t] = (const Fr*)d_polys[t];
+        memcpy(&T.c[t], (const char*)coeffs + 32 * t, 32);
+    }
+    k_lin_comb<<<grid_for(n, 256, 148u * 16u), 256, 0, stream>>>((Fr*)d_acc, T, (uint32_t)count, n, accumulate);
+    H2B_LAUNCHED("k_lin_comb");
     return ok();
 }

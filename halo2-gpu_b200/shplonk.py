@@ -92,12 +92,14 @@ class Shplonk:
         return ws[off:off + 32]
 
     def eval_many(self, items):
-        """[p(x) for (p, x) in items] as ints, with one synchronisation."""
+        """[p(x) for (p, x) in items] as ints: up to 64 evaluations per
+        h2b_eval_many_device call, one synchronisation."""
         if not items:
             return []
-        views = [self.eval_device(d, x) for d, x in items]
         torch = __import__("torch")
-        packed = torch.cat(views).cpu().numpy().view("<u8").reshape(-1, 4)
+        outs = [self.h2b.eval_many_device([d for d, _ in items[i:i + 64]], [x for _, x in items[i:i + 64]], self.n,
+                                          stream=self.st) for i in range(0, len(items), 64)]
+        packed = torch.cat(outs).cpu().numpy().view("<u8").reshape(-1, 4)
         return F.fr_from_mont_limbs(packed)
 
     def eval(self, d_poly, x):
@@ -106,8 +108,14 @@ class Shplonk:
 
     def madd(self, d_acc, d_in, c):
         """acc += c * in over n coefficients."""
-        self.h2b.call("_halo2_poly_multiply_add", self.h2b.ptr(d_acc), self.h2b.ptr(d_in),
-                      self.h2b.ptr(self._scalar(c)), self.n, self.sh)
+        self.combine(d_acc, [d_in], [c])
+
+    def combine(self, d_acc, d_polys, coeffs, accumulate=True):
+        """acc = (acc if accumulate else 0) + sum_t coeffs[t] polys[t], one
+        pass per 64 terms (h2b_poly_linear_combination)."""
+        for i in range(0, max(len(d_polys), 1), 64):
+            self.h2b.linear_combination_device(d_acc, d_polys[i:i + 64], coeffs[i:i + 64], self.n,
+                                               accumulate=accumulate or i > 0, stream=self.st)
 
     def sub_short(self, d_acc, coeffs):
         d = self.h2b.to_dev(F.fr_mont_limbs([c % P for c in coeffs]), self.st)
@@ -156,13 +164,12 @@ def open_queries(h2b, queries, challenges, commit, stream=None, on_evals=None):
     lin_terms = []
     for i, (pts, keys) in enumerate(sets.items()):
         num = bufs[0]
-        num.zero_()
         short = [0] * len(pts)
         for j, key in enumerate(keys):
             yj = pow(y, j, P)
-            sp.madd(num, polys[key], yj)
             r = _interpolate(list(pts), [point_sets[key][x] for x in pts])
             short = [(a + yj * b) % P for a, b in zip(short, r)]
+        sp.combine(num, [polys[key] for key in keys], [pow(y, j, P) for j in range(len(keys))], accumulate=False)
         sp.sub_short(num, short)
         cur, other = bufs
         for pt in pts:                   # divide by (X - s) for every point of the set
@@ -179,14 +186,18 @@ def open_queries(h2b, queries, challenges, commit, stream=None, on_evals=None):
     lin_terms = [(keys, vi * _vanishing_at(diff, u) * z0_diff_inv % P, _eval_host(short, u))
                  for keys, vi, diff, short in lin_terms]
     # L / Z_{T\S_0}(u) = sum_i v^i Z_{T\S_i}(u) / Z_{T\S_0}(u) sum_j y^j (p_ij - r_ij(u)) - Z_{S_0}(u) h
-    lx = sp.zeros()
+    lx = h2b.dev_empty(32 * n)
     const = 0
+    terms, coeffs = [], []
     for keys, c_i, r_at_u in lin_terms:
         for j, key in enumerate(keys):
-            sp.madd(lx, polys[key], c_i * pow(y, j, P))
+            terms.append(polys[key])
+            coeffs.append(c_i * pow(y, j, P))
         const = (const + c_i * r_at_u) % P
+    terms.append(h)
+    coeffs.append(-_vanishing_at(list(sets)[0], u))
+    sp.combine(lx, terms, coeffs, accumulate=False)
     h2b.call("_halo2_poly_sub_scalar_at_zero", h2b.ptr(lx), h2b.ptr(sp._scalar(const)), sp.sh)
-    sp.madd(lx, h, -_vanishing_at(list(sets)[0], u))
     l_at_u = sp.eval(lx, u)
     q = sp.zeros()
     sp.div_linear(lx, q, u)

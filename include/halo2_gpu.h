@@ -187,6 +187,18 @@ RustError _halo2_kate_division_device(const void* d_a, void* d_q, const void* d_
 RustError _halo2_kate_division_device_padded(const void* d_a, void* d_q, const void* d_u, uint64_t n,
                                              uint64_t out_len, void* scratch, uint64_t scratch_bytes,
                                              h2b_stream_t stream);
+/* No counterpart in the reference (its batch evaluation and multiopen calculation stage HOST polynomial
+ * chunks): out[i] = sum_j polys[i][j] points[i]^j for count <= 64 DEVICE polynomials of n coefficients
+ * (host array of device pointers, host 32-byte points), device outputs (count x 32 B), scratch of
+ * h2b_eval_many_workspace_size(n, count) bytes; one launch sequence for all, no synchronisation. */
+uint64_t h2b_eval_many_workspace_size(uint64_t n, uint64_t count);
+RustError h2b_eval_many_device(const void* const* d_polys, const void* points, uint64_t count, uint64_t n,
+                               void* d_out, void* scratch, uint64_t scratch_bytes, h2b_stream_t stream);
+/* No counterpart in the reference: acc[i] = (accumulate ? acc[i] : 0) + sum_t coeffs[t] polys[t][i] for
+ * i < n, count <= 64 device polynomials (host array of device pointers, host 32-byte coefficients), one
+ * pass over memory, no scratch, no synchronisation. */
+RustError h2b_poly_linear_combination(void* d_acc, const void* const* d_polys, const void* coeffs, uint64_t count,
+                                      uint64_t n, int accumulate, h2b_stream_t stream);
 /* culib.rs:401-405 ; multiopen.cu:30-45 */
 uint64_t _halo2_multiopen_poly_max_len(uint64_t poly_length, uint64_t batch_size, uint64_t free_bytes);
 /* culib.rs:407-410 ; multiopen.cu:47-53 */

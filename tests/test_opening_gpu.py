@@ -191,3 +191,58 @@ def test_batch_invert_assigned_rejects_bad_layouts(h2b, cuda):
     for stride, no, do in ((72, 8, 41), (70, 8, 40), (72, 8, 48), (72, 0, 40)):
         with pytest.raises(h2b.Halo2GpuError, match="layout"):
             h2b.batch_invert_assigned_device([d], [d], 8, stride, no, do)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 1000, (1 << 16) + 3])
+def test_eval_many_device_matches_single_evaluations(h2b, orc, cuda, n):
+    """h2b_eval_many_device over 64 device polynomials (points 0, 1, -1 and
+    random) gives the bytes of _halo2_eval_polynomial per polynomial; more
+    than 64 is an error."""
+    import ctypes
+    import random
+    f = h2b.fields
+    rng = random.Random(n)
+    polys = [h2b.to_dev(orc.chacha_fr(500 + i, n)) for i in range(64)]
+    pts = [0, 1, f.R_MOD - 1] + [rng.randrange(f.R_MOD) for _ in range(61)]
+    got = h2b.to_host(h2b.eval_many_device(polys, pts, n))
+    ws = h2b.dev_empty(h2b.lib()._halo2_eval_polynomial_workspace_size(n))
+    for i, (d, z) in enumerate(zip(polys, pts)):
+        res = ctypes.c_void_p()
+        h2b.call("_halo2_eval_polynomial", h2b.ptr(d), ctypes.byref(h2b.host_ffi(f.fr_mont_limbs([z]))),
+                 ctypes.byref(res), n, h2b.ptr(ws), ws.numel(), h2b.stream_handle())
+        off = res.value - ws.data_ptr()
+        assert h2b.to_host(ws[off:off + 32]).tobytes() == got[i].tobytes(), i
+    with pytest.raises(h2b.Halo2GpuError, match="more than 64"):
+        h2b.eval_many_device(polys + polys[:1], pts + [5], n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("count", [0, 1, 7, 64])
+def test_linear_combination_matches_multiply_add(h2b, orc, cuda, count):
+    """h2b_poly_linear_combination (accumulating or not) gives the bytes of
+    one _halo2_poly_multiply_add per term; more than 64 terms is an error."""
+    import random
+    f = h2b.fields
+    n = 5000
+    rng = random.Random(count)
+    polys = [h2b.to_dev(orc.chacha_fr(700 + i, n)) for i in range(count)]
+    coeffs = [rng.randrange(f.R_MOD) for _ in range(count)]
+    start = orc.chacha_fr(699, n)
+    want = h2b.to_dev(start)
+    for d, c in zip(polys, coeffs):
+        h2b.call("_halo2_poly_multiply_add", h2b.ptr(want), h2b.ptr(d), h2b.ptr(h2b.to_dev(f.fr_mont_limbs([c]))), n,
+                 h2b.stream_handle())
+    acc = h2b.to_dev(start)
+    h2b.linear_combination_device(acc, polys, coeffs, n, accumulate=True)
+    assert h2b.to_host(acc).tobytes() == h2b.to_host(want).tobytes()
+    fresh = h2b.to_dev(orc.chacha_fr(698, n))          # overwritten: starts from zero
+    h2b.linear_combination_device(fresh, polys, coeffs, n, accumulate=False)
+    zero = h2b.to_dev(np.zeros((n, 4), np.uint64))
+    for d, c in zip(polys, coeffs):
+        h2b.call("_halo2_poly_multiply_add", h2b.ptr(zero), h2b.ptr(d), h2b.ptr(h2b.to_dev(f.fr_mont_limbs([c]))), n,
+                 h2b.stream_handle())
+    assert h2b.to_host(fresh).tobytes() == h2b.to_host(zero).tobytes()
+    if count == 64:
+        with pytest.raises(h2b.Halo2GpuError, match="more than 64"):
+            h2b.linear_combination_device(acc, polys + polys[:1], coeffs + [1], n)
