@@ -150,41 +150,63 @@ class UtilSampler:
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling during the timed region.
+
+    start() returns once the first sample has arrived (nvidia-smi takes a
+    moment to begin), so the timed region is sampled from its start; begin()
+    and end() mark the region, and stop() reports the samples that arrived
+    inside it (all samples when the region was shorter than one interval)."""
+
+    INTERVAL_MS = 50
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
+        self.t_begin = self.t_end = None
 
-    def start(self):
+    def start(self, wait_s=5.0):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.first.wait(wait_s)
         except OSError:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+            self.first.set()
+
+    def begin(self):
+        self.t_begin = time.monotonic()
+
+    def end(self):
+        self.t_end = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
+        time.sleep(2 * self.INTERVAL_MS / 1000)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        lines = self.lines
+        inside = []
+        if self.t_begin is not None and self.t_end is not None:
+            inside = [x for x in lines if self.t_begin <= x[0] <= self.t_end + self.INTERVAL_MS / 1000]
+            lines = inside or lines
         sms, mx, reasons = [], None, set()
-        for ln in self.lines:
+        for _, ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -198,7 +220,8 @@ class ClockSampler:
                     reasons.add(name)
         sms.sort()
         med = sms[len(sms) // 2] if sms else None
-        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sms)}
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sms),
+                "interval_ms": self.INTERVAL_MS, "samples_inside_timed_region": bool(inside)}
 
 
 def ncu_traffic(name):
@@ -577,7 +600,7 @@ def serving_section(h2b, torch, count=24, slots=4, kmax=22, seed=9, loads=(0.5, 
                                                   for j in range(2)])
         service[k] = (lat[1], torch.cuda.max_memory_allocated() / 1e9)
         _, _, proof, public = r["outputs"][0]
-        verified[str(k)] = bool(V.verify_proof(res.verifying_key(k), public, proof, res.tau))
+        verified[str(k)] = bool(V.verify_proof(res.verifying_key(k), public, proof, res.verifier_params()))
     served.serve([(0.0, k, 9 + k) for k in ks for _ in range(slots)])   # untimed: every worker's pools warm
     mean_s = sum(w * service[k][0] for k, w in zip(ks, weights))
     # what concurrency buys per k: a burst of same-k requests one at a time
@@ -1050,11 +1073,13 @@ def main():
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    clocks.begin()
     t0.record(stream)
     for i in range(args.steps):
         step(evs[i])
     t1.record(stream)
     torch.cuda.synchronize()
+    clocks.end()
     if dist is not None:
         dist.barrier()
     clk = clocks.stop()

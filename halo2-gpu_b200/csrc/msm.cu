@@ -99,7 +99,8 @@ static int choose_c(uint64_t n, bool plain = false)
         if (tuned) return tuned;
         // plain-base widths from autotuner runs on B200 (witness-like scalar
         // mix): 16 bits from 2^20 (5.40 -> 4.36 ms with the chunk rule below),
-        // 13 bits from 2^14 (2^16: 1.79 -> 1.45 ms)
+        // 13 bits from 2^14 (2^16: 1.79 -> 1.45 ms); 17 to 20 bits measured
+        // slower from 2^20 to 2^22 (2^22: 11.30 ms at 16, 13.4-19.6 ms wider)
         if (lg >= 20) return 16;
         if (lg >= 19) return 15;
         if (lg >= 14) return 13;

@@ -34,7 +34,8 @@ points, in the reference's phase order:
 Challenges come from the Fiat-Shamir transcript (transcript.py) when
 `transcript=True`, and from a seeded generator otherwise (same device work,
 no proof bytes).  `verify.verify_proof` checks a proof from its bytes, the
-public inputs and the verifying key.  Blinding values come from this
+public inputs, the verifying key and the SRS's G2 elements
+(`Resident.verifier_params`), ending in the reference's pairing check.  Blinding values come from this
 library's seeded device generator, not the reference's ChaCha RNG, so proof
 bytes are this build's own; parity of the bytes is unpinned.
 
@@ -183,6 +184,12 @@ class Resident:
             rep = int.from_bytes(h.digest(), "little") % F.R_MOD
             self._vk[k] = V.VerifyingKey(k, pts[:3], pts[3:], rep)
         return self._vk[k]
+
+    def verifier_params(self):
+        """The SRS's G2 elements for the verifier's pairing check
+        (verify.KZGVerifierParams: [1]_2 and [s]_2 = tau [1]_2)."""
+        from . import verify as V
+        return V.params_from_tau(self.tau)
 
     def vk_repr(self, k, stream=None):
         """One Fr scalar standing for the 2^k verifying key in the transcript:

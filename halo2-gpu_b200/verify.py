@@ -17,19 +17,23 @@ column is evaluated from the public inputs, verifier.rs:162-198):
    folded with y, give the expected h(x) = fold / (x^n - 1); the h
    commitment is sum_i x^(n i) H_i;
 3. the SHPLONK opening of every query (shplonk/verifier.rs:60-135) against
-   the commitments, with that h(x) as the claimed evaluation of h.
+   the commitments, with that h(x) as the claimed evaluation of h, ending in
+   the reference's pairing product (poly/kzg/msm.rs:159-176)
+       e(W', [s]_2) * e(F + u W', -[1]_2) == 1,
+   F = sum_i v^i (Z_{T\\S_i}(u) / Z_{T\\S_0}(u)) (sum_j y^j C_ij - r_i(u) G)
+       - Z_{S_0}(u) W,
+   computed by pairing.py's optimal ate pairing.
 
-The final pairing check of step 3, e(W', [tau]_2) = e(F + u W', [1]_2) with
-    F = sum_i v^i (Z_{T\\S_i}(u) / Z_{T\\S_0}(u)) (sum_j y^j C_ij - r_i(u) G)
-        - Z_{S_0}(u) W,
-holds exactly when F = (tau - u) W' in G1, because e is non-degenerate.  For
-a synthetic SRS whose trapdoor tau is known ([tau^i] G with a seeded tau,
-never a ceremony) `shplonk_check_trapdoor` checks that G1 form directly, so
-no pairing is needed; with a real SRS the pairing form is the only option,
-and it is not built here.
+The SRS here is synthetic ([tau^i] G with a seeded tau, never a ceremony),
+so its G2 elements are [1]_2 = the standard generator and [s]_2 = tau [1]_2,
+as the reference's setup makes them (poly/kzg/commitment.rs:188-189).
+Because e is non-degenerate the pairing product is 1 exactly when
+F + u W' = tau W' in G1; `shplonk_check_trapdoor` checks that G1 form
+directly (no pairing), and the tests hold both checks to the same verdicts.
 """
 from . import circuit as C
 from . import fields as F
+from . import pairing as E
 from . import transcript as T
 from .shplonk import _eval_host, _interpolate, _vanishing_at
 
@@ -62,14 +66,39 @@ def _mul(pt, s):
     return F.g1_mul(pt, s)
 
 
-def shplonk_check_trapdoor(commitments, queries, evals, y, v, u, w, w2, tau):
-    """commitments: {label: affine point or None}; queries: [(label, point)]
+class KZGVerifierParams:
+    """The SRS's G2 elements the final check needs: [1]_2 and [s]_2
+    (ParamsKZG's g2 and s_g2, poly/kzg/commitment.rs:32-33)."""
+
+    def __init__(self, g2, s_g2):
+        if not (E.g2_on_curve(g2) and E.g2_on_curve(s_g2)):
+            raise ValueError("G2 element off the twist")
+        self.g2, self.s_g2 = g2, s_g2
+
+
+_PARAMS = {}
+
+
+def params_from_tau(tau):
+    """[1]_2 = the standard G2 generator and [s]_2 = tau [1]_2 for the
+    synthetic SRS with trapdoor tau (cached per tau)."""
+    tau %= P
+    if tau not in _PARAMS:
+        _PARAMS[tau] = KZGVerifierParams(E.G2_GENERATOR, E.g2_mul(E.G2_GENERATOR, tau))
+    return _PARAMS[tau]
+
+
+def shplonk_dual_msm(commitments, queries, evals, y, v, u, w, w2):
+    """The two G1 sums of the final check, (left, right) = (W', F + u W').
+
+    commitments: {label: affine point or None}; queries: [(label, point)]
     in query order; evals: the claimed evaluations; y, v, u: the SHPLONK
-    challenges; w, w2: W and W' (affine); tau: the SRS trapdoor.  Mirrors
-    shplonk/verifier.rs:60-131: rotation sets in the order of their first
-    commitment, each set's coefficient Z_{T\\S_i}(u) normalised by the first
-    set's (so set 0 enters with 1), r_outer = sum_i v^i z_i sum_j y^j r_ij(u),
-    and F = outer - r_outer G - Z_{S_0}(u) W.  True when F + u W' = tau W'."""
+    challenges; w, w2: W and W' (affine).  Mirrors shplonk/verifier.rs:60-131:
+    rotation sets in the order of their first commitment, each set's
+    coefficient Z_{T\\S_i}(u) normalised by the first set's (so set 0 enters
+    with 1), r_outer = sum_i v^i z_i sum_j y^j r_ij(u), and
+    F = outer - r_outer G - Z_{S_0}(u) W; left gets W' (msm_accumulator.left),
+    right gets F + u W' (msm_accumulator.right)."""
     point_sets = {}
     for (lab, x), e in zip(queries, evals):
         point_sets.setdefault(lab, {})[x % P] = e % P
@@ -98,7 +127,22 @@ def shplonk_check_trapdoor(commitments, queries, evals, y, v, u, w, w2, tau):
     outer = F.g1_add(outer, _mul(F.G1_GENERATOR, -r_outer))
     outer = F.g1_add(outer, _mul(w, -z_0))
     outer = F.g1_add(outer, _mul(w2, u))
-    return outer == _mul(w2, tau)
+    return w2, outer
+
+
+def shplonk_check_pairing(commitments, queries, evals, y, v, u, w, w2, params):
+    """The reference's final check (poly/kzg/msm.rs:159-176):
+    e(left, [s]_2) * e(right, -[1]_2) == 1."""
+    if isinstance(params, int):
+        params = params_from_tau(params)
+    left, right = shplonk_dual_msm(commitments, queries, evals, y, v, u, w, w2)
+    return E.pairing_check([(left, params.s_g2), (right, E.g2_neg(params.g2))])
+
+
+def shplonk_check_trapdoor(commitments, queries, evals, y, v, u, w, w2, tau):
+    """The same check in G1 with the SRS trapdoor tau: right == tau left."""
+    left, right = shplonk_dual_msm(commitments, queries, evals, y, v, u, w, w2)
+    return right == _mul(left, tau)
 
 
 def lagrange_at(dom, x, i):
@@ -156,11 +200,12 @@ def expressions(dom, ev, public_eval, theta, beta, gamma, x):
     return out
 
 
-def verify_proof(vk, public, proof, tau):
+def verify_proof(vk, public, proof, params):
     """True when `proof` (bytes) is a valid proof of the circuit with public
-    inputs `public` (ints) under `vk`, checked against the synthetic SRS with
-    trapdoor `tau`.  A malformed proof (a point off the curve, a
-    non-canonical scalar, missing or extra bytes) is rejected."""
+    inputs `public` (ints) under `vk`, its opening checked by the pairing
+    product against `params` (KZGVerifierParams, or the synthetic SRS's
+    trapdoor tau, from which they are made).  A malformed proof (a point off
+    the curve, a non-canonical scalar, missing or extra bytes) is rejected."""
     from .prover import open_queries_for, transcript_eval_order
     dom, B = vk.dom, C.BLINDING_FACTORS
     try:
@@ -218,4 +263,4 @@ def verify_proof(vk, public, proof, tau):
     values = dict(evals)
     values[("h", x)] = expected_h
     claimed = [values[lab] for lab in labels]
-    return shplonk_check_trapdoor(cm, labels, claimed, sy, sv, u, w, w2, tau)
+    return shplonk_check_pairing(cm, labels, claimed, sy, sv, u, w, w2, params)

@@ -3,7 +3,7 @@ issues the same device work per proof) and the serving loop around it.
 
 A proof of a satisfying witness verifies (verify.verify_proof: the
 vanishing argument at x from the opened evaluations and the SHPLONK opening
-in its trapdoor form) at k = 10, 16 and 20; one wrong witness cell, one
+ending in the reference's pairing check) at k = 10, 16 and 20; one wrong witness cell, one
 changed commitment, one changed evaluation or a wrong public input makes it
 fail.  The device-synthesised witness satisfies every gate, copy and lookup
 on the host.  Proofs are the same bytes alone and in a concurrent mix."""
@@ -157,7 +157,7 @@ def test_served_outputs_match_alone(h2b):
         assert a[2] == m[2]
     # every proof verifies
     for (_, k, _), out in zip(reqs, alone):
-        assert V.verify_proof(res.verifying_key(k), out[3], out[2], res.tau)
+        assert V.verify_proof(res.verifying_key(k), out[3], out[2], res.verifier_params())
     c, e = _bytes(alone[0])
     assert len(c) == 96 * 15 and len(e) == 32 * P.NUM_EVALS
     assert len(alone[0][2]) == 32 * (15 + P.NUM_EVALS)
@@ -225,7 +225,7 @@ def test_proof_verifies_and_rejects_changes(h2b):
     w, commits, evals = _prove(h2b, res, k, 21, check_degree=True)
     assert w.h_degree_ok
     proof, public = w.proof, w.public
-    assert V.verify_proof(vk, public, proof, res.tau)
+    assert V.verify_proof(vk, public, proof, res.verifier_params())
     pts = [T.commitment_to_affine(c.cpu().numpy().view(np.uint64)) for c in commits]
     assert [T.decompress(proof[32 * i: 32 * i + 32]) for i in range(10)] == pts[:10]
     assert pts[9] == F.G1_GENERATOR                                   # the constant random polynomial
@@ -233,13 +233,13 @@ def test_proof_verifies_and_rejects_changes(h2b):
     at = 32 * 13 + 32 * 2
     bad = bytearray(proof)
     bad[at] ^= 1
-    assert not V.verify_proof(vk, public, bytes(bad), res.tau)
+    assert not V.verify_proof(vk, public, bytes(bad), res.verifier_params())
     bad = bytearray(proof)
     bad[32: 64] = T.compress(F.G1_GENERATOR)
-    assert not V.verify_proof(vk, public, bytes(bad), res.tau)
-    assert not V.verify_proof(vk, [public[0] + 1] + public[1:], proof, res.tau)
-    assert not V.verify_proof(vk, public, proof[:-32], res.tau)
-    assert not V.verify_proof(vk, public, proof + bytes(32), res.tau)
+    assert not V.verify_proof(vk, public, bytes(bad), res.verifier_params())
+    assert not V.verify_proof(vk, [public[0] + 1] + public[1:], proof, res.verifier_params())
+    assert not V.verify_proof(vk, public, proof[:-32], res.verifier_params())
+    assert not V.verify_proof(vk, public, proof + bytes(32), res.verifier_params())
     # one wrong witness cell: the quotient is no longer a polynomial
     n = 1 << k
     one = h2b.to_dev(F.fr_mont_limbs([1]))
@@ -260,7 +260,7 @@ def test_proof_verifies_and_rejects_changes(h2b):
     for tamper in (add_one(C.ADV_C, 7), add_one(C.ADV_D, 100), add_one(C.ADV_B, int(b_rows[3]))):
         wt, _, _ = _prove(h2b, res, k, 21, tamper, check_degree=True)
         assert wt.h_degree_ok is False
-        assert not V.verify_proof(vk, wt.public, wt.proof, res.tau)
+        assert not V.verify_proof(vk, wt.public, wt.proof, res.verifier_params())
     # a lookup input outside the table: the prover refuses at the permute-sort, as the
     # reference's permute_expression_pair does (lookup/prover.rs:788-880)
     with pytest.raises(h2b.Halo2GpuError, match="not found in the table"):
@@ -286,10 +286,10 @@ def test_proof_verifies_at_config_sizes(h2b, k):
     res = P.Resident(h2b, k)
     w, _, _ = _prove(h2b, res, k, 1000 + k, check_degree=True)
     assert w.h_degree_ok, "h must have degree < 3n when every constraint holds"
-    assert V.verify_proof(res.verifying_key(k), w.public, w.proof, res.tau)
+    assert V.verify_proof(res.verifying_key(k), w.public, w.proof, res.verifier_params())
     if k == 20:
         w2, _, _ = _prove(h2b, res, k, 1000 + k, fused_quotient=False, merged_msm=True)
         assert w2.proof == w.proof, "fused quotient and merged MSMs must not change the proof"
     bad = bytearray(w.proof)
     bad[-32 * 3] ^= 4                                 # inside the last evaluations
-    assert not V.verify_proof(res.verifying_key(k), w.public, bytes(bad), res.tau)
+    assert not V.verify_proof(res.verifying_key(k), w.public, bytes(bad), res.verifier_params())

@@ -1,14 +1,23 @@
-"""The G1 (trapdoor) form of SHPLONK's final pairing check
-(halo2-gpu_b200/verify.py) against an opening made by a pure-Python
-restatement of the SHPLONK prover, all on the host: a correct opening
-passes; a changed evaluation, challenge, commitment or W' fails."""
+"""SHPLONK's final check (halo2-gpu_b200/verify.py), in the reference's
+pairing form and in the G1 (trapdoor) form, against an opening made by a
+pure-Python restatement of the SHPLONK prover, all on the host: a correct
+opening passes both; a changed evaluation, challenge, commitment or W'
+fails both."""
 import importlib
 import random
 
 from test_shplonk_gpu import _restate
 
 
-def test_trapdoor_check_accepts_opening_and_rejects_changes(h2b):
+def _both(V, *args):
+    """The pairing and trapdoor verdicts, which must agree."""
+    tr = V.shplonk_check_trapdoor(*args)
+    pr = V.shplonk_check_pairing(*args)
+    assert tr == pr
+    return pr
+
+
+def test_final_check_accepts_opening_and_rejects_changes(h2b):
     F = h2b.fields
     S = importlib.import_module(h2b.__name__ + ".shplonk")
     V = importlib.import_module(h2b.__name__ + ".verify")
@@ -26,18 +35,18 @@ def test_trapdoor_check_accepts_opening_and_rejects_changes(h2b):
     cm = {i: commit(c) for i, c in enumerate(polys)}
     W, W2 = commit(h), commit(q)
     evals = [S._eval_host(polys[k], pt) for k, pt in queries]
-    assert V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, W, W2, tau)
+    assert _both(V, cm, queries, evals, y, v, u, W, W2, tau)
     bad = list(evals)
     bad[4] = (bad[4] + 1) % p
-    assert not V.shplonk_check_trapdoor(cm, queries, bad, y, v, u, W, W2, tau)
-    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, (v + 1) % p, u, W, W2, tau)
-    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, W, F.g1_add(W2, F.G1_GENERATOR), tau)
+    assert not _both(V, cm, queries, bad, y, v, u, W, W2, tau)
+    assert not _both(V, cm, queries, evals, y, (v + 1) % p, u, W, W2, tau)
+    assert not _both(V, cm, queries, evals, y, v, u, W, F.g1_add(W2, F.G1_GENERATOR), tau)
     cm2 = dict(cm)
     cm2[3] = F.g1_add(cm[3], F.G1_GENERATOR)
-    assert not V.shplonk_check_trapdoor(cm2, queries, evals, y, v, u, W, W2, tau)
+    assert not _both(V, cm2, queries, evals, y, v, u, W, W2, tau)
 
 
-def test_trapdoor_check_rejects_an_unnormalised_w2(h2b):
+def test_final_check_rejects_an_unnormalised_w2(h2b):
     """W' must be the commitment to L(X) / ((X - u) Z_{T\\S_0}(u)), as the
     reference's prover scales it (shplonk/prover.rs:423-430): the quotient
     without the factor fails the check whenever Z_{T\\S_0}(u) != 1."""
@@ -54,8 +63,8 @@ def test_trapdoor_check_rejects_an_unnormalised_w2(h2b):
     commit = lambda c: F.g1_mul(F.G1_GENERATOR, S._eval_host(c, tau))  # noqa: E731
     cm = {i: commit(c) for i, c in enumerate(polys)}
     evals = [S._eval_host(polys[k], pt) for k, pt in queries]
-    assert V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, commit(h), commit(q), tau)
+    assert _both(V, cm, queries, evals, y, v, u, commit(h), commit(q), tau)
     z0_diff = S._vanishing_at([x * w % p], u)          # T \ S_0 for S_0 = {x}
     assert z0_diff != 1
     raw = [c * z0_diff % p for c in q]
-    assert not V.shplonk_check_trapdoor(cm, queries, evals, y, v, u, commit(h), commit(raw), tau)
+    assert not _both(V, cm, queries, evals, y, v, u, commit(h), commit(raw), tau)
