@@ -202,6 +202,96 @@ __global__ void k_bitrev_inplace(NttBatch B, int k, bool scale, Zeta3 z3)
     }
 }
 
+// Tiled bit reversal for 2^k arrays with k >= 10.  Index i splits as
+// (h: top 5 bits, m: middle k - 10 bits, l: low 5 bits) and
+// bitrev_k(i) = (rev5(l), rev_{k-10}(m), rev5(h)): the 1024 elements with
+// middle index m (32 runs of 32 consecutive elements, one run per h) are
+// exactly the images of the elements with middle index rev(m).  One CTA
+// carries tile m and its partner tile rev(m) through shared memory, so every
+// global load and store is one warp's contiguous 1 KB run instead of a
+// 32-byte access n/2 away from its neighbour's.
+constexpr int BR_LOG = 5, BR_SIDE = 1 << BR_LOG, BR_THREADS = 256;
+constexpr int BR_MIN_LOG = 2 * BR_LOG;
+constexpr int BR_TILE = BR_SIDE * BR_SIDE;
+constexpr size_t BR_SMEM = 2 * BR_TILE * sizeof(Fr);  // two tiles, 64 KB
+
+__device__ __forceinline__ uint32_t rev5(uint32_t x) { return __brev(x) >> (32 - BR_LOG); }
+
+// slot of element (row r, column c) of a tile: the column is XOR-swizzled by
+// the row, so a warp reading one column across 32 rows touches four bank
+// groups per 16-byte access instead of one (two-way conflicts at most; rows
+// are read and written conflict-light as well)
+__device__ __forceinline__ uint32_t br_slot(uint32_t r, uint32_t c) { return r * BR_SIDE + (c ^ ((r >> 2) & 3)); }
+
+__device__ __forceinline__ uint64_t br_index(uint32_t h, uint64_t m, uint32_t l, int k)
+{
+    return ((uint64_t)h << (k - BR_LOG)) | (m << BR_LOG) | l;
+}
+
+// In place: a[bitrev(j)] and a[j] swap; with `scale` the element landing at
+// index j is multiplied by z3.f[j mod 3] (as k_bitrev_inplace).
+__global__ void __launch_bounds__(BR_THREADS) k_bitrev_tiled(NttBatch B, int k, bool scale, Zeta3 z3)
+{
+    extern __shared__ uint4 br_sh[];
+    Fr* tile = reinterpret_cast<Fr*>(br_sh);
+    Fr* __restrict__ a = B.dst[blockIdx.y];
+    const int km = k - BR_MIN_LOG;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = BR_THREADS / 32;
+    for (uint64_t m = blockIdx.x; m < (1ull << km); m += gridDim.x) {
+        const uint64_t mr = bitrev(m, km);
+        if (m > mr) continue;  // the CTA of the partner tile moves both
+        const int nt = (m == mr) ? 1 : 2;
+        for (int t = 0; t < nt; t++) {
+            const uint64_t mm = t ? mr : m;
+            for (uint32_t h = warp; h < BR_SIDE; h += nw)
+                st(&tile[t * BR_TILE + br_slot(h, lane)], ld(&a[br_index(h, mm, lane, k)]));
+        }
+        __syncthreads();
+        // tile t holds middle index mm; its element (h, l) lands at
+        // (rev5(l), rev(mm), rev5(h)), so output run h of tile rev(mm) reads
+        // column rev5(h) of tile t at rows rev5(lane)
+        for (int t = 0; t < nt; t++) {
+            const uint64_t md = t ? m : mr;
+            for (uint32_t h = warp; h < BR_SIDE; h += nw) {
+                Fr v = ld(&tile[t * BR_TILE + br_slot(rev5(lane), rev5(h))]);
+                const uint64_t j = br_index(h, md, lane, k);
+                if (scale) v = v * z3.f[j % 3];
+                st(&a[j], v);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// k_twist_bitrev_stage0 on tiles (out of place, output size 2^L, L >= 10):
+// output tile m takes its inputs from input tile rev(m), twisted as they are
+// loaded (twist_in), and writes the first DIT stage's pairs (l, l ^ 1) of
+// each output run.
+__global__ void __launch_bounds__(BR_THREADS) k_twist_bitrev_stage0_tiled(NttBatch B, uint64_t n_in, int L, int mode,
+                                                                          const Fr* __restrict__ cpow, Zeta3 z3)
+{
+    extern __shared__ uint4 br_sh[];
+    Fr* tile = reinterpret_cast<Fr*>(br_sh);
+    const Fr* __restrict__ in = B.src[blockIdx.y];
+    Fr* __restrict__ out = B.dst[blockIdx.y];
+    const int km = L - BR_MIN_LOG;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = BR_THREADS / 32;
+    for (uint64_t m = blockIdx.x; m < (1ull << km); m += gridDim.x) {
+        const uint64_t mi = bitrev(m, km);
+        for (uint32_t h = warp; h < BR_SIDE; h += nw)
+            st(&tile[br_slot(h, lane)], twist_in(in, br_index(h, mi, lane, L), n_in, mode, cpow, z3));
+        __syncthreads();
+        for (uint32_t h = warp; h < BR_SIDE; h += nw) {
+            // output (h, m, l) holds input (rev5(l), mi, rev5(h)); DIT stage 0
+            // pairs outputs l and l ^ 1: (x_even + x_odd, x_even - x_odd)
+            const Fr x = ld(&tile[br_slot(rev5(lane), rev5(h))]);
+            const Fr y = ld(&tile[br_slot(rev5(lane ^ 1), rev5(h))]);
+            st(&out[br_index(h, m, lane, L)], (lane & 1) ? y - x : x + y);
+        }
+        __syncthreads();
+    }
+}
+
 // One shared-memory pass of `nst` radix-2 stages starting at stage s0.
 //   DIT: stage s pairs (i, i + 2^s), twiddle w^((i mod 2^s) * n/2^(s+1)),
 //        groups: 2^nst elements at stride S = 2^s0 inside blocks of S*2^nst.
@@ -499,6 +589,26 @@ static bool ntt4_smem_ready()
     return state == 1;
 }
 
+// The tiled bit reversals take 64 KB of shared memory (opt-in above the
+// 48 KB default), set once per process; without it the scatter kernels run.
+static bool br_smem_ready()
+{
+    static int state = 0;
+    if (state == 0) {
+        bool ok_ = cudaFuncSetAttribute(k_bitrev_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)BR_SMEM) == cudaSuccess &&
+                   cudaFuncSetAttribute(k_twist_bitrev_stage0_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)BR_SMEM) == cudaSuccess;
+        state = ok_ ? 1 : 2;
+    }
+    return state == 1;
+}
+
+static dim3 br_grid(int logn, int count)
+{
+    return dim3((unsigned)std::min<uint64_t>(1ull << (logn - BR_MIN_LOG), 8192), (unsigned)count);
+}
+
 // Runs radix-2 stages [first, logn) of `count` transforms in passes of at
 // most g_max_pass_stages stages.  The first pass reads B.src and writes B.dst;
 // the later ones work in place on B.dst.
@@ -629,6 +739,20 @@ static Zeta3 scale_factors(const host::Fr64& scale)
     return out;
 }
 
+// In-place bit reversal (and optional scale) of `count` arrays of 2^logn.
+static RustError bitrev_group(NttBatch D, int count, int logn, bool scale, Zeta3 z3, cudaStream_t st)
+{
+    if (logn >= BR_MIN_LOG && br_smem_ready()) {
+        k_bitrev_tiled<<<br_grid(logn, count), BR_THREADS, BR_SMEM, st>>>(D, logn, scale, z3);
+        H2B_LAUNCHED("k_bitrev_tiled");
+    } else {
+        const uint64_t n = 1ull << logn;
+        k_bitrev_inplace<<<dim3(grid_for(n, 256), (unsigned)count), 256, 0, st>>>(D, logn, scale, z3);
+        H2B_LAUNCHED("k_bitrev_inplace");
+    }
+    return ok();
+}
+
 // Core: `count` (<= NTT_MAX_BATCH) transforms of one type and size, B.src[i]
 // -> B.dst[i], all on the device.  `alias`: every B.src[i] == B.dst[i].
 //   log_n   : input length (and transform size except for coset types)
@@ -672,8 +796,15 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
         const uint64_t nthreads = nt / SC_CHUNK + (nt % SC_CHUNK ? 1 : 0);
         if (!alias) {
             // the fused input stage also runs DIT stage 0
-            k_twist_bitrev_stage0<<<grid(nt / 2), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.cpow, z3);
-            H2B_LAUNCHED("k_twist_bitrev_stage0");
+            if (logt >= BR_MIN_LOG && br_smem_ready()) {
+                k_twist_bitrev_stage0_tiled<<<br_grid(logt, count), BR_THREADS, BR_SMEM, st>>>(
+                    B, type == 3 ? nin : nt, logt, mode, s.cpow, z3);
+                H2B_LAUNCHED("k_twist_bitrev_stage0_tiled");
+            } else {
+                k_twist_bitrev_stage0<<<grid(nt / 2), 256, 0, st>>>(B, type == 3 ? nin : nt, logt, mode, s.cpow,
+                                                                      z3);
+                H2B_LAUNCHED("k_twist_bitrev_stage0");
+            }
             return run_passes(D, count, s.tw, logt, true, st, 1);
         } else {
             if (type == 3 && nt != nin) {
@@ -685,8 +816,7 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
                 k_twist_inplace<<<grid(nthreads), 256, 0, st>>>(D, nt, mode, s.cpow, z3);
                 H2B_LAUNCHED("k_twist_inplace");
             }
-            k_bitrev_inplace<<<grid(nt), 256, 0, st>>>(D, logt, false, none);
-            H2B_LAUNCHED("k_bitrev_inplace");
+            H2B_TRY(bitrev_group(D, count, logt, false, none, st));
         }
         return run_passes(D, count, s.tw, logt, true, st);
     }
@@ -702,9 +832,7 @@ static RustError transform_group(int type, int log_n, int log_ext, NttBatch B, i
         }
         H2B_TRY(run_passes(P, count, s.tw, logt, false, st));
         Zeta3 z3 = (type == 4) ? zeta_factors(*h_divisor, true) : scale_factors(*h_divisor);
-        k_bitrev_inplace<<<grid(nt), 256, 0, st>>>(D, logt, true, z3);
-        H2B_LAUNCHED("k_bitrev_inplace");
-        return ok();
+        return bitrev_group(D, count, logt, true, z3, st);
     }
     return err(-1, "unsupported ntt_type");
 }
