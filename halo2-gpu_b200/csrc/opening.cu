@@ -24,16 +24,23 @@
 //
 // Kate division is the linear recurrence Y_t = r_t + u Y_{t-1} over the
 // reversed coefficients r_t = a_{n-1-t} (q_{n-2-t} = Y_t).  With a constant
-// multiplier it scans like a prefix sum: tiles of KD_T * KD_E values are
-// solved with zero carry-in (thread-sequential, then a Hillis-Steele scan of
-// the thread totals with multipliers v^(8 * 2^d)); the tile totals form the
-// same recurrence one level up with multiplier v^2048; the down pass adds
-// v^(position + 1) * carry to every value of a tile.  Scratch is a few
-// small per-level arrays instead of two n-length state arrays.
+// multiplier it scans like a prefix sum over tiles of T = KD_T * KD_E = 2048
+// values.  The coefficients' own level (level 0) is a weighted prefix sum:
+// in tile k with local index j, the solution with zero carry-in is
+// u^j P_j, P_j = sum_{s <= j} r_{kT+s} u^-s (one product per value, then
+// additions only), and with the true value C before the tile
+// Y_t = u^j (P_j + u C) (one product per value); u^j and u^-j for j < T are
+// tables built once per division (one inversion of u).  The tile totals
+// u^(T-1) P_{T-1} form the same recurrence one level up with multiplier
+// u^T, solved by thread-sequential tiles and a Hillis-Steele scan of the
+// thread totals with multipliers v^(8 * 2^d), whose down pass adds
+// v^(position + 1) * carry.  Scratch is the two tables and a few small
+// per-level arrays instead of n-length state arrays.
 #define H2B_INLINE_MUL 1
 #include <algorithm>
 #include "abi.cuh"
 #include "field.cuh"
+#include "inverse.cuh"
 
 namespace h2b {
 
@@ -293,6 +300,109 @@ static __global__ void __launch_bounds__(KD_T) k_kd_down(KdLevel L, const Fr* __
     }
 }
 
+// u^j and u^-j for j < KD_TILE (U and W), one CTA: thread 0 inverts u (0
+// stays 0) and forms u^(8 * 2^d), u^-(8 * 2^d); thread c then builds
+// entries 8c .. 8c + 7 from u^(8c) and u^-(8c).
+static __global__ void __launch_bounds__(KD_T) k_kd_pow(const Fr* __restrict__ u_in, Fr* __restrict__ U,
+                                                         Fr* __restrict__ W)
+{
+    __shared__ Fr base[2][9];  // [0]: u, u^8, u^16, ...; [1]: the same for u^-1
+    const int c = threadIdx.x;
+    if (c == 0) {
+        Fr x[2];
+        x[0] = ld(u_in);
+        x[1] = finv_fast(x[0]);
+        for (int s = 0; s < 2; s++) {
+            base[s][0] = x[s];
+            Fr p = x[s] * x[s];
+            p = p * p;
+            p = p * p;  // x^8
+            for (int d = 0; d < 8; d++) {
+                base[s][1 + d] = p;
+                p = p * p;
+            }
+        }
+    }
+    __syncthreads();
+    for (int s = 0; s < 2; s++) {
+        Fr p = Fr::one();
+        for (int d = 0; d < 8; d++)
+            if ((c >> d) & 1) p = p * base[s][1 + d];
+        Fr* out = s ? W : U;
+        const Fr x = base[s][0];
+#pragma unroll 1
+        for (int k = 0; k < KD_E; k++) {
+            st(&out[c * KD_E + k], p);
+            if (k + 1 < KD_E) p = p * x;
+        }
+    }
+}
+
+// Level 0 up: P_j = sum_{s <= j} r_{kT+s} u^-s within the tile, written to q
+// (below qlim); the tile's zero-carry end value u^(T-1) P_{T-1} to tot.
+static __global__ void __launch_bounds__(KD_T, 2) k_kd0_up(KdLevel L, const Fr* __restrict__ a,
+                                                            const Fr* __restrict__ U, const Fr* __restrict__ W,
+                                                            Fr* __restrict__ tot)
+{
+    __shared__ Fr sm[2][KD_T];
+    const int c = threadIdx.x;
+    const uint64_t t0 = blockIdx.x * KD_TILE + (uint64_t)c * KD_E;
+    Fr y[KD_E];
+#pragma unroll
+    for (int k = 0; k < KD_E; k++) {
+        const uint64_t t = t0 + k;
+        y[k] = t < L.m ? ld(&a[L.n - 1 - t]) * ldg(&W[c * KD_E + k]) : Fr::zero();
+    }
+#pragma unroll
+    for (int k = 1; k < KD_E; k++) y[k] = y[k] + y[k - 1];
+    // inclusive scan of the thread totals (additions)
+    Fr s = y[KD_E - 1];
+    int buf = 0;
+    sm[buf][c] = s;
+    __syncthreads();
+    for (int d = 0; (1 << d) < KD_T; d++) {
+        if (c >= (1 << d)) s = s + sm[buf][c - (1 << d)];
+        buf ^= 1;
+        sm[buf][c] = s;
+        __syncthreads();
+    }
+    if (c > 0) {
+        const Fr ex = sm[buf][c - 1];
+#pragma unroll
+        for (int k = 0; k < KD_E; k++) y[k] = y[k] + ex;
+    }
+#pragma unroll
+    for (int k = 0; k < KD_E; k++) {
+        const uint64_t t = t0 + k;
+        if (t >= L.m) break;
+        const uint64_t q = kd_qidx(L, t);
+        if (q < L.qlim) st(&L.arr[q], y[k]);
+    }
+    if (c == KD_T - 1) st(&tot[blockIdx.x], ldg(&U[KD_TILE - 1]) * s);
+}
+
+// Level 0 down: Y_t = u^j (P_j + u C), C = tot[k - 1] (the solved value
+// before tile k; 0 for tile 0).  With u = 0, Y_t = r_t.
+static __global__ void __launch_bounds__(KD_T) k_kd0_down(KdLevel L, const Fr* __restrict__ a,
+                                                           const Fr* __restrict__ U, const Fr* __restrict__ tot)
+{
+    const uint64_t b = blockIdx.x;
+    const int c = threadIdx.x;
+    const uint64_t t0 = b * KD_TILE + (uint64_t)c * KD_E;
+    if (t0 >= L.m) return;
+    const Fr u = ldg(&U[1]);
+    const bool u_zero = u.is_zero();
+    const Fr uc = b > 0 ? u * ld(&tot[b - 1]) : Fr::zero();
+#pragma unroll
+    for (int k = 0; k < KD_E; k++) {
+        const uint64_t t = t0 + k;
+        if (t >= L.m) break;
+        const uint64_t q = kd_qidx(L, t);
+        if (q >= L.qlim) continue;
+        st(&L.arr[q], u_zero ? ld(&a[L.n - 1 - t]) : ldg(&U[c * KD_E + k]) * (ld(&L.arr[q]) + uc));
+    }
+}
+
 struct KdPlan {
     int levels = 0;          // levels above 0
     uint64_t m[KD_MAX_LEVELS + 1];
@@ -316,6 +426,7 @@ static void kd_plan_scratch(ScratchPlan& sp, uint64_t n)
     sp.add_n<Fr>((uint64_t)KD_TAB * (P.levels + 1));          // power tables
     for (int l = 1; l <= P.levels; l++) sp.add_n<Fr>(P.m[l]);  // level values
     sp.add_n<Fr>(1);                                            // top-level total (unused)
+    sp.add_n<Fr>(2 * KD_TILE);                                  // u^j, u^-j for level 0
 }
 
 static RustError kd_run(const Fr* a, Fr* q, const Fr* u, uint64_t n, uint64_t qlim, void* scratch, uint64_t bytes,
@@ -330,6 +441,8 @@ static RustError kd_run(const Fr* a, Fr* q, const Fr* u, uint64_t n, uint64_t ql
     Fr* lv[KD_MAX_LEVELS + 2] = {nullptr};
     for (int l = 1; l <= P.levels; l++) lv[l] = ar.take_n<Fr>(P.m[l]);
     Fr* top = ar.take_n<Fr>(1);
+    Fr* upow = ar.take_n<Fr>(KD_TILE);
+    Fr* wpow = ar.take_n<Fr>(KD_TILE);
     if (!ar.good()) {
         ScratchPlan sp;
         kd_plan_scratch(sp, n);
@@ -352,18 +465,25 @@ static RustError kd_run(const Fr* a, Fr* q, const Fr* u, uint64_t n, uint64_t ql
         L.qlim = qlim;
         return L;
     };
-    for (int l = 0; l <= P.levels; l++) {
+    k_kd_pow<<<1, KD_T, 0, st>>>(u, upow, wpow);
+    H2B_LAUNCHED("k_kd_pow");
+    const unsigned tiles0 = (unsigned)((P.m[0] + KD_TILE - 1) / KD_TILE);
+    k_kd0_up<<<tiles0, KD_T, 0, st>>>(level(0), a, upow, wpow, lv[1]);
+    H2B_LAUNCHED("k_kd0_up");
+    for (int l = 1; l <= P.levels; l++) {
         const uint64_t tiles = (P.m[l] + KD_TILE - 1) / KD_TILE;
         k_kd_up<<<(unsigned)tiles, KD_T, 0, st>>>(level(l), a, tabs + (uint64_t)KD_TAB * l, lv[l + 1]);
         H2B_LAUNCHED("k_kd_up");
     }
-    for (int l = P.levels - 1; l >= 0; l--) {
+    for (int l = P.levels - 1; l >= 1; l--) {
         const uint64_t tiles = (P.m[l] + KD_TILE - 1) / KD_TILE;
         if (tiles > 1) {
             k_kd_down<<<(unsigned)(tiles - 1), KD_T, 0, st>>>(level(l), tabs + (uint64_t)KD_TAB * l, lv[l + 1]);
             H2B_LAUNCHED("k_kd_down");
         }
     }
+    k_kd0_down<<<tiles0, KD_T, 0, st>>>(level(0), a, upow, lv[1]);
+    H2B_LAUNCHED("k_kd0_down");
     return ok();
 }
 
