@@ -206,9 +206,15 @@ __device__ __forceinline__ uint64_t bi_index(uint64_t t, int j)
     return (t / BI_GT) * (BI_GT * BI_E) + (uint64_t)j * BI_GT + (t % BI_GT);
 }
 
+// With `pre` (an n-length array laid out like d), the up pass also stores the
+// group's running products P_j (nonzero elements up to j, j < BI_E - 1) at
+// pre[bi_index(t, j)], and the down pass reads P_{j-1} instead of
+// recomputing it: three products per element instead of four, for one more
+// write and read of the array (the passes are product-bound, the memory
+// traffic overlaps).
 template <class C>
 __global__ void __launch_bounds__(128) k_bi_up(const Fp<C>* __restrict__ d, uint64_t n, uint64_t nt,
-                                               Fp<C>* __restrict__ totals)
+                                               Fp<C>* __restrict__ totals, Fp<C>* __restrict__ pre)
 {
     using F = Fp<C>;
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt; t += (uint64_t)gridDim.x * blockDim.x) {
@@ -219,6 +225,7 @@ __global__ void __launch_bounds__(128) k_bi_up(const Fp<C>* __restrict__ d, uint
             if (i < n) {
                 const F x = ld(&d[i]);
                 if (!x.is_zero()) acc = acc * x;
+                if (pre && j < BI_E - 1) st(&pre[i], acc);
             }
         }
         st(&totals[t], acc);
@@ -227,18 +234,20 @@ __global__ void __launch_bounds__(128) k_bi_up(const Fp<C>* __restrict__ d, uint
 
 template <class C>
 __global__ void __launch_bounds__(128) k_bi_down(Fp<C>* __restrict__ d, uint64_t n, uint64_t nt,
-                                                 const Fp<C>* __restrict__ inv_totals)
+                                                 const Fp<C>* __restrict__ inv_totals, const Fp<C>* __restrict__ stored)
 {
     using F = Fp<C>;
     __shared__ F pre[BI_E][128];                           // per thread: product of the nonzero elements before j
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nt; t += (uint64_t)gridDim.x * blockDim.x) {
-        F acc = F::one();
+        if (!stored) {
+            F acc = F::one();
 #pragma unroll 1
-        for (int j = 0; j < BI_E; j++) {
-            const uint64_t i = bi_index(t, j);
-            const F x = i < n ? ld(&d[i]) : F::zero();
-            pre[j][threadIdx.x] = acc;
-            if (!x.is_zero()) acc = acc * x;
+            for (int j = 0; j < BI_E; j++) {
+                const uint64_t i = bi_index(t, j);
+                const F x = i < n ? ld(&d[i]) : F::zero();
+                pre[j][threadIdx.x] = acc;
+                if (!x.is_zero()) acc = acc * x;
+            }
         }
         F inv = ld(&inv_totals[t]);                        // (product of all nonzero elements)^-1
 #pragma unroll 1
@@ -247,7 +256,8 @@ __global__ void __launch_bounds__(128) k_bi_down(Fp<C>* __restrict__ d, uint64_t
             if (i >= n) continue;
             const F x = ld(&d[i]);                         // read again (still the input: i is written last)
             if (x.is_zero()) continue;                     // zero stays zero
-            const F out = inv * pre[j][threadIdx.x];
+            const F before = !stored ? pre[j][threadIdx.x] : (j > 0 ? ld(&stored[bi_index(t, j - 1)]) : F::one());
+            const F out = inv * before;
             inv = inv * x;
             st(&d[i], out);
         }
@@ -258,6 +268,7 @@ static uint64_t groups_of(uint64_t n) { return (n + BI_GT * BI_E - 1) / (BI_GT *
 
 static void plan_batch_invert_groups(ScratchPlan& p, uint64_t n)
 {
+    if (n > BI_TILE) p.add(n * 32);  // the top level's stored running products
     while (n > BI_TILE) {
         n = groups_of(n);
         p.add(n * 32);
@@ -269,13 +280,14 @@ static RustError batch_invert_groups(Fp<C>* d, uint64_t n, ScratchArena& ar, cud
 {
     if (n <= BI_TILE) return batch_invert_local<C>(d, n, st);
     const uint64_t nt = groups_of(n);
+    Fp<C>* pre = top ? ar.take_n<Fp<C>>(n) : nullptr;
     Fp<C>* tot = ar.take_n<Fp<C>>(nt);
     if (!ar.good()) return err(cudaErrorInvalidValue, "batch_invert: scratch too small");
-    k_bi_up<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot);
+    k_bi_up<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot, pre);
     H2B_LAUNCHED("k_bi_up");
     H2B_TRY(batch_invert_groups<C>(tot, nt, ar, st, false));
     if (top) prof_begin(PROF_BATCH_INVERT, st);
-    k_bi_down<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot);
+    k_bi_down<C><<<grid_for(nt, 128, 148u * 16u), 128, 0, st>>>(d, n, nt, tot, pre);
     if (top) prof_end(PROF_BATCH_INVERT, st);
     H2B_LAUNCHED("k_bi_down");
     return ok();
