@@ -881,6 +881,10 @@ def main():
                                        "prove", "table_widths"],
                     help="run one kernel family (profiling runs) or the served-prover section only")
     ap.add_argument("--log-n", type=int, default=21, help="size for --case")
+    ap.add_argument("--widths", default="10,12,13,14,15,16,17,18",
+                    help="window widths for --case table_widths")
+    ap.add_argument("--tables", default="10,11,12,13,14,15,16,17,18,19,20",
+                    help="log2 table sizes for --case table_widths")
     ap.add_argument("--requests", type=int, default=24, help="requests per trace for --case serve")
     ap.add_argument("--loads", default="0.5,1.0,1.5", help="load factors (x plain capacity) for --case serve")
     ap.add_argument("--no-tune", action="store_true",
@@ -914,22 +918,26 @@ def main():
                                                                       loads=loads)}))
         return
     if args.case == "table_widths":
-        # MSMs over window tables of 2^10..2^20 points built at each window
-        # width 10..18 (uniform and witness-mix scalars at the table's size,
-        # uniform at 1/16 of it); outputs must agree across widths
+        # MSMs over window tables (--tables, log2 sizes) built at each window
+        # width (--widths): uniform and witness-mix scalars at the table's
+        # size, uniform at 1/16 of it, and 2^16 uniform scalars over tables
+        # above 2^18 points (a small proof's commitments over a served SRS);
+        # outputs must agree across widths
         import hashlib
         import torch
         torch.cuda.set_device(0)
         h2b = load_pkg()
         L = h2b.lib()
         out_rows = {}
-        for lg in range(10, 21):
+        for lg in [int(x) for x in args.tables.split(",")]:
             tn = 1 << lg
             srs = h2b.srs_device(0x7AB1E + lg, tn)
             scs = {(tn, 1): h2b.random_fr_device(tn, 60 + lg, 1), (tn, 0): h2b.random_fr_device(tn, 70 + lg, 0),
                    (max(tn >> 4, 1), 0): h2b.random_fr_device(max(tn >> 4, 1), 80 + lg, 0)}
+            if lg > 18:
+                scs[(1 << 16, 0)] = h2b.random_fr_device(1 << 16, 90 + lg, 0)
             ref = {}
-            for c in (10, 12, 13, 14, 15, 16, 17, 18):
+            for c in [int(x) for x in args.widths.split(",")]:
                 L.h2b_msm_set_tuning(c, 0)
                 table = h2b.msm_table_precompute(srs, tn)
                 row = {}
@@ -950,7 +958,9 @@ def main():
                     ref.setdefault(key, digest)
                     row[key] = {"ms": round(e0.elapsed_time(e1) / 5, 3), "same": digest == ref[key]}
                 out_rows[f"2^{lg} table, c={c}"] = row
+                print(json.dumps({f"2^{lg} table, c={c}": row}), file=sys.stderr, flush=True)
                 del table
+                torch.cuda.empty_cache()
             L.h2b_msm_set_tuning(0, 0)
         print(json.dumps({"case": "table_widths", "rows": out_rows}))
         return

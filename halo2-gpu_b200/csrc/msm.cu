@@ -50,6 +50,10 @@ static constexpr int GLV_BITS = 127;
 // 32-bit sorted-entry offsets: 2 halves x 8 windows x n < 2^32
 static constexpr uint64_t MSM_MAX_LENGTH = 1ull << 27;
 static constexpr uint32_t SIGN_BIT = 0x80000000u;
+// widest window the tuning override accepts (22 bits: 6 windows per GLV half)
+static constexpr int MSM_MAX_WINDOW = 22;
+// segment sums per CTA of a bit sum before it is split (reduction step 2)
+static constexpr uint32_t BITSUM_ITEMS = 4096;
 static constexpr uint32_t DENSE_LIMIT = 32;     // chunks per bucket summed serially in fixup
 static constexpr int DENSE_PIECES = 32;          // CTAs per dense bucket
 static constexpr uint64_t ACC_TARGET_CHUNKS = 148ull * 3 * 128 * 4;  // accumulation threads x 4
@@ -93,7 +97,7 @@ static int floor_log2(uint64_t n)
 static int choose_c(uint64_t n, bool plain = false)
 {
     const int lg = floor_log2(n);
-    if (g_msm_window_override >= 4 && g_msm_window_override <= 20) return g_msm_window_override;
+    if (g_msm_window_override >= 4 && g_msm_window_override <= MSM_MAX_WINDOW) return g_msm_window_override;
     if (plain) {
         const int tuned = tune_value(0, lg);
         if (tuned) return tuned;
@@ -176,6 +180,10 @@ static MsmPlan plan_core(uint64_t n, int c, uint64_t tn, uint32_t concurrent = 1
     p.LOGL = 31 - __builtin_clz(L);
     p.S = p.H / L;
     p.NBITS = p.S > 1 ? 31 - __builtin_clz(p.S) : 0;
+    // a bit sum of more than BITSUM_ITEMS segment sums is split over CTAs
+    // (wide windows over a table: one bucket set of 2^(c-1) buckets, a
+    // single reduction window, so only NBITS + 1 bit sums to spread)
+    p.BP = std::max<uint32_t>(1u, (p.S + BITSUM_ITEMS - 1) / BITSUM_ITEMS);
     // a bucket spanning more than DENSE_LIMIT chunks holds > DENSE_LIMIT*K entries
     p.max_dense = final_entries / ((uint64_t)DENSE_LIMIT * p.Kf) + 1;
     return p;
@@ -218,6 +226,7 @@ void msm_plan_scratch(const MsmPlan& p, ScratchPlan& sp, bool scalar_host, bool 
     sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment weighted sums
     sp.add_n<G1Xyzz>((uint64_t)p.Wr * p.S);           // segment plain sums
     sp.add_n<G1Xyzz>((uint64_t)std::max(p.W, p.Wr) * (p.NBITS + 1));  // per-bit sums
+    if (p.BP > 1) sp.add_n<G1Xyzz>((uint64_t)p.Wr * (p.NBITS + 1) * p.BP);  // their parts
     sp.add_n<G1Xyzz>(std::max(p.W, p.Wr));                            // window sums
     sp.add_n<G1Jac>(1);                               // result
     if (p.R >= 1) sp.add_n<G1Affine>(p.cap[1]);       // round outputs 1, 3
@@ -253,6 +262,7 @@ MsmScratch msm_carve(const MsmPlan& p, ScratchArena& ar, bool scalar_host, bool 
     s.segacc = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
     s.segrun = ar.take_n<G1Xyzz>((uint64_t)p.Wr * p.S);
     s.bits = ar.take_n<G1Xyzz>((uint64_t)std::max(p.W, p.Wr) * (p.NBITS + 1));
+    s.bitparts = p.BP > 1 ? ar.take_n<G1Xyzz>((uint64_t)p.Wr * (p.NBITS + 1) * p.BP) : nullptr;
     s.wins = ar.take_n<G1Xyzz>(std::max(p.W, p.Wr));
     s.result = ar.take_n<G1Jac>(1);
     s.pts[0] = p.R >= 1 ? ar.take_n<G1Affine>(p.cap[1]) : nullptr;
@@ -906,21 +916,37 @@ __global__ void __launch_bounds__(128) k_msm_segments(const G1Xyzz* __restrict__
     }
 }
 
+// CTA (w, k, part): part `part` of BP of bit sum (w, k); with BP = 1 the
+// CTA writes the bit sum itself, else its partial (out[(w, k) * BP + part]).
 __global__ void __launch_bounds__(256) k_msm_bitsums(const G1Xyzz* __restrict__ segacc,
                                                      const G1Xyzz* __restrict__ segrun, uint32_t S, int nbits,
-                                                     G1Xyzz* __restrict__ bits)
+                                                     uint32_t BP, G1Xyzz* __restrict__ out)
 {
-    const uint32_t w = blockIdx.x / (nbits + 1);
-    const int k = (int)(blockIdx.x % (nbits + 1));
+    const uint32_t wk = blockIdx.x / BP, part = blockIdx.x % BP;
+    const uint32_t w = wk / (nbits + 1);
+    const int k = (int)(wk % (nbits + 1));
     // k == nbits: all S weighted sums; else the S/2 plain sums with bit k set,
     // s = (hi << (k+1)) | (1 << k) | lo
     const bool all = (k == nbits);
     const uint64_t lo_mask = all ? 0 : (1ull << k) - 1;
-    G1Xyzz r = block_sum_xyzz(all ? S : S / 2, [&](uint64_t j) {
+    const uint64_t items = all ? S : S / 2;
+    const uint64_t per = (items + BP - 1) / BP;
+    const uint64_t j0 = std::min<uint64_t>(items, (uint64_t)part * per);
+    const uint64_t j1 = std::min<uint64_t>(items, j0 + per);
+    G1Xyzz r = block_sum_xyzz(j1 - j0, [&](uint64_t jj) {
+        const uint64_t j = j0 + jj;
         if (all) return ld_xyzz(&segacc[(uint64_t)w * S + j]);
         uint64_t s = ((j & ~lo_mask) << 1) | (1ull << k) | (j & lo_mask);
         return ld_xyzz(&segrun[(uint64_t)w * S + s]);
     });
+    if (threadIdx.x == 0) st_xyzz(&out[blockIdx.x], r);
+}
+
+// CTA (w, k): the BP partials of bit sum (w, k).
+__global__ void __launch_bounds__(256) k_msm_bitparts(const G1Xyzz* __restrict__ parts, uint32_t BP,
+                                                      G1Xyzz* __restrict__ bits)
+{
+    G1Xyzz r = block_sum_xyzz(BP, [&](uint64_t j) { return ld_xyzz(&parts[(uint64_t)blockIdx.x * BP + j]); });
     if (threadIdx.x == 0) st_xyzz(&bits[blockIdx.x], r);
 }
 
@@ -990,6 +1016,20 @@ __global__ void k_msm_final_each(const G1Xyzz* __restrict__ wins, uint32_t J, co
     st(&outs.p[j]->X, r.X);
     st(&outs.p[j]->Y, r.Y);
     st(&outs.p[j]->Z, r.Z);
+}
+
+// Per-bit sums of the segment sums (reduction step 2), in BP parts per sum
+// when the segments are many.
+static RustError msm_bitsums(const MsmPlan& p, const MsmScratch& s, cudaStream_t st)
+{
+    const uint32_t nbs = (uint32_t)p.Wr * (uint32_t)(p.NBITS + 1);
+    k_msm_bitsums<<<nbs * p.BP, 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, p.BP, p.BP > 1 ? s.bitparts : s.bits);
+    H2B_LAUNCHED("k_msm_bitsums");
+    if (p.BP > 1) {
+        k_msm_bitparts<<<nbs, 256, 0, st>>>(s.bitparts, p.BP, s.bits);
+        H2B_LAUNCHED("k_msm_bitparts");
+    }
+    return ok();
 }
 
 // Runs steps 1-7 on device buffers; result (96 bytes) lands in s.result.
@@ -1109,8 +1149,7 @@ static RustError msm_finish(const MsmPlan& p, const MsmScratch& s, const G1Affin
     uint64_t nseg = (uint64_t)p.Wr * p.S;
     k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.Wr, p.H, p.L, p.S, s.segacc, s.segrun);
     H2B_LAUNCHED("k_msm_segments");
-    k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
-    H2B_LAUNCHED("k_msm_bitsums");
+    H2B_TRY(msm_bitsums(p, s, st));
     k_msm_wincombine<<<(p.Wr + 7) / 8, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
     H2B_LAUNCHED("k_msm_wincombine");
     k_msm_final<<<1, 32 * std::min(p.Wr, 8), 0, st>>>(s.wins, p.Wr, p.c, s.result);
@@ -1184,8 +1223,7 @@ RustError msm_run_merged(const MsmPlan& p, const MsmScratch& s, uint32_t J, cons
     const uint64_t nseg = (uint64_t)p.Wr * p.S;
     k_msm_segments<<<grid_for(nseg, 128, sm_cap), 128, 0, st>>>(s.buckets, p.Wr, p.H, p.L, p.S, s.segacc, s.segrun);
     H2B_LAUNCHED("k_msm_segments");
-    k_msm_bitsums<<<p.Wr * (p.NBITS + 1), 256, 0, st>>>(s.segacc, s.segrun, p.S, p.NBITS, s.bits);
-    H2B_LAUNCHED("k_msm_bitsums");
+    H2B_TRY(msm_bitsums(p, s, st));
     k_msm_wincombine<<<(p.Wr + 7) / 8, 32 * std::min(p.Wr, 8), 0, st>>>(s.bits, p.Wr, p.NBITS, p.LOGL, s.wins);
     H2B_LAUNCHED("k_msm_wincombine");
     MsmOuts o;

@@ -27,6 +27,7 @@ struct MsmPlan {
     uint32_t Kf;         // entries per XYZZ accumulation chunk after the rounds
     uint64_t tn;         // points per window slice of a precomputed table (0: plain bases)
     int Wr;              // windows in the bucket reduction (W, or 1 with a table)
+    uint32_t BP;         // CTAs per bit sum of the reduction (partials summed by a second kernel when > 1)
 };
 
 struct MsmScratch {
@@ -45,6 +46,7 @@ struct MsmScratch {
     G1Xyzz* segacc;
     G1Xyzz* segrun;
     G1Xyzz* bits;
+    G1Xyzz* bitparts;    // per-part bit sums (BP > 1)
     G1Xyzz* wins;
     G1Jac* result;
     G1Affine* rbases;    // plain bases P_i, then phi(P_i), in the lazy x 2^261 form (no pairing rounds)

@@ -460,7 +460,8 @@ RustError _halo2_quotient_permutation(void* values, const void* l0, const void* 
  * result to d_out on `stream` without synchronising. */
 RustError h2b_msm_device(const void* d_scalar, const void* d_bases, void* d_out, uint64_t length, void* scratch,
                          uint64_t scratch_bytes, h2b_stream_t stream);
-/* Window bits (0 = automatic) and sorted entries per accumulation chunk (0 = automatic). */
+/* Window bits (0 = automatic; 4..22 accepted, other values also mean automatic) and sorted entries per
+ * accumulation chunk (0 = automatic). */
 void h2b_msm_set_tuning(int window_bits, int chunk);
 /* Form of the MSM bucket-accumulation kernel: 6 = lazy R' = 2^260 limbs of 52 bits on the FP64 pipe
  * (default; window-table MSMs use it too); 0 = lazy R = 2^261 limbs of 29 bits with one-step carries on the
