@@ -185,3 +185,31 @@ def test_merged_argument_errors(h2b, cuda, table4k):
     need = L.h2b_msm_merged_workspace_size(ok, 1)
     with pytest.raises(h2b.Halo2GpuError):
         h2b.msm_merged(ok, 1, h2b.dev_empty(need - 256))
+
+
+def test_wide_windows_split_bit_sums(h2b, orc, cuda):
+    """Window widths 17-19 give bucket reductions whose bit sums span more
+    than 4096 segment sums, split over several CTAs and summed by a second
+    kernel: a table MSM and a plain MSM at those widths equal the oracle."""
+    L = h2b.lib()
+    n = 1 << 12
+    tau = h2b.fields.fr_mont_limbs([0x51DE])
+    srs = orc.srs(tau, n)
+    d_srs = h2b.to_dev(srs)
+    sc = orc.chacha_fr(77, n)
+    sc[::5] = 0
+    want = orc.msm(sc, srs)
+    d_sc = h2b.to_dev(sc)
+    try:
+        for c in (17, 19):
+            L.h2b_msm_set_tuning(c, 0)
+            assert L.h2b_msm_window_bits(n) == c
+            table = h2b.msm_table_precompute(d_srs, n)
+            out = h2b.dev_empty(96)
+            h2b.msm_device_table(d_sc, table, n, out, n)
+            assert_limbs_equal(h2b.to_host(out, (12,)), want, f"table msm at {c} bits")
+            out2 = h2b.dev_empty(96)
+            h2b.msm_device(d_sc, d_srs, out2, n, h2b.msm_workspace(n))
+            assert_limbs_equal(h2b.to_host(out2, (12,)), want, f"plain msm at {c} bits")
+    finally:
+        L.h2b_msm_set_tuning(0, 0)
