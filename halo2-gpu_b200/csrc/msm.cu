@@ -324,18 +324,37 @@ __device__ __forceinline__ uint32_t window_bits(const uint4& s, int bit, int c)
     return (uint32_t)(v & ((1ull << c) - 1));
 }
 
+// Signed digit w of a virtual scalar (carry in/out through `carry`) and its
+// bucket key w*H + |d| - 1, or ~0 for a zero digit or an invalid lane.
+// With a window table every window shares one bucket set, based at `kb`
+// (the job's bucket set in a merged run, 0 otherwise).  The histogram and
+// the scatter both take their keys from here, so their counts agree.
+__device__ __forceinline__ uint32_t digit_key(const uint4& s, int w, int c, uint32_t H, uint32_t& carry, bool valid,
+                                              uint64_t tn, uint32_t kb, int32_t& d)
+{
+    const uint32_t v = window_bits(s, w * c, c) + carry;
+    if (v > H) { d = (int32_t)v - (int32_t)(1u << c); carry = 1; }
+    else { d = (int32_t)v; carry = 0; }
+    return (valid && d != 0) ? (tn ? kb : (uint32_t)w * H) + (uint32_t)(d < 0 ? -d : d) - 1u : 0xffffffffu;
+}
+
+// Warp-aggregated count of one key per lane (all 32 lanes call it together).
+__device__ __forceinline__ void hist_key(uint32_t key, uint32_t* __restrict__ counts)
+{
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key != 0xffffffffu && (int)lane == __ffs(peers) - 1) atomicAdd(&counts[key], __popc(peers));
+}
+
 // For each digit: key = w*H + |d| - 1 (or ~0 for zero digits); the entry's
 // sign is the digit's sign flipped by the virtual scalar's sign.
 // Virtual points v0 <= i < n.
-// With a window table every window shares one bucket set, based at `kb`
-// (the job's bucket set in a merged run, 0 otherwise).
 template <bool SCATTER>
 __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t n, int c, int W, uint32_t H,
                            uint32_t* __restrict__ counts_or_cursor, uint32_t* __restrict__ sorted, uint64_t tn,
                            uint32_t kb)
 {
     const unsigned lane = threadIdx.x & 31;
-    const uint32_t full = 1u << c;
     for (uint64_t base = v0 + blockIdx.x * (uint64_t)blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t i = base + threadIdx.x;
         bool valid = i < n;
@@ -343,12 +362,8 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t 
         const bool sneg = (s.w >> 31) != 0;
         uint32_t carry = 0;
         for (int w = 0; w < W; w++) {
-            uint32_t v = window_bits(s, w * c, c) + carry;
             int32_t d;
-            if (v > H) { d = (int32_t)v - (int32_t)full; carry = 1; }
-            else { d = (int32_t)v; carry = 0; }
-            uint32_t key = 0xffffffffu;
-            if (valid && d != 0) key = (tn ? kb : (uint32_t)w * H) + (uint32_t)(d < 0 ? -d : d) - 1u;
+            const uint32_t key = digit_key(s, w, c, H, carry, valid, tn, kb, d);
             unsigned peers = __match_any_sync(0xffffffffu, key);
             int leader = __ffs(peers) - 1;
             if (!SCATTER) {
@@ -364,6 +379,42 @@ __global__ void k_msm_sort(const uint4* __restrict__ vsc, uint64_t v0, uint64_t 
                     sorted[b + rank] = v | (((d < 0) != sneg) ? SIGN_BIT : 0u);
                 }
             }
+        }
+    }
+}
+
+// The GLV split and base conversion of k_msm_glv fused with the digit
+// histogram of k_msm_sort<false> for the two halves of each scalar: the
+// histogram's atomics overlap the split's memory traffic, and the halves are
+// counted from registers instead of re-read.  Loops are block-uniform so
+// that every lane reaches the warp-wide match.
+__global__ void k_msm_glv_hist(const Fr* __restrict__ sc, uint4* __restrict__ vs, uint64_t lo, uint64_t hi,
+                               const G1Affine* __restrict__ bases, G1Affine* __restrict__ rb, uint64_t n, int c,
+                               int W, uint32_t H, uint32_t* __restrict__ counts, uint64_t tn)
+{
+    const Fq beta = glv::beta();
+    for (uint64_t base = lo + blockIdx.x * (uint64_t)blockDim.x; base < hi; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = base + threadIdx.x;
+        const bool valid = i < hi;
+        uint4 a = make_uint4(0u, 0u, 0u, 0u), b = a;
+        if (valid) {
+            glv::decompose(from_mont(ldg(&sc[i])), a, b);
+            vs[2 * i] = a;
+            vs[2 * i + 1] = b;
+            if (rb) {
+                const G1Affine q = ld_affine(&bases[i]);
+                const Fq y = to_r261(q.y);
+                st(&rb[i].x, to_r261(q.x));
+                st(&rb[i].y, y);
+                st(&rb[n + i].x, to_r261(q.x * beta));     // infinity (0, 0) stays (0, 0)
+                st(&rb[n + i].y, y);
+            }
+        }
+        uint32_t ca = 0, cb = 0;
+        for (int w = 0; w < W; w++) {
+            int32_t d;
+            hist_key(digit_key(a, w, c, H, ca, valid, tn, 0u, d), counts);
+            hist_key(digit_key(b, w, c, H, cb, valid, tn, 0u, d), counts);
         }
     }
 }
@@ -1059,12 +1110,10 @@ static RustError msm_split(const MsmPlan& p, const MsmScratch& s, const Fr* d_sc
     if (hi <= lo) return ok();
     const unsigned sm_cap = 148u * 16u;
     uint4* vsc = reinterpret_cast<uint4*>(s.canon);  // 2n x 16 B in the n x 32 B slot
-    k_msm_glv<<<grid_for(hi - lo, 256, sm_cap), 256, 0, st>>>(d_scalars, vsc, lo, hi, d_bases,
-                                                              msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr, p.n);
-    H2B_LAUNCHED("k_msm_glv");
-    k_msm_sort<false><<<grid_for(2 * (hi - lo), 256, sm_cap), 256, 0, st>>>(vsc, 2 * lo, 2 * hi, p.c, p.W, p.H,
-                                                                              s.counts, nullptr, p.tn, 0u);
-    H2B_LAUNCHED("k_msm_sort<hist>");
+    k_msm_glv_hist<<<grid_for(hi - lo, 256, sm_cap), 256, 0, st>>>(
+        d_scalars, vsc, lo, hi, d_bases, msm_lazy(p) && p.tn == 0 ? s.rbases : nullptr, p.n, p.c, p.W, p.H, s.counts,
+        p.tn);
+    H2B_LAUNCHED("k_msm_glv_hist");
     return ok();
 }
 
